@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Benchmark: DSEM right-hand side + low-storage RK stage, FP64, p = 8.
+
+Workload: the reference-scale Taylor-Green case (22^3 periodic hex elements on
+[0,2pi]^3, p = 8, 729 Gauss points per element, 38,811,960 conserved
+unknowns, Re = 1600, Mach 0.1, Carpenter-Kennedy 2N-storage RK with 5 stages,
+dt = 0.5 x the inviscid limit).  A "step" is one RK time step (5 stages) of
+the whole mesh.  Metric: DOF-RK-stages/s = unknowns x 5 x steps / seconds.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value : device-resident throughput, CUDA events on the library's stream
+        around exactly K steps (CUDA graph per step), max over ranks.
+e2e   : the same metric through the C-ABI with host buffers: each step uploads
+        the state from pinned host memory, advances one step and downloads it.
+Multi-GPU (torchrun): replicas only -- every rank advances its own copy of the
+case, no data-path collective; value sums the ranks' unknowns.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NEX, P = 22, 8
+RE = 1600.0
+CFL = 0.5
+STAGES = 5
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nex", type=int, default=NEX)
+    ap.add_argument("--p", type=int, default=P)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- op counts
+# Counted from the kernel source (division and sqrt counted as one flop each;
+# an FMA as two).  G = p+1 Gauss points, L = G+1 Lobatto points per direction.
+VIS_FLOPS = 87     # one directional viscous flux vector (vis_flux_x/y/z)
+EUL_FLOPS = 20     # one directional Euler flux vector
+ROE_FLOPS = 161    # Roe flux + average + signed copies per mortar point
+FVIS_FLOPS = 30    # viscous BR1 average per mortar point
+
+
+def vol_flops(G):
+    L, G2, NG = G + 1, G * G, G ** 3
+    chain = lambda n: 2 * n - 1
+    f = 5 * NG  # Q*jacob
+    f += 3 * (5 * G2 * (L - 2) * chain(G) + 5 * G2 * G * chain(L) + 5 * NG)  # Lobatto, derivative, gradient
+    f += 2 * 5 * NG  # Q*jacob reloads
+    f += 3 * (5 * G2 * (L - 2) * chain(G) + 11 * G2 * L * chain(G))  # Lobatto rebuild, 11 gradient fields to grid
+    f += 3 * (2 * G2 * (VIS_FLOPS + 5) + (L - 2) * G2 * (VIS_FLOPS + 5 + EUL_FLOPS + 5 + 10))  # fluxes
+    f += 3 * 5 * G2 * G * chain(L - 2) + 2 * 5 * NG  # interior divergence + accumulation
+    return f
+
+
+def stage_flops(G):
+    G2, NG = G * G, G ** 3
+    upd = 30 * G2 * 2 + 5 * NG * 17 + 30 * G2 * (2 * G - 1)
+    faces = 3 * G2 * (ROE_FLOPS + FVIS_FLOPS)  # three mortars per element
+    return vol_flops(G) + upd + faces
+
+
+def vol_bytes(G):
+    L, G2, NG, NL = G + 1, G * G, G ** 3, (G + 1) * G * G
+    return 8 * (5 * NG + NG + 3 * NG + 3 * NL + 30 * G2 + 30 * G2 + 5 * NG)
+
+
+def stage_bytes(G):
+    L, G2, NG, NL = G + 1, G * G, G ** 3, (G + 1) * G * G
+    face_inv = 8 * (30 * G2 * 3 + 3 * G2 * 4)
+    face_vis = 8 * (30 * G2 * 2 + 3 * G2)
+    upd = 8 * (5 * NG * 5 + NG + 30 * G2 * 3)
+    return face_inv + vol_bytes(G) + face_vis + upd
+
+
+# ------------------------------------------------------------------- clocks
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def fp64_gemm_peak(torch, dev):
+    """cuBLAS FP64 GEMM throughput (burst), TFLOP/s: the FP64 arithmetic ceiling."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize(dev)
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def profiled_traffic():
+    p = os.path.join(ROOT, "profiles", "k_vol_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_baseline(desc, q, dt, dof):
+    from oracle import oracle
+    cores = oracle.set_threads(os.cpu_count() or 1)
+    c = oracle.Case.from_desc(desc)
+    c.set_phys(re=RE)
+    c.set_q(q)
+    t0 = time.perf_counter()
+    for kk in range(1, STAGES + 1):
+        c.stage(0.0, dt, kk, want_qt=False)
+    t = time.perf_counter() - t0
+    return {"value": dof * STAGES / t, "unit": "DOF-RK-stages/s", "cores": cores, "kind": "port",
+            "sample": "1 RK step (5 stages) of the same 22^3 p=8 case, C++ oracle with OpenMP over elements"}
+
+
+def run_reference(args):
+    """Reference arm: the CPU restatement of DSEM's FP64 path on all host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from dsem_b200 import mesh
+    from oracle import oracle
+    cores = oracle.set_threads(os.cpu_count() or 1)
+    box = mesh.Box(args.nex, args.nex, args.nex, args.p)
+    q = mesh.taylor_green(box)
+    dt = CFL * mesh.dtcalc(box, q)
+    dof = 5 * box.nel * (args.p + 1) ** 3
+    c = oracle.Case.from_desc(box.desc())
+    c.set_phys(re=RE)
+    c.set_q(q)
+    kk = 0
+    for _ in range(args.warmup):
+        kk = kk % STAGES + 1
+        c.stage(0.0, dt, kk, want_qt=False)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        kk = kk % STAGES + 1
+        c.stage(0.0, dt, kk, want_qt=False)
+    t = time.perf_counter() - t0
+    v = dof * args.steps / t
+    line = {"metric": "DOF-RK-stages/s FP64 at p=8", "value": v, "unit": "DOF-RK-stages/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"taylor-green {args.nex}^3 hex p={args.p}, Re=1600, Mach 0.1",
+                       "unknowns": dof, "step": "one RK stage per sample"},
+            "cpu_baseline": {"value": v, "unit": "DOF-RK-stages/s", "cores": cores, "kind": "port",
+                             "sample": "one RK stage of the full case per step (C++ oracle, OpenMP)"},
+            "e2e": {"value": v, "unit": "DOF-RK-stages/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from dsem_b200 import mesh
+    from dsem_b200.solver import Solver
+
+    box = mesh.Box(args.nex, args.nex, args.nex, args.p)
+    desc = box.desc()
+    q = mesh.taylor_green(box)
+    dt = CFL * mesh.dtcalc(box, q)
+    G = args.p + 1
+    dof = 5 * box.nel * G ** 3
+    s = Solver(desc, re=RE)
+    s.upload(q)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    # ---- device-resident throughput
+    s.step(dt, args.warmup)
+    barrier()
+    with Clocks(local) as clk:
+        s.step(dt, args.steps)
+        barrier()
+    ms, launches = s.last_timing()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * dof * STAGES * args.steps / (ms_max * 1e-3)
+
+    # ---- end to end through the C-ABI with host buffers (pinned), ldx = nx = p+2
+    ldx = G + 1
+    hq = torch.empty((box.nel, 5, ldx, ldx, ldx), dtype=torch.float64, pin_memory=True)
+    hq_np = hq.numpy()
+    s.download(out=hq_np)
+    barrier()
+    k_e2e = max(1, min(args.steps, 10))
+    t0 = time.perf_counter()
+    for _ in range(k_e2e):
+        s.upload(hq_np)
+        s.step(dt, 1)
+        s.download(out=hq_np)
+    barrier()
+    te = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e = world * dof * STAGES * k_e2e / float(te.item())
+    nbytes = hq_np.nbytes
+
+    # ---- per-kernel device times (CUDA events on the library stream)
+    prof = s.profile_rhs(5)
+    t_vol = prof[1] * 1e-3
+    peaks, src = measured_peaks()
+    out = None
+    if rank == 0:
+        fp64_peak = fp64_gemm_peak(torch, "cuda")
+        achieved = vol_flops(G) * box.nel / t_vol / 1e12
+        hbm_ach = vol_bytes(G) * box.nel / t_vol / 1e9
+        tr = profiled_traffic()
+        roof = {"bound": "tensor", "pipe": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak, "kernel": "k_vol",
+                "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                "traffic": (tr["bytes_per_launch"] if tr else None),
+                "hbm": {"achieved": hbm_ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": hbm_ach / peaks["hbm_gbs"], "peak_source": src},
+                "kernel_ms": {"face_inv": prof[0], "vol": prof[1], "face_vis": prof[2], "update": prof[3]},
+                "flops_per_element_stage": stage_flops(G), "vol_flops_per_element": vol_flops(G),
+                "vol_bytes_per_element": vol_bytes(G)}
+        stage_ms = ms_max / (args.steps * STAGES)
+        step_tf = stage_flops(G) * box.nel / (stage_ms * 1e-3) / 1e12
+        out = {"metric": "DOF-RK-stages/s FP64 at p=8", "value": value, "unit": "DOF-RK-stages/s",
+               "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+               "data": "synthetic (analytic Taylor-Green initial condition)",
+               "config": {"workload": f"taylor-green {args.nex}^3 hex p={args.p}, Re=1600, Mach 0.1, 5-stage LSRK",
+                          "unknowns_per_gpu": dof, "elements": box.nel, "parallelism": f"replicas x{world}",
+                          "l2": "inputs larger than L2 (state 310 MB + face buffers 620 MB)",
+                          "stage_tflops_fp64": step_tf},
+               "e2e": {"value": e2e, "unit": "DOF-RK-stages/s", "h2d_bytes_per_step": nbytes,
+                       "d2h_bytes_per_step": nbytes, "steps": k_e2e},
+               "gpu_launches": launches, "clocks": clk.summary(), "roofline": roof}
+        if world == 1:
+            out["cpu_baseline"] = cpu_baseline(desc, q, dt, dof)
+        print(json.dumps(out), flush=True)
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

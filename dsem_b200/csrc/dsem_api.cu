@@ -1,0 +1,918 @@
+// dsem_api.cu -- C-ABI of include/dsem_gpu.h: context set-up, layout
+// conversion, mortar tables, stage orchestration (one CUDA graph per time
+// step), diagnostics.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/dsem_gpu.h"
+#include "dsem_host_math.h"
+#include "dsem_launch.h"
+#include "dsem_stage.cuh"
+
+using namespace dsem;
+
+namespace {
+
+thread_local std::string g_create_err;
+
+template <class F> cudaError_t with_G(int G, F &&f) {
+  switch (G) {
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 5: return f(std::integral_constant<int, 5>{});
+    case 6: return f(std::integral_constant<int, 6>{});
+    case 7: return f(std::integral_constant<int, 7>{});
+    case 8: return f(std::integral_constant<int, 8>{});
+    case 9: return f(std::integral_constant<int, 9>{});
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+struct Group {
+  int G = 0, nel = 0;
+  bool diag = true;
+  long long e0 = 0;  // first internal element
+  long long q0 = 0;  // offset of the group's state (doubles)
+  long long f0 = 0;  // offset of the group's face slots (doubles)
+  double *jac = nullptr, *gg = nullptr, *gm = nullptr, *hd = nullptr;
+  double *muhg = nullptr, *EVB = nullptr, *kew = nullptr;
+  int *int2ext = nullptr;  // device: caller element id of each group element
+};
+
+struct MList {  // conforming mortars of one order
+  int G = 0, n = 0;
+  MortarC *mc = nullptr;
+  double *nh = nullptr, *nrm = nullptr;
+};
+
+// ---------------------------------------------------------- layout kernels
+__global__ void k_pack(const double *__restrict__ src, int ldx, const int *__restrict__ ext, int G, int nf,
+                       double *__restrict__ dst, int to_internal) {
+  // one block per group element; nf fields of G^3 points
+  const int k = blockIdx.x;
+  const long long L3 = (long long)ldx * ldx * ldx;
+  const int NG = G * G * G;
+  const long long e = ext[k];
+  for (int i = threadIdx.x; i < nf * NG; i += blockDim.x) {
+    const int v = i / NG, p = i - v * NG;
+    const int n = p % G, m = (p / G) % G, l = p / (G * G);
+    const long long s = (e * nf + v) * L3 + n + (long long)ldx * (m + (long long)ldx * l);
+    const long long d = (long long)k * nf * NG + i;
+    if (to_internal)
+      dst[d] = src[s];
+    else
+      dst[s] = src[d];
+  }
+}
+
+// Per-element partial sums for the diagnostics, one thread per element, in the
+// oracle's loop order: [0..2] sum u^2 w, v^2 w, w^2 w; [3] sum |w|^2 J; [4] sum J.
+__global__ void k_diag(const double *__restrict__ JQ, const double *__restrict__ jac, const double *__restrict__ EVB,
+                       const double *__restrict__ kew, int G, int nel, int have_grad, double *__restrict__ part) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nel) return;
+  const int NG = G * G * G;
+  const double *Q = JQ + (long long)k * 5 * NG;
+  const double *J = jac + (long long)k * NG;
+  double su = 0, sv = 0, sw = 0;
+  for (int i = 0; i < G; ++i)
+    for (int j = 0; j < G; ++j)
+      for (int l = 0; l < G; ++l) {
+        const int p = i + G * (j + G * l);
+        const double q1 = Q[p];
+        const double u = Q[NG + p] / q1, v = Q[2 * NG + p] / q1, w = Q[3 * NG + p] / q1;
+        const double b = kew[p];
+        su = su + (u * u) * b;
+        sv = sv + (v * v) * b;
+        sw = sw + (w * w) * b;
+      }
+  double s = 0.0, s2 = 0.0;
+  if (have_grad) {  // energydissipation.f90:19-78
+    const double *E = EVB + (long long)k * 15 * NG;
+    for (int l = 0; l < G; ++l)
+      for (int m = 0; m < G; ++m)
+        for (int n = 0; n < G; ++n) {
+          const int p = l + G * (m + G * n);
+          const double Q1 = Q[p], Q2 = Q[NG + p], Q3 = Q[2 * NG + p], Q4 = Q[3 * NG + p];
+          const double jc = J[p];
+          const double Qx0 = E[0 * NG + p], Qy0 = E[1 * NG + p], Qz0 = E[2 * NG + p];
+          const double Qy1 = E[4 * NG + p], Qz1 = E[5 * NG + p];
+          const double Qx2 = E[6 * NG + p], Qz2 = E[8 * NG + p];
+          const double Qx3 = E[9 * NG + p], Qy3 = E[10 * NG + p];
+          const double udery = ((Qy1 - (Q2 / Q1) * Qy0)) / Q1;
+          const double uderz = ((Qz1 - (Q2 / Q1) * Qz0)) / Q1;
+          const double vderx = ((Qx2 - (Q3 / Q1) * Qx0)) / Q1;
+          const double vderz = ((Qz2 - (Q3 / Q1) * Qz0)) / Q1;
+          const double wderx = ((Qx3 - (Q4 / Q1) * Qx0)) / Q1;
+          const double wdery = ((Qy3 - (Q4 / Q1) * Qy0)) / Q1;
+          const double c1 = (wdery - vderz) / jc, c2 = (uderz - wderx) / jc, c3 = (vderx - udery) / jc;
+          double vort = c1 * c1 + c2 * c2 + c3 * c3;
+          vort = vort / jc;
+          s2 = s2 + 1.0 / jc;
+          s = s + vort;
+        }
+  }
+  double *o = part + (long long)k * 5;
+  o[0] = su;
+  o[1] = sv;
+  o[2] = sw;
+  o[3] = s;
+  o[4] = s2;
+}
+
+}  // namespace
+
+struct dsem_ctx {
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  int ngrid = 0, nmort = 0;
+  Phys P{};
+  int shock = 0, iord = 4, kord = 5;
+  double ark[5] = {}, brk[5] = {}, crk[5] = {};
+  std::vector<Group> groups;
+  std::vector<MList> mlists;
+  std::vector<int> ext_group, ext_k;  // caller element -> (group, index in group)
+  double *JQ = nullptr, *gQ = nullptr, *QTI = nullptr, *QF = nullptr, *FF = nullptr, *VF = nullptr;
+  double *Qt = nullptr, *stage = nullptr, *part = nullptr;
+  size_t nq = 0, nface = 0, nstage = 0;
+  int stage_ldx = 0;
+  int *flag = nullptr;
+  bool traces_valid = false;
+  bool grad_valid = false;     // EVB holds the Q gradients of the last Fluxes call
+  bool ev_grad_valid = false;  // ... and the temperature gradients (EV)
+  double prestep = 0.0;
+  int keep_grad = 0;
+  cudaGraphExec_t gexec = nullptr;
+  double graph_dt = 0.0;
+  int graph_key = -1;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  double last_ms = 0.0;
+  long long last_launches = 0;
+  std::string err;
+  std::vector<double> host_part;
+};
+
+namespace {
+
+int fail(dsem_ctx *c, int code, const std::string &msg) {
+  if (c)
+    c->err = msg;
+  else
+    g_create_err = msg;
+  return code;
+}
+int cuda_fail(dsem_ctx *c, cudaError_t e, const char *where) {
+  return fail(c, DSEM_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+#define CK(call)                                          \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, #call); \
+  } while (0)
+
+void rkcoefs(dsem_ctx *c, int iord) {  // Independentroutines/baselib.f90:86-160
+  for (int i = 0; i < 5; ++i) c->ark[i] = c->brk[i] = c->crk[i] = 0.0;
+  if (iord == 3) {
+    c->kord = 3;
+    c->ark[1] = -5.0 / 9.0;
+    c->ark[2] = -153.0 / 128.0;
+    c->brk[1] = 1.0 / 3.0;
+    c->brk[2] = 3.0 / 4.0;
+    c->crk[0] = 1.0 / 3.0;
+    c->crk[1] = 15.0 / 16.0;
+    c->crk[2] = 8.0 / 15.0;
+  } else if (iord == 2) {
+    c->kord = 2;
+    c->ark[1] = -1.0;
+    c->brk[1] = 1.0;
+    c->crk[0] = 1.0;
+    c->crk[1] = 0.5;
+  } else if (iord == 1) {
+    c->kord = 1;
+    c->crk[0] = 1.0;
+  } else {
+    c->kord = 5;
+    c->ark[1] = -0.4178904745;
+    c->ark[2] = -1.192151694643;
+    c->ark[3] = -1.697784692471;
+    c->ark[4] = -1.514183444257;
+    c->brk[1] = 0.1496590219993;
+    c->brk[2] = 0.3704009573644;
+    c->brk[3] = 0.6222557631345;
+    c->brk[4] = 0.9582821306748;
+    c->crk[0] = 0.1496590219993;
+    c->crk[1] = 0.3792103129999;
+    c->crk[2] = 0.8229550293869;
+    c->crk[3] = 0.6994504559488;
+    c->crk[4] = 0.1530572479681;
+  }
+}
+
+int upload_ops(dsem_ctx *c) {
+  static std::vector<double> table;
+  if (table.empty()) {
+    table.assign(OPS_TOTAL, 0.0);
+    for (int G = GMIN; G <= GMAX; ++G) {
+      const int L = G + 1;
+      hostmath::operators(G, &table[ops_off(G)], &table[ops_off(G) + G * L]);
+    }
+  }
+  for (int G = GMIN; G <= GMAX; ++G) {
+    cudaError_t e = with_G(G, [&](auto g) { return Launch<decltype(g)::value>::set_ops(table.data(), OPS_TOTAL); });
+    if (e != cudaSuccess) return cuda_fail(c, e, "set_ops");
+  }
+  return DSEM_OK;
+}
+
+int vol_mode(const dsem_ctx *c, bool save) {
+  if (c->shock) return save ? VOL_EV_SAVE : VOL_EV;
+  return save ? VOL_SAVE : VOL_PLAIN;
+}
+
+// One evaluation of Fluxes and the flux divergence, plus the update when kk > 0.
+int enqueue_stage(dsem_ctx *c, int kk, double dt, bool save, double *qt_out, long long *launches) {
+  const double gamma = c->P.gamma;
+  for (auto &ml : c->mlists) {
+    CK(with_G(ml.G, [&](auto g) {
+      return Launch<decltype(g)::value>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, gamma, c->st);
+    }));
+    ++*launches;
+  }
+  const int mode = vol_mode(c, save);
+  for (auto &g : c->groups) {
+    VolArgs a{};
+    a.JQ = c->JQ + g.q0;
+    a.sq = 5LL * g.G * g.G * g.G;
+    a.jac = g.jac;
+    a.gg = g.gg;
+    a.gm = g.gm;
+    a.muhg = g.muhg;
+    a.QF = c->QF + g.f0;
+    a.VF = c->VF + g.f0;
+    a.QTI = c->QTI + g.q0;
+    a.EVB = g.EVB;
+    a.P = c->P;
+    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::vol(a, g.nel, g.diag, mode, c->st); }));
+    ++*launches;
+  }
+  for (auto &ml : c->mlists) {
+    CK(with_G(ml.G, [&](auto g) { return Launch<decltype(g)::value>::face_vis(ml.mc, ml.n, c->VF, ml.nrm, c->st); }));
+    ++*launches;
+  }
+  for (auto &g : c->groups) {
+    UpdArgs u{};
+    u.JQ = c->JQ + g.q0;
+    u.gQ = c->gQ + g.q0;
+    u.sq = 5LL * g.G * g.G * g.G;
+    u.jac = g.jac;
+    u.QTI = c->QTI + g.q0;
+    u.FF = c->FF + g.f0;
+    u.VF = c->VF + g.f0;
+    u.QF = c->QF + g.f0;
+    u.Qt_out = qt_out ? qt_out + g.q0 : nullptr;
+    u.flag = c->flag;
+    u.re = c->P.re;
+    u.update = kk > 0;
+    u.first = kk == 1;
+    u.ark = kk > 0 ? c->ark[kk - 1] : 0.0;
+    u.cdt = kk > 0 ? c->crk[kk - 1] * dt : 0.0;
+    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::update(u, g.nel, c->st); }));
+    ++*launches;
+  }
+  return DSEM_OK;
+}
+
+int enqueue_ev(dsem_ctx *c, long long *launches) {
+  for (auto &g : c->groups) {
+    EvArgs a{};
+    a.JQ = c->JQ + g.q0;
+    a.sq = 5LL * g.G * g.G * g.G;
+    a.jac = g.jac;
+    a.hd = g.hd;
+    a.EVB = g.EVB;
+    a.muhg = g.muhg;
+    a.valid = c->ev_grad_valid ? 1 : 0;
+    a.P = c->P;
+    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::ev(a, g.nel, c->st); }));
+    ++*launches;
+  }
+  return DSEM_OK;
+}
+
+int enqueue_traces(dsem_ctx *c, long long *launches) {
+  for (auto &g : c->groups) {
+    TraceArgs a{};
+    a.JQ = c->JQ + g.q0;
+    a.sq = 5LL * g.G * g.G * g.G;
+    a.jac = g.jac;
+    a.QF = c->QF + g.f0;
+    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::trace(a, g.nel, c->st); }));
+    ++*launches;
+  }
+  c->traces_valid = true;
+  return DSEM_OK;
+}
+
+// one full time step (tstep.f90:36-116): EV, g_Q = 0 (folded into stage 1), kord stages
+int enqueue_step(dsem_ctx *c, double dt, bool save_last, long long *launches) {
+  if (c->shock) {
+    int r = enqueue_ev(c, launches);
+    if (r) return r;
+  }
+  for (int kk = 1; kk <= c->kord; ++kk) {
+    int r = enqueue_stage(c, kk, dt, save_last && kk == c->kord, nullptr, launches);
+    if (r) return r;
+  }
+  return DSEM_OK;
+}
+
+int ensure_stage_buf(dsem_ctx *c, int ldx, int nf) {
+  const size_t need = (size_t)c->ngrid * nf * ldx * ldx * ldx;
+  if (need > c->nstage) {
+    if (c->stage) cudaFree(c->stage);
+    c->stage = nullptr;
+    CK(cudaMalloc(&c->stage, need * sizeof(double)));
+    c->nstage = need;
+  }
+  return DSEM_OK;
+}
+
+int check_ldx(dsem_ctx *c, int ldx) {
+  for (auto &g : c->groups)
+    if (ldx < g.G) return fail(c, DSEM_ERR_INVALID_ARG, "ldx smaller than the number of Gauss points");
+  return DSEM_OK;
+}
+
+// device internal [group elements][nf][G^3] <-> caller [ngrid][nf][ldx^3]
+int unpack_to_host(dsem_ctx *c, const double *dev_internal, double *host, int ldx, int nf, const std::vector<long long> &offs) {
+  int r = ensure_stage_buf(c, ldx, nf);
+  if (r) return r;
+  const size_t n = (size_t)c->ngrid * nf * ldx * ldx * ldx;
+  CK(cudaMemsetAsync(c->stage, 0, n * sizeof(double), c->st));
+  for (size_t gi = 0; gi < c->groups.size(); ++gi) {
+    auto &g = c->groups[gi];
+    if (g.nel == 0) continue;
+    k_pack<<<g.nel, 256, 0, c->st>>>(dev_internal + offs[gi], ldx, g.int2ext, g.G, nf, c->stage, 0);
+    CK(cudaGetLastError());
+  }
+  CK(cudaMemcpyAsync(host, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return DSEM_OK;
+}
+
+std::vector<long long> state_offs(const dsem_ctx *c) {
+  std::vector<long long> o;
+  for (auto &g : c->groups) o.push_back(g.q0);
+  return o;
+}
+
+int check_flag(dsem_ctx *c) {
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (h & 1) return fail(c, DSEM_ERR_NONFINITE, "NaN or Inf in the stage right-hand side");
+  return DSEM_OK;
+}
+
+}  // namespace
+
+// =================================================================== C-ABI
+namespace {
+int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m);
+}
+
+extern "C" {
+
+const char *dsem_last_error(const dsem_ctx *c) { return c ? c->err.c_str() : g_create_err.c_str(); }
+
+int dsem_create(const dsem_mesh_desc *m, const dsem_phys *ph, dsem_ctx **out) {
+  dsem_ctx *c = nullptr;
+  if (!m || !ph || !out) return fail(nullptr, DSEM_ERR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (m->ngrid <= 0 || m->nmort < 0 || m->ldx <= 0 || !m->ncg || !m->jacob || !m->gmetg || !m->gmet ||
+      (m->nmort > 0 && (!m->mortar || !m->n_hat || !m->norm)))
+    return fail(nullptr, DSEM_ERR_INVALID_ARG, "incomplete mesh descriptor");
+  const int ldx = m->ldx;
+  for (int e = 0; e < m->ngrid; ++e) {
+    const int G = m->ncg[3 * e];
+    if (m->ncg[3 * e + 1] != G || m->ncg[3 * e + 2] != G)
+      return fail(nullptr, DSEM_ERR_UNSUPPORTED, "anisotropic element orders are not supported");
+    if (G < GMIN || G > GMAX) return fail(nullptr, DSEM_ERR_UNSUPPORTED, "element order outside 1..8");
+    if (ldx < G + 1) return fail(nullptr, DSEM_ERR_INVALID_ARG, "ldx must be at least ncg+1");
+  }
+  c = new dsem_ctx();
+  cudaGetDevice(&c->dev);
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return fail(nullptr, DSEM_ERR_CUDA, "cudaStreamCreate failed (no usable CUDA device?)");
+  }
+  c->ngrid = m->ngrid;
+  c->nmort = m->nmort;
+  c->P.gamma = ph->gamma;
+  c->P.re = ph->re;
+  c->P.pr = ph->pr;
+  c->P.mach = ph->mach;
+  c->P.cmu = ph->cmu;
+  c->P.mumax = ph->mumax;
+  c->P.ducros = (ph->shock & 2) ? 1 : 0;
+  c->shock = ph->shock ? 1 : 0;
+  c->iord = ph->iord;
+  rkcoefs(c, ph->iord);
+  const int r = setup_ctx(c, m);
+  if (r) {
+    g_create_err = c->err;
+    dsem_destroy(c);
+    return r;
+  }
+  *out = c;
+  return DSEM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m) {
+  const int ldx = m->ldx;
+  int r = upload_ops(c);
+  if (r) return r;
+
+  // ---- groups: elements sorted by order
+  const size_t L3 = (size_t)ldx * ldx * ldx;
+  c->ext_group.assign(m->ngrid, -1);
+  c->ext_k.assign(m->ngrid, -1);
+  long long q0 = 0, f0 = 0, e0 = 0;
+  for (int G = GMIN; G <= GMAX; ++G) {
+    std::vector<int> ids;
+    for (int e = 0; e < m->ngrid; ++e)
+      if (m->ncg[3 * e] == G) ids.push_back(e);
+    if (ids.empty()) continue;
+    Group g;
+    g.G = G;
+    g.nel = (int)ids.size();
+    g.e0 = e0;
+    g.q0 = q0;
+    g.f0 = f0;
+    const int L = G + 1, NG = G * G * G, NL = L * G * G;
+    // metric layout: diagonal when every off-diagonal entry is exactly zero
+    bool diag = true;
+    for (int e : ids) {
+      for (int l = 0; l < L && diag; ++l)
+        for (int mm = 0; mm < L && diag; ++mm)
+          for (int n = 0; n < L && diag; ++n) {
+            const size_t q = (size_t)e * L3 + n + (size_t)ldx * (mm + (size_t)ldx * l);
+            if (n < G && mm < G && l < G)
+              for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j)
+                  if (i != j && m->gmetg[q * 9 + i + 3 * j] != 0.0) diag = false;
+            const int idx[3] = {n, mm, l};
+            for (int d = 0; d < 3; ++d) {
+              bool ok = true;
+              for (int a = 0; a < 3; ++a)
+                if (idx[a] >= (a == d ? L : G)) ok = false;
+              if (!ok) continue;
+              for (int j = 0; j < 3; ++j)
+                if (j != d && m->gmet[q * 9 + d + 3 * j] != 0.0) diag = false;
+            }
+          }
+      if (!diag) break;
+    }
+    g.diag = diag;
+    std::vector<double> jac((size_t)g.nel * NG), hd((size_t)g.nel * NG);
+    std::vector<double> gg((size_t)g.nel * (diag ? 3 : 9) * NG), gmv((size_t)g.nel * (diag ? 3 : 9) * NL);
+    for (int k = 0; k < g.nel; ++k) {
+      const int e = ids[k];
+      c->ext_group[e] = (int)c->groups.size();
+      c->ext_k[e] = k;
+      for (int l = 0; l < G; ++l)
+        for (int mm = 0; mm < G; ++mm)
+          for (int n = 0; n < G; ++n) {
+            const size_t q = (size_t)e * L3 + n + (size_t)ldx * (mm + (size_t)ldx * l);
+            const int p = n + G * (mm + G * l);
+            jac[(size_t)k * NG + p] = m->jacob[q];
+            hd[(size_t)k * NG + p] =  // delta_g (turbulence/staticSmago/staticSmag.f90:191-201)
+                std::pow(std::fabs(1.0 / m->jacob[q]), 1.0 / 3.0) / std::pow((double)(G * G * G), 1.0 / 3.0);
+            for (int i = 0; i < 3; ++i)
+              for (int j = 0; j < 3; ++j) {
+                const double v = m->gmetg[q * 9 + i + 3 * j];
+                if (diag) {
+                  if (i == j) gg[((size_t)k * 3 + i) * NG + p] = v;
+                } else {
+                  gg[((size_t)k * NG + p) * 9 + i + 3 * j] = v;
+                }
+              }
+          }
+      for (int d = 0; d < 3; ++d) {
+        const int ext[3] = {d == 0 ? L : G, d == 1 ? L : G, d == 2 ? L : G};
+        for (int l = 0; l < ext[2]; ++l)
+          for (int mm = 0; mm < ext[1]; ++mm)
+            for (int n = 0; n < ext[0]; ++n) {
+              const size_t q = (size_t)e * L3 + n + (size_t)ldx * (mm + (size_t)ldx * l);
+              const int pl = d == 0 ? n + L * (mm + G * l) : (d == 1 ? n + G * (mm + L * l) : n + G * (mm + G * l));
+              if (diag) {
+                gmv[((size_t)k * 3 + d) * NL + pl] = m->gmet[q * 9 + d + 3 * d];
+              } else {
+                for (int j = 0; j < 3; ++j) gmv[(((size_t)k * 3 + d) * NL + pl) * 3 + j] = m->gmet[q * 9 + d + 3 * j];
+              }
+            }
+      }
+    }
+    CK(cudaMalloc(&g.jac, jac.size() * sizeof(double)));
+    CK(cudaMalloc(&g.hd, hd.size() * sizeof(double)));
+    CK(cudaMalloc(&g.gg, gg.size() * sizeof(double)));
+    CK(cudaMalloc(&g.gm, gmv.size() * sizeof(double)));
+    CK(cudaMemcpy(g.jac, jac.data(), jac.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(g.hd, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(g.gg, gg.data(), gg.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(g.gm, gmv.data(), gmv.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&g.muhg, (size_t)g.nel * NG * sizeof(double)));
+    CK(cudaMemset(g.muhg, 0, (size_t)g.nel * NG * sizeof(double)));
+    CK(cudaMalloc(&g.EVB, (size_t)g.nel * 15 * NG * sizeof(double)));
+    CK(cudaMemset(g.EVB, 0, (size_t)g.nel * 15 * NG * sizeof(double)));
+    CK(cudaMalloc(&g.int2ext, ids.size() * sizeof(int)));
+    CK(cudaMemcpy(g.int2ext, ids.data(), ids.size() * sizeof(int), cudaMemcpyHostToDevice));
+    std::vector<double> kw(NG);
+    hostmath::ke_weights(G, kw.data());
+    CK(cudaMalloc(&g.kew, NG * sizeof(double)));
+    CK(cudaMemcpy(g.kew, kw.data(), NG * sizeof(double), cudaMemcpyHostToDevice));
+    c->groups.push_back(g);
+    q0 += 5LL * g.nel * NG;
+    f0 += 30LL * g.nel * G * G;
+    e0 += g.nel;
+  }
+  c->nq = (size_t)q0;
+  c->nface = (size_t)f0;
+
+  // ---- mortars
+  std::vector<std::vector<MortarC>> mcs(GMAX + 1);
+  std::vector<std::vector<double>> nhs(GMAX + 1), nrs(GMAX + 1);
+  for (int j = 0; j < m->nmort; ++j) {
+    const int *t = m->mortar + (size_t)DSEM_MORTAR_INTS * j;
+    const int id1 = t[0] - 1, id2 = t[1] - 1;
+    if (id1 < 0 || id1 >= m->ngrid) return fail(c, DSEM_ERR_INVALID_ARG, "mortar master id out of range");
+    if (id2 < 0) return fail(c, DSEM_ERR_UNSUPPORTED, "boundary mortars (id(2)=0) are not supported: the implemented path is fully periodic");
+    if (id2 >= m->ngrid) return fail(c, DSEM_ERR_INVALID_ARG, "mortar slave id out of range");
+    const int f1 = t[2], f2 = t[3], orient = t[10];
+    if (f1 < 1 || f1 > 6 || f2 < 1 || f2 > 6 || orient < 0 || orient > 7)
+      return fail(c, DSEM_ERR_INVALID_ARG, "bad mortar face or orientation");
+    const int Gm = m->ncg[3 * id1], Gs = m->ncg[3 * id2];
+    const bool conf = t[13] && t[14] && t[15] && t[16];
+    if (!conf || Gm != Gs || t[8] != Gm || t[9] != Gm)
+      return fail(c, DSEM_ERR_UNSUPPORTED, "nonconforming mortars are not supported by this build");
+    const int G = Gm, G2 = G * G;
+    const Group &gm = c->groups[c->ext_group[id1]];
+    const Group &gs = c->groups[c->ext_group[id2]];
+    MortarC mc;
+    mc.ms = gm.f0 + (long long)c->ext_k[id1] * 30 * G2 + (long long)(f1 - 1) * 5 * G2;
+    mc.ss = gs.f0 + (long long)c->ext_k[id2] * 30 * G2 + (long long)(f2 - 1) * 5 * G2;
+    mc.geo = (int)mcs[G].size();
+    const bool low = (f1 == 1 || f1 == 3 || f1 == 6);
+    mc.flags = orient | ((t[11] < 0) << 3) | ((t[12] < 0) << 4) | (low << 5);
+    mcs[G].push_back(mc);
+    for (int jj = 0; jj < G; ++jj)
+      for (int i = 0; i < G; ++i) {
+        const size_t q = (size_t)j * ldx * ldx + i + (size_t)ldx * jj;
+        nrs[G].push_back(m->norm[q]);
+        for (int k = 0; k < 3; ++k) nhs[G].push_back(m->n_hat[q * 3 + k]);
+      }
+  }
+  for (int G = GMIN; G <= GMAX; ++G) {
+    if (mcs[G].empty()) continue;
+    MList ml;
+    ml.G = G;
+    ml.n = (int)mcs[G].size();
+    CK(cudaMalloc(&ml.mc, mcs[G].size() * sizeof(MortarC)));
+    CK(cudaMemcpy(ml.mc, mcs[G].data(), mcs[G].size() * sizeof(MortarC), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&ml.nh, nhs[G].size() * sizeof(double)));
+    CK(cudaMemcpy(ml.nh, nhs[G].data(), nhs[G].size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&ml.nrm, nrs[G].size() * sizeof(double)));
+    CK(cudaMemcpy(ml.nrm, nrs[G].data(), nrs[G].size() * sizeof(double), cudaMemcpyHostToDevice));
+    c->mlists.push_back(ml);
+  }
+
+  // ---- state and face buffers
+  CK(cudaMalloc(&c->JQ, c->nq * sizeof(double)));
+  CK(cudaMalloc(&c->gQ, c->nq * sizeof(double)));
+  CK(cudaMalloc(&c->QTI, c->nq * sizeof(double)));
+  CK(cudaMalloc(&c->Qt, c->nq * sizeof(double)));
+  CK(cudaMemset(c->JQ, 0, c->nq * sizeof(double)));
+  CK(cudaMemset(c->gQ, 0, c->nq * sizeof(double)));
+  CK(cudaMalloc(&c->QF, c->nface * sizeof(double)));
+  CK(cudaMalloc(&c->FF, c->nface * sizeof(double)));
+  CK(cudaMalloc(&c->VF, c->nface * sizeof(double)));
+  CK(cudaMalloc(&c->part, (size_t)m->ngrid * 5 * sizeof(double)));
+  CK(cudaMalloc(&c->flag, sizeof(int)));
+  CK(cudaMemset(c->flag, 0, sizeof(int)));
+  CK(cudaEventCreate(&c->e0));
+  CK(cudaEventCreate(&c->e1));
+  // set the shared-memory attribute of every volume variant outside any capture
+  for (auto &g : c->groups)
+    for (int mode = 0; mode < 4; ++mode) {
+      VolArgs a{};
+      CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::vol(a, 0, g.diag, mode, c->st); }));
+    }
+  return DSEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void dsem_destroy(dsem_ctx *c) {
+  if (!c) return;
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  for (auto &g : c->groups) {
+    cudaFree(g.jac);
+    cudaFree(g.gg);
+    cudaFree(g.gm);
+    cudaFree(g.hd);
+    cudaFree(g.muhg);
+    cudaFree(g.EVB);
+    cudaFree(g.kew);
+    cudaFree(g.int2ext);
+  }
+  for (auto &ml : c->mlists) {
+    cudaFree(ml.mc);
+    cudaFree(ml.nh);
+    cudaFree(ml.nrm);
+  }
+  cudaFree(c->JQ);
+  cudaFree(c->gQ);
+  cudaFree(c->QTI);
+  cudaFree(c->Qt);
+  cudaFree(c->QF);
+  cudaFree(c->FF);
+  cudaFree(c->VF);
+  cudaFree(c->stage);
+  cudaFree(c->part);
+  cudaFree(c->flag);
+  if (c->e0) cudaEventDestroy(c->e0);
+  if (c->e1) cudaEventDestroy(c->e1);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+int dsem_upload_q(dsem_ctx *c, const double *JQ, int ldx) {
+  if (!c || !JQ) return fail(c, DSEM_ERR_INVALID_ARG, "null argument");
+  int r = check_ldx(c, ldx);
+  if (r) return r;
+  r = ensure_stage_buf(c, ldx, 5);
+  if (r) return r;
+  const size_t n = (size_t)c->ngrid * 5 * ldx * ldx * ldx;
+  CK(cudaMemcpyAsync(c->stage, JQ, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  for (auto &g : c->groups) {
+    k_pack<<<g.nel, 256, 0, c->st>>>(c->stage, ldx, g.int2ext, g.G, 5, c->JQ + g.q0, 1);
+    CK(cudaGetLastError());
+  }
+  long long l = 0;
+  r = enqueue_traces(c, &l);
+  if (r) return r;
+  CK(cudaStreamSynchronize(c->st));
+  return DSEM_OK;
+}
+
+int dsem_download_q(dsem_ctx *c, double *JQ, int ldx) {
+  if (!c || !JQ) return fail(c, DSEM_ERR_INVALID_ARG, "null argument");
+  int r = check_ldx(c, ldx);
+  if (r) return r;
+  return unpack_to_host(c, c->JQ, JQ, ldx, 5, state_offs(c));
+}
+
+int dsem_rhs(dsem_ctx *c, double tk, double *Qt, int ldx) {
+  (void)tk;
+  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (Qt) {
+    int r = check_ldx(c, ldx);
+    if (r) return r;
+  }
+  long long l = 0;
+  int r;
+  if (!c->traces_valid && (r = enqueue_traces(c, &l))) return r;
+  CK(cudaMemsetAsync(c->flag, 0, sizeof(int), c->st));
+  r = enqueue_stage(c, 0, 0.0, true, c->Qt, &l);
+  if (r) return r;
+  c->grad_valid = true;
+  c->ev_grad_valid = c->shock != 0;
+  if (Qt && (r = unpack_to_host(c, c->Qt, Qt, ldx, 5, state_offs(c)))) return r;
+  return check_flag(c);
+}
+
+int dsem_stage(dsem_ctx *c, double time, double dt, int kk, double *Qt, int ldx) {
+  (void)time;
+  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (kk < 1 || kk > c->kord) return fail(c, DSEM_ERR_INVALID_ARG, "stage index outside 1..kord");
+  if (Qt) {
+    int r = check_ldx(c, ldx);
+    if (r) return r;
+  }
+  long long l = 0;
+  int r;
+  if (!c->traces_valid && (r = enqueue_traces(c, &l))) return r;
+  CK(cudaMemsetAsync(c->flag, 0, sizeof(int), c->st));
+  if (kk == 1 && c->shock && (r = enqueue_ev(c, &l))) return r;
+  r = enqueue_stage(c, kk, dt, true, Qt ? c->Qt : nullptr, &l);
+  if (r) return r;
+  c->grad_valid = true;
+  c->ev_grad_valid = c->shock != 0;
+  if (Qt && (r = unpack_to_host(c, c->Qt, Qt, ldx, 5, state_offs(c)))) return r;
+  return check_flag(c);
+}
+
+int dsem_step(dsem_ctx *c, double time, double dt, int nsteps) {
+  (void)time;
+  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (nsteps < 0) return fail(c, DSEM_ERR_INVALID_ARG, "negative step count");
+  long long l = 0;
+  int r;
+  if (!c->traces_valid && (r = enqueue_traces(c, &l))) return r;
+  CK(cudaMemsetAsync(c->flag, 0, sizeof(int), c->st));
+  const bool save = c->shock || c->keep_grad;
+  const int key = (save ? 1 : 0) | (c->ev_grad_valid ? 2 : 0);
+  long long per_step = 0;
+  // the first step of a run may need EV without valid gradients: run it eagerly
+  if (nsteps > 0 && c->shock && !c->ev_grad_valid) {
+    CK(cudaEventRecord(c->e0, c->st));
+    if ((r = enqueue_step(c, dt, save, &per_step))) return r;
+    c->ev_grad_valid = true;
+    c->grad_valid = true;
+    --nsteps;
+  } else {
+    CK(cudaEventRecord(c->e0, c->st));
+  }
+  long long launches = per_step;
+  if (nsteps > 0) {
+    if (!c->gexec || c->graph_dt != dt || c->graph_key != key) {
+      if (c->gexec) cudaGraphExecDestroy(c->gexec);
+      c->gexec = nullptr;
+      cudaGraph_t graph;
+      CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+      long long cnt = 0;
+      r = enqueue_step(c, dt, save, &cnt);
+      cudaError_t ec = cudaStreamEndCapture(c->st, &graph);
+      if (r) return r;
+      if (ec != cudaSuccess) return cuda_fail(c, ec, "cudaStreamEndCapture");
+      ec = cudaGraphInstantiate(&c->gexec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ec != cudaSuccess) return cuda_fail(c, ec, "cudaGraphInstantiate");
+      c->graph_dt = dt;
+      c->graph_key = key;
+      c->last_launches = cnt;
+    }
+    long long cnt = 0;
+    {
+      // launches per graph replay: recount without enqueueing
+      cnt = (long long)c->kord * (2 * (long long)c->mlists.size() + 2 * (long long)c->groups.size()) +
+            (c->shock ? (long long)c->groups.size() : 0);
+    }
+    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->gexec, c->st));
+    launches += cnt * nsteps;
+    c->grad_valid = c->grad_valid || save;
+    c->ev_grad_valid = c->ev_grad_valid || c->shock;
+  }
+  CK(cudaEventRecord(c->e1, c->st));
+  CK(cudaEventSynchronize(c->e1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c->e0, c->e1));
+  c->last_ms = ms;
+  c->last_launches = launches;
+  if (save) c->grad_valid = true;
+  return check_flag(c);
+}
+
+int dsem_diag(dsem_ctx *c, double dt, int first, double *ke, double *dkdt, double *eps) {
+  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  c->keep_grad = 1;
+  const bool have = c->grad_valid;
+  for (auto &g : c->groups) {
+    k_diag<<<(g.nel + 127) / 128, 128, 0, c->st>>>(c->JQ + g.q0, g.jac, g.EVB, g.kew, g.G, g.nel, have ? 1 : 0,
+                                                    c->part + g.e0 * 5);
+    CK(cudaGetLastError());
+  }
+  c->host_part.resize((size_t)c->ngrid * 5);
+  CK(cudaMemcpyAsync(c->host_part.data(), c->part, c->host_part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double us = 0, vs = 0, ws = 0, s = 0, s2 = 0;
+  for (int e = 0; e < c->ngrid; ++e) {  // caller element order
+    const auto &g = c->groups[c->ext_group[e]];
+    const double *p = &c->host_part[(size_t)(g.e0 + c->ext_k[e]) * 5];
+    us += p[0];
+    vs += p[1];
+    ws += p[2];
+    s += p[3];
+    s2 += p[4];
+  }
+  // jacob(1,1,1) of element 1
+  double j0 = 0.0;
+  {
+    const auto &g = c->groups[c->ext_group[0]];
+    CK(cudaMemcpy(&j0, g.jac + (size_t)c->ext_k[0] * g.G * g.G * g.G, sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  us /= j0;
+  vs /= j0;
+  ws /= j0;
+  const double PI = hostmath::PI;
+  const double tk = 0.5 * (us + vs + ws) / (8.0 * PI * PI * PI);
+  if (first) c->prestep = 0.0;
+  if (ke) *ke = tk;
+  if (dkdt) *dkdt = (c->prestep - tk) / dt;
+  c->prestep = tk;
+  if (eps) *eps = (have && s2 > 0) ? 100.0 * (s / s2) * (1.0 / c->P.re) : 0.0;
+  return DSEM_OK;
+}
+
+int dsem_get_muhg(dsem_ctx *c, double *mu, int ldx) {
+  if (!c || !mu) return fail(c, DSEM_ERR_INVALID_ARG, "null argument");
+  int r = check_ldx(c, ldx);
+  if (r) return r;
+  std::vector<long long> offs;
+  // muhg lives in per-group arrays: unpack group by group
+  r = ensure_stage_buf(c, ldx, 1);
+  if (r) return r;
+  const size_t n = (size_t)c->ngrid * ldx * ldx * ldx;
+  CK(cudaMemsetAsync(c->stage, 0, n * sizeof(double), c->st));
+  for (auto &g : c->groups) {
+    k_pack<<<g.nel, 256, 0, c->st>>>(g.muhg, ldx, g.int2ext, g.G, 1, c->stage, 0);
+    CK(cudaGetLastError());
+  }
+  CK(cudaMemcpyAsync(mu, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return DSEM_OK;
+}
+
+int dsem_profile_rhs(dsem_ctx *c, int reps, double *ms) {
+  if (!c || !ms || reps <= 0) return fail(c, DSEM_ERR_INVALID_ARG, "bad argument");
+  long long l = 0;
+  int r;
+  if (!c->traces_valid && (r = enqueue_traces(c, &l))) return r;
+  cudaEvent_t ev[5];
+  for (auto &e : ev) CK(cudaEventCreate(&e));
+  double acc[4] = {0, 0, 0, 0};
+  const int mode = vol_mode(c, false);
+  for (int it = 0; it < reps; ++it) {
+    CK(cudaEventRecord(ev[0], c->st));
+    for (auto &ml : c->mlists)
+      CK(with_G(ml.G, [&](auto g) {
+        return Launch<decltype(g)::value>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st);
+      }));
+    CK(cudaEventRecord(ev[1], c->st));
+    for (auto &g : c->groups) {
+      VolArgs a{};
+      a.JQ = c->JQ + g.q0;
+      a.sq = 5LL * g.G * g.G * g.G;
+      a.jac = g.jac;
+      a.gg = g.gg;
+      a.gm = g.gm;
+      a.muhg = g.muhg;
+      a.QF = c->QF + g.f0;
+      a.VF = c->VF + g.f0;
+      a.QTI = c->QTI + g.q0;
+      a.EVB = g.EVB;
+      a.P = c->P;
+      CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::vol(a, g.nel, g.diag, mode, c->st); }));
+    }
+    CK(cudaEventRecord(ev[2], c->st));
+    for (auto &ml : c->mlists)
+      CK(with_G(ml.G, [&](auto g) { return Launch<decltype(g)::value>::face_vis(ml.mc, ml.n, c->VF, ml.nrm, c->st); }));
+    CK(cudaEventRecord(ev[3], c->st));
+    for (auto &g : c->groups) {
+      UpdArgs u{};
+      u.JQ = c->JQ + g.q0;
+      u.gQ = c->gQ + g.q0;
+      u.sq = 5LL * g.G * g.G * g.G;
+      u.jac = g.jac;
+      u.QTI = c->QTI + g.q0;
+      u.FF = c->FF + g.f0;
+      u.VF = c->VF + g.f0;
+      u.QF = c->QF + g.f0;
+      u.flag = c->flag;
+      u.re = c->P.re;
+      u.update = 0;
+      CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::update(u, g.nel, c->st); }));
+    }
+    CK(cudaEventRecord(ev[4], c->st));
+    CK(cudaEventSynchronize(ev[4]));
+    for (int k = 0; k < 4; ++k) {
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+      acc[k] += t;
+    }
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  for (int k = 0; k < 4; ++k) ms[k] = acc[k] / reps;
+  return DSEM_OK;
+}
+
+int dsem_last_timing(const dsem_ctx *c, double *ms, long long *launches) {
+  if (!c) return DSEM_ERR_INVALID_ARG;
+  if (ms) *ms = c->last_ms;
+  if (launches) *launches = c->last_launches;
+  return DSEM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,87 @@
+// dsem_inst.cuh -- definitions of Launch<G>; included once per order by inst_g*.cu.
+#pragma once
+#include "dsem_launch.h"
+#include "dsem_stage.cuh"
+
+namespace dsem {
+
+template <int G> cudaError_t Launch<G>::set_ops(const double *h, int n) {
+  if (n != OPS_TOTAL) return cudaErrorInvalidValue;
+  return cudaMemcpyToSymbol(c_ops, h, sizeof(double) * OPS_TOTAL);
+}
+
+template <int G, bool DIAG, bool EV, int SAVE> static cudaError_t vol_one(const VolArgs &a, int nel, cudaStream_t s) {
+  using C = VolCfg<G, DIAG, EV, SAVE>;
+  auto kern = k_vol<G, DIAG, EV, SAVE>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  if (nel <= 0) return cudaSuccess;
+  kern<<<nel, C::NT, C::SMEM, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int G> size_t Launch<G>::vol_smem(bool diag, int mode) {
+  switch (mode) {
+    case VOL_SAVE: return diag ? VolCfg<G, true, false, 1>::SMEM : VolCfg<G, false, false, 1>::SMEM;
+    case VOL_EV: return diag ? VolCfg<G, true, true, 0>::SMEM : VolCfg<G, false, true, 0>::SMEM;
+    case VOL_EV_SAVE: return diag ? VolCfg<G, true, true, 2>::SMEM : VolCfg<G, false, true, 2>::SMEM;
+    default: return diag ? VolCfg<G, true, false, 0>::SMEM : VolCfg<G, false, false, 0>::SMEM;
+  }
+}
+template <int G> int Launch<G>::vol_threads(bool diag, int mode) {
+  (void)diag;
+  (void)mode;
+  return VolCfg<G, true, false, 0>::NT;
+}
+
+template <int G> cudaError_t Launch<G>::vol(const VolArgs &a, int nel, bool diag, int mode, cudaStream_t s) {
+  switch (mode) {
+    case VOL_SAVE: return diag ? vol_one<G, true, false, 1>(a, nel, s) : vol_one<G, false, false, 1>(a, nel, s);
+    case VOL_EV: return diag ? vol_one<G, true, true, 0>(a, nel, s) : vol_one<G, false, true, 0>(a, nel, s);
+    case VOL_EV_SAVE: return diag ? vol_one<G, true, true, 2>(a, nel, s) : vol_one<G, false, true, 2>(a, nel, s);
+    default: return diag ? vol_one<G, true, false, 0>(a, nel, s) : vol_one<G, false, false, 0>(a, nel, s);
+  }
+}
+
+template <int G> cudaError_t Launch<G>::update(const UpdArgs &a, int nel, cudaStream_t s) {
+  if (nel <= 0) return cudaSuccess;
+  const size_t smem = sizeof(double) * (30 * G * G + 5 * G * G * G);
+  k_update<G><<<nel, 256, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int G> cudaError_t Launch<G>::trace(const TraceArgs &a, int nel, cudaStream_t s) {
+  if (nel <= 0) return cudaSuccess;
+  k_trace<G><<<nel, 256, sizeof(double) * 5 * G * G * G, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int G> cudaError_t Launch<G>::ev(const EvArgs &a, int nel, cudaStream_t s) {
+  if (nel <= 0) return cudaSuccess;
+  k_ev<G><<<nel, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int G>
+cudaError_t Launch<G>::face_inv(const MortarC *mc, int nm, double *QF, double *FF, const double *nh, const double *nrm,
+                                double gamma, cudaStream_t s) {
+  if (nm <= 0) return cudaSuccess;
+  const long long n = (long long)nm * G * G;
+  k_face_inv<G><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(mc, nm, QF, FF, nh, nrm, gamma);
+  return cudaGetLastError();
+}
+
+template <int G> cudaError_t Launch<G>::face_vis(const MortarC *mc, int nm, double *VF, const double *nrm, cudaStream_t s) {
+  if (nm <= 0) return cudaSuccess;
+  const long long n = (long long)nm * G * G;
+  k_face_vis<G><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(mc, nm, VF, nrm);
+  return cudaGetLastError();
+}
+
+}  // namespace dsem
+
+#define DSEM_INSTANTIATE(GG) template struct dsem::Launch<GG>;

@@ -1,0 +1,31 @@
+// dsem_launch.h -- host-side launch interface of the per-order kernel
+// instantiations (one translation unit per order G = p+1, see inst_g*.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace dsem {
+
+struct Phys;
+struct VolArgs;
+struct UpdArgs;
+struct TraceArgs;
+struct EvArgs;
+struct MortarC;
+
+// volume kernel variants: metric layout x entropy viscosity x saved gradients
+enum VolMode { VOL_PLAIN = 0, VOL_SAVE = 1, VOL_EV = 2, VOL_EV_SAVE = 3 };
+
+template <int G> struct Launch {
+  static cudaError_t set_ops(const double *host_ops, int n);  // copies the operator table to constant memory
+  static size_t vol_smem(bool diag, int mode);
+  static int vol_threads(bool diag, int mode);
+  static cudaError_t vol(const VolArgs &a, int nel, bool diag, int mode, cudaStream_t s);
+  static cudaError_t update(const UpdArgs &a, int nel, cudaStream_t s);
+  static cudaError_t trace(const TraceArgs &a, int nel, cudaStream_t s);
+  static cudaError_t ev(const EvArgs &a, int nel, cudaStream_t s);
+  static cudaError_t face_inv(const MortarC *mc, int nm, double *QF, double *FF, const double *nh, const double *nrm,
+                              double gamma, cudaStream_t s);
+  static cudaError_t face_vis(const MortarC *mc, int nm, double *VF, const double *nrm, cudaStream_t s);
+};
+
+}  // namespace dsem

@@ -1,0 +1,495 @@
+// dsem_stage.cuh -- the per-stage kernels.
+//
+//  k_trace   : physical Q traces on the six faces          (Int_fluxes face slots)
+//  k_face_inv: Roe flux + averaged state per mortar point  (interface_flux, V_Avg_Soln,
+//                                                           send_flux_to_faces, send_q_to_faces)
+//  k_vol     : Lobatto arrays, Gauss gradients, viscous + inviscid fluxes on the three
+//              staggered grids, interior flux divergence   (Int_fluxes, Vis_Fluxes,
+//                                                           Gauss_Deriv, update_interior)
+//  k_face_vis: BR1 average of the viscous normal flux      (send_flux_to_mortars,
+//                                                           mortar_vis_flux, send_flux_to_faces_add)
+//  k_update  : face terms of the divergence, 2N-storage update, next-stage traces
+//  k_ev      : entropy-viscosity coefficient at Gauss points (RHS_ent_trans, Entropy_Viscosity)
+#pragma once
+#include "dsem_kernels.cuh"
+
+namespace dsem {
+
+// ------------------------------------------------------------------ traces
+template <int G, int HI> __device__ __forceinline__ double trace_of(const double *x, int xs) {
+  constexpr int n = HI ? G : 0;  // Lobatto end point (L-1 = G)
+  double acc = Op<G>::B(n, 0) * x[0];
+#pragma unroll
+  for (int j = 1; j < G; ++j) acc = __fma_rn(Op<G>::B(n, j), x[j * xs], acc);
+  return acc;
+}
+
+// all six face traces of the 5 fields in q (Gauss layout, smem) -> QF slots
+template <int G> __device__ __forceinline__ void write_traces(const double *q, double *QF, int tid, int nt) {
+  constexpr int G2 = G * G, NG = G * G * G;
+  for (int t = tid; t < 30 * G2; t += nt) {
+    const int f = t / (5 * G2);  // 0..5 -> faces 1..6
+    const int r = t - f * 5 * G2;
+    const int v = r / G2, ln = r - v * G2;
+    const int a = ln % G, b = ln / G;
+    const int face = f + 1;
+    const int d = (face == 4 || face == 6) ? 0 : ((face == 1 || face == 2) ? 1 : 2);
+    const double *x = q + v * NG;
+    double val;
+    if (d == 0) {
+      x += gbase<G>(0, a, b);
+      val = (face == 4) ? trace_of<G, 1>(x, 1) : trace_of<G, 0>(x, 1);
+    } else if (d == 1) {
+      x += gbase<G>(1, a, b);
+      val = (face == 2) ? trace_of<G, 1>(x, G) : trace_of<G, 0>(x, G);
+    } else {
+      x += gbase<G>(2, a, b);
+      val = (face == 5) ? trace_of<G, 1>(x, G2) : trace_of<G, 0>(x, G2);
+    }
+    QF[t] = val;
+  }
+}
+
+struct TraceArgs {
+  const double *JQ;
+  long long sq;
+  const double *jac;
+  double *QF;
+};
+
+template <int G> __global__ void __launch_bounds__(256) k_trace(TraceArgs A) {
+  constexpr int G2 = G * G, NG = G * G * G;
+  extern __shared__ double sm[];
+  const int k = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+  const double *JQ = A.JQ + (long long)k * A.sq;
+  const double *jac = A.jac + (long long)k * NG;
+  for (int i = tid; i < 5 * NG; i += nt) sm[i] = JQ[i] * jac[i % NG];
+  __syncthreads();
+  write_traces<G>(sm, A.QF + (long long)k * 30 * G2, tid, nt);
+}
+
+// --------------------------------------------------------------- face kernels
+// Conforming mortar: master slot, slave slot (offsets in the face buffers),
+// geometry index, flags = orient | (sign<0)<<3 | (nsign<0)<<4 | (master face low)<<5.
+struct MortarC {
+  long long ms, ss;
+  int geo, flags;
+};
+
+// mortar index (i,j) -> slave face index (rotate_to_mortar inverse, mortar_operations.f90:461-605)
+template <int G> __device__ __forceinline__ void slave_index(int orient, int i, int j, int &si, int &sj) {
+  switch (orient) {
+    case 3: si = i; sj = G - 1 - j; break;          // F1B2
+    case 2: si = G - 1 - i; sj = G - 1 - j; break;  // B1B2
+    case 1: si = G - 1 - i; sj = j; break;          // B1F2
+    case 4: si = j; sj = i; break;                  // F2F1
+    case 5: si = j; sj = G - 1 - i; break;          // B2F1
+    case 6: si = G - 1 - j; sj = G - 1 - i; break;  // B2B1
+    case 7: si = G - 1 - j; sj = i; break;          // F2B1
+    default: si = i; sj = j; break;
+  }
+}
+
+template <int G>
+__global__ void __launch_bounds__(128) k_face_inv(const MortarC *__restrict__ mc, int nm, double *__restrict__ QF,
+                                                   double *__restrict__ FF, const double *__restrict__ nh,
+                                                   const double *__restrict__ nrm, double gamma) {
+  constexpr int G2 = G * G;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nm * G2) return;
+  const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
+  const MortarC M = mc[m];
+  const int i = pt % G, j = pt / G;
+  int si, sj;
+  slave_index<G>(M.flags & 7, i, j, si, sj);
+  const int sp = si + G * sj;
+  double Q1[NV], Q2[NV], f[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    Q1[v] = QF[M.ms + v * G2 + pt];
+    Q2[v] = QF[M.ss + v * G2 + sp];
+  }
+  const long long gp = (long long)M.geo * G2 + pt;
+  const double n3[3] = {nh[gp * 3], nh[gp * 3 + 1], nh[gp * 3 + 2]};
+  const bool low = (M.flags >> 5) & 1;
+  riemann(n3, nrm[gp], low ? Q2 : Q1, low ? Q1 : Q2, gamma, f);
+  const double sgn = ((M.flags >> 3) & 1) ? -1.0 : 1.0;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double avg = (Q1[v] + Q2[v]) * 0.5;
+    FF[M.ms + v * G2 + pt] = f[v];
+    FF[M.ss + v * G2 + sp] = sgn * f[v];
+    QF[M.ms + v * G2 + pt] = avg;
+    QF[M.ss + v * G2 + sp] = avg;
+  }
+}
+
+template <int G>
+__global__ void __launch_bounds__(128) k_face_vis(const MortarC *__restrict__ mc, int nm, double *__restrict__ VF,
+                                                   const double *__restrict__ nrm) {
+  constexpr int G2 = G * G;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nm * G2) return;
+  const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
+  const MortarC M = mc[m];
+  const int i = pt % G, j = pt / G;
+  int si, sj;
+  slave_index<G>(M.flags & 7, i, j, si, sj);
+  const int sp = si + G * sj;
+  const long long g0 = (long long)M.geo * G2;
+  const double nm_m = nrm[g0 + pt], nm_s = nrm[g0 + sp];
+  const bool neg_n = (M.flags >> 4) & 1, neg_s = (M.flags >> 3) & 1;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double fv1 = VF[M.ms + v * G2 + pt] / nm_m;
+    const double fv2 = VF[M.ss + v * G2 + sp] / nm_s;
+    const double Qs = neg_n ? -fv2 : fv2;
+    const double qb = 0.5 * (fv1 + Qs) * nm_m;
+    VF[M.ms + v * G2 + pt] = qb;
+    VF[M.ss + v * G2 + sp] = neg_s ? -qb : qb;
+  }
+}
+
+// ------------------------------------------------------------------ volume
+struct VolArgs {
+  const double *JQ;
+  long long sq;
+  const double *jac, *gg, *gm;  // metrics, layout per DIAG
+  const double *muhg;           // [elem][G^3] entropy viscosity (EV)
+  const double *QF;             // [elem][6][5][G^2] averaged face state
+  double *VF;                   // [elem][6][5][G^2] out: viscous normal flux at faces
+  double *QTI;                  // [elem][5][G^3]   out: interior divergence sum
+  double *EVB;                  // [elem][15][G^3]  out: gradients kept for EV / diagnostics
+  Phys P;
+};
+
+template <int G, bool DIAG, bool EV, int SAVE> struct VolCfg {
+  static constexpr int L = G + 1, NG = G * G * G, NL = L * G * G;
+  static constexpr int NCH = DIAG ? 11 : 15;
+  static constexpr int NLB = (EV || SAVE == 2) ? 6 : 5;
+  static constexpr size_t SMEM = sizeof(double) * (size_t)(15 * NG + NLB * NL + NCH * NL);
+  static constexpr int NT = G >= 8 ? 384 : 256;
+};
+
+template <int G, int D>
+__device__ __forceinline__ void build_lobatto(const double *q, const double *QF, double *LB, int tid, int nt) {
+  constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
+  for (int t = tid; t < 5 * G2; t += nt) {
+    const int v = t / G2, ln = t - v * G2, a = ln % G, b = ln / G;
+    double *y = LB + v * NL + lbase<G>(D, a, b);
+    constexpr int ys = D == 0 ? 1 : G;
+    constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
+    contract<G, false, 1, L - 1, 0, G>(q + v * NG + gbase<G>(D, a, b), xs, y, ys);
+    y[0] = QF[(face_lo(D) - 1) * 5 * G2 + v * G2 + ln];
+    y[(L - 1) * ys] = QF[(face_hi(D) - 1) * 5 * G2 + v * G2 + ln];
+  }
+}
+
+template <int G, bool DIAG, bool EV, int SAVE, int D>
+__device__ __forceinline__ void vol_pass1(const VolArgs &A, const double *q, const double *QF, const double *gg,
+                                          double *GR, double *LB, double *EVB, int tid, int nt) {
+  constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
+  constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
+  constexpr int ls = D == 0 ? 1 : G;
+  build_lobatto<G, D>(q, QF, LB, tid, nt);
+  if (SAVE == 2) {
+    __syncthreads();
+    const double gamma = A.P.gamma;
+    for (int p = tid; p < NL; p += nt) {  // temperature on the Lobatto grid (RHS.f90:66-83)
+      const double q1 = LB[p], q2 = LB[NL + p], q3 = LB[2 * NL + p], q4 = LB[3 * NL + p], q5 = LB[4 * NL + p];
+      const double P = (gamma - 1.0) * (q5 - 0.5 * q1 * ((q2 / q1) * (q2 / q1) + (q3 / q1) * (q3 / q1) + (q4 / q1) * (q4 / q1)));
+      LB[5 * NL + p] = P * gamma / q1;
+    }
+  }
+  __syncthreads();
+  constexpr int NF = SAVE == 2 ? 6 : 5;
+  for (int t = tid; t < NF * G2; t += nt) {
+    const int f = t / G2, ln = t - f * G2, a = ln % G, b = ln / G;
+    double w[G];
+    contract_reg<G, true, 0, G, 0, L>(LB + f * NL + lbase<G>(D, a, b), ls, w);
+    const int p0 = gbase<G>(D, a, b);
+#pragma unroll
+    for (int k = 0; k < G; ++k) {
+      const int p = p0 + k * xs;
+      if (f < 5) {
+        if (DIAG) {
+          GR[(f * 3 + D) * NG + p] = gg[D * NG + p] * w[k];
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const double val = gg[p * 9 + D + 3 * c] * w[k];
+            GR[(f * 3 + c) * NG + p] = (D == 0) ? val : GR[(f * 3 + c) * NG + p] + val;
+          }
+        }
+      } else {
+        if (DIAG) {
+          EVB[(12 + D) * NG + p] = gg[D * NG + p] * w[k];
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const double val = gg[p * 9 + D + 3 * c] * w[k];
+            EVB[(12 + c) * NG + p] = (D == 0) ? val : EVB[(12 + c) * NG + p] + val;
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template <int G, bool DIAG, bool EV, int SAVE, int D>
+__device__ __forceinline__ void vol_pass2(const VolArgs &A, const double *JQ, const double *jac, const double *QF,
+                                          const double *gm, const double *muhg, double *GR, double *LB, double *CH,
+                                          double *VF, double *QTI, int tid, int nt) {
+  constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
+  constexpr int NCH = DIAG ? 11 : 15;
+  constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
+  constexpr int ls = D == 0 ? 1 : G;
+  if (D > 0) {
+    for (int i = tid; i < 5 * NG; i += nt) CH[i] = JQ[i] * jac[i % NG];
+    __syncthreads();
+  }
+  build_lobatto<G, D>(CH, QF, LB, tid, nt);
+  if (EV) {  // EV_Prolong (Prolong_gtol.f90:7-51)
+    for (int t = tid; t < G2; t += nt) {
+      const int a = t % G, b = t / G;
+      contract<G, false, 0, L, 0, G>(muhg + gbase<G>(D, a, b), xs, LB + 5 * NL + lbase<G>(D, a, b), ls);
+    }
+  }
+  __syncthreads();
+  for (int t = tid; t < NCH * G2; t += nt) {  // gradients to grid D (Vis_Fluxes_new.f90:84-109)
+    const int jf = t / G2, ln = t - jf * G2, a = ln % G, b = ln / G;
+    const int src = DIAG ? diag_field(D, jf) : jf;
+    contract<G, false, 0, L, 0, G>(GR + src * NG + gbase<G>(D, a, b), xs, CH + jf * NL + lbase<G>(D, a, b), ls);
+  }
+  __syncthreads();
+  const Phys P = A.P;
+  for (int p = tid; p < NL; p += nt) {  // fluxes on grid D (Vis_Fluxes_new.f90:115-228, fluxesH_newa.f90:276-352)
+    int s, a, b;
+    ldecode<G>(D, p, s, a, b);
+    double Q[NV], Qx[NV], Qy[NV], Qz[NV], r[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Q[v] = LB[v * NL + p];
+    double amu = 1.0;
+    if (EV) amu = amu + LB[5 * NL + p];
+    const bool face = (s == 0 || s == L - 1);
+    if (DIAG) {
+      double c[11];
+#pragma unroll
+      for (int jf = 0; jf < 11; ++jf) c[jf] = CH[jf * NL + p];
+      double fl[NV];
+      if (D == 0) {
+        Qx[0] = c[0]; Qx[1] = c[1]; Qx[2] = c[2]; Qx[3] = c[3]; Qx[4] = c[4];
+        Qy[0] = c[5]; Qy[1] = c[6]; Qy[2] = c[7]; Qy[3] = 0.0; Qy[4] = 0.0;
+        Qz[0] = c[8]; Qz[1] = c[9]; Qz[3] = c[10]; Qz[2] = 0.0; Qz[4] = 0.0;
+        vis_flux_x(Q, Qx, Qy, Qz, amu, P, fl);
+      } else if (D == 1) {
+        Qy[0] = c[0]; Qy[1] = c[1]; Qy[2] = c[2]; Qy[3] = c[3]; Qy[4] = c[4];
+        Qx[0] = c[5]; Qx[1] = c[6]; Qx[2] = c[7]; Qx[3] = 0.0; Qx[4] = 0.0;
+        Qz[0] = c[8]; Qz[2] = c[9]; Qz[3] = c[10]; Qz[1] = 0.0; Qz[4] = 0.0;
+        vis_flux_y(Q, Qx, Qy, Qz, amu, P, fl);
+      } else {
+        Qz[0] = c[0]; Qz[1] = c[1]; Qz[2] = c[2]; Qz[3] = c[3]; Qz[4] = c[4];
+        Qx[0] = c[5]; Qx[1] = c[6]; Qx[3] = c[7]; Qx[2] = 0.0; Qx[4] = 0.0;
+        Qy[0] = c[8]; Qy[2] = c[9]; Qy[3] = c[10]; Qy[1] = 0.0; Qy[4] = 0.0;
+        vis_flux_z(Q, Qx, Qy, Qz, amu, P, fl);
+      }
+      const double g = gm[D * NL + p];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) r[v] = g * fl[v];
+      if (face) {
+        const int fc = s == 0 ? face_lo(D) : face_hi(D);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) VF[(fc - 1) * 5 * G2 + v * G2 + a + G * b] = r[v];
+      } else {
+        double fi[NV];
+        euler_flux(D, Q, P.gamma, fi);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) CH[v * NL + p] = g * fi[v] - r[v] / P.re;
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        Qx[v] = CH[(v * 3 + 0) * NL + p];
+        Qy[v] = CH[(v * 3 + 1) * NL + p];
+        Qz[v] = CH[(v * 3 + 2) * NL + p];
+      }
+      double f[NV], g[NV], h[NV];
+      vis_flux_x(Q, Qx, Qy, Qz, amu, P, f);
+      vis_flux_y(Q, Qx, Qy, Qz, amu, P, g);
+      vis_flux_z(Q, Qx, Qy, Qz, amu, P, h);
+      const double *g3 = gm + ((long long)D * NL + p) * 3;
+      const double m0 = g3[0], m1 = g3[1], m2 = g3[2];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) r[v] = m0 * f[v] + m1 * g[v] + m2 * h[v];
+      if (face) {
+        const int fc = s == 0 ? face_lo(D) : face_hi(D);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) VF[(fc - 1) * 5 * G2 + v * G2 + a + G * b] = r[v];
+      } else {
+        euler_fluxes3(Q, P.gamma, f, g, h);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) CH[v * NL + p] = (m0 * f[v] + m1 * g[v] + m2 * h[v]) - r[v] / P.re;
+      }
+    }
+  }
+  __syncthreads();
+  for (int t = tid; t < 5 * G2; t += nt) {  // interior divergence along D (updatea.f90:100-113)
+    const int v = t / G2, ln = t - v * G2, a = ln % G, b = ln / G;
+    double S[G];
+    contract_reg<G, true, 0, G, 1, L - 1>(CH + v * NL + lbase<G>(D, a, b), ls, S);
+    const int p0 = gbase<G>(D, a, b);
+#pragma unroll
+    for (int k = 0; k < G; ++k) {
+      const int p = v * NG + p0 + k * xs;
+      QTI[p] = (D == 0) ? S[k] : QTI[p] + S[k];
+    }
+  }
+  __syncthreads();
+}
+
+template <int G, bool DIAG, bool EV, int SAVE>
+__global__ void __launch_bounds__(VolCfg<G, DIAG, EV, SAVE>::NT, 1) k_vol(VolArgs A) {
+  using C = VolCfg<G, DIAG, EV, SAVE>;
+  constexpr int G2 = G * G, NG = C::NG, NL = C::NL;
+  extern __shared__ double sm[];
+  double *GR = sm;
+  double *LB = GR + 15 * NG;
+  double *CH = LB + C::NLB * NL;
+  const int k = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+  const double *JQ = A.JQ + (long long)k * A.sq;
+  const double *jac = A.jac + (long long)k * NG;
+  const double *QF = A.QF + (long long)k * 30 * G2;
+  double *VF = A.VF + (long long)k * 30 * G2;
+  double *QTI = A.QTI + (long long)k * 5 * NG;
+  double *EVB = SAVE ? A.EVB + (long long)k * 15 * NG : nullptr;
+  const double *gg = A.gg + (long long)k * 3 * NG * (DIAG ? 1 : 3);
+  const double *gm = A.gm + (long long)k * 3 * NL * (DIAG ? 1 : 3);
+  const double *muhg = EV ? A.muhg + (long long)k * NG : nullptr;
+
+  for (int i = tid; i < 5 * NG; i += nt) CH[i] = JQ[i] * jac[i % NG];  // Q*jacob (fluxesH_newa.f90:262-272)
+  __syncthreads();
+  vol_pass1<G, DIAG, EV, SAVE, 0>(A, CH, QF, gg, GR, LB, EVB, tid, nt);
+  vol_pass1<G, DIAG, EV, SAVE, 1>(A, CH, QF, gg, GR, LB, EVB, tid, nt);
+  vol_pass1<G, DIAG, EV, SAVE, 2>(A, CH, QF, gg, GR, LB, EVB, tid, nt);
+  if (SAVE) {
+    for (int i = tid; i < 12 * NG; i += nt) EVB[i] = GR[i];
+  }
+  vol_pass2<G, DIAG, EV, SAVE, 0>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QTI, tid, nt);
+  vol_pass2<G, DIAG, EV, SAVE, 1>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QTI, tid, nt);
+  vol_pass2<G, DIAG, EV, SAVE, 2>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QTI, tid, nt);
+}
+
+// ------------------------------------------------------------------ update
+struct UpdArgs {
+  double *JQ, *gQ;
+  long long sq;
+  const double *jac;
+  const double *QTI, *FF, *VF;
+  double *QF;      // out: traces of the updated state
+  double *Qt_out;  // optional: [elem][5][G^3]
+  int *flag;       // bit 0: non-finite Qt
+  double ark, cdt, re;
+  int first, update;
+};
+
+template <int G> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
+  constexpr int L = G + 1, G2 = G * G, NG = G * G * G;
+  extern __shared__ double sm[];
+  double *FB = sm;          // 30*G2 face fluxes
+  double *QN = FB + 30 * G2;  // 5*NG updated physical Q
+  __shared__ double Dlo[G], Dhi[G];
+  const int k = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+  const double *FF = A.FF + (long long)k * 30 * G2;
+  const double *VF = A.VF + (long long)k * 30 * G2;
+  for (int i = tid; i < 30 * G2; i += nt) FB[i] = FF[i] - VF[i] / A.re;  // send_flux_to_faces_add
+  for (int i = tid; i < G; i += nt) {
+    Dlo[i] = Op<G>::D(i, 0);
+    Dhi[i] = Op<G>::D(i, L - 1);
+  }
+  __syncthreads();
+  double *JQ = A.JQ + (long long)k * A.sq;
+  double *gQ = A.gQ + (long long)k * A.sq;
+  const double *QTI = A.QTI + (long long)k * 5 * NG;
+  const double *jac = A.jac + (long long)k * NG;
+  bool bad = false;
+  for (int i = tid; i < 5 * NG; i += nt) {
+    const int v = i / NG, p = i - v * NG;
+    const int n = p % G, m = (p / G) % G, l = p / G2;
+    const double *F = FB + v * G2;
+    double acc = QTI[i];
+    acc = __fma_rn(Dlo[n], F[5 * 5 * G2 + m + G * l], acc);  // face 6 (x = 0)
+    acc = __fma_rn(Dhi[n], F[3 * 5 * G2 + m + G * l], acc);  // face 4 (x = 1)
+    acc = __fma_rn(Dlo[m], F[0 * 5 * G2 + n + G * l], acc);  // face 1 (y = 0)
+    acc = __fma_rn(Dhi[m], F[1 * 5 * G2 + n + G * l], acc);  // face 2 (y = 1)
+    acc = __fma_rn(Dlo[l], F[2 * 5 * G2 + n + G * m], acc);  // face 3 (z = 0)
+    acc = __fma_rn(Dhi[l], F[4 * 5 * G2 + n + G * m], acc);  // face 5 (z = 1)
+    const double Qt = -acc;
+    if (!isfinite(Qt)) bad = true;
+    if (A.Qt_out) A.Qt_out[(long long)k * 5 * NG + i] = Qt;
+    double q = JQ[i];
+    if (A.update) {  // updatea.f90:213-227
+      const double g0 = A.first ? 0.0 : gQ[i];
+      const double g = A.ark * g0 + Qt;
+      q = q + A.cdt * g;
+      gQ[i] = g;
+      JQ[i] = q;
+    }
+    QN[i] = q * jac[p];
+  }
+  if (__any_sync(0xffffffffu, bad) && (tid & 31) == 0) atomicOr(A.flag, 1);
+  __syncthreads();
+  write_traces<G>(QN, A.QF + (long long)k * 30 * G2, tid, nt);
+}
+
+// --------------------------------------------------------------------- EV
+struct EvArgs {
+  const double *JQ;
+  long long sq;
+  const double *jac, *hd, *EVB;
+  double *muhg;
+  int valid;
+  Phys P;
+};
+
+// RHS_ent_trans + Entropy_Viscosity at Gauss points (RHS.f90:21-278, EViscosity_GL.f90:19-101)
+template <int G> __global__ void __launch_bounds__(256) k_ev(EvArgs A) {
+  constexpr int NG = G * G * G;
+  const int k = blockIdx.x;
+  const double *JQ = A.JQ + (long long)k * A.sq;
+  const double *jac = A.jac + (long long)k * NG;
+  const double *hd = A.hd + (long long)k * NG;
+  const double *EVB = A.EVB + (long long)k * 15 * NG;
+  double *mu = A.muhg + (long long)k * NG;
+  for (int p = threadIdx.x; p < NG; p += blockDim.x) {
+    double out = 0.0;
+    if (A.valid) {
+      double Q[NV], Qx[NV], Qy[NV], Qz[NV], T1[3];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) Q[v] = JQ[v * NG + p] * jac[p];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        Qx[v] = EVB[(v * 3 + 0) * NG + p];
+        Qy[v] = EVB[(v * 3 + 1) * NG + p];
+        Qz[v] = EVB[(v * 3 + 2) * NG + p];
+      }
+      Qx[4] = Qy[4] = Qz[4] = 0.0;
+      T1[0] = EVB[12 * NG + p];
+      T1[1] = EVB[13 * NG + p];
+      T1[2] = EVB[14 * NG + p];
+      double duc;
+      const double biS = ev_residual(A.P, Q, Qx, Qy, Qz, T1, duc);
+      const double rho = JQ[p] * jac[p];
+      const double h = hd[p];
+      double mur = A.P.cmu * A.P.re * rho * (h * h) * fabs(biS);
+      if (A.P.ducros) mur = mur * duc;
+      const double mx = mur >= 0.0 ? mur : 0.0;
+      double m = mx <= A.P.mumax ? mx : A.P.mumax;
+      if (!isfinite(m)) m = 0.0;
+      out = m;
+    }
+    mu[p] = out;
+  }
+}
+
+}  // namespace dsem

@@ -1,0 +1,158 @@
+"""ctypes front end of libdsem_b200.so (include/dsem_gpu.h).
+
+`Solver` mirrors the Fortran call sites the library replaces: construction
+packs the geometry (after 3DDriver_parfmdf.f90:307), `step` replaces the body
+of tstep (src/tstep.f90:36-116), `diag` the KE/dissipation diagnostics.
+There is no CPU fallback: a missing library or CUDA device raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "libdsem_b200.so")
+
+DSEM_OK = 0
+ERRORS = {-1: "INVALID_ARG", -2: "CUDA", -3: "NONFINITE", -4: "TIMEOUT", -5: "UNSUPPORTED", -6: "NOMEM"}
+EXPORTS = ("dsem_create", "dsem_destroy", "dsem_last_error", "dsem_upload_q", "dsem_download_q", "dsem_step",
+           "dsem_stage", "dsem_rhs", "dsem_diag", "dsem_get_muhg", "dsem_last_timing", "dsem_profile_rhs")
+
+
+class DsemError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"dsem error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("ngrid", C.c_int), ("nmort", C.c_int), ("ldx", C.c_int), ("ncg", C.POINTER(C.c_int)),
+                ("jacob", C.POINTER(C.c_double)), ("gmetg", C.POINTER(C.c_double)), ("gmet", C.POINTER(C.c_double)),
+                ("mortar", C.POINTER(C.c_int)), ("n_hat", C.POINTER(C.c_double)), ("norm", C.POINTER(C.c_double))]
+
+
+class Phys(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("re", C.c_double), ("pr", C.c_double), ("mach", C.c_double),
+                ("cmu", C.c_double), ("mumax", C.c_double), ("shock", C.c_int), ("iord", C.c_int)]
+
+
+_lib = None
+
+
+def lib(path=None):
+    """Loads the in-tree library (building it with nvcc when it is missing)."""
+    global _lib
+    if _lib is None:
+        p = path or LIB
+        if not os.path.exists(p):
+            from . import build
+            build.build()
+        L = C.CDLL(p)
+        vp = C.c_void_p
+        dp = C.POINTER(C.c_double)
+        L.dsem_create.argtypes = [C.POINTER(MeshDesc), C.POINTER(Phys), C.POINTER(vp)]
+        L.dsem_destroy.argtypes = [vp]
+        L.dsem_last_error.argtypes = [vp]
+        L.dsem_last_error.restype = C.c_char_p
+        L.dsem_upload_q.argtypes = [vp, dp, C.c_int]
+        L.dsem_download_q.argtypes = [vp, dp, C.c_int]
+        L.dsem_step.argtypes = [vp, C.c_double, C.c_double, C.c_int]
+        L.dsem_stage.argtypes = [vp, C.c_double, C.c_double, C.c_int, dp, C.c_int]
+        L.dsem_rhs.argtypes = [vp, C.c_double, dp, C.c_int]
+        L.dsem_diag.argtypes = [vp, C.c_double, C.c_int, dp, dp, dp]
+        L.dsem_get_muhg.argtypes = [vp, dp, C.c_int]
+        L.dsem_last_timing.argtypes = [vp, dp, C.POINTER(C.c_longlong)]
+        L.dsem_profile_rhs.argtypes = [vp, C.c_int, dp]
+        _lib = L
+    return _lib
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _iptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+class Solver:
+    """One device context: geometry + state resident in HBM."""
+
+    def __init__(self, desc, gamma=1.4, re=1600.0, pr=0.72, mach=1.0, cmu=0.0, mumax=0.0, shock=0, iord=4):
+        L = lib()
+        self._arrays = {k: np.ascontiguousarray(desc[k]) for k in ("ncg", "jacob", "gmetg", "gmet", "mortar",
+                                                                  "n_hat", "norm")}
+        a = self._arrays
+        assert a["ncg"].dtype == np.int32 and a["mortar"].dtype == np.int32
+        self.ngrid, self.nmort, self.ldx = int(desc["ngrid"]), int(desc["nmort"]), int(desc["ldx"])
+        md = MeshDesc(self.ngrid, self.nmort, self.ldx, _iptr(a["ncg"]), _dptr(a["jacob"]), _dptr(a["gmetg"]),
+                      _dptr(a["gmet"]), _iptr(a["mortar"]), _dptr(a["n_hat"]), _dptr(a["norm"]))
+        ph = Phys(gamma, re, pr, mach, cmu, mumax, int(shock), int(iord))
+        h = C.c_void_p()
+        rc = L.dsem_create(C.byref(md), C.byref(ph), C.byref(h))
+        if rc != DSEM_OK:
+            raise DsemError(rc, L.dsem_last_error(None).decode())
+        self.h = h
+        self.kord = 5 if iord == 4 else iord
+
+    def _check(self, rc):
+        if rc != DSEM_OK:
+            raise DsemError(rc, lib().dsem_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dsem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def qshape(self, ldx=None):
+        ldx = ldx or self.ldx
+        return (self.ngrid, 5, ldx, ldx, ldx)
+
+    def upload(self, JQ):
+        JQ = np.ascontiguousarray(JQ, dtype=np.float64)
+        self._check(lib().dsem_upload_q(self.h, _dptr(JQ), JQ.shape[-1]))
+
+    def download(self, out=None, ldx=None):
+        out = np.zeros(self.qshape(ldx)) if out is None else out
+        self._check(lib().dsem_download_q(self.h, _dptr(out), out.shape[-1]))
+        return out
+
+    def step(self, dt, nsteps=1, time=0.0):
+        self._check(lib().dsem_step(self.h, time, dt, nsteps))
+
+    def stage(self, dt, kk, time=0.0, want_qt=True):
+        q = np.zeros(self.qshape()) if want_qt else None
+        self._check(lib().dsem_stage(self.h, time, dt, kk, _dptr(q) if want_qt else None, self.ldx))
+        return q
+
+    def rhs(self, tk=0.0):
+        q = np.zeros(self.qshape())
+        self._check(lib().dsem_rhs(self.h, tk, _dptr(q), self.ldx))
+        return q
+
+    def diag(self, dt, first=False):
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        self._check(lib().dsem_diag(self.h, dt, int(first), C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def muhg(self):
+        m = np.zeros((self.ngrid, self.ldx, self.ldx, self.ldx))
+        self._check(lib().dsem_get_muhg(self.h, _dptr(m), self.ldx))
+        return m
+
+    def profile_rhs(self, reps=5):
+        """Mean device milliseconds per RHS of {inviscid face, volume, viscous face, update}."""
+        ms = np.zeros(4)
+        self._check(lib().dsem_profile_rhs(self.h, int(reps), _dptr(ms)))
+        return ms
+
+    def last_timing(self):
+        ms, n = C.c_double(), C.c_longlong()
+        self._check(lib().dsem_last_timing(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value

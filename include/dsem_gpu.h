@@ -1,0 +1,125 @@
+/*
+ * dsem_gpu.h -- C-ABI of the B200 implementation of DSEM's right-hand side
+ * and low-storage Runge-Kutta stage (FP64, sm_100a).
+ *
+ * The library replaces the body of DSEM's
+ *     SUBROUTINE tstep(time,dt,d,ngrid,mrtr,nmort,resid)        (src/tstep.f90:12-120)
+ * called from the time loop at src/3DDriver_parfmdf.f90:466.  DSEM's Fortran
+ * keeps the mesh, the case input and the time loop; it packs the geometry of
+ * TYPE(domain) d(:) and TYPE(mortar) mrtr(:) (src/paraFMDF/initializationsc2.f90:50-215)
+ * once, after the setup at src/3DDriver_parfmdf.f90:307, and calls dsem_create.
+ * From then on all element and interface state stays resident in HBM.
+ *
+ * Conventions
+ *  - Plain C types only; host arrays are caller-owned and read (or written)
+ *    only during the call.  Device state is library-owned.
+ *  - Every function returns 0 (DSEM_OK) or a negative DSEM_ERR_* code; the
+ *    text of the last error is available from dsem_last_error().  Nothing
+ *    exits or aborts.
+ *  - One context per host thread; calls on a context are not re-entrant and
+ *    are synchronous on return (one CUDA stream per context).
+ *  - Per-element arrays use DSEM's Fortran column-major layout padded to the
+ *    caller's extent ldx (the `nx` of size.f90): element e, variable v,
+ *    point (n,m,l) (0-based) sits at  n + ldx*(m + ldx*(l + ldx*(v + 5*e))).
+ */
+#ifndef DSEM_GPU_H
+#define DSEM_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DSEM_OK 0
+#define DSEM_ERR_INVALID_ARG (-1)
+#define DSEM_ERR_CUDA (-2)
+#define DSEM_ERR_NONFINITE (-3)   /* mirrors the NaN/Inf abort of 3DDriver_parfmdf.f90:489-499 */
+#define DSEM_ERR_TIMEOUT (-4)     /* a bounded device-side wait gave up */
+#define DSEM_ERR_UNSUPPORTED (-5) /* mesh feature outside the implemented path */
+#define DSEM_ERR_NOMEM (-6)
+
+/* Integers per mortar in dsem_mesh_desc.mortar, mirroring TYPE(mortar)
+ * (src/paraFMDF/initializationsc2.f90:193-215):
+ *  [0] id(1)  master element (1-based)     [1] id(2) slave element (1-based)
+ *  [2] iface(1) (1..6)                     [3] iface(2)
+ *  [4] len(1,1) [5] len(2,1) [6] len(1,2) [7] len(2,2)
+ *  [8] lenmortar(1) [9] lenmortar(2)       [10] orient (Edge_Mappings: 0..7)
+ *  [11] sign  [12] nsign                   [13..16] conforming(1,1),(2,1),(1,2),(2,2) as 0/1 */
+#define DSEM_MORTAR_INTS 17
+
+typedef struct dsem_ctx dsem_ctx; /* opaque, owned by the library */
+
+/* Geometry packed from d(:) and mrtr(:).  ldx is the padded extent of the
+ * caller's arrays (>= ncg+1 of every element). */
+typedef struct {
+  int ngrid;             /* number of elements (ngrid in tstep)                        */
+  int nmort;             /* number of mortars (nmort in tstep)                         */
+  int ldx;               /* padded extent nx of the caller's per-element arrays        */
+  const int *ncg;        /* [ngrid][3] Gauss points per direction, d%ncg               */
+  const double *jacob;   /* [ngrid][ldx^3]       d%jacob   (1/J at Gauss points)       */
+  const double *gmetg;   /* [ngrid][ldx^3][3][3] d%gmetg(3,3,nx,ny,nz) (grad xi)       */
+  const double *gmet;    /* [ngrid][ldx^3][3][3] d%gmet(3,3,nx,ny,nz) (J grad xi on the
+                            staggered grids; row i on grid i)                          */
+  const int *mortar;     /* [nmort][DSEM_MORTAR_INTS]                                   */
+  const double *n_hat;   /* [nmort][ldx][ldx][3]  mrtr%n_hat(3,nmax,nmax)               */
+  const double *norm;    /* [nmort][ldx][ldx]     mrtr%norm(nmax,nmax)                  */
+} dsem_mesh_desc;
+
+/* Physics and time-integration parameters (MODULE physics, input_data, rk_coefs). */
+typedef struct {
+  double gamma, re, pr, mach; /* NS_data.f90:51-201                                    */
+  double cmu, mumax;          /* entropy-viscosity coefficients                        */
+  int shock;                  /* 1: entropy viscosity (tstep.f90:36-38); 3: also the
+                                 Ducros sensor (input keyword `ducros`)                */
+  int iord;                   /* rkcoefs order: 3 (3 stages) or 4 (5 stages)           */
+} dsem_phys;
+
+/* Creates a context on the current CUDA device and copies the geometry to HBM.
+ * Replaces nothing in DSEM itself: it is the one-time upload that precedes the
+ * time loop (3DDriver_parfmdf.f90:307). */
+int dsem_create(const dsem_mesh_desc *mesh, const dsem_phys *phys, dsem_ctx **out);
+void dsem_destroy(dsem_ctx *ctx);
+const char *dsem_last_error(const dsem_ctx *ctx); /* ctx may be NULL (creation errors) */
+
+/* J*Q state in/out (d%Q, stored as Q/jacob, 3DDriver_parfmdf.f90:290-300). */
+int dsem_upload_q(dsem_ctx *ctx, const double *JQ, int ldx);
+int dsem_download_q(dsem_ctx *ctx, double *JQ, int ldx);
+
+/* Replaces the body of tstep (tstep.f90:36-116), nsteps times:
+ * entropy viscosity (if enabled), g_Q = 0, kord stages of Fluxes + update.
+ * dt is the global step (delta_t(1)).  Returns DSEM_ERR_NONFINITE when the
+ * stage residual max|Qt| is not finite (checked once per dsem_step call). */
+int dsem_step(dsem_ctx *ctx, double time, double dt, int nsteps);
+
+/* One Runge-Kutta stage kk (1-based).  kk==1 also evaluates the entropy
+ * viscosity and zeroes g_Q.  Qt (may be NULL) receives the stage Qt. */
+int dsem_stage(dsem_ctx *ctx, double time, double dt, int kk, double *Qt, int ldx);
+
+/* Parity hook: one evaluation of Fluxes (fluxesH_newa.f90:17) and the flux
+ * divergence Qt (updatea.f90:100-113) without the update. */
+int dsem_rhs(dsem_ctx *ctx, double tk, double *Qt, int ldx);
+
+/* Diagnostics of the current state, the do_user_stuff / energydissipation
+ * analogue (caseFiles/tgv/BackstepProblem-stoch.f90:463-709,
+ * Energydissipation/energydissipation.f90:2-89):
+ *   ke   = 1/2 <u.u> over the periodic [0,2pi]^3 box          (fort.22)
+ *   dkdt = (ke_prev - ke)/dt, ke_prev = 0 when first != 0     (fort.23)
+ *   eps  = 100 <|w|^2>/Re from the last stage's gradients      (dissipated) */
+int dsem_diag(dsem_ctx *ctx, double dt, int first, double *ke, double *dkdt, double *eps);
+
+/* Entropy-viscosity coefficient muhg at Gauss points (ldx layout, one field). */
+int dsem_get_muhg(dsem_ctx *ctx, double *mu, int ldx);
+
+/* Device time of the last dsem_step call, and the number of kernel launches
+ * it made (for benchmarking). */
+int dsem_last_timing(const dsem_ctx *ctx, double *ms, long long *launches);
+
+/* Benchmark hook (no DSEM counterpart): times reps evaluations of each
+ * kernel of a right-hand side with CUDA events on the context's stream and
+ * returns the mean milliseconds per evaluation in ms[4] = {inviscid face,
+ * volume, viscous face, divergence + update}.  The state is left unchanged. */
+int dsem_profile_rhs(dsem_ctx *ctx, int reps, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DSEM_GPU_H */
