@@ -49,7 +49,7 @@ template <int G> cudaError_t Launch<G>::vol(const VolArgs &a, int nel, bool diag
 
 template <int G> cudaError_t Launch<G>::update(const UpdArgs &a, int nel, cudaStream_t s) {
   if (nel <= 0) return cudaSuccess;
-  const size_t smem = sizeof(double) * (30 * G * G + 5 * G * G * G);
+  const size_t smem = sizeof(double) * (30 * G * G + 5 * G * G * G + 2 * G);
   k_update<G><<<nel, 256, smem, s>>>(a);
   return cudaGetLastError();
 }

@@ -62,7 +62,7 @@ template <int G> __device__ __forceinline__ int lbase(int d, int a, int b) {
   constexpr int L = G + 1;
   return d == 0 ? L * (a + G * b) : (d == 1 ? a + G * L * b : a + G * b);
 }
-template <int G> __device__ __forceinline__ int lstride(int d) { return d == 0 ? 1 : G; }
+template <int G> __device__ __forceinline__ int lstride(int d) { return d == 0 ? 1 : (d == 1 ? G : G * G); }
 // faces at the low/high Lobatto ends of direction d (DSEM numbering 1..6)
 __device__ __forceinline__ int face_lo(int d) { return d == 0 ? 6 : (d == 1 ? 1 : 3); }
 __device__ __forceinline__ int face_hi(int d) { return d == 0 ? 4 : (d == 1 ? 2 : 5); }

@@ -177,7 +177,7 @@ __device__ __forceinline__ void build_lobatto(const double *q, const double *QF,
   for (int t = tid; t < 5 * G2; t += nt) {
     const int v = t / G2, ln = t - v * G2, a = ln % G, b = ln / G;
     double *y = LB + v * NL + lbase<G>(D, a, b);
-    constexpr int ys = D == 0 ? 1 : G;
+    constexpr int ys = D == 0 ? 1 : (D == 1 ? G : G2);
     constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
     contract<G, false, 1, L - 1, 0, G>(q + v * NG + gbase<G>(D, a, b), xs, y, ys);
     y[0] = QF[(face_lo(D) - 1) * 5 * G2 + v * G2 + ln];
@@ -190,7 +190,7 @@ __device__ __forceinline__ void vol_pass1(const VolArgs &A, const double *q, con
                                           double *GR, double *LB, double *EVB, int tid, int nt) {
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
   constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
-  constexpr int ls = D == 0 ? 1 : G;
+  constexpr int ls = D == 0 ? 1 : (D == 1 ? G : G2);
   build_lobatto<G, D>(q, QF, LB, tid, nt);
   if (SAVE == 2) {
     __syncthreads();
@@ -244,7 +244,7 @@ __device__ __forceinline__ void vol_pass2(const VolArgs &A, const double *JQ, co
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
   constexpr int NCH = DIAG ? 11 : 15;
   constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
-  constexpr int ls = D == 0 ? 1 : G;
+  constexpr int ls = D == 0 ? 1 : (D == 1 ? G : G2);
   if (D > 0) {
     for (int i = tid; i < 5 * NG; i += nt) CH[i] = JQ[i] * jac[i % NG];
     __syncthreads();
@@ -396,9 +396,10 @@ struct UpdArgs {
 template <int G> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G;
   extern __shared__ double sm[];
-  double *FB = sm;          // 30*G2 face fluxes
+  double *FB = sm;            // 30*G2 face fluxes
   double *QN = FB + 30 * G2;  // 5*NG updated physical Q
-  __shared__ double Dlo[G], Dhi[G];
+  double *Dlo = QN + 5 * NG;  // first and last columns of dmx
+  double *Dhi = Dlo + G;
   const int k = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
   const double *FF = A.FF + (long long)k * 30 * G2;
   const double *VF = A.VF + (long long)k * 30 * G2;
@@ -437,7 +438,7 @@ template <int G> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
     }
     QN[i] = q * jac[p];
   }
-  if (__any_sync(0xffffffffu, bad) && (tid & 31) == 0) atomicOr(A.flag, 1);
+  if (bad) atomicOr(A.flag, 1);
   __syncthreads();
   write_traces<G>(QN, A.QF + (long long)k * 30 * G2, tid, nt);
 }

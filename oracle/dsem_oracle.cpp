@@ -1769,6 +1769,14 @@ int orc_set_threads(int n) {
 #endif
 }
 int orc_kord(const orc_case *h) { return h->c->kord; }
+void orc_riemann(const double *nh, double ds, const double *Ql, const double *Qr, double gamma, double *flux) {
+  riemann(nh, ds, Ql, Qr, gamma, flux);
+}
+void orc_euler(const double *Q, double gamma, double *f, double *g, double *h) { euler_fluxes(Q, gamma, f, g, h); }
+void orc_vis(const double *Q, const double *Qx, const double *Qy, const double *Qz, double amu, double gamma,
+             double pr, double mach, double *f, double *g, double *h) {
+  vis_fluxes(Q, Qx, Qy, Qz, amu, gamma, pr, mach, f, g, h);
+}
 void orc_rk(const orc_case *h, double *a, double *b, double *c) {
   for (int i = 0; i < 5; ++i) {
     a[i] = h->c->ark[i];

@@ -79,6 +79,12 @@ void orc_diag(orc_case *c, double dt, int first, double *turbk, double *dissp, d
 void orc_get_muhg(const orc_case *c, double *mu, int ldx);
 int orc_set_threads(int n);
 int orc_kord(const orc_case *c);
+/* Pointwise physics for unit tests: Roe flux (PhysLib.f90:231-320), Euler and
+ * viscous fluxes (PhysLib.f90:17-124, 419-583). */
+void orc_riemann(const double *n_hat, double ds, const double *Ql, const double *Qr, double gamma, double *flux);
+void orc_euler(const double *Q, double gamma, double *f, double *g, double *h);
+void orc_vis(const double *Q, const double *Qx, const double *Qy, const double *Qz, double amu, double gamma,
+             double pr, double mach, double *f, double *g, double *h);
 void orc_rk(const orc_case *c, double *ark, double *brk, double *crk);
 
 #ifdef __cplusplus

@@ -59,6 +59,9 @@ def lib():
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_set_threads.restype = C.c_int
         L.orc_rk.argtypes = [vp, _dp, _dp, _dp]
+        L.orc_riemann.argtypes = [_dp, C.c_double, _dp, _dp, C.c_double, _dp]
+        L.orc_euler.argtypes = [_dp, C.c_double, _dp, _dp, _dp]
+        L.orc_vis.argtypes = [_dp] * 4 + [C.c_double] * 4 + [_dp] * 3
         _lib = L
     return _lib
 
@@ -82,6 +85,19 @@ def ke_weights(G):
     w = np.zeros(G ** 3)
     lib().orc_ke_weights(G, w)
     return w.reshape(G, G, G, order="F")
+
+
+def riemann(n_hat, ds, Ql, Qr, gamma=1.4):
+    f = np.zeros(5)
+    lib().orc_riemann(np.ascontiguousarray(n_hat, float), ds, np.ascontiguousarray(Ql, float),
+                      np.ascontiguousarray(Qr, float), gamma, f)
+    return f
+
+
+def euler(Q, gamma=1.4):
+    f, g, h = np.zeros(5), np.zeros(5), np.zeros(5)
+    lib().orc_euler(np.ascontiguousarray(Q, float), gamma, f, g, h)
+    return f, g, h
 
 
 def set_threads(n):

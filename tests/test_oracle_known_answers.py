@@ -1,0 +1,193 @@
+"""Known-answer tests that pin the CPU oracle.
+
+DSEM ships no test suite, fixtures or golden vectors, and its Fortran cannot
+be built here, so the restatement is pinned by properties of the mathematics
+the reference implements: exactness of the spectral operators, the mortar L2
+projections and the quadrature; Roe-flux consistency and symmetry; freestream
+preservation and discrete conservation of the full right-hand side; invariance
+under rotated element frames; analytic Taylor-Green invariants.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from dsem_b200 import mesh
+
+
+def cheb(G):
+    return mesh.gauss_points(G), mesh.lobatto_points(G + 1)
+
+
+@pytest.mark.parametrize("p", [1, 2, 4, 6, 8])
+def test_derivative_matrix_exact(oracle_mod, p):
+    """dmx differentiates polynomials of degree <= p+1 exactly (dermat, matrices.f90:144-178)."""
+    dmx, bx = oracle_mod.operators(p)
+    xg, xl = cheb(p + 1)
+    for deg in range(p + 2):
+        f = xl ** deg
+        df = deg * xg ** (deg - 1) if deg else 0 * xg
+        assert np.abs(dmx @ f - df).max() <= 1e-11 * max(1, deg * deg)
+    assert np.abs(dmx.sum(axis=1)).max() <= 1e-12
+
+
+@pytest.mark.parametrize("p", [1, 3, 5, 8])
+def test_interpolation_matrix_exact(oracle_mod, p):
+    """bx interpolates polynomials of degree <= p exactly (intrpmat, matrices.f90:185-207)."""
+    dmx, bx = oracle_mod.operators(p)
+    xg, xl = cheb(p + 1)
+    for deg in range(p + 1):
+        assert np.abs(bx @ xg ** deg - xl ** deg).max() <= 1e-13
+    assert np.abs(bx.sum(axis=1) - 1).max() <= 1e-13
+
+
+@pytest.mark.parametrize("nin,nout", [(5, 7), (7, 9), (4, 9)])
+def test_mortar_projection(oracle_mod, nin, nout):
+    """Prolongation is exact interpolation; restriction(prolongation) = identity;
+    restriction is the L2 projection (compute_pmat, mortarLib.f90:242-420)."""
+    P, R = oracle_mod.projection(nin, nout)
+    xi = mesh.gauss_points(nin)
+    xo = mesh.gauss_points(nout)
+    for deg in range(nin):
+        assert np.abs(P @ xi ** deg - xo ** deg).max() <= 1e-12
+    assert np.abs(R @ P - np.eye(nin)).max() <= 1e-12
+    # R keeps polynomials of degree < nin
+    for deg in range(nin):
+        assert np.abs(R @ xo ** deg - xi ** deg).max() <= 1e-12
+
+
+@pytest.mark.parametrize("G", [3, 5, 9])
+def test_ke_weights_integrate(oracle_mod, G):
+    """bmatu1b integrates the Gauss-node interpolant over the unit cube exactly."""
+    w = oracle_mod.ke_weights(G)
+    assert abs(w.sum() - 1.0) <= 1e-14
+    x = mesh.gauss_points(G)
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    f = X ** (G - 1) * Y * (1 - Z) ** 2
+    exact = (1.0 / G) * 0.5 * (1.0 / 3.0)
+    assert abs(np.sum(w * f) - exact) <= 1e-14
+
+
+def _state(rng):
+    rho = 0.5 + rng.random()
+    u = rng.standard_normal(3) * 0.3
+    p = 1.0 + rng.random()
+    return np.array([rho, rho * u[0], rho * u[1], rho * u[2], p / 0.4 + 0.5 * rho * u @ u])
+
+
+def test_roe_consistency_and_symmetry(oracle_mod):
+    """riemann(n, ds, Q, Q) = ds n.F(Q); swapping sides and flipping n negates the flux."""
+    rng = np.random.default_rng(3)
+    for _ in range(20):
+        n = rng.standard_normal(3)
+        n /= np.linalg.norm(n)
+        ds = 0.3 + rng.random()
+        Q = _state(rng)
+        f, g, h = oracle_mod.euler(Q)
+        ref = ds * (n[0] * f + n[1] * g + n[2] * h)
+        assert np.allclose(oracle_mod.riemann(n, ds, Q, Q), ref, rtol=1e-13, atol=1e-13)
+        Q2 = _state(rng)
+        a = oracle_mod.riemann(n, ds, Q, Q2)
+        b = oracle_mod.riemann(-n, ds, Q2, Q)
+        assert np.allclose(a, -b, rtol=1e-11, atol=1e-12)
+
+
+def _case(oracle_mod, box, re=400.0):
+    c = oracle_mod.Case.from_desc(box.desc())
+    c.set_phys(re=re)
+    return c
+
+
+@pytest.mark.parametrize("rot", [None, 13])
+def test_freestream_preservation(oracle_mod, rot):
+    n, p = 3, 4
+    r = None
+    if rot is not None:
+        r = [0] * 27
+        r[13] = rot
+    box = mesh.Box(n, n, n, p, rot=r)
+    c = _case(oracle_mod, box)
+    q = np.zeros(box.qshape()).reshape(box.nel, 5, -1)
+    st = np.array([1.1, 0.2, -0.3, 0.4, 0.0])
+    st[4] = 2.0 / 0.4 + 0.5 * (st[1] ** 2 + st[2] ** 2 + st[3] ** 2) / st[0]
+    m = box.jacob != 0
+    for v in range(5):
+        q[:, v][m] = st[v] / box.jacob[m]
+    c.set_q(q.reshape(box.qshape()))
+    qt = c.rhs()
+    scale = np.abs(q).max()
+    assert np.abs(qt).max() <= 1e-13 * scale
+
+
+def test_conservation(oracle_mod):
+    """Sum over elements of the quadrature-weighted Qt vanishes (periodic box)."""
+    n, p = 3, 5
+    box = mesh.Box(n, n, n, p)
+    c = _case(oracle_mod, box)
+    c.set_q(mesh.taylor_green(box))
+    qt = c.rhs()
+    G = p + 1
+    w = oracle_mod.ke_weights(G)  # (i, j, l) = (x, y, z)
+    q5 = qt[:, :, :G, :G, :G]  # [e][v][z][y][x]
+    tot = np.einsum("evzyx,xyz->v", q5, w)
+    mag = np.einsum("evzyx,xyz->v", np.abs(q5), w)
+    assert np.all(np.abs(tot) <= 1e-12 * mag)
+
+
+def test_rotated_frame_invariance(oracle_mod):
+    """An interior element with a rotated local frame gives the same RHS at the same physical points."""
+    n, p = 3, 4
+    r = [0] * 27
+    r[13] = 17
+    b1, b0 = mesh.Box(n, n, n, p, rot=r), mesh.Box(n, n, n, p)
+    c1, c0 = _case(oracle_mod, b1), _case(oracle_mod, b0)
+    c1.set_q(mesh.taylor_green(b1))
+    c0.set_q(mesh.taylor_green(b0))
+    q1, q0 = c1.rhs(), c0.rhs()
+    scale = np.abs(q0).max()
+    x1, x0 = b1.xg[13], b0.xg[13]
+    idx = {tuple(np.round(x, 11)): i for i, x in enumerate(x0) if b0.jacob[13, i] != 0}
+    diff = 0.0
+    for i in np.where(b1.jacob[13] != 0)[0]:
+        j = idx[tuple(np.round(x1[i], 11))]
+        diff = max(diff, np.abs(q1[13].reshape(5, -1)[:, i] - q0[13].reshape(5, -1)[:, j]).max())
+    assert diff <= 1e-10 * scale
+    assert np.abs(np.delete(q1, 13, 0) - np.delete(q0, 13, 0)).max() <= 1e-10 * scale
+
+
+def test_taylor_green_invariants(oracle_mod):
+    """KE0 = 1/8 and 100 <|w|^2>/Re = 75/Re at t = 0 (spectral accuracy)."""
+    box = mesh.Box(4, 4, 4, 6)
+    c = _case(oracle_mod, box, re=1600.0)
+    c.set_q(mesh.taylor_green(box))
+    c.rhs()
+    ke, _, eps = c.diag(1.0, True)
+    assert abs(ke - 0.125) <= 1e-10
+    assert abs(eps - 75.0 / 1600.0) <= 1e-3 * 75.0 / 1600.0
+
+
+def test_kinetic_energy_decays(oracle_mod):
+    box = mesh.Box(3, 3, 3, 4)
+    c = _case(oracle_mod, box, re=100.0)
+    c.set_q(mesh.taylor_green(box))
+    dt = 0.5 * c.dtcalc()
+    kes = []
+    for k in range(6):
+        c.step(0.0, dt, 1)
+        kes.append(c.diag(dt, k == 0)[0])
+    assert all(b < a for a, b in zip(kes, kes[1:]))
+
+
+def test_rk_coefficients(oracle_mod):
+    """Carpenter-Kennedy 2N-storage (iord 4) integrates y' = y to fourth order per step."""
+    box = mesh.Box(2, 2, 2, 2)
+    c = _case(oracle_mod, box)
+    a, b, cc = c.rk()
+    assert c.kord() == 5
+    for h in (0.1, 0.05):
+        y, g = 1.0, 0.0
+        for k in range(5):
+            g = a[k] * g + y
+            y = y + cc[k] * h * g
+        err = abs(y - math.exp(h))
+        assert err <= 2e-3 * h ** 5 * 10
