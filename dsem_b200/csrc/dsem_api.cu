@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -138,6 +139,9 @@ struct dsem_ctx {
   double ark[5] = {}, brk[5] = {}, crk[5] = {};
   std::vector<Group> groups;
   std::vector<MList> mlists;
+  MortarNC *nc = nullptr;  // p-nonconforming mortars
+  int nnc = 0;
+  double *nc_nh = nullptr, *nc_nrm = nullptr, *nc_mats = nullptr;
   std::vector<int> ext_group, ext_k;  // caller element -> (group, index in group)
   double *JQ = nullptr, *gQ = nullptr, *QTI = nullptr, *QF = nullptr, *FF = nullptr, *VF = nullptr;
   double *Qt = nullptr, *stage = nullptr, *part = nullptr;
@@ -245,6 +249,11 @@ int enqueue_stage(dsem_ctx *c, int kk, double dt, bool save, double *qt_out, lon
     }));
     ++*launches;
   }
+  if (c->nnc > 0) {
+    k_face_nc_inv<<<c->nnc, 128, 0, c->st>>>(c->nc, c->QF, c->FF, c->nc_nh, c->nc_nrm, c->nc_mats, gamma);
+    CK(cudaGetLastError());
+    ++*launches;
+  }
   const int mode = vol_mode(c, save);
   for (auto &g : c->groups) {
     VolArgs a{};
@@ -264,6 +273,11 @@ int enqueue_stage(dsem_ctx *c, int kk, double dt, bool save, double *qt_out, lon
   }
   for (auto &ml : c->mlists) {
     CK(with_G(ml.G, [&](auto g) { return Launch<decltype(g)::value>::face_vis(ml.mc, ml.n, c->VF, ml.nrm, c->st); }));
+    ++*launches;
+  }
+  if (c->nnc > 0) {
+    k_face_nc_vis<<<c->nnc, 128, 0, c->st>>>(c->nc, c->VF, c->nc_nrm, c->nc_mats);
+    CK(cudaGetLastError());
     ++*launches;
   }
   for (auto &g : c->groups) {
@@ -551,6 +565,9 @@ int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m) {
 
   // ---- mortars
   std::vector<std::vector<MortarC>> mcs(GMAX + 1);
+  std::vector<MortarNC> ncs;
+  std::vector<double> nc_nh, nc_nrm, mats;
+  std::map<long long, std::pair<int, int>> mat_off;
   std::vector<std::vector<double>> nhs(GMAX + 1), nrs(GMAX + 1);
   for (int j = 0; j < m->nmort; ++j) {
     const int *t = m->mortar + (size_t)DSEM_MORTAR_INTS * j;
@@ -563,8 +580,54 @@ int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m) {
       return fail(c, DSEM_ERR_INVALID_ARG, "bad mortar face or orientation");
     const int Gm = m->ncg[3 * id1], Gs = m->ncg[3 * id2];
     const bool conf = t[13] && t[14] && t[15] && t[16];
-    if (!conf || Gm != Gs || t[8] != Gm || t[9] != Gm)
-      return fail(c, DSEM_ERR_UNSUPPORTED, "nonconforming mortars are not supported by this build");
+    if (t[4] != Gm || t[5] != Gm || t[6] != Gs || t[7] != Gs || t[8] != std::max(Gm, Gs) || t[9] != std::max(Gm, Gs))
+      return fail(c, DSEM_ERR_UNSUPPORTED, "mortar lengths must match the element orders (geometrically conforming faces)");
+    if (!conf || Gm != Gs) {  // p-nonconforming mortar
+      MortarNC nc{};
+      const int G2m = Gm * Gm, G2s = Gs * Gs;
+      nc.ms = c->groups[c->ext_group[id1]].f0 + (long long)c->ext_k[id1] * 30 * G2m + (long long)(f1 - 1) * 5 * G2m;
+      nc.ss = c->groups[c->ext_group[id2]].f0 + (long long)c->ext_k[id2] * 30 * G2s + (long long)(f2 - 1) * 5 * G2s;
+      nc.gm = Gm;
+      nc.gs = Gs;
+      nc.lm1 = t[8];
+      nc.lm2 = t[9];
+      nc.orient = orient;
+      nc.sign = t[11];
+      nc.nsign = t[12];
+      nc.low = (f1 == 1 || f1 == 3 || f1 == 6);
+      for (int k = 0; k < 4; ++k) nc.conf[k] = t[13 + k];
+      nc.geo = (int)nc_nrm.size();
+      for (int side = 0; side < 2; ++side)
+        for (int dir = 0; dir < 2; ++dir) {
+          nc.P[side][dir] = nc.R[side][dir] = -1;
+          if (nc.conf[2 * side + dir]) continue;
+          const int nin = side == 0 ? Gm : Gs, nout = t[8 + dir];
+          const long long key = (long long)nin * 100 + nout;
+          auto it = mat_off.find(key);
+          if (it == mat_off.end()) {
+            std::vector<double> ci(nin), co(nout), P((size_t)nout * nin), R((size_t)nin * nout);
+            hostmath::gauss_points(nin, ci.data());
+            hostmath::gauss_points(nout, co.data());
+            hostmath::projection(ci.data(), nin, co.data(), nout, P.data());
+            hostmath::projection(co.data(), nout, ci.data(), nin, R.data());
+            const int po = (int)mats.size();
+            mats.insert(mats.end(), P.begin(), P.end());
+            const int ro = (int)mats.size();
+            mats.insert(mats.end(), R.begin(), R.end());
+            it = mat_off.emplace(key, std::make_pair(po, ro)).first;
+          }
+          nc.P[side][dir] = it->second.first;
+          nc.R[side][dir] = it->second.second;
+        }
+      for (int jj = 0; jj < t[9]; ++jj)
+        for (int i = 0; i < t[8]; ++i) {
+          const size_t q = (size_t)j * ldx * ldx + i + (size_t)ldx * jj;
+          nc_nrm.push_back(m->norm[q]);
+          for (int k = 0; k < 3; ++k) nc_nh.push_back(m->n_hat[q * 3 + k]);
+        }
+      ncs.push_back(nc);
+      continue;
+    }
     const int G = Gm, G2 = G * G;
     const Group &gm = c->groups[c->ext_group[id1]];
     const Group &gs = c->groups[c->ext_group[id2]];
@@ -594,6 +657,18 @@ int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m) {
     CK(cudaMalloc(&ml.nrm, nrs[G].size() * sizeof(double)));
     CK(cudaMemcpy(ml.nrm, nrs[G].data(), nrs[G].size() * sizeof(double), cudaMemcpyHostToDevice));
     c->mlists.push_back(ml);
+  }
+
+  if (!ncs.empty()) {
+    c->nnc = (int)ncs.size();
+    CK(cudaMalloc(&c->nc, ncs.size() * sizeof(MortarNC)));
+    CK(cudaMemcpy(c->nc, ncs.data(), ncs.size() * sizeof(MortarNC), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->nc_nh, nc_nh.size() * sizeof(double)));
+    CK(cudaMemcpy(c->nc_nh, nc_nh.data(), nc_nh.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->nc_nrm, nc_nrm.size() * sizeof(double)));
+    CK(cudaMemcpy(c->nc_nrm, nc_nrm.data(), nc_nrm.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->nc_mats, std::max<size_t>(1, mats.size()) * sizeof(double)));
+    if (!mats.empty()) CK(cudaMemcpy(c->nc_mats, mats.data(), mats.size() * sizeof(double), cudaMemcpyHostToDevice));
   }
 
   // ---- state and face buffers
@@ -637,6 +712,10 @@ void dsem_destroy(dsem_ctx *c) {
     cudaFree(g.kew);
     cudaFree(g.int2ext);
   }
+  cudaFree(c->nc);
+  cudaFree(c->nc_nh);
+  cudaFree(c->nc_nrm);
+  cudaFree(c->nc_mats);
   for (auto &ml : c->mlists) {
     cudaFree(ml.mc);
     cudaFree(ml.nh);
@@ -767,7 +846,8 @@ int dsem_step(dsem_ctx *c, double time, double dt, int nsteps) {
     long long cnt = 0;
     {
       // launches per graph replay: recount without enqueueing
-      cnt = (long long)c->kord * (2 * (long long)c->mlists.size() + 2 * (long long)c->groups.size()) +
+      cnt = (long long)c->kord * (2 * (long long)c->mlists.size() + 2 * (long long)c->groups.size() +
+                                  (c->nnc > 0 ? 2 : 0)) +
             (c->shock ? (long long)c->groups.size() : 0);
     }
     for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->gexec, c->st));

@@ -150,6 +150,303 @@ __global__ void __launch_bounds__(128) k_face_vis(const MortarC *__restrict__ mc
   }
 }
 
+// ------------------------------------------------------- nonconforming faces
+// One CTA per p-nonconforming mortar (lenmortar > len on at least one side).
+// Mirrors interface_flux / map_to_mortar_space / map_to_face_space /
+// rotate_to_mortar / rotate_flux_to_face (mortar_operations.f90:151-758) with
+// the consistent prolong -> flux/average -> restrict sequence.  Arrays are
+// [var][j*NMX + i] in shared memory.
+constexpr int NMX = GMAX + 1;  // mortar extents never exceed GMAX
+struct MortarNC {
+  long long ms, ss;          // face slot offsets (master, slave)
+  int gm, gs;                // Gauss points per direction on each side
+  int lm1, lm2;              // lenmortar
+  int orient, sign, nsign, low;
+  int conf[4];               // conforming (dir1,side1) (dir2,side1) (dir1,side2) (dir2,side2)
+  int geo;                   // offset of the mortar's points in n_hat/norm (lm1*lm2 points)
+  int P[2][2], R[2][2];      // offsets of prolong/restrict matrices in the matrix pool, -1 if none
+};
+
+static __device__ __forceinline__ void nc_rotate_to_mortar(const MortarNC &M, const double *src, double *dst, int tid, int nt) {
+  const int l1 = M.gs, l2 = M.gs;
+  for (int t = tid; t < NV * l1 * l2; t += nt) {
+    const int v = t / (l1 * l2), r = t - v * l1 * l2, i = r % l1, j = r / l1;
+    int ni = i, nj = j;
+    switch (M.orient) {
+      case 3: ni = i; nj = l2 - 1 - j; break;
+      case 2: ni = l1 - 1 - i; nj = l2 - 1 - j; break;
+      case 1: ni = l1 - 1 - i; nj = j; break;
+      case 4: ni = j; nj = i; break;
+      case 5: ni = l2 - 1 - j; nj = i; break;
+      case 6: ni = l2 - 1 - j; nj = l1 - 1 - i; break;
+      case 7: ni = j; nj = l1 - 1 - i; break;
+      default: break;
+    }
+    dst[v * NMX * NMX + nj * NMX + ni] = src[v * NMX * NMX + j * NMX + i];
+  }
+}
+static __device__ __forceinline__ void nc_rotate_to_face(const MortarNC &M, const double *src, double *dst, int tid, int nt) {
+  const int l1 = M.gs, l2 = M.gs;
+  for (int t = tid; t < NV * l1 * l2; t += nt) {
+    const int v = t / (l1 * l2), r = t - v * l1 * l2, i = r % l1, j = r / l1;
+    int si = i, sj = j;
+    switch (M.orient) {
+      case 3: si = i; sj = l2 - 1 - j; break;
+      case 2: si = l1 - 1 - i; sj = l2 - 1 - j; break;
+      case 1: si = l1 - 1 - i; sj = j; break;
+      case 4: si = j; sj = i; break;
+      case 5: si = l2 - 1 - j; sj = i; break;
+      case 6: si = l2 - 1 - j; sj = l1 - 1 - i; break;
+      case 7: si = j; sj = l1 - 1 - i; break;
+      default: break;
+    }
+    dst[v * NMX * NMX + j * NMX + i] = src[v * NMX * NMX + sj * NMX + si];
+  }
+}
+// y = A[nout][nin] x along one direction of a [var][j][i] array (FMA chain)
+static __device__ __forceinline__ double nc_apply(const double *A, int nin, int i, const double *x, int xs) {
+  double acc = A[i * nin] * x[0];
+  for (int k = 1; k < nin; ++k) acc = __fma_rn(A[i * nin + k], x[k * xs], acc);
+  return acc;
+}
+// map_to_mortar_space: a (mortar orientation, face extents) -> mortar extents, in place via tmp
+static __device__ void nc_to_mortar(const MortarNC &M, int side, const double *mats, double *a, double *tmp, int tid, int nt) {
+  const bool c1 = M.conf[2 * side], c2 = M.conf[2 * side + 1];
+  if (c1 && c2) return;
+  const int n = side == 0 ? M.gm : M.gs;  // isotropic: len(idir) = len(jdir)
+  if (!c1) {
+    const double *A = mats + M.P[side][0];
+    for (int t = tid; t < NV * n * M.lm1; t += nt) {
+      const int v = t / (n * M.lm1), r = t - v * n * M.lm1, i = r % M.lm1, j = r / M.lm1;
+      tmp[v * NMX * NMX + j * NMX + i] = nc_apply(A, n, i, a + v * NMX * NMX + j * NMX, 1);
+    }
+    __syncthreads();
+    for (int t = tid; t < NV * n * M.lm1; t += nt) {
+      const int v = t / (n * M.lm1), r = t - v * n * M.lm1, i = r % M.lm1, j = r / M.lm1;
+      a[v * NMX * NMX + j * NMX + i] = tmp[v * NMX * NMX + j * NMX + i];
+    }
+    __syncthreads();
+  }
+  const int m1 = c1 ? n : M.lm1;
+  if (!c2) {
+    const double *A = mats + M.P[side][1];
+    for (int t = tid; t < NV * m1 * M.lm2; t += nt) {
+      const int v = t / (m1 * M.lm2), r = t - v * m1 * M.lm2, i = r % m1, j = r / m1;
+      tmp[v * NMX * NMX + j * NMX + i] = nc_apply(A, n, j, a + v * NMX * NMX + i, NMX);
+    }
+    __syncthreads();
+    for (int t = tid; t < NV * m1 * M.lm2; t += nt) {
+      const int v = t / (m1 * M.lm2), r = t - v * m1 * M.lm2, i = r % m1, j = r / m1;
+      a[v * NMX * NMX + j * NMX + i] = tmp[v * NMX * NMX + j * NMX + i];
+    }
+    __syncthreads();
+  }
+}
+// map_to_face_space: mortar extents -> face extents (restriction), a -> out
+static __device__ void nc_to_face(const MortarNC &M, int side, const double *mats, const double *a, double *out, double *tmp,
+                           int tid, int nt) {
+  const bool c1 = M.conf[2 * side], c2 = M.conf[2 * side + 1];
+  for (int t = tid; t < NV * NMX * NMX; t += nt) out[t] = a[t];
+  __syncthreads();
+  if (c1 && c2) return;
+  const int n = side == 0 ? M.gm : M.gs;
+  if (!c1) {
+    const double *A = mats + M.R[side][0];
+    for (int t = tid; t < NV * M.lm2 * n; t += nt) {
+      const int v = t / (M.lm2 * n), r = t - v * M.lm2 * n, i = r % n, j = r / n;
+      tmp[v * NMX * NMX + j * NMX + i] = nc_apply(A, M.lm1, i, out + v * NMX * NMX + j * NMX, 1);
+    }
+    __syncthreads();
+    for (int t = tid; t < NV * M.lm2 * n; t += nt) {
+      const int v = t / (M.lm2 * n), r = t - v * M.lm2 * n, i = r % n, j = r / n;
+      out[v * NMX * NMX + j * NMX + i] = tmp[v * NMX * NMX + j * NMX + i];
+    }
+    __syncthreads();
+  }
+  const int m1 = c1 ? M.lm1 : n;
+  if (!c2) {
+    const double *A = mats + M.R[side][1];
+    for (int t = tid; t < NV * m1 * n; t += nt) {
+      const int v = t / (m1 * n), r = t - v * m1 * n, i = r % m1, j = r / m1;
+      tmp[v * NMX * NMX + j * NMX + i] = nc_apply(A, M.lm2, j, out + v * NMX * NMX + i, NMX);
+    }
+    __syncthreads();
+    for (int t = tid; t < NV * m1 * n; t += nt) {
+      const int v = t / (m1 * n), r = t - v * m1 * n, i = r % m1, j = r / m1;
+      out[v * NMX * NMX + j * NMX + i] = tmp[v * NMX * NMX + j * NMX + i];
+    }
+    __syncthreads();
+  }
+}
+
+static __global__ void __launch_bounds__(128) k_face_nc_inv(const MortarNC *__restrict__ mn, double *__restrict__ QF,
+                                                     double *__restrict__ FF, const double *__restrict__ nh,
+                                                     const double *__restrict__ nrm, const double *__restrict__ mats,
+                                                     double gamma) {
+  __shared__ double A1[NV * NMX * NMX], A2[NV * NMX * NMX], T0[NV * NMX * NMX], FL[NV * NMX * NMX],
+      AV[NV * NMX * NMX];
+  const MortarNC M = mn[blockIdx.x];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int gm2 = M.gm * M.gm, gs2 = M.gs * M.gs;
+  for (int t = tid; t < NV * NMX * NMX; t += nt) A1[t] = A2[t] = T0[t] = FL[t] = AV[t] = 0.0;
+  __syncthreads();
+  for (int t = tid; t < NV * gm2; t += nt) {
+    const int v = t / gm2, p = t - v * gm2;
+    A1[v * NMX * NMX + (p / M.gm) * NMX + p % M.gm] = QF[M.ms + t];
+  }
+  for (int t = tid; t < NV * gs2; t += nt) {
+    const int v = t / gs2, p = t - v * gs2;
+    T0[v * NMX * NMX + (p / M.gs) * NMX + p % M.gs] = QF[M.ss + t];
+  }
+  __syncthreads();
+  if (M.orient) {
+    nc_rotate_to_mortar(M, T0, A2, tid, nt);
+  } else {
+    for (int t = tid; t < NV * NMX * NMX; t += nt) A2[t] = T0[t];
+  }
+  __syncthreads();
+  nc_to_mortar(M, 0, mats, A1, T0, tid, nt);
+  nc_to_mortar(M, 1, mats, A2, T0, tid, nt);
+  for (int t = tid; t < M.lm1 * M.lm2; t += nt) {
+    const int i = t % M.lm1, j = t / M.lm1;
+    double Q1[NV], Q2[NV], f[NV];
+    for (int v = 0; v < NV; ++v) {
+      Q1[v] = A1[v * NMX * NMX + j * NMX + i];
+      Q2[v] = A2[v * NMX * NMX + j * NMX + i];
+    }
+    const long long gp = (long long)M.geo + t;
+    const double n3[3] = {nh[gp * 3], nh[gp * 3 + 1], nh[gp * 3 + 2]};
+    riemann(n3, nrm[gp], M.low ? Q2 : Q1, M.low ? Q1 : Q2, gamma, f);
+    for (int v = 0; v < NV; ++v) {
+      FL[v * NMX * NMX + j * NMX + i] = f[v];
+      AV[v * NMX * NMX + j * NMX + i] = (Q1[v] + Q2[v]) * 0.5;
+    }
+  }
+  __syncthreads();
+  // master side: restrict flux and average, write face slots
+  nc_to_face(M, 0, mats, FL, A1, T0, tid, nt);
+  for (int t = tid; t < NV * gm2; t += nt) {
+    const int v = t / gm2, p = t - v * gm2;
+    FF[M.ms + t] = A1[v * NMX * NMX + (p / M.gm) * NMX + p % M.gm];
+  }
+  __syncthreads();
+  nc_to_face(M, 0, mats, AV, A1, T0, tid, nt);
+  for (int t = tid; t < NV * gm2; t += nt) {
+    const int v = t / gm2, p = t - v * gm2;
+    QF[M.ms + t] = A1[v * NMX * NMX + (p / M.gm) * NMX + p % M.gm];
+  }
+  __syncthreads();
+  // slave side: restrict, rotate to the face, sign on the flux
+  const double sgn = (double)M.sign;
+  nc_to_face(M, 1, mats, FL, A1, T0, tid, nt);
+  if (M.orient) {
+    nc_rotate_to_face(M, A1, A2, tid, nt);
+  } else {
+    for (int t = tid; t < NV * NMX * NMX; t += nt) A2[t] = A1[t];
+  }
+  __syncthreads();
+  for (int t = tid; t < NV * gs2; t += nt) {
+    const int v = t / gs2, p = t - v * gs2;
+    FF[M.ss + t] = sgn * A2[v * NMX * NMX + (p / M.gs) * NMX + p % M.gs];
+  }
+  __syncthreads();
+  nc_to_face(M, 1, mats, AV, A1, T0, tid, nt);
+  if (M.orient) {
+    nc_rotate_to_face(M, A1, A2, tid, nt);
+  } else {
+    for (int t = tid; t < NV * NMX * NMX; t += nt) A2[t] = A1[t];
+  }
+  __syncthreads();
+  for (int t = tid; t < NV * gs2; t += nt) {
+    const int v = t / gs2, p = t - v * gs2;
+    QF[M.ss + t] = A2[v * NMX * NMX + (p / M.gs) * NMX + p % M.gs];
+  }
+}
+
+static __global__ void __launch_bounds__(128) k_face_nc_vis(const MortarNC *__restrict__ mn, double *__restrict__ VF,
+                                                     const double *__restrict__ nrm, const double *__restrict__ mats) {
+  __shared__ double R1[NV * NMX * NMX], R2[NV * NMX * NMX], T0[NV * NMX * NMX], QB[NV * NMX * NMX],
+      T1[NV * NMX * NMX];
+  const MortarNC M = mn[blockIdx.x];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int gm2 = M.gm * M.gm, gs2 = M.gs * M.gs;
+  const bool conf1 = M.conf[0] && M.conf[1], conf2 = M.conf[2] && M.conf[3];
+  const double *nm = nrm + M.geo;  // mortar points, index i + lm1*j
+  for (int t = tid; t < NV * NMX * NMX; t += nt) R1[t] = R2[t] = T0[t] = QB[t] = T1[t] = 0.0;
+  __syncthreads();
+  for (int t = tid; t < NV * gm2; t += nt) {
+    const int v = t / gm2, p = t - v * gm2;
+    R1[v * NMX * NMX + (p / M.gm) * NMX + p % M.gm] = VF[M.ms + t];
+  }
+  for (int t = tid; t < NV * gs2; t += nt) {
+    const int v = t / gs2, p = t - v * gs2;
+    R2[v * NMX * NMX + (p / M.gs) * NMX + p % M.gs] = VF[M.ss + t];
+  }
+  __syncthreads();
+  // fv1: master side on mortar points
+  if (!conf1) nc_to_mortar(M, 0, mats, R1, T0, tid, nt);
+  for (int t = tid; t < NV * M.lm1 * M.lm2; t += nt) {
+    const int v = t / (M.lm1 * M.lm2), r = t - v * M.lm1 * M.lm2, i = r % M.lm1, j = r / M.lm1;
+    R1[v * NMX * NMX + j * NMX + i] = R1[v * NMX * NMX + j * NMX + i] / nm[i + M.lm1 * j];
+  }
+  __syncthreads();
+  // fv2: slave side (conforming: divide in face indexing, then rotate)
+  if (conf2) {
+    for (int t = tid; t < NV * gs2; t += nt) {
+      const int v = t / gs2, p = t - v * gs2, i = p % M.gs, j = p / M.gs;
+      R2[v * NMX * NMX + j * NMX + i] = R2[v * NMX * NMX + j * NMX + i] / nm[i + M.lm1 * j];
+    }
+    __syncthreads();
+    if (M.orient) {
+      nc_rotate_to_mortar(M, R2, T1, tid, nt);
+      __syncthreads();
+      for (int t = tid; t < NV * NMX * NMX; t += nt) R2[t] = T1[t];
+      __syncthreads();
+    }
+  } else {
+    if (M.orient) {
+      nc_rotate_to_mortar(M, R2, T1, tid, nt);
+      __syncthreads();
+      for (int t = tid; t < NV * NMX * NMX; t += nt) R2[t] = T1[t];
+      __syncthreads();
+    }
+    nc_to_mortar(M, 1, mats, R2, T0, tid, nt);
+    for (int t = tid; t < NV * M.lm1 * M.lm2; t += nt) {
+      const int v = t / (M.lm1 * M.lm2), r = t - v * M.lm1 * M.lm2, i = r % M.lm1, j = r / M.lm1;
+      R2[v * NMX * NMX + j * NMX + i] = R2[v * NMX * NMX + j * NMX + i] / nm[i + M.lm1 * j];
+    }
+    __syncthreads();
+  }
+  for (int t = tid; t < NV * M.lm1 * M.lm2; t += nt) {
+    const int v = t / (M.lm1 * M.lm2), r = t - v * M.lm1 * M.lm2, i = r % M.lm1, j = r / M.lm1;
+    double Qs = R2[v * NMX * NMX + j * NMX + i];
+    if (M.nsign == -1) Qs = -Qs;
+    const double Qm = R1[v * NMX * NMX + j * NMX + i];
+    QB[v * NMX * NMX + j * NMX + i] = 0.5 * (Qm + Qs) * nm[i + M.lm1 * j];
+  }
+  __syncthreads();
+  nc_to_face(M, 0, mats, QB, R1, T0, tid, nt);
+  for (int t = tid; t < NV * gm2; t += nt) {
+    const int v = t / gm2, p = t - v * gm2;
+    VF[M.ms + t] = R1[v * NMX * NMX + (p / M.gm) * NMX + p % M.gm];
+  }
+  __syncthreads();
+  if (M.sign == -1)
+    for (int t = tid; t < NV * NMX * NMX; t += nt) QB[t] = -QB[t];
+  __syncthreads();
+  nc_to_face(M, 1, mats, QB, R1, T0, tid, nt);
+  if (M.orient) {
+    nc_rotate_to_face(M, R1, R2, tid, nt);
+  } else {
+    for (int t = tid; t < NV * NMX * NMX; t += nt) R2[t] = R1[t];
+  }
+  __syncthreads();
+  for (int t = tid; t < NV * gs2; t += nt) {
+    const int v = t / gs2, p = t - v * gs2;
+    VF[M.ss + t] = R2[v * NMX * NMX + (p / M.gs) * NMX + p % M.gs];
+  }
+}
+
 // ------------------------------------------------------------------ volume
 struct VolArgs {
   const double *JQ;

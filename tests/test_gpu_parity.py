@@ -140,3 +140,51 @@ def test_nonfinite_state_reports_error(oracle_mod):
     # the context stays usable after the error
     s.upload(mesh.taylor_green(box))
     s.step(1e-3, 1)
+
+
+def _band(n, p_out, p_in):
+    orders = np.full(n ** 3, p_out)
+    for iz in range(n):
+        for ix in range(n):
+            for iy in range(n):
+                if n // 3 <= ix < n - n // 3:
+                    orders[iy + n * (ix + n * iz)] = p_in
+    return orders
+
+
+@pytest.mark.parametrize("p_out,p_in", [(4, 6), (6, 8)])
+def test_rhs_nonconforming_band(oracle_mod, p_out, p_in):
+    """p-nonconforming mortars (consistent L2 prolong / restrict) against the oracle."""
+    box = mesh.Box(3, 3, 3, _band(3, p_out, p_in))
+    assert (~box.mortar[:, 13:17].all(axis=1)).any()
+    q = mesh.taylor_green(box)
+    s, c = _pair(oracle_mod, box, q, re=800.0)
+    assert relmax(s.rhs(), c.rhs()) <= RHS_TOL
+
+
+def test_entropy_viscosity_steps(oracle_mod):
+    """EV (shock on): coefficient and state after 4 steps against the oracle."""
+    box = mesh.Box(3, 3, 3, 5)
+    q = mesh.random_isotropic(box, seed=11)
+    phys = dict(re=400.0, cmu=1.0, mumax=0.5, shock=1)
+    s, c = _pair(oracle_mod, box, q, **phys)
+    dt = 0.3 * c.dtcalc()
+    for k in range(4):
+        s.step(dt, 1)
+        c.step(0.0, dt, 1)
+        mo, mg = c.muhg(), s.muhg()
+        assert np.abs(mg - mo).max() <= 1e-12 * max(np.abs(mo).max(), 1e-300), k
+    assert np.abs(c.muhg()).max() > 0
+    assert relmax(s.download(), c.get_q()) <= 1e-12
+
+
+def test_cfg3_layout_small(oracle_mod):
+    """cfg 3 ingredients on a small box: p-nonconforming band + EV + isotropic turbulence."""
+    box = mesh.Box(3, 3, 3, _band(3, 6, 8))
+    q = mesh.random_isotropic(box, seed=5)
+    phys = dict(re=800.0, cmu=1.0, mumax=0.2, shock=1)
+    s, c = _pair(oracle_mod, box, q, **phys)
+    dt = 0.3 * c.dtcalc()
+    s.step(dt, 3)
+    c.step(0.0, dt, 3)
+    assert relmax(s.download(), c.get_q()) <= 1e-12

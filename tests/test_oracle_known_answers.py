@@ -191,3 +191,55 @@ def test_rk_coefficients(oracle_mod):
             y = y + cc[k] * h * g
         err = abs(y - math.exp(h))
         assert err <= 2e-3 * h ** 5 * 10
+
+
+def band_orders(n, p_out=6, p_in=8):
+    """cfg 3 layout: the middle third in x at a higher order (p-nonconforming band)."""
+    orders = np.full(n ** 3, p_out)
+    for iz in range(n):
+        for ix in range(n):
+            for iy in range(n):
+                if n // 3 <= ix < n - n // 3:
+                    orders[iy + n * (ix + n * iz)] = p_in
+    return orders
+
+
+def test_nonconforming_band_freestream_and_conservation(oracle_mod):
+    n = 3
+    box = mesh.Box(n, n, n, band_orders(n, 4, 6))
+    assert (~box.mortar[:, 13:17].all(axis=1)).any()
+    c = _case(oracle_mod, box)
+    # freestream
+    q = np.zeros(box.qshape()).reshape(box.nel, 5, -1)
+    st = np.array([1.0, 0.3, 0.1, -0.2, 0.0])
+    st[4] = 2.0 / 0.4 + 0.5 * (st[1] ** 2 + st[2] ** 2 + st[3] ** 2) / st[0]
+    m = box.jacob != 0
+    for v in range(5):
+        q[:, v][m] = st[v] / box.jacob[m]
+    c.set_q(q.reshape(box.qshape()))
+    assert np.abs(c.rhs()).max() <= 1e-12 * np.abs(q).max()
+    # conservation across the nonconforming faces
+    c.set_q(mesh.taylor_green(box))
+    qt = c.rhs()
+    tot = np.zeros(5)
+    mag = np.zeros(5)
+    for e in range(box.nel):
+        G = int(box.G[e])
+        w = oracle_mod.ke_weights(G)
+        q5 = qt[e, :, :G, :G, :G]
+        tot += np.einsum("vzyx,xyz->v", q5, w)
+        mag += np.einsum("vzyx,xyz->v", np.abs(q5), w)
+    assert np.all(np.abs(tot) <= 1e-12 * mag)
+
+
+def test_entropy_viscosity_bounds(oracle_mod):
+    box = mesh.Box(3, 3, 3, 4)
+    c = _case(oracle_mod, box, re=400.0)
+    c.set_phys(re=400.0, cmu=1.0, mumax=0.5, shock=1)
+    c.set_q(mesh.random_isotropic(box, seed=7))
+    dt = 0.3 * c.dtcalc()
+    c.step(0.0, dt, 1)
+    assert np.all(c.muhg() == 0.0)  # no Lobatto arrays before the first Fluxes call
+    c.step(0.0, dt, 2)
+    mu = c.muhg()[:, :5, :5, :5]
+    assert mu.max() > 0.0 and mu.min() >= 0.0 and mu.max() <= 0.5
