@@ -402,6 +402,9 @@ namespace {
 int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m);
 }
 
+// error text of calls made without a context (read by dsem_last_error(NULL))
+void dsem_set_thread_error(const std::string &msg) { g_create_err = msg; }
+
 extern "C" {
 
 const char *dsem_last_error(const dsem_ctx *c) { return c ? c->err.c_str() : g_create_err.c_str(); }

@@ -119,6 +119,38 @@ int dsem_last_timing(const dsem_ctx *ctx, double *ms, long long *launches);
  * volume, viscous face, divergence + update}.  The state is left unchanged. */
 int dsem_profile_rhs(dsem_ctx *ctx, int reps, double *ms);
 
+/* Size of the static device array that holds the working buffers of
+ * dsem_rhs_noalloc: 2^20 doubles (8 MiB) on every GPU that loads the library. */
+#define DSEM_NOALLOC_SCRATCH_DOUBLES (1 << 20)
+
+/* No counterpart in the reference (DSEM's Fortran allocates all its arrays at
+ * start-up and has no GPU path).  The right-hand side of dsem_rhs for callers
+ * that cannot allocate device memory -- applications whose GPU memory is owned
+ * by their own pool allocator or fixed at start-up, where a cudaMalloc inside a
+ * library fails or breaks their budget.  It allocates nothing: inputs and output
+ * are the caller's device arrays, and the working buffers live in one static
+ * device array of DSEM_NOALLOC_SCRATCH_DOUBLES doubles.
+ *   Limits: one order p (1..8) for every element, fully periodic conforming
+ *   mesh, axis-aligned (diagonal) metrics, and
+ *   nel*(90*(p+1)^2 + 5*(p+1)^3) + 1 <= DSEM_NOALLOC_SCRATCH_DOUBLES
+ *   (95 elements at p = 8, 364 at p = 4); larger meshes are rejected with
+ *   DSEM_ERR_INVALID_ARG and a message from dsem_last_error(NULL).
+ *   Device arrays (G = p+1, L = p+2, element-major, x fastest):
+ *     mortar      [nmort][DSEM_MORTAR_INTS]  same rows as dsem_mesh_desc.mortar
+ *     n_hat, norm [nmort][G*G][3], [nmort][G*G]  (mortar point i + G*j)
+ *     JQ, Qt      [nel][5][G^3]   (Qt is the output, the rest are read)
+ *     jac         [nel][G^3]      d%jacob
+ *     gmetg_diag  [nel][3][G^3]   gmetg(d,d) at the Gauss points
+ *     gmet_diag   [nel][3][L*G^2] gmet(d,d) on staggered grid d
+ *   The first call on a device does a one-time set-up with that device current
+ *   (scratch address, operator tables); make it before any stream capture.
+ *   Every call shares the scratch array and leaves its contents behind: calls
+ *   whose work overlaps on the GPU race on it.  The call runs on `stream`
+ *   (cudaStream_t, NULL = default stream) and waits for it before returning. */
+int dsem_rhs_noalloc(int nel, int p, int nmort, const int *mortar, const double *n_hat, const double *norm,
+                     const double *JQ, const double *jac, const double *gmetg_diag, const double *gmet_diag,
+                     double gamma, double re, double pr, double mach, double *Qt, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,88 @@
+"""dsem_rhs_noalloc: the right-hand side for callers that cannot allocate device
+memory (applications whose GPU memory belongs to their own pool allocator or
+is fixed at start-up).  The caller owns every input and output buffer -- here
+torch allocates them, standing in for such an application -- and the library
+works in its static scratch array.  The result must equal dsem_rhs on the same
+state, on two calls in a row (the second call reuses the scratch array the
+first one left behind).
+
+This file is collected last so that a failure here cannot hide the result of
+any other test; it also passes on its own in a fresh process.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from dsem_b200 import mesh
+
+pytestmark = pytest.mark.gpu
+
+RHS_TOL = 1e-12
+
+
+def internal_arrays(box, q):
+    """Device-layout inputs: element-major, x fastest, no padding."""
+    G, L, ldx, ne = int(box.G[0]), int(box.G[0]) + 1, box.ldx, box.nel
+    jq = np.ascontiguousarray(q[:, :, :G, :G, :G])
+    jac = np.ascontiguousarray(box.jacob.reshape(ne, ldx, ldx, ldx)[:, :G, :G, :G])
+    gmg = box.gmetg.reshape(ne, ldx, ldx, ldx, 9)
+    gg = np.ascontiguousarray(np.stack([gmg[:, :G, :G, :G, d + 3 * d] for d in range(3)], axis=1))
+    gm5 = box.gmet.reshape(ne, ldx, ldx, ldx, 9)
+    gm = np.stack([gm5[:, :G, :G, :L, 0].reshape(ne, -1), gm5[:, :G, :L, :G, 4].reshape(ne, -1),
+                   gm5[:, :L, :G, :G, 8].reshape(ne, -1)], axis=1)
+    nh = np.ascontiguousarray(box.n_hat[:, :G, :G, :])
+    nrm = np.ascontiguousarray(box.norm[:, :G, :G])
+    return dict(JQ=jq, jac=jac, gg=gg, gm=np.ascontiguousarray(gm), nh=nh, nrm=nrm,
+                mortar=np.ascontiguousarray(box.mortar))
+
+
+def call_noalloc(lib, box, arrs, torch, p, re=1600.0):
+    dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in arrs.items()}
+    G = p + 1
+    qt = torch.zeros((box.nel, 5, G, G, G), dtype=torch.float64, device="cuda")
+    dp = lambda t: C.c_void_p(t.data_ptr())
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = lib.dsem_rhs_noalloc(box.nel, p, box.nmort, dp(dev["mortar"]), dp(dev["nh"]), dp(dev["nrm"]), dp(dev["JQ"]),
+                              dp(dev["jac"]), dp(dev["gg"]), dp(dev["gm"]), C.c_double(1.4), C.c_double(re),
+                              C.c_double(0.72), C.c_double(1.0), dp(qt), stream)
+    return rc, qt.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from dsem_b200 import solver
+    L = solver.lib()
+    L.dsem_rhs_noalloc.restype = C.c_int
+    L.dsem_rhs_noalloc.argtypes = [C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 7 + [C.c_double] * 4 + \
+        [C.c_void_p, C.c_void_p]
+    return L
+
+
+@pytest.mark.parametrize("n,p", [(3, 4), (2, 8)])
+def test_noalloc_matches_rhs_twice(lib, n, p):
+    import torch
+    from dsem_b200.solver import Solver
+    box = mesh.Box(n, n, n, p)
+    q = mesh.taylor_green(box)
+    s = Solver(box.desc(), re=1600.0)
+    s.upload(q)
+    G = p + 1
+    ref = s.rhs()[:, :, :G, :G, :G]
+    arrs = internal_arrays(box, q)
+    for call in range(2):
+        rc, got = call_noalloc(lib, box, arrs, torch, p)
+        assert rc == 0, lib.dsem_last_error(None)
+        err = float(np.abs(got - ref).max() / np.abs(ref).max())
+        assert err <= RHS_TOL, (call, err)
+
+
+def test_noalloc_rejects_oversized_mesh(lib):
+    """Sizes beyond the static scratch are refused with a clear message, before any device work."""
+    p = 8
+    nel = 96  # 96 * (90*81 + 5*729) + 1 > 2^20
+    rc = lib.dsem_rhs_noalloc(nel, p, 0, None, None, None, C.c_void_p(1), C.c_void_p(1), C.c_void_p(1),
+                              C.c_void_p(1), C.c_double(1.4), C.c_double(1600.0), C.c_double(0.72), C.c_double(1.0),
+                              C.c_void_p(1), None)
+    assert rc == -1
+    assert b"too large" in lib.dsem_last_error(None)
