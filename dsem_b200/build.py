@@ -14,11 +14,12 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-OBJ = os.path.join(HERE, "_build")
-LIB = os.path.join(HERE, "libdsem_b200.so")
+OBJ = os.environ.get("DSEM_BUILD_DIR", os.path.join(HERE, "_build"))
+LIB = os.environ.get("DSEM_LIB_OUT", os.path.join(HERE, "libdsem_b200.so"))
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "--fmad=false", "-lineinfo",
-         "-Xcompiler", "-fPIC", "-ccbin", "/usr/bin/g++", "-I", os.path.join(HERE, "..", "include")]
+         "-Xcompiler", "-fPIC", "-ccbin", "/usr/bin/g++", "-I", os.path.join(HERE, "..", "include")] + \
+    os.environ.get("DSEM_NVCC_EXTRA", "").split()
 
 
 def _sources():

@@ -293,6 +293,7 @@ int enqueue_stage(dsem_ctx *c, int kk, double dt, bool save, double *qt_out, lon
     u.Qt_out = qt_out ? qt_out + g.q0 : nullptr;
     u.flag = c->flag;
     u.re = c->P.re;
+    u.r_re = c->P.r_re;
     u.update = kk > 0;
     u.first = kk == 1;
     u.ark = kk > 0 ? c->ark[kk - 1] : 0.0;
@@ -439,6 +440,7 @@ int dsem_create(const dsem_mesh_desc *m, const dsem_phys *ph, dsem_ctx **out) {
   c->P.cmu = ph->cmu;
   c->P.mumax = ph->mumax;
   c->P.ducros = (ph->shock & 2) ? 1 : 0;
+  phys_recips(c->P);
   c->shock = ph->shock ? 1 : 0;
   c->iord = ph->iord;
   rkcoefs(c, ph->iord);
@@ -975,6 +977,7 @@ int dsem_profile_rhs(dsem_ctx *c, int reps, double *ms) {
       u.QF = c->QF + g.f0;
       u.flag = c->flag;
       u.re = c->P.re;
+      u.r_re = c->P.r_re;
       u.update = 0;
       CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::update(u, g.nel, c->st); }));
     }

@@ -50,7 +50,29 @@ template <int G> struct Op {
 struct Phys {
   double gamma, re, pr, mach, cmu, mumax;
   int ducros;
+  // correctly rounded reciprocals of the constant divisors, filled on the host
+  double r_gm1, r_3, r_den, r_re;  // 1/(gamma-1), 1/3, 1/(pr*mach*mach*(gamma-1)), 1/re
 };
+
+// Fills the reciprocals of Phys from its constants (host side, IEEE division).
+inline void phys_recips(Phys &P) {
+  P.r_gm1 = 1.0 / (P.gamma - 1.0);
+  P.r_3 = 1.0 / 3.0;
+  P.r_den = 1.0 / (P.pr * P.mach * P.mach * (P.gamma - 1.0));
+  P.r_re = 1.0 / P.re;
+}
+
+// Correctly rounded a/b from rb = RN(1/b): one Newton correction on the
+// product, q = q0 + (a - b q0) rb with the residual exact through an FMA
+// (P. Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Develop. 34(1), 1990).  Equal to the
+// IEEE quotient for the operand ranges of this solver (no overflow or
+// underflow); the parity tests compare against plain division bit for bit.
+__device__ __forceinline__ double ddiv(double a, double b, double rb) {
+  const double q0 = a * rb;
+  const double r = __fma_rn(-q0, b, a);
+  return __fma_rn(r, rb, q0);
+}
 
 // ------------------------------------------------------------ line helpers
 // Line (a,b) of direction d.  Gauss arrays: base/stride; grid-d arrays: base/stride.
@@ -118,9 +140,9 @@ __device__ __forceinline__ void contract_reg(const double *__restrict__ x, int x
 
 // -------------------------------------------------------------- physics
 // Euler flux of direction d (PhysLib.f90:17-124)
-__device__ __forceinline__ void euler_flux(int d, const double *Q, double gamma, double *f) {
+__device__ __forceinline__ void euler_flux(int d, const double *Q, double rr, double gamma, double *f) {
   double rho = Q[0], rhou = Q[1], rhov = Q[2], rhow = Q[3], rhoe = Q[4];
-  double u = rhou / rho, v = rhov / rho, w = rhow / rho;
+  double u = ddiv(rhou, rho, rr), v = ddiv(rhov, rho, rr), w = ddiv(rhow, rho, rr);
   double p = (gamma - 1.0) * (rhoe - 0.5 * rho * (u * u + v * v + w * w));
   if (d == 0) {
     f[0] = rhou; f[1] = p + rhou * u; f[2] = rhou * v; f[3] = rhou * w; f[4] = u * (rhoe + p);
@@ -130,9 +152,9 @@ __device__ __forceinline__ void euler_flux(int d, const double *Q, double gamma,
     f[0] = rhow; f[1] = rhou * w; f[2] = rhov * w; f[3] = p + rhow * w; f[4] = w * (rhoe + p);
   }
 }
-__device__ __forceinline__ void euler_fluxes3(const double *Q, double gamma, double *f, double *g, double *h) {
+__device__ __forceinline__ void euler_fluxes3(const double *Q, double rr, double gamma, double *f, double *g, double *h) {
   double rho = Q[0], rhou = Q[1], rhov = Q[2], rhow = Q[3], rhoe = Q[4];
-  double u = rhou / rho, v = rhov / rho, w = rhow / rho;
+  double u = ddiv(rhou, rho, rr), v = ddiv(rhov, rho, rr), w = ddiv(rhow, rho, rr);
   double p = (gamma - 1.0) * (rhoe - 0.5 * rho * (u * u + v * v + w * w));
   f[0] = rhou; f[1] = p + rhou * u; f[2] = rhou * v; f[3] = rhou * w; f[4] = u * (rhoe + p);
   g[0] = rhov; g[1] = rhou * v; g[2] = p + rhov * v; g[3] = rhow * v; g[4] = v * (rhoe + p);
@@ -196,65 +218,65 @@ __device__ __forceinline__ void riemann(const double *nh, double ds, const doubl
 // Viscous fluxes (PhysLib.f90:419-583).  GX/GY/GZ hold the gradient
 // components of the five conserved variables (x, y, z derivatives).
 // The directional versions compute only what their flux vector reads.
-__device__ __forceinline__ void vis_flux_x(const double *Q, const double *Qx, const double *Qy, const double *Qz,
-                                           double amu, const Phys &P, double *f) {
+__device__ __forceinline__ void vis_flux_x(const double *Q, double rr, const double *Qx, const double *Qy,
+                                           const double *Qz, double amu, const Phys &P, double *f) {
   const double gamma = P.gamma;
   double rho = Q[0], rhou = Q[1], rhov = Q[2], rhow = Q[3], rhoe = Q[4];
-  double u = rhou / rho, v = rhov / rho, w = rhow / rho;
+  double u = ddiv(rhou, rho, rr), v = ddiv(rhov, rho, rr), w = ddiv(rhow, rho, rr);
   double p = (gamma - 1.0) * (rhoe - 0.5 * rho * (u * u + v * v + w * w));
-  double ux = (Qx[1] - u * Qx[0]) / rho, uy = (Qy[1] - u * Qy[0]) / rho, uz = (Qz[1] - u * Qz[0]) / rho;
-  double vx = (Qx[2] - v * Qx[0]) / rho, vy = (Qy[2] - v * Qy[0]) / rho;
-  double wx = (Qx[3] - w * Qx[0]) / rho, wz = (Qz[3] - w * Qz[0]) / rho;
+  double ux = ddiv(Qx[1] - u * Qx[0], rho, rr), uy = ddiv(Qy[1] - u * Qy[0], rho, rr), uz = ddiv(Qz[1] - u * Qz[0], rho, rr);
+  double vx = ddiv(Qx[2] - v * Qx[0], rho, rr), vy = ddiv(Qy[2] - v * Qy[0], rho, rr);
+  double wx = ddiv(Qx[3] - w * Qx[0], rho, rr), wz = ddiv(Qz[3] - w * Qz[0], rho, rr);
   double px = (gamma - 1.0) * (Qx[4] - 0.5 * Qx[0] * (u * u + v * v + w * w) - rho * (u * ux + v * vx + w * wx));
-  double tx = (px - p * Qx[0] / rho) * P.mach * P.mach * gamma / rho;
-  double akappa = 1.0 + (amu - 1.0) * 2.0e-1 / (gamma - 1.0);
+  double tx = ddiv((px - ddiv(p * Qx[0], rho, rr)) * P.mach * P.mach * gamma, rho, rr);
+  double akappa = 1.0 + ddiv((amu - 1.0) * 2.0e-1, gamma - 1.0, P.r_gm1);
   double div = ux + vy + wz;
   double sxy = uy + vx, sxz = wx + uz;
   f[0] = 0.0;
-  f[1] = 2.0 * amu * (ux - div / 3.0);
+  f[1] = 2.0 * amu * (ux - ddiv(div, 3.0, P.r_3));
   f[2] = amu * sxy;
   f[3] = amu * sxz;
-  f[4] = u * f[1] + v * f[2] + w * f[3] + akappa * tx / (P.pr * P.mach * P.mach * (gamma - 1.0));
+  f[4] = u * f[1] + v * f[2] + w * f[3] + ddiv(akappa * tx, P.pr * P.mach * P.mach * (gamma - 1.0), P.r_den);
 }
-__device__ __forceinline__ void vis_flux_y(const double *Q, const double *Qx, const double *Qy, const double *Qz,
-                                           double amu, const Phys &P, double *g) {
+__device__ __forceinline__ void vis_flux_y(const double *Q, double rr, const double *Qx, const double *Qy,
+                                           const double *Qz, double amu, const Phys &P, double *g) {
   const double gamma = P.gamma;
   double rho = Q[0], rhou = Q[1], rhov = Q[2], rhow = Q[3], rhoe = Q[4];
-  double u = rhou / rho, v = rhov / rho, w = rhow / rho;
+  double u = ddiv(rhou, rho, rr), v = ddiv(rhov, rho, rr), w = ddiv(rhow, rho, rr);
   double p = (gamma - 1.0) * (rhoe - 0.5 * rho * (u * u + v * v + w * w));
-  double ux = (Qx[1] - u * Qx[0]) / rho, uy = (Qy[1] - u * Qy[0]) / rho;
-  double vx = (Qx[2] - v * Qx[0]) / rho, vy = (Qy[2] - v * Qy[0]) / rho, vz = (Qz[2] - v * Qz[0]) / rho;
-  double wy = (Qy[3] - w * Qy[0]) / rho, wz = (Qz[3] - w * Qz[0]) / rho;
+  double ux = ddiv(Qx[1] - u * Qx[0], rho, rr), uy = ddiv(Qy[1] - u * Qy[0], rho, rr);
+  double vx = ddiv(Qx[2] - v * Qx[0], rho, rr), vy = ddiv(Qy[2] - v * Qy[0], rho, rr), vz = ddiv(Qz[2] - v * Qz[0], rho, rr);
+  double wy = ddiv(Qy[3] - w * Qy[0], rho, rr), wz = ddiv(Qz[3] - w * Qz[0], rho, rr);
   double py = (gamma - 1.0) * (Qy[4] - 0.5 * Qy[0] * (u * u + v * v + w * w) - rho * (u * uy + v * vy + w * wy));
-  double ty = (py - p * Qy[0] / rho) * P.mach * P.mach * gamma / rho;
-  double akappa = 1.0 + (amu - 1.0) * 2.0e-1 / (gamma - 1.0);
+  double ty = ddiv((py - ddiv(p * Qy[0], rho, rr)) * P.mach * P.mach * gamma, rho, rr);
+  double akappa = 1.0 + ddiv((amu - 1.0) * 2.0e-1, gamma - 1.0, P.r_gm1);
   double div = ux + vy + wz;
   double sxy = uy + vx, syz = wy + vz;
   g[0] = 0.0;
   g[1] = amu * sxy;
-  g[2] = 2.0 * amu * (vy - div / 3.0);
+  g[2] = 2.0 * amu * (vy - ddiv(div, 3.0, P.r_3));
   g[3] = amu * syz;
-  g[4] = v * g[2] + u * g[1] + w * g[3] + akappa * ty / (P.pr * P.mach * P.mach * (gamma - 1.0));
+  g[4] = v * g[2] + u * g[1] + w * g[3] + ddiv(akappa * ty, P.pr * P.mach * P.mach * (gamma - 1.0), P.r_den);
 }
-__device__ __forceinline__ void vis_flux_z(const double *Q, const double *Qx, const double *Qy, const double *Qz,
-                                           double amu, const Phys &P, double *h) {
+__device__ __forceinline__ void vis_flux_z(const double *Q, double rr, const double *Qx, const double *Qy,
+                                           const double *Qz, double amu, const Phys &P, double *h) {
   const double gamma = P.gamma;
   double rho = Q[0], rhou = Q[1], rhov = Q[2], rhow = Q[3], rhoe = Q[4];
-  double u = rhou / rho, v = rhov / rho, w = rhow / rho;
+  double u = ddiv(rhou, rho, rr), v = ddiv(rhov, rho, rr), w = ddiv(rhow, rho, rr);
   double p = (gamma - 1.0) * (rhoe - 0.5 * rho * (u * u + v * v + w * w));
-  double ux = (Qx[1] - u * Qx[0]) / rho, uz = (Qz[1] - u * Qz[0]) / rho;
-  double vy = (Qy[2] - v * Qy[0]) / rho, vz = (Qz[2] - v * Qz[0]) / rho;
-  double wx = (Qx[3] - w * Qx[0]) / rho, wy = (Qy[3] - w * Qy[0]) / rho, wz = (Qz[3] - w * Qz[0]) / rho;
+  double ux = ddiv(Qx[1] - u * Qx[0], rho, rr), uz = ddiv(Qz[1] - u * Qz[0], rho, rr);
+  double vy = ddiv(Qy[2] - v * Qy[0], rho, rr), vz = ddiv(Qz[2] - v * Qz[0], rho, rr);
+  double wx = ddiv(Qx[3] - w * Qx[0], rho, rr), wy = ddiv(Qy[3] - w * Qy[0], rho, rr), wz = ddiv(Qz[3] - w * Qz[0], rho, rr);
   double pz = (gamma - 1.0) * (Qz[4] - 0.5 * Qz[0] * (u * u + v * v + w * w) - rho * (u * uz + v * vz + w * wz));
-  double tz = (pz - p * Qz[0] / rho) * P.mach * P.mach * gamma / rho;
-  double akappa = 1.0 + (amu - 1.0) * 2.0e-1 / (gamma - 1.0);
+  double tz = ddiv((pz - ddiv(p * Qz[0], rho, rr)) * P.mach * P.mach * gamma, rho, rr);
+  double akappa = 1.0 + ddiv((amu - 1.0) * 2.0e-1, gamma - 1.0, P.r_gm1);
   double div = ux + vy + wz;
   double sxz = wx + uz, syz = wy + vz;
   h[0] = 0.0;
   h[1] = amu * sxz;
   h[2] = amu * syz;
-  h[3] = 2.0 * amu * (wz - div / 3.0);
-  h[4] = v * h[2] + u * h[1] + w * h[3] + akappa * tz / (P.pr * P.mach * P.mach * (gamma - 1.0));
+  h[3] = 2.0 * amu * (wz - ddiv(div, 3.0, P.r_3));
+  h[4] = v * h[2] + u * h[1] + w * h[3] + ddiv(akappa * tz, P.pr * P.mach * P.mach * (gamma - 1.0), P.r_den);
 }
 
 // EV residual (EV_routines/Main/RHS.f90:207-278): D = ((phi+gam)/T)/Re

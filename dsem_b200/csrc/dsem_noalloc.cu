@@ -189,6 +189,7 @@ int run(double *scratch, int nel, int nmort, const int *rows, const double *nh, 
   va.P.re = re;
   va.P.pr = pr;
   va.P.mach = mach;
+  phys_recips(va.P);
   NK(Launch<G>::vol(va, nel, true, VOL_PLAIN, st));
   if (nmort > 0) {
     k_face_vis_rows<G><<<nb, 128, 0, st>>>(rows, nmort, VF, nrm);
@@ -206,6 +207,7 @@ int run(double *scratch, int nel, int nmort, const int *rows, const double *nh, 
   ua.Qt_out = Qt;
   ua.flag = flag;
   ua.re = re;
+  ua.r_re = 1.0 / re;
   ua.update = 0;
   NK(Launch<G>::update(ua, nel, st));
   int h = 0;

@@ -13,6 +13,27 @@
 #pragma once
 #include "dsem_kernels.cuh"
 
+#ifdef DSEM_PHASE_TIMING
+// development probe: cycles per phase of the volume kernel, summed over blocks
+__device__ unsigned long long g_phase_cycles[32];
+#define PHASE_MARK(i)                                                  \
+  do {                                                                 \
+    if (threadIdx.x == 0) {                                            \
+      long long now_ = clock64();                                      \
+      atomicAdd(&g_phase_cycles[i], (unsigned long long)(now_ - t_ph_)); \
+      t_ph_ = now_;                                                    \
+    }                                                                  \
+  } while (0)
+#else
+#define PHASE_MARK(i) \
+  do {                \
+  } while (0)
+#endif
+
+#ifndef DSEM_VOL_THREADS_P8
+#define DSEM_VOL_THREADS_P8 448  // threads per volume CTA for p >= 7 (fastest of 384/448/512 at p = 8)
+#endif
+
 namespace dsem {
 
 // ------------------------------------------------------------------ traces
@@ -462,160 +483,182 @@ struct VolArgs {
 
 template <int G, bool DIAG, bool EV, int SAVE> struct VolCfg {
   static constexpr int L = G + 1, NG = G * G * G, NL = L * G * G;
-  static constexpr int NCH = DIAG ? 11 : 15;
-  static constexpr int NLB = (EV || SAVE == 2) ? 6 : 5;
-  static constexpr size_t SMEM = sizeof(double) * (size_t)(15 * NG + NLB * NL + NCH * NL);
-  static constexpr int NT = G >= 8 ? 384 : 256;
+  static constexpr int NCH = DIAG ? 11 : 15;          // gradient fields interpolated to each grid
+  static constexpr int NLB = EV ? 6 : 5;              // Lobatto slots (+ EV coefficient)
+  static constexpr size_t MAXS = 232448;              // dynamic shared memory per CTA on sm_100
+  static constexpr size_t bytes(bool pad, bool qsm) {
+    return sizeof(double) *
+           (size_t)(15 * NG + (NLB + NCH) * ((pad ? (L | 1) : L) * G * G) + (qsm ? 5 * NG : 0));
+  }
+  static constexpr bool QSM = bytes(false, true) <= MAXS;  // divergence sum kept in shared memory
+  static constexpr bool PAD = QSM ? bytes(true, true) <= MAXS : bytes(true, false) <= MAXS;
+  static constexpr int LX = PAD ? (L | 1) : L;        // x-grid line stride (odd: no bank conflicts)
+  static constexpr int NLS = LX * G * G;              // stride of one field on a Lobatto grid
+  static constexpr size_t SMEM = bytes(PAD, QSM);
+  static constexpr int NT = G >= 8 ? DSEM_VOL_THREADS_P8 : 256;
 };
 
-template <int G, int D>
-__device__ __forceinline__ void build_lobatto(const double *q, const double *QF, double *LB, int tid, int nt) {
-  constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
-  for (int t = tid; t < 5 * G2; t += nt) {
-    const int v = t / G2, ln = t - v * G2, a = ln % G, b = ln / G;
-    double *y = LB + v * NL + lbase<G>(D, a, b);
-    constexpr int ys = D == 0 ? 1 : (D == 1 ? G : G2);
-    constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
-    contract<G, false, 1, L - 1, 0, G>(q + v * NG + gbase<G>(D, a, b), xs, y, ys);
-    y[0] = QF[(face_lo(D) - 1) * 5 * G2 + v * G2 + ln];
-    y[(L - 1) * ys] = QF[(face_hi(D) - 1) * 5 * G2 + v * G2 + ln];
-  }
+// Line (a,b) of direction D on a Lobatto-grid array with x-stride LX.
+template <int G, int LX, int D> __device__ __forceinline__ int lb_base(int a, int b) {
+  return D == 0 ? LX * (a + G * b) : (D == 1 ? a + G * (G + 1) * b : a + G * b);
+}
+template <int G, int D> __device__ __forceinline__ constexpr int lb_stride() { return D == 0 ? 1 : (D == 1 ? G : G * G); }
+template <int G, int D> __device__ __forceinline__ constexpr int g_stride() { return D == 0 ? 1 : (D == 1 ? G : G * G); }
+
+// Interior Lobatto points of the 5 fields along D from q (Gauss layout); face
+// points from the averaged face state.  Tasks [t0, t0 + 5*G^2) of a merged phase.
+template <int G, int LX, int D>
+__device__ __forceinline__ void build_task(int t, const double *q, const double *QF, double *LB, int NLS) {
+  constexpr int L = G + 1, G2 = G * G, NG = G * G * G;
+  const int v = t / G2, ln = t - v * G2, a = ln % G, b = ln / G;
+  const double flo = QF[(face_lo(D) - 1) * 5 * G2 + v * G2 + ln];
+  const double fhi = QF[(face_hi(D) - 1) * 5 * G2 + v * G2 + ln];
+  double *y = LB + v * NLS + lb_base<G, LX, D>(a, b);
+  constexpr int ys = lb_stride<G, D>();
+  contract<G, false, 1, L - 1, 0, G>(q + v * NG + gbase<G>(D, a, b), g_stride<G, D>(), y, ys);
+  y[0] = flo;
+  y[(L - 1) * ys] = fhi;
 }
 
-template <int G, bool DIAG, bool EV, int SAVE, int D>
-__device__ __forceinline__ void vol_pass1(const VolArgs &A, const double *q, const double *QF, const double *gg,
-                                          double *GR, double *LB, double *EVB, int tid, int nt) {
-  constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
-  constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
-  constexpr int ls = D == 0 ? 1 : (D == 1 ? G : G2);
-  build_lobatto<G, D>(q, QF, LB, tid, nt);
-  if (SAVE == 2) {
-    __syncthreads();
-    const double gamma = A.P.gamma;
-    for (int p = tid; p < NL; p += nt) {  // temperature on the Lobatto grid (RHS.f90:66-83)
-      const double q1 = LB[p], q2 = LB[NL + p], q3 = LB[2 * NL + p], q4 = LB[3 * NL + p], q5 = LB[4 * NL + p];
-      const double P = (gamma - 1.0) * (q5 - 0.5 * q1 * ((q2 / q1) * (q2 / q1) + (q3 / q1) * (q3 / q1) + (q4 / q1) * (q4 / q1)));
-      LB[5 * NL + p] = P * gamma / q1;
+// Derivative along D of Lobatto field f (f == 5: temperature, computed on the
+// fly from the five fields, RHS.f90:66-83) and its contribution to the Gauss
+// gradients (Gauss_Deriv, SolnDerivsc.f90:36-80).
+template <int G, int LX, bool DIAG, int D>
+__device__ __forceinline__ void deriv_task(int t, const double *LB, int NLS, const double *gg, double *GR, double *EVB,
+                                           double gamma) {
+  constexpr int L = G + 1, G2 = G * G, NG = G * G * G;
+  const int f = t / G2, ln = t - f * G2, a = ln % G, b = ln / G;
+  constexpr int ls = lb_stride<G, D>(), xs = g_stride<G, D>();
+  const int l0 = lb_base<G, LX, D>(a, b);
+  double w[G];
+  if (f < 5) {
+    contract_reg<G, true, 0, G, 0, L>(LB + f * NLS + l0, ls, w);
+  } else {
+    double T[L];
+#pragma unroll
+    for (int n = 0; n < L; ++n) {
+      const int p = l0 + n * ls;
+      const double q1 = LB[p], q2 = LB[NLS + p], q3 = LB[2 * NLS + p], q4 = LB[3 * NLS + p], q5 = LB[4 * NLS + p];
+      const double r1 = 1.0 / q1, u = ddiv(q2, q1, r1), v = ddiv(q3, q1, r1), w = ddiv(q4, q1, r1);
+      const double P = (gamma - 1.0) * (q5 - 0.5 * q1 * (u * u + v * v + w * w));
+      T[n] = ddiv(P * gamma, q1, r1);
     }
+    contract_reg<G, true, 0, G, 0, L>(T, 1, w);
   }
-  __syncthreads();
-  constexpr int NF = SAVE == 2 ? 6 : 5;
-  for (int t = tid; t < NF * G2; t += nt) {
-    const int f = t / G2, ln = t - f * G2, a = ln % G, b = ln / G;
-    double w[G];
-    contract_reg<G, true, 0, G, 0, L>(LB + f * NL + lbase<G>(D, a, b), ls, w);
-    const int p0 = gbase<G>(D, a, b);
+  const int p0 = gbase<G>(D, a, b);
+  double *dst = f < 5 ? GR : EVB + 12 * NG;
+  const int fo = f < 5 ? f * 3 : 0;
 #pragma unroll
-    for (int k = 0; k < G; ++k) {
-      const int p = p0 + k * xs;
-      if (f < 5) {
-        if (DIAG) {
-          GR[(f * 3 + D) * NG + p] = gg[D * NG + p] * w[k];
-        } else {
+  for (int k = 0; k < G; ++k) {
+    const int p = p0 + k * xs;
+    if (DIAG) {
+      dst[(fo + D) * NG + p] = gg[D * NG + p] * w[k];
+    } else {
 #pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const double val = gg[p * 9 + D + 3 * c] * w[k];
-            GR[(f * 3 + c) * NG + p] = (D == 0) ? val : GR[(f * 3 + c) * NG + p] + val;
-          }
-        }
-      } else {
-        if (DIAG) {
-          EVB[(12 + D) * NG + p] = gg[D * NG + p] * w[k];
-        } else {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const double val = gg[p * 9 + D + 3 * c] * w[k];
-            EVB[(12 + c) * NG + p] = (D == 0) ? val : EVB[(12 + c) * NG + p] + val;
-          }
-        }
+      for (int c = 0; c < 3; ++c) {
+        const double val = gg[p * 9 + D + 3 * c] * w[k];
+        dst[(fo + c) * NG + p] = (D == 0) ? val : dst[(fo + c) * NG + p] + val;
       }
     }
   }
-  __syncthreads();
 }
 
+// Pass 2 for one direction: gradients to grid D, fluxes, interior divergence.
 template <int G, bool DIAG, bool EV, int SAVE, int D>
-__device__ __forceinline__ void vol_pass2(const VolArgs &A, const double *JQ, const double *jac, const double *QF,
-                                          const double *gm, const double *muhg, double *GR, double *LB, double *CH,
-                                          double *VF, double *QTI, int tid, int nt) {
+__device__ __forceinline__ void vol_dir(const VolArgs &A, const double *JQ, const double *jac, const double *QF,
+                                        const double *gm, const double *muhg, const double *GR, double *LB, double *CH,
+                                        double *VF, double *QT, int tid, int nt, long long &t_ph_) {
+  using C = VolCfg<G, DIAG, EV, SAVE>;
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
-  constexpr int NCH = DIAG ? 11 : 15;
-  constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
-  constexpr int ls = D == 0 ? 1 : (D == 1 ? G : G2);
-  if (D > 0) {
-    for (int i = tid; i < 5 * NG; i += nt) CH[i] = JQ[i] * jac[i % NG];
-    __syncthreads();
+  constexpr int LX = C::LX, NLS = C::NLS, NCH = C::NCH;
+  constexpr int xs = g_stride<G, D>(), ls = lb_stride<G, D>();
+  double *qpre = CH + 5 * NLS;  // state prefetched during the previous divergence phase
+  if (D != 2) {
+    for (int t = tid; t < 5 * G2; t += nt) build_task<G, LX, D>(t, qpre, QF, LB, NLS);
   }
-  build_lobatto<G, D>(CH, QF, LB, tid, nt);
   if (EV) {  // EV_Prolong (Prolong_gtol.f90:7-51)
     for (int t = tid; t < G2; t += nt) {
       const int a = t % G, b = t / G;
-      contract<G, false, 0, L, 0, G>(muhg + gbase<G>(D, a, b), xs, LB + 5 * NL + lbase<G>(D, a, b), ls);
+      contract<G, false, 0, L, 0, G>(muhg + gbase<G>(D, a, b), xs, LB + 5 * NLS + lb_base<G, LX, D>(a, b), ls);
     }
   }
-  __syncthreads();
+  if (D != 2 || EV) __syncthreads();
+  PHASE_MARK(8 + 4 * D);
   for (int t = tid; t < NCH * G2; t += nt) {  // gradients to grid D (Vis_Fluxes_new.f90:84-109)
     const int jf = t / G2, ln = t - jf * G2, a = ln % G, b = ln / G;
     const int src = DIAG ? diag_field(D, jf) : jf;
-    contract<G, false, 0, L, 0, G>(GR + src * NG + gbase<G>(D, a, b), xs, CH + jf * NL + lbase<G>(D, a, b), ls);
+    contract<G, false, 0, L, 0, G>(GR + src * NG + gbase<G>(D, a, b), xs, CH + jf * NLS + lb_base<G, LX, D>(a, b), ls);
   }
   __syncthreads();
+  PHASE_MARK(9 + 4 * D);
   const Phys P = A.P;
-  for (int p = tid; p < NL; p += nt) {  // fluxes on grid D (Vis_Fluxes_new.f90:115-228, fluxesH_newa.f90:276-352)
-    int s, a, b;
-    ldecode<G>(D, p, s, a, b);
+  for (int qi = tid; qi < NL; qi += nt) {  // fluxes on grid D (Vis_Fluxes_new.f90:115-228, fluxesH_newa.f90:276-352)
+    int s, a, b, p, pg;
+    if (D == 0) {
+      s = qi % L;
+      const int r = qi / L;
+      a = r % G;
+      b = r / G;
+      p = s + LX * r;
+      pg = qi;
+    } else {
+      ldecode<G>(D, qi, s, a, b);
+      p = qi;
+      pg = qi;
+    }
+    const double gdiag = DIAG ? gm[D * NL + pg] : 0.0;
     double Q[NV], Qx[NV], Qy[NV], Qz[NV], r[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) Q[v] = LB[v * NL + p];
+    for (int v = 0; v < NV; ++v) Q[v] = LB[v * NLS + p];
+    const double rr = 1.0 / Q[0];
     double amu = 1.0;
-    if (EV) amu = amu + LB[5 * NL + p];
+    if (EV) amu = amu + LB[5 * NLS + p];
     const bool face = (s == 0 || s == L - 1);
     if (DIAG) {
       double c[11];
 #pragma unroll
-      for (int jf = 0; jf < 11; ++jf) c[jf] = CH[jf * NL + p];
+      for (int jf = 0; jf < 11; ++jf) c[jf] = CH[jf * NLS + p];
       double fl[NV];
       if (D == 0) {
         Qx[0] = c[0]; Qx[1] = c[1]; Qx[2] = c[2]; Qx[3] = c[3]; Qx[4] = c[4];
         Qy[0] = c[5]; Qy[1] = c[6]; Qy[2] = c[7]; Qy[3] = 0.0; Qy[4] = 0.0;
         Qz[0] = c[8]; Qz[1] = c[9]; Qz[3] = c[10]; Qz[2] = 0.0; Qz[4] = 0.0;
-        vis_flux_x(Q, Qx, Qy, Qz, amu, P, fl);
+        vis_flux_x(Q, rr, Qx, Qy, Qz, amu, P, fl);
       } else if (D == 1) {
         Qy[0] = c[0]; Qy[1] = c[1]; Qy[2] = c[2]; Qy[3] = c[3]; Qy[4] = c[4];
         Qx[0] = c[5]; Qx[1] = c[6]; Qx[2] = c[7]; Qx[3] = 0.0; Qx[4] = 0.0;
         Qz[0] = c[8]; Qz[2] = c[9]; Qz[3] = c[10]; Qz[1] = 0.0; Qz[4] = 0.0;
-        vis_flux_y(Q, Qx, Qy, Qz, amu, P, fl);
+        vis_flux_y(Q, rr, Qx, Qy, Qz, amu, P, fl);
       } else {
         Qz[0] = c[0]; Qz[1] = c[1]; Qz[2] = c[2]; Qz[3] = c[3]; Qz[4] = c[4];
         Qx[0] = c[5]; Qx[1] = c[6]; Qx[3] = c[7]; Qx[2] = 0.0; Qx[4] = 0.0;
         Qy[0] = c[8]; Qy[2] = c[9]; Qy[3] = c[10]; Qy[1] = 0.0; Qy[4] = 0.0;
-        vis_flux_z(Q, Qx, Qy, Qz, amu, P, fl);
+        vis_flux_z(Q, rr, Qx, Qy, Qz, amu, P, fl);
       }
-      const double g = gm[D * NL + p];
 #pragma unroll
-      for (int v = 0; v < NV; ++v) r[v] = g * fl[v];
+      for (int v = 0; v < NV; ++v) r[v] = gdiag * fl[v];
       if (face) {
         const int fc = s == 0 ? face_lo(D) : face_hi(D);
 #pragma unroll
         for (int v = 0; v < NV; ++v) VF[(fc - 1) * 5 * G2 + v * G2 + a + G * b] = r[v];
       } else {
         double fi[NV];
-        euler_flux(D, Q, P.gamma, fi);
+        euler_flux(D, Q, rr, P.gamma, fi);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) CH[v * NL + p] = g * fi[v] - r[v] / P.re;
+        for (int v = 0; v < NV; ++v) CH[v * NLS + p] = gdiag * fi[v] - ddiv(r[v], P.re, P.r_re);
       }
     } else {
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        Qx[v] = CH[(v * 3 + 0) * NL + p];
-        Qy[v] = CH[(v * 3 + 1) * NL + p];
-        Qz[v] = CH[(v * 3 + 2) * NL + p];
+        Qx[v] = CH[(v * 3 + 0) * NLS + p];
+        Qy[v] = CH[(v * 3 + 1) * NLS + p];
+        Qz[v] = CH[(v * 3 + 2) * NLS + p];
       }
       double f[NV], g[NV], h[NV];
-      vis_flux_x(Q, Qx, Qy, Qz, amu, P, f);
-      vis_flux_y(Q, Qx, Qy, Qz, amu, P, g);
-      vis_flux_z(Q, Qx, Qy, Qz, amu, P, h);
-      const double *g3 = gm + ((long long)D * NL + p) * 3;
+      vis_flux_x(Q, rr, Qx, Qy, Qz, amu, P, f);
+      vis_flux_y(Q, rr, Qx, Qy, Qz, amu, P, g);
+      vis_flux_z(Q, rr, Qx, Qy, Qz, amu, P, h);
+      const double *g3 = gm + ((long long)D * NL + pg) * 3;
       const double m0 = g3[0], m1 = g3[1], m2 = g3[2];
 #pragma unroll
       for (int v = 0; v < NV; ++v) r[v] = m0 * f[v] + m1 * g[v] + m2 * h[v];
@@ -624,57 +667,99 @@ __device__ __forceinline__ void vol_pass2(const VolArgs &A, const double *JQ, co
 #pragma unroll
         for (int v = 0; v < NV; ++v) VF[(fc - 1) * 5 * G2 + v * G2 + a + G * b] = r[v];
       } else {
-        euler_fluxes3(Q, P.gamma, f, g, h);
+        euler_fluxes3(Q, rr, P.gamma, f, g, h);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) CH[v * NL + p] = (m0 * f[v] + m1 * g[v] + m2 * h[v]) - r[v] / P.re;
+        for (int v = 0; v < NV; ++v) CH[v * NLS + p] = (m0 * f[v] + m1 * g[v] + m2 * h[v]) - ddiv(r[v], P.re, P.r_re);
       }
     }
   }
   __syncthreads();
-  for (int t = tid; t < 5 * G2; t += nt) {  // interior divergence along D (updatea.f90:100-113)
+  PHASE_MARK(10 + 4 * D);
+  // interior divergence along D (updatea.f90:100-113), and the state for the next direction
+  for (int t = tid; t < 5 * G2; t += nt) {
     const int v = t / G2, ln = t - v * G2, a = ln % G, b = ln / G;
     double S[G];
-    contract_reg<G, true, 0, G, 1, L - 1>(CH + v * NL + lbase<G>(D, a, b), ls, S);
-    const int p0 = gbase<G>(D, a, b);
+    contract_reg<G, true, 0, G, 1, L - 1>(CH + v * NLS + lb_base<G, LX, D>(a, b), ls, S);
+    const int p0 = v * NG + gbase<G>(D, a, b);
 #pragma unroll
     for (int k = 0; k < G; ++k) {
-      const int p = v * NG + p0 + k * xs;
-      QTI[p] = (D == 0) ? S[k] : QTI[p] + S[k];
+      const int p = p0 + k * xs;
+      QT[p] = (D == 2) ? S[k] : QT[p] + S[k];
     }
   }
+  if (D != 0) {
+    for (int i = tid; i < 5 * NG; i += nt) qpre[i] = JQ[i] * jac[i % NG];
+  }
   __syncthreads();
+  PHASE_MARK(11 + 4 * D);
 }
 
 template <int G, bool DIAG, bool EV, int SAVE>
 __global__ void __launch_bounds__(VolCfg<G, DIAG, EV, SAVE>::NT, 1) k_vol(VolArgs A) {
   using C = VolCfg<G, DIAG, EV, SAVE>;
-  constexpr int G2 = G * G, NG = C::NG, NL = C::NL;
+  constexpr int G2 = G * G, NG = C::NG, NL = C::NL, LX = C::LX, NLS = C::NLS;
   extern __shared__ double sm[];
   double *GR = sm;
   double *LB = GR + 15 * NG;
-  double *CH = LB + C::NLB * NL;
+  double *CH = LB + C::NLB * NLS;
+  double *QTS = CH + C::NCH * NLS;  // divergence sum (when it fits)
   const int k = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
   const double *JQ = A.JQ + (long long)k * A.sq;
   const double *jac = A.jac + (long long)k * NG;
   const double *QF = A.QF + (long long)k * 30 * G2;
   double *VF = A.VF + (long long)k * 30 * G2;
   double *QTI = A.QTI + (long long)k * 5 * NG;
+  double *QT = C::QSM ? QTS : QTI;
   double *EVB = SAVE ? A.EVB + (long long)k * 15 * NG : nullptr;
   const double *gg = A.gg + (long long)k * 3 * NG * (DIAG ? 1 : 3);
   const double *gm = A.gm + (long long)k * 3 * NL * (DIAG ? 1 : 3);
   const double *muhg = EV ? A.muhg + (long long)k * NG : nullptr;
+  const double gamma = A.P.gamma;
+  long long t_ph_ = 0;
+#ifdef DSEM_PHASE_TIMING
+  t_ph_ = clock64();
+#endif
 
-  for (int i = tid; i < 5 * NG; i += nt) CH[i] = JQ[i] * jac[i % NG];  // Q*jacob (fluxesH_newa.f90:262-272)
+  // Q*jacob (fluxesH_newa.f90:262-272)
+  for (int i = tid; i < 5 * NG; i += nt) CH[i] = JQ[i] * jac[i % NG];
   __syncthreads();
-  vol_pass1<G, DIAG, EV, SAVE, 0>(A, CH, QF, gg, GR, LB, EVB, tid, nt);
-  vol_pass1<G, DIAG, EV, SAVE, 1>(A, CH, QF, gg, GR, LB, EVB, tid, nt);
-  vol_pass1<G, DIAG, EV, SAVE, 2>(A, CH, QF, gg, GR, LB, EVB, tid, nt);
+  PHASE_MARK(0);
+  // pass 1: Lobatto arrays and Gauss gradients, Lobatto array double-buffered
+  double *LB2 = CH + 5 * NG;
+  constexpr int NF = SAVE == 2 ? 6 : 5;
+  for (int t = tid; t < 5 * G2; t += nt) build_task<G, LX, 0>(t, CH, QF, LB, NLS);
+  __syncthreads();
+  PHASE_MARK(1);
+  for (int t = tid; t < (NF + 5) * G2; t += nt) {
+    if (t < NF * G2)
+      deriv_task<G, LX, DIAG, 0>(t, LB, NLS, gg, GR, EVB, gamma);
+    else
+      build_task<G, LX, 1>(t - NF * G2, CH, QF, LB2, NLS);
+  }
+  __syncthreads();
+  PHASE_MARK(2);
+  for (int t = tid; t < (NF + 5) * G2; t += nt) {
+    if (t < NF * G2)
+      deriv_task<G, LX, DIAG, 1>(t, LB2, NLS, gg, GR, EVB, gamma);
+    else
+      build_task<G, LX, 2>(t - NF * G2, CH, QF, LB, NLS);
+  }
+  __syncthreads();
+  PHASE_MARK(3);
+  for (int t = tid; t < NF * G2; t += nt) deriv_task<G, LX, DIAG, 2>(t, LB, NLS, gg, GR, EVB, gamma);
+  __syncthreads();
+  PHASE_MARK(4);
   if (SAVE) {
     for (int i = tid; i < 12 * NG; i += nt) EVB[i] = GR[i];
   }
-  vol_pass2<G, DIAG, EV, SAVE, 0>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QTI, tid, nt);
-  vol_pass2<G, DIAG, EV, SAVE, 1>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QTI, tid, nt);
-  vol_pass2<G, DIAG, EV, SAVE, 2>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QTI, tid, nt);
+  // pass 2: z (reusing the last Lobatto array), y, x
+  vol_dir<G, DIAG, EV, SAVE, 2>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QT, tid, nt, t_ph_);
+  vol_dir<G, DIAG, EV, SAVE, 1>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QT, tid, nt, t_ph_);
+  vol_dir<G, DIAG, EV, SAVE, 0>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QT, tid, nt, t_ph_);
+  if (C::QSM) {
+    for (int i = tid; i < 5 * NG; i += nt) QTI[i] = QTS[i];
+  }
+  PHASE_MARK(20);
 }
 
 // ------------------------------------------------------------------ update
@@ -686,7 +771,7 @@ struct UpdArgs {
   double *QF;      // out: traces of the updated state
   double *Qt_out;  // optional: [elem][5][G^3]
   int *flag;       // bit 0: non-finite Qt
-  double ark, cdt, re;
+  double ark, cdt, re, r_re;  // r_re = 1/re
   int first, update;
 };
 
@@ -700,7 +785,7 @@ template <int G> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
   const int k = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
   const double *FF = A.FF + (long long)k * 30 * G2;
   const double *VF = A.VF + (long long)k * 30 * G2;
-  for (int i = tid; i < 30 * G2; i += nt) FB[i] = FF[i] - VF[i] / A.re;  // send_flux_to_faces_add
+  for (int i = tid; i < 30 * G2; i += nt) FB[i] = FF[i] - ddiv(VF[i], A.re, A.r_re);  // send_flux_to_faces_add
   for (int i = tid; i < G; i += nt) {
     Dlo[i] = Op<G>::D(i, 0);
     Dhi[i] = Op<G>::D(i, L - 1);

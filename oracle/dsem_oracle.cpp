@@ -868,7 +868,7 @@ template <class T> void element_qt(const Elem<T> &E, std::vector<T> &Qt) {
         for (int n = 0; n < G; ++n) {
           size_t p = gidx(G, n, m, l);
           const T *F0 = &E.F[0][v * nl], *F1 = &E.F[1][v * nl], *F2 = &E.F[2][v * nl];
-          T acc = S[0][p] + S[1][p] + S[2][p];
+          T acc = S[2][p] + S[1][p] + S[0][p];  // z, y, x: the CUDA kernel's pass order
           acc = fmac(o.dmx[n * L + 0], F0[lidx(0, G, L, 0, m, l)], acc);
           acc = fmac(o.dmx[n * L + L - 1], F0[lidx(0, G, L, L - 1, m, l)], acc);
           acc = fmac(o.dmx[m * L + 0], F1[lidx(1, G, L, n, 0, l)], acc);
