@@ -8,6 +8,7 @@ dt = 0.5 x the inviscid limit).  A "step" is one RK time step (5 stages) of
 the whole mesh.  Metric: DOF-RK-stages/s = unknowns x 5 x steps / seconds.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --workload ensemble [--steps K] [--warmup W]
 
 value : device-resident throughput, CUDA events on the library's stream
         around exactly K steps (CUDA graph per step), max over ranks.
@@ -15,6 +16,12 @@ e2e   : the same metric through the C-ABI with host buffers: each step uploads
         the state from pinned host memory, advances one step and downloads it.
 Multi-GPU (torchrun): replicas only -- every rank advances its own copy of the
 case, no data-path collective; value sums the ranks' unknowns.
+
+--workload ensemble: 64 independent cases drawn from a seed (E in {4^3, 6^3,
+8^3, 10^3, 12^3}, p in {4, 6, 8}, Re ~ U[400, 3200], Mach ~ U[0.05, 0.3] set
+through the reference pressure, Taylor-Green or isotropic initial condition),
+advanced together by one ensemble context (dsem_create_batch) against the same
+64 cases run one after another through single-case contexts.
 """
 import argparse
 import json
@@ -44,6 +51,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nex", type=int, default=NEX)
     ap.add_argument("--p", type=int, default=P)
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "ensemble"])
+    ap.add_argument("--cases", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=2024)
     return ap.parse_args()
 
 
@@ -224,10 +234,92 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- ensemble
+ENS_SIZES = (4, 6, 8, 10, 12)
+ENS_ORDERS = (4, 6, 8)
+
+
+def ensemble_cases(n, seed):
+    """(nex, p, Re, Mach, initial condition) of n cases drawn from seed."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nex = int(rng.choice(ENS_SIZES))
+        p = int(rng.choice(ENS_ORDERS))
+        re = float(rng.uniform(400.0, 3200.0))
+        ma = float(rng.uniform(0.05, 0.3))
+        ic = "tgv" if rng.random() < 0.5 else "iso"
+        out.append((nex, p, re, ma, ic))
+    return out
+
+
+def ensemble_inputs(cases, seed):
+    from dsem_b200 import mesh
+    boxes, descs, qs, dts = {}, [], [], []
+    for k, (nex, p, re, ma, ic) in enumerate(cases):
+        if (nex, p) not in boxes:
+            b = mesh.Box(nex, nex, nex, p)
+            boxes[(nex, p)] = (b, b.desc())
+        b, d = boxes[(nex, p)]
+        twall = 1.0 / (ma * ma)  # rho0 = V0 = 1: Mach = V0 / sqrt(gamma p0 / rho0), p0 = twall / gamma
+        q = mesh.taylor_green(b, twall=twall) if ic == "tgv" else \
+            mesh.random_isotropic(b, seed=seed * 1000 + k, k0=2.0, mach_t=ma, twall=twall)
+        descs.append(d)
+        qs.append(q)
+        dts.append(CFL * mesh.dtcalc(b, q))
+    return descs, qs, np.array(dts)
+
+
+def run_ensemble(args):
+    import torch
+    from dsem_b200.solver import Ensemble, Solver
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    cases = ensemble_cases(args.cases, args.seed)
+    descs, qs, dts = ensemble_inputs(cases, args.seed)
+    dof = np.array([5 * int(d["ngrid"]) * (c[1] + 1) ** 3 for d, c in zip(descs, cases)])
+    work = float(dof.sum()) * STAGES * args.steps
+    # one ensemble context
+    ens = Ensemble(descs, [c[2] for c in cases])
+    for k, q in enumerate(qs):
+        ens.upload_case(k, q)
+    ens.step_batch(dts, args.warmup)
+    torch.cuda.synchronize()
+    with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        ens.step_batch(dts, args.steps)
+    ms_b, launches_b = ens.last_timing()
+    ens.close()
+    # the same cases one after another
+    ms_s, launches_s = 0.0, 0
+    for d, q, dt, c in zip(descs, qs, dts, cases):
+        s = Solver(d, re=c[2])
+        s.upload(q)
+        s.step(dt, args.warmup)
+        s.step(dt, args.steps)
+        m, n = s.last_timing()
+        ms_s += m
+        launches_s += n
+        s.close()
+    out = {"metric": "DOF-RK-stages/s FP64, 64-case ensemble", "value": work / (ms_b * 1e-3),
+           "unit": "DOF-RK-stages/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": ms_b / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic (seeded Taylor-Green / isotropic initial conditions)",
+           "config": {"workload": f"ensemble of {len(cases)} cases, seed {args.seed}: E in 4^3..12^3, p in 4/6/8, "
+                                  "Re U[400,3200], Mach U[0.05,0.3]", "cases": len(cases),
+                      "unknowns": int(dof.sum()), "elements": int(sum(int(d["ngrid"]) for d in descs))},
+           "sequential": {"value": work / (ms_s * 1e-3), "ms_per_step": ms_s / args.steps,
+                          "gpu_launches": launches_s},
+           "speedup_vs_sequential": ms_s / ms_b, "gpu_launches": launches_b, "clocks": clk.summary()}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "ensemble":
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_ensemble(args)
         return
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))

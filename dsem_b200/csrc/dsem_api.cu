@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <map>
 #include <string>
 #include <type_traits>
@@ -45,6 +46,8 @@ struct Group {
   double *jac = nullptr, *gg = nullptr, *gm = nullptr, *hd = nullptr;
   double *muhg = nullptr, *EVB = nullptr, *kew = nullptr;
   int *int2ext = nullptr;  // device: caller element id of each group element
+  int *ecase = nullptr;    // device: case of each group element
+  std::vector<int> case_lo, case_hi;  // group elements [lo, hi) of each case
 };
 
 struct MList {  // conforming mortars of one order
@@ -54,13 +57,13 @@ struct MList {  // conforming mortars of one order
 };
 
 // ---------------------------------------------------------- layout kernels
-__global__ void k_pack(const double *__restrict__ src, int ldx, const int *__restrict__ ext, int G, int nf,
+__global__ void k_pack(const double *__restrict__ src, int ldx, const int *__restrict__ ext, int ext0, int G, int nf,
                        double *__restrict__ dst, int to_internal) {
   // one block per group element; nf fields of G^3 points
   const int k = blockIdx.x;
   const long long L3 = (long long)ldx * ldx * ldx;
   const int NG = G * G * G;
-  const long long e = ext[k];
+  const long long e = ext[k] - ext0;
   for (int i = threadIdx.x; i < nf * NG; i += blockDim.x) {
     const int v = i / NG, p = i - v * NG;
     const int n = p % G, m = (p / G) % G, l = p / (G * G);
@@ -151,16 +154,25 @@ struct dsem_ctx {
   bool traces_valid = false;
   bool grad_valid = false;     // EVB holds the Q gradients of the last Fluxes call
   bool ev_grad_valid = false;  // ... and the temperature gradients (EV)
-  double prestep = 0.0;
   int keep_grad = 0;
   cudaGraphExec_t gexec = nullptr;
-  double graph_dt = 0.0;
   int graph_key = -1;
+  long long graph_launches = 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   double last_ms = 0.0;
   long long last_launches = 0;
   std::string err;
   std::vector<double> host_part;
+  // ensemble: independent cases sharing the launches (a single case is an ensemble of one)
+  int ncase = 1;
+  std::vector<int> case_el0;         // first caller element of each case (+ total)
+  std::vector<double> case_re, case_dt, case_prestep;
+  double *d_rec = nullptr;           // device: per case {re, 1/re}
+  double *d_dtc = nullptr;           // device: per case dt of the current call
+  // order groups run as parallel branches of the stream (and of the captured graph)
+  std::vector<cudaStream_t> aux;
+  std::vector<cudaEvent_t> ev_join;
+  cudaEvent_t ev_fork = nullptr;
 };
 
 namespace {
@@ -235,27 +247,58 @@ int upload_ops(dsem_ctx *c) {
   return DSEM_OK;
 }
 
+// Runs f(j, stream) for jobs j = 0..n-1. With more than one job each gets its
+// own stream, forked from the context stream and joined back into it, so that
+// independent order groups (and mortar lists) overlap on the device and form
+// parallel branches of a captured graph.
+template <class F> int fork_jobs(dsem_ctx *c, size_t n, F &&f) {
+  if (n <= 1) {
+    for (size_t j = 0; j < n; ++j) {
+      const int r = f(j, c->st);
+      if (r) return r;
+    }
+    return DSEM_OK;
+  }
+  if (n > c->aux.size()) return fail(c, DSEM_ERR_INVALID_ARG, "more parallel jobs than auxiliary streams");
+  CK(cudaEventRecord(c->ev_fork, c->st));
+  for (size_t j = 0; j < n; ++j) {
+    CK(cudaStreamWaitEvent(c->aux[j], c->ev_fork, 0));
+    const int r = f(j, c->aux[j]);
+    if (r) return r;
+    CK(cudaEventRecord(c->ev_join[j], c->aux[j]));
+  }
+  for (size_t j = 0; j < n; ++j) CK(cudaStreamWaitEvent(c->st, c->ev_join[j], 0));
+  return DSEM_OK;
+}
+
 int vol_mode(const dsem_ctx *c, bool save) {
   if (c->shock) return save ? VOL_EV_SAVE : VOL_EV;
   return save ? VOL_SAVE : VOL_PLAIN;
 }
 
 // One evaluation of Fluxes and the flux divergence, plus the update when kk > 0.
-int enqueue_stage(dsem_ctx *c, int kk, double dt, bool save, double *qt_out, long long *launches) {
+// The update reads dt per case from d_dtc (written before the stage is enqueued
+// or the graph replayed).
+int enqueue_stage(dsem_ctx *c, int kk, bool save, double *qt_out, long long *launches) {
   const double gamma = c->P.gamma;
-  for (auto &ml : c->mlists) {
-    CK(with_G(ml.G, [&](auto g) {
-      return Launch<decltype(g)::value>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, gamma, c->st);
-    }));
-    ++*launches;
-  }
-  if (c->nnc > 0) {
-    k_face_nc_inv<<<c->nnc, 128, 0, c->st>>>(c->nc, c->QF, c->FF, c->nc_nh, c->nc_nrm, c->nc_mats, gamma);
-    CK(cudaGetLastError());
-    ++*launches;
-  }
+  const size_t nml = c->mlists.size(), nfj = nml + (c->nnc > 0 ? 1 : 0);
+  int r = fork_jobs(c, nfj, [&](size_t j, cudaStream_t st) -> int {
+    if (j < nml) {
+      auto &ml = c->mlists[j];
+      CK(with_G(ml.G, [&](auto g) {
+        return Launch<decltype(g)::value>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, gamma, st);
+      }));
+    } else {
+      k_face_nc_inv<<<c->nnc, 128, 0, st>>>(c->nc, c->QF, c->FF, c->nc_nh, c->nc_nrm, c->nc_mats, gamma);
+      CK(cudaGetLastError());
+    }
+    return DSEM_OK;
+  });
+  if (r) return r;
+  *launches += (long long)nfj;
   const int mode = vol_mode(c, save);
-  for (auto &g : c->groups) {
+  r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
+    auto &g = c->groups[j];
     VolArgs a{};
     a.JQ = c->JQ + g.q0;
     a.sq = 5LL * g.G * g.G * g.G;
@@ -268,19 +311,27 @@ int enqueue_stage(dsem_ctx *c, int kk, double dt, bool save, double *qt_out, lon
     a.QTI = c->QTI + g.q0;
     a.EVB = g.EVB;
     a.P = c->P;
-    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::vol(a, g.nel, g.diag, mode, c->st); }));
-    ++*launches;
-  }
-  for (auto &ml : c->mlists) {
-    CK(with_G(ml.G, [&](auto g) { return Launch<decltype(g)::value>::face_vis(ml.mc, ml.n, c->VF, ml.nrm, c->st); }));
-    ++*launches;
-  }
-  if (c->nnc > 0) {
-    k_face_nc_vis<<<c->nnc, 128, 0, c->st>>>(c->nc, c->VF, c->nc_nrm, c->nc_mats);
-    CK(cudaGetLastError());
-    ++*launches;
-  }
-  for (auto &g : c->groups) {
+    a.ecase = g.ecase;
+    a.rec = c->d_rec;
+    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::vol(a, g.nel, g.diag, mode, st); }));
+    return DSEM_OK;
+  });
+  if (r) return r;
+  *launches += (long long)c->groups.size();
+  r = fork_jobs(c, nfj, [&](size_t j, cudaStream_t st) -> int {
+    if (j < nml) {
+      auto &ml = c->mlists[j];
+      CK(with_G(ml.G, [&](auto g) { return Launch<decltype(g)::value>::face_vis(ml.mc, ml.n, c->VF, ml.nrm, st); }));
+    } else {
+      k_face_nc_vis<<<c->nnc, 128, 0, st>>>(c->nc, c->VF, c->nc_nrm, c->nc_mats);
+      CK(cudaGetLastError());
+    }
+    return DSEM_OK;
+  });
+  if (r) return r;
+  *launches += (long long)nfj;
+  r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
+    auto &g = c->groups[j];
     UpdArgs u{};
     u.JQ = c->JQ + g.q0;
     u.gQ = c->gQ + g.q0;
@@ -297,15 +348,21 @@ int enqueue_stage(dsem_ctx *c, int kk, double dt, bool save, double *qt_out, lon
     u.update = kk > 0;
     u.first = kk == 1;
     u.ark = kk > 0 ? c->ark[kk - 1] : 0.0;
-    u.cdt = kk > 0 ? c->crk[kk - 1] * dt : 0.0;
-    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::update(u, g.nel, c->st); }));
-    ++*launches;
-  }
+    u.crk = kk > 0 ? c->crk[kk - 1] : 0.0;
+    u.ecase = g.ecase;
+    u.rec = c->d_rec;
+    u.dtc = c->d_dtc;
+    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::update(u, g.nel, st); }));
+    return DSEM_OK;
+  });
+  if (r) return r;
+  *launches += (long long)c->groups.size();
   return DSEM_OK;
 }
 
 int enqueue_ev(dsem_ctx *c, long long *launches) {
-  for (auto &g : c->groups) {
+  const int r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
+    auto &g = c->groups[j];
     EvArgs a{};
     a.JQ = c->JQ + g.q0;
     a.sq = 5LL * g.G * g.G * g.G;
@@ -315,34 +372,41 @@ int enqueue_ev(dsem_ctx *c, long long *launches) {
     a.muhg = g.muhg;
     a.valid = c->ev_grad_valid ? 1 : 0;
     a.P = c->P;
-    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::ev(a, g.nel, c->st); }));
-    ++*launches;
-  }
+    a.ecase = g.ecase;
+    a.rec = c->d_rec;
+    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::ev(a, g.nel, st); }));
+    return DSEM_OK;
+  });
+  if (r) return r;
+  *launches += (long long)c->groups.size();
   return DSEM_OK;
 }
 
 int enqueue_traces(dsem_ctx *c, long long *launches) {
-  for (auto &g : c->groups) {
+  const int r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
+    auto &g = c->groups[j];
     TraceArgs a{};
     a.JQ = c->JQ + g.q0;
     a.sq = 5LL * g.G * g.G * g.G;
     a.jac = g.jac;
     a.QF = c->QF + g.f0;
-    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::trace(a, g.nel, c->st); }));
-    ++*launches;
-  }
+    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::trace(a, g.nel, st); }));
+    return DSEM_OK;
+  });
+  if (r) return r;
+  *launches += (long long)c->groups.size();
   c->traces_valid = true;
   return DSEM_OK;
 }
 
 // one full time step (tstep.f90:36-116): EV, g_Q = 0 (folded into stage 1), kord stages
-int enqueue_step(dsem_ctx *c, double dt, bool save_last, long long *launches) {
+int enqueue_step(dsem_ctx *c, bool save_last, long long *launches) {
   if (c->shock) {
     int r = enqueue_ev(c, launches);
     if (r) return r;
   }
   for (int kk = 1; kk <= c->kord; ++kk) {
-    int r = enqueue_stage(c, kk, dt, save_last && kk == c->kord, nullptr, launches);
+    int r = enqueue_stage(c, kk, save_last && kk == c->kord, nullptr, launches);
     if (r) return r;
   }
   return DSEM_OK;
@@ -374,7 +438,7 @@ int unpack_to_host(dsem_ctx *c, const double *dev_internal, double *host, int ld
   for (size_t gi = 0; gi < c->groups.size(); ++gi) {
     auto &g = c->groups[gi];
     if (g.nel == 0) continue;
-    k_pack<<<g.nel, 256, 0, c->st>>>(dev_internal + offs[gi], ldx, g.int2ext, g.G, nf, c->stage, 0);
+    k_pack<<<g.nel, 256, 0, c->st>>>(dev_internal + offs[gi], ldx, g.int2ext, 0, g.G, nf, c->stage, 0);
     CK(cudaGetLastError());
   }
   CK(cudaMemcpyAsync(host, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -400,41 +464,58 @@ int check_flag(dsem_ctx *c) {
 
 // =================================================================== C-ABI
 namespace {
-int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m);
-}
 
-// error text of calls made without a context (read by dsem_last_error(NULL))
-void dsem_set_thread_error(const std::string &msg) { g_create_err = msg; }
+// The cases of a context, each a caller descriptor with its own padding ldx;
+// caller element e of case k is context element case_el0[k] + e (no copy of
+// the caller's arrays is made).
+struct MeshSet {
+  std::vector<const dsem_mesh_desc *> m;
+  std::vector<int> el0, mo0;  // first element / mortar of each case (+ totals)
+  int case_of(int e) const {
+    return (int)(std::upper_bound(el0.begin(), el0.end(), e) - el0.begin()) - 1;
+  }
+  int ngrid() const { return el0.back(); }
+  int nmort() const { return mo0.back(); }
+  int G(int e) const {
+    const int k = case_of(e);
+    return m[k]->ncg[3 * (e - el0[k])];
+  }
+  // caller point (n, mm, l) of element e: descriptor, flat point index, ldx
+  const dsem_mesh_desc *at(int e, int n, int mm, int l, size_t &q) const {
+    const int k = case_of(e);
+    const size_t ld = (size_t)m[k]->ldx;
+    q = (size_t)(e - el0[k]) * ld * ld * ld + n + ld * (mm + ld * l);
+    return m[k];
+  }
+};
 
-extern "C" {
+int setup_ctx(dsem_ctx *c, const MeshSet &ms);
 
-const char *dsem_last_error(const dsem_ctx *c) { return c ? c->err.c_str() : g_create_err.c_str(); }
-
-int dsem_create(const dsem_mesh_desc *m, const dsem_phys *ph, dsem_ctx **out) {
-  dsem_ctx *c = nullptr;
-  if (!m || !ph || !out) return fail(nullptr, DSEM_ERR_INVALID_ARG, "null argument");
-  *out = nullptr;
+int check_desc(const dsem_mesh_desc *m) {
   if (m->ngrid <= 0 || m->nmort < 0 || m->ldx <= 0 || !m->ncg || !m->jacob || !m->gmetg || !m->gmet ||
       (m->nmort > 0 && (!m->mortar || !m->n_hat || !m->norm)))
     return fail(nullptr, DSEM_ERR_INVALID_ARG, "incomplete mesh descriptor");
-  const int ldx = m->ldx;
   for (int e = 0; e < m->ngrid; ++e) {
     const int G = m->ncg[3 * e];
     if (m->ncg[3 * e + 1] != G || m->ncg[3 * e + 2] != G)
       return fail(nullptr, DSEM_ERR_UNSUPPORTED, "anisotropic element orders are not supported");
     if (G < GMIN || G > GMAX) return fail(nullptr, DSEM_ERR_UNSUPPORTED, "element order outside 1..8");
-    if (ldx < G + 1) return fail(nullptr, DSEM_ERR_INVALID_ARG, "ldx must be at least ncg+1");
+    if (m->ldx < G + 1) return fail(nullptr, DSEM_ERR_INVALID_ARG, "ldx must be at least ncg+1");
   }
-  c = new dsem_ctx();
+  return DSEM_OK;
+}
+
+int create_ctx(const MeshSet &ms, const dsem_phys *ph, const std::vector<double> &re, dsem_ctx **out) {
+  dsem_ctx *c = new dsem_ctx();
   cudaGetDevice(&c->dev);
   if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
     delete c;
     return fail(nullptr, DSEM_ERR_CUDA, "cudaStreamCreate failed (no usable CUDA device?)");
   }
-  c->ngrid = m->ngrid;
-  c->nmort = m->nmort;
+  c->ngrid = ms.ngrid();
+  c->nmort = ms.nmort();
   c->P.gamma = ph->gamma;
-  c->P.re = ph->re;
+  c->P.re = re[0];
   c->P.pr = ph->pr;
   c->P.mach = ph->mach;
   c->P.cmu = ph->cmu;
@@ -444,7 +525,12 @@ int dsem_create(const dsem_mesh_desc *m, const dsem_phys *ph, dsem_ctx **out) {
   c->shock = ph->shock ? 1 : 0;
   c->iord = ph->iord;
   rkcoefs(c, ph->iord);
-  const int r = setup_ctx(c, m);
+  c->ncase = (int)ms.m.size();
+  c->case_el0 = ms.el0;
+  c->case_re = re;
+  c->case_dt.assign(c->ncase, 0.0);
+  c->case_prestep.assign(c->ncase, 0.0);
+  const int r = setup_ctx(c, ms);
   if (r) {
     g_create_err = c->err;
     dsem_destroy(c);
@@ -454,23 +540,70 @@ int dsem_create(const dsem_mesh_desc *m, const dsem_phys *ph, dsem_ctx **out) {
   return DSEM_OK;
 }
 
+}  // namespace
+
+// error text of calls made without a context (read by dsem_last_error(NULL))
+void dsem_set_thread_error(const std::string &msg) { g_create_err = msg; }
+
+extern "C" {
+
+const char *dsem_last_error(const dsem_ctx *c) { return c ? c->err.c_str() : g_create_err.c_str(); }
+
+int dsem_create(const dsem_mesh_desc *m, const dsem_phys *ph, dsem_ctx **out) {
+  if (!m || !ph || !out) return fail(nullptr, DSEM_ERR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  int r = check_desc(m);
+  if (r) return r;
+  MeshSet ms;
+  ms.m = {m};
+  ms.el0 = {0, m->ngrid};
+  ms.mo0 = {0, m->nmort};
+  return create_ctx(ms, ph, {ph->re}, out);
+}
+
+int dsem_create_batch(int ncase, const dsem_mesh_desc *meshes, const dsem_phys *phys, dsem_ctx **out) {
+  if (!meshes || !phys || !out || ncase <= 0) return fail(nullptr, DSEM_ERR_INVALID_ARG, "null argument or ncase < 1");
+  *out = nullptr;
+  MeshSet ms;
+  ms.el0 = {0};
+  ms.mo0 = {0};
+  std::vector<double> re;
+  for (int k = 0; k < ncase; ++k) {
+    const dsem_mesh_desc *m = &meshes[k];
+    const dsem_phys *p = &phys[k];
+    int r = check_desc(m);
+    if (r) return r;
+    if (p->gamma != phys[0].gamma || p->pr != phys[0].pr || p->mach != phys[0].mach || p->cmu != phys[0].cmu ||
+        p->mumax != phys[0].mumax || p->shock != phys[0].shock || p->iord != phys[0].iord)
+      return fail(nullptr, DSEM_ERR_UNSUPPORTED,
+                  "cases of one batch must share gamma, pr, mach, cmu, mumax, shock and iord (re and dt may differ)");
+    if (!(p->re > 0.0)) return fail(nullptr, DSEM_ERR_INVALID_ARG, "re must be positive");
+    if ((long long)ms.el0.back() + m->ngrid > 0x7fffffffLL || (long long)ms.mo0.back() + m->nmort > 0x7fffffffLL)
+      return fail(nullptr, DSEM_ERR_INVALID_ARG, "batch too large");
+    ms.m.push_back(m);
+    ms.el0.push_back(ms.el0.back() + m->ngrid);
+    ms.mo0.push_back(ms.mo0.back() + m->nmort);
+    re.push_back(p->re);
+  }
+  return create_ctx(ms, &phys[0], re, out);
+}
+
 }  // extern "C"
 
 namespace {
-int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m) {
-  const int ldx = m->ldx;
+int setup_ctx(dsem_ctx *c, const MeshSet &ms) {
   int r = upload_ops(c);
   if (r) return r;
+  const int ngrid = ms.ngrid();
 
   // ---- groups: elements sorted by order
-  const size_t L3 = (size_t)ldx * ldx * ldx;
-  c->ext_group.assign(m->ngrid, -1);
-  c->ext_k.assign(m->ngrid, -1);
+  c->ext_group.assign(ngrid, -1);
+  c->ext_k.assign(ngrid, -1);
   long long q0 = 0, f0 = 0, e0 = 0;
   for (int G = GMIN; G <= GMAX; ++G) {
     std::vector<int> ids;
-    for (int e = 0; e < m->ngrid; ++e)
-      if (m->ncg[3 * e] == G) ids.push_back(e);
+    for (int e = 0; e < ngrid; ++e)
+      if (ms.G(e) == G) ids.push_back(e);
     if (ids.empty()) continue;
     Group g;
     g.G = G;
@@ -485,7 +618,8 @@ int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m) {
       for (int l = 0; l < L && diag; ++l)
         for (int mm = 0; mm < L && diag; ++mm)
           for (int n = 0; n < L && diag; ++n) {
-            const size_t q = (size_t)e * L3 + n + (size_t)ldx * (mm + (size_t)ldx * l);
+            size_t q;
+            const dsem_mesh_desc *m = ms.at(e, n, mm, l, q);
             if (n < G && mm < G && l < G)
               for (int i = 0; i < 3; ++i)
                 for (int j = 0; j < 3; ++j)
@@ -505,14 +639,22 @@ int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m) {
     g.diag = diag;
     std::vector<double> jac((size_t)g.nel * NG), hd((size_t)g.nel * NG);
     std::vector<double> gg((size_t)g.nel * (diag ? 3 : 9) * NG), gmv((size_t)g.nel * (diag ? 3 : 9) * NL);
+    std::vector<int> ec(ids.size());
+    g.case_lo.assign(c->ncase, 0);
+    g.case_hi.assign(c->ncase, 0);
     for (int k = 0; k < g.nel; ++k) {
       const int e = ids[k];
+      const int cs = ms.case_of(e);
+      ec[k] = cs;
+      if (g.case_hi[cs] == 0) g.case_lo[cs] = k;  // ids increase and cases are contiguous
+      g.case_hi[cs] = k + 1;
       c->ext_group[e] = (int)c->groups.size();
       c->ext_k[e] = k;
       for (int l = 0; l < G; ++l)
         for (int mm = 0; mm < G; ++mm)
           for (int n = 0; n < G; ++n) {
-            const size_t q = (size_t)e * L3 + n + (size_t)ldx * (mm + (size_t)ldx * l);
+            size_t q;
+            const dsem_mesh_desc *m = ms.at(e, n, mm, l, q);
             const int p = n + G * (mm + G * l);
             jac[(size_t)k * NG + p] = m->jacob[q];
             hd[(size_t)k * NG + p] =  // delta_g (turbulence/staticSmago/staticSmag.f90:191-201)
@@ -532,7 +674,8 @@ int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m) {
         for (int l = 0; l < ext[2]; ++l)
           for (int mm = 0; mm < ext[1]; ++mm)
             for (int n = 0; n < ext[0]; ++n) {
-              const size_t q = (size_t)e * L3 + n + (size_t)ldx * (mm + (size_t)ldx * l);
+              size_t q;
+              const dsem_mesh_desc *m = ms.at(e, n, mm, l, q);
               const int pl = d == 0 ? n + L * (mm + G * l) : (d == 1 ? n + G * (mm + L * l) : n + G * (mm + G * l));
               if (diag) {
                 gmv[((size_t)k * 3 + d) * NL + pl] = m->gmet[q * 9 + d + 3 * d];
@@ -556,6 +699,8 @@ int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m) {
     CK(cudaMemset(g.EVB, 0, (size_t)g.nel * 15 * NG * sizeof(double)));
     CK(cudaMalloc(&g.int2ext, ids.size() * sizeof(int)));
     CK(cudaMemcpy(g.int2ext, ids.data(), ids.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&g.ecase, ec.size() * sizeof(int)));
+    CK(cudaMemcpy(g.ecase, ec.data(), ec.size() * sizeof(int), cudaMemcpyHostToDevice));
     std::vector<double> kw(NG);
     hostmath::ke_weights(G, kw.data());
     CK(cudaMalloc(&g.kew, NG * sizeof(double)));
@@ -574,16 +719,19 @@ int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m) {
   std::vector<double> nc_nh, nc_nrm, mats;
   std::map<long long, std::pair<int, int>> mat_off;
   std::vector<std::vector<double>> nhs(GMAX + 1), nrs(GMAX + 1);
+  for (int cs = 0; cs < c->ncase; ++cs) {
+  const dsem_mesh_desc *m = ms.m[cs];
+  const int ldx = m->ldx;
   for (int j = 0; j < m->nmort; ++j) {
     const int *t = m->mortar + (size_t)DSEM_MORTAR_INTS * j;
-    const int id1 = t[0] - 1, id2 = t[1] - 1;
-    if (id1 < 0 || id1 >= m->ngrid) return fail(c, DSEM_ERR_INVALID_ARG, "mortar master id out of range");
-    if (id2 < 0) return fail(c, DSEM_ERR_UNSUPPORTED, "boundary mortars (id(2)=0) are not supported: the implemented path is fully periodic");
-    if (id2 >= m->ngrid) return fail(c, DSEM_ERR_INVALID_ARG, "mortar slave id out of range");
+    if (t[0] - 1 < 0 || t[0] - 1 >= m->ngrid) return fail(c, DSEM_ERR_INVALID_ARG, "mortar master id out of range");
+    if (t[1] - 1 < 0) return fail(c, DSEM_ERR_UNSUPPORTED, "boundary mortars (id(2)=0) are not supported: the implemented path is fully periodic");
+    if (t[1] - 1 >= m->ngrid) return fail(c, DSEM_ERR_INVALID_ARG, "mortar slave id out of range");
+    const int id1 = t[0] - 1 + ms.el0[cs], id2 = t[1] - 1 + ms.el0[cs];
     const int f1 = t[2], f2 = t[3], orient = t[10];
     if (f1 < 1 || f1 > 6 || f2 < 1 || f2 > 6 || orient < 0 || orient > 7)
       return fail(c, DSEM_ERR_INVALID_ARG, "bad mortar face or orientation");
-    const int Gm = m->ncg[3 * id1], Gs = m->ncg[3 * id2];
+    const int Gm = ms.G(id1), Gs = ms.G(id2);
     const bool conf = t[13] && t[14] && t[15] && t[16];
     if (t[4] != Gm || t[5] != Gm || t[6] != Gs || t[7] != Gs || t[8] != std::max(Gm, Gs) || t[9] != std::max(Gm, Gs))
       return fail(c, DSEM_ERR_UNSUPPORTED, "mortar lengths must match the element orders (geometrically conforming faces)");
@@ -650,6 +798,7 @@ int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m) {
         for (int k = 0; k < 3; ++k) nhs[G].push_back(m->n_hat[q * 3 + k]);
       }
   }
+  }  // cases
   for (int G = GMIN; G <= GMAX; ++G) {
     if (mcs[G].empty()) continue;
     MList ml;
@@ -686,11 +835,38 @@ int setup_ctx(dsem_ctx *c, const dsem_mesh_desc *m) {
   CK(cudaMalloc(&c->QF, c->nface * sizeof(double)));
   CK(cudaMalloc(&c->FF, c->nface * sizeof(double)));
   CK(cudaMalloc(&c->VF, c->nface * sizeof(double)));
-  CK(cudaMalloc(&c->part, (size_t)m->ngrid * 5 * sizeof(double)));
+  CK(cudaMalloc(&c->part, (size_t)ngrid * 5 * sizeof(double)));
   CK(cudaMalloc(&c->flag, sizeof(int)));
   CK(cudaMemset(c->flag, 0, sizeof(int)));
   CK(cudaEventCreate(&c->e0));
   CK(cudaEventCreate(&c->e1));
+  // per-case tables
+  {
+    std::vector<double> rec(2 * (size_t)c->ncase);
+    for (int k = 0; k < c->ncase; ++k) {
+      rec[2 * k] = c->case_re[k];
+      rec[2 * k + 1] = 1.0 / c->case_re[k];
+    }
+    CK(cudaMalloc(&c->d_rec, rec.size() * sizeof(double)));
+    CK(cudaMemcpy(c->d_rec, rec.data(), rec.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->d_dtc, (size_t)c->ncase * sizeof(double)));
+    CK(cudaMemset(c->d_dtc, 0, (size_t)c->ncase * sizeof(double)));
+  }
+  // streams for the parallel branches of a stage
+  {
+    const size_t nj = std::max(c->groups.size(), c->mlists.size() + (c->nnc > 0 ? 1 : 0));
+    if (nj > 1) {
+      CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+      for (size_t j = 0; j < nj; ++j) {
+        cudaStream_t s;
+        cudaEvent_t e;
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        c->aux.push_back(s);
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c->ev_join.push_back(e);
+      }
+    }
+  }
   // set the shared-memory attribute of every volume variant outside any capture
   for (auto &g : c->groups)
     for (int mode = 0; mode < 4; ++mode) {
@@ -716,7 +892,13 @@ void dsem_destroy(dsem_ctx *c) {
     cudaFree(g.EVB);
     cudaFree(g.kew);
     cudaFree(g.int2ext);
+    cudaFree(g.ecase);
   }
+  cudaFree(c->d_rec);
+  cudaFree(c->d_dtc);
+  for (auto s : c->aux) cudaStreamDestroy(s);
+  for (auto e : c->ev_join) cudaEventDestroy(e);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   cudaFree(c->nc);
   cudaFree(c->nc_nh);
   cudaFree(c->nc_nrm);
@@ -751,7 +933,7 @@ int dsem_upload_q(dsem_ctx *c, const double *JQ, int ldx) {
   const size_t n = (size_t)c->ngrid * 5 * ldx * ldx * ldx;
   CK(cudaMemcpyAsync(c->stage, JQ, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
   for (auto &g : c->groups) {
-    k_pack<<<g.nel, 256, 0, c->st>>>(c->stage, ldx, g.int2ext, g.G, 5, c->JQ + g.q0, 1);
+    k_pack<<<g.nel, 256, 0, c->st>>>(c->stage, ldx, g.int2ext, 0, g.G, 5, c->JQ + g.q0, 1);
     CK(cudaGetLastError());
   }
   long long l = 0;
@@ -779,7 +961,7 @@ int dsem_rhs(dsem_ctx *c, double tk, double *Qt, int ldx) {
   int r;
   if (!c->traces_valid && (r = enqueue_traces(c, &l))) return r;
   CK(cudaMemsetAsync(c->flag, 0, sizeof(int), c->st));
-  r = enqueue_stage(c, 0, 0.0, true, c->Qt, &l);
+  r = enqueue_stage(c, 0, true, c->Qt, &l);
   if (r) return r;
   c->grad_valid = true;
   c->ev_grad_valid = c->shock != 0;
@@ -787,76 +969,55 @@ int dsem_rhs(dsem_ctx *c, double tk, double *Qt, int ldx) {
   return check_flag(c);
 }
 
-int dsem_stage(dsem_ctx *c, double time, double dt, int kk, double *Qt, int ldx) {
-  (void)time;
-  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
-  if (kk < 1 || kk > c->kord) return fail(c, DSEM_ERR_INVALID_ARG, "stage index outside 1..kord");
-  if (Qt) {
-    int r = check_ldx(c, ldx);
-    if (r) return r;
+}  // extern "C"
+
+namespace {
+// dt of every case for the stages enqueued next (read by k_update)
+int set_dt(dsem_ctx *c, const double *dt) {
+  for (int k = 0; k < c->ncase; ++k) {
+    if (!std::isfinite(dt[k])) return fail(c, DSEM_ERR_INVALID_ARG, "dt is not finite");
+    c->case_dt[k] = dt[k];
   }
-  long long l = 0;
-  int r;
-  if (!c->traces_valid && (r = enqueue_traces(c, &l))) return r;
-  CK(cudaMemsetAsync(c->flag, 0, sizeof(int), c->st));
-  if (kk == 1 && c->shock && (r = enqueue_ev(c, &l))) return r;
-  r = enqueue_stage(c, kk, dt, true, Qt ? c->Qt : nullptr, &l);
-  if (r) return r;
-  c->grad_valid = true;
-  c->ev_grad_valid = c->shock != 0;
-  if (Qt && (r = unpack_to_host(c, c->Qt, Qt, ldx, 5, state_offs(c)))) return r;
-  return check_flag(c);
+  CK(cudaMemcpyAsync(c->d_dtc, c->case_dt.data(), (size_t)c->ncase * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  return DSEM_OK;
 }
 
-int dsem_step(dsem_ctx *c, double time, double dt, int nsteps) {
-  (void)time;
-  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
-  if (nsteps < 0) return fail(c, DSEM_ERR_INVALID_ARG, "negative step count");
+int step_impl(dsem_ctx *c, int nsteps) {
   long long l = 0;
   int r;
   if (!c->traces_valid && (r = enqueue_traces(c, &l))) return r;
   CK(cudaMemsetAsync(c->flag, 0, sizeof(int), c->st));
   const bool save = c->shock || c->keep_grad;
-  const int key = (save ? 1 : 0) | (c->ev_grad_valid ? 2 : 0);
   long long per_step = 0;
   // the first step of a run may need EV without valid gradients: run it eagerly
+  CK(cudaEventRecord(c->e0, c->st));
   if (nsteps > 0 && c->shock && !c->ev_grad_valid) {
-    CK(cudaEventRecord(c->e0, c->st));
-    if ((r = enqueue_step(c, dt, save, &per_step))) return r;
+    if ((r = enqueue_step(c, save, &per_step))) return r;
     c->ev_grad_valid = true;
     c->grad_valid = true;
     --nsteps;
-  } else {
-    CK(cudaEventRecord(c->e0, c->st));
   }
   long long launches = per_step;
   if (nsteps > 0) {
-    if (!c->gexec || c->graph_dt != dt || c->graph_key != key) {
+    const int key = (save ? 1 : 0) | (c->ev_grad_valid ? 2 : 0);
+    if (!c->gexec || c->graph_key != key) {
       if (c->gexec) cudaGraphExecDestroy(c->gexec);
       c->gexec = nullptr;
       cudaGraph_t graph;
       CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
       long long cnt = 0;
-      r = enqueue_step(c, dt, save, &cnt);
+      r = enqueue_step(c, save, &cnt);
       cudaError_t ec = cudaStreamEndCapture(c->st, &graph);
       if (r) return r;
       if (ec != cudaSuccess) return cuda_fail(c, ec, "cudaStreamEndCapture");
       ec = cudaGraphInstantiate(&c->gexec, graph, 0);
       cudaGraphDestroy(graph);
       if (ec != cudaSuccess) return cuda_fail(c, ec, "cudaGraphInstantiate");
-      c->graph_dt = dt;
       c->graph_key = key;
-      c->last_launches = cnt;
-    }
-    long long cnt = 0;
-    {
-      // launches per graph replay: recount without enqueueing
-      cnt = (long long)c->kord * (2 * (long long)c->mlists.size() + 2 * (long long)c->groups.size() +
-                                  (c->nnc > 0 ? 2 : 0)) +
-            (c->shock ? (long long)c->groups.size() : 0);
+      c->graph_launches = cnt;
     }
     for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->gexec, c->st));
-    launches += cnt * nsteps;
+    launches += c->graph_launches * nsteps;
     c->grad_valid = c->grad_valid || save;
     c->ev_grad_valid = c->ev_grad_valid || c->shock;
   }
@@ -870,8 +1031,8 @@ int dsem_step(dsem_ctx *c, double time, double dt, int nsteps) {
   return check_flag(c);
 }
 
-int dsem_diag(dsem_ctx *c, double dt, int first, double *ke, double *dkdt, double *eps) {
-  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+// KE, -dKE/dt and the enstrophy dissipation of every case
+int diag_impl(dsem_ctx *c, const double *dt, int first, double *ke, double *dkdt, double *eps) {
   c->keep_grad = 1;
   const bool have = c->grad_valid;
   for (auto &g : c->groups) {
@@ -882,32 +1043,140 @@ int dsem_diag(dsem_ctx *c, double dt, int first, double *ke, double *dkdt, doubl
   c->host_part.resize((size_t)c->ngrid * 5);
   CK(cudaMemcpyAsync(c->host_part.data(), c->part, c->host_part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
-  double us = 0, vs = 0, ws = 0, s = 0, s2 = 0;
-  for (int e = 0; e < c->ngrid; ++e) {  // caller element order
-    const auto &g = c->groups[c->ext_group[e]];
-    const double *p = &c->host_part[(size_t)(g.e0 + c->ext_k[e]) * 5];
-    us += p[0];
-    vs += p[1];
-    ws += p[2];
-    s += p[3];
-    s2 += p[4];
-  }
-  // jacob(1,1,1) of element 1
-  double j0 = 0.0;
-  {
-    const auto &g = c->groups[c->ext_group[0]];
-    CK(cudaMemcpy(&j0, g.jac + (size_t)c->ext_k[0] * g.G * g.G * g.G, sizeof(double), cudaMemcpyDeviceToHost));
-  }
-  us /= j0;
-  vs /= j0;
-  ws /= j0;
   const double PI = hostmath::PI;
-  const double tk = 0.5 * (us + vs + ws) / (8.0 * PI * PI * PI);
-  if (first) c->prestep = 0.0;
-  if (ke) *ke = tk;
-  if (dkdt) *dkdt = (c->prestep - tk) / dt;
-  c->prestep = tk;
-  if (eps) *eps = (have && s2 > 0) ? 100.0 * (s / s2) * (1.0 / c->P.re) : 0.0;
+  for (int k = 0; k < c->ncase; ++k) {
+    double us = 0, vs = 0, ws = 0, s = 0, s2 = 0;
+    for (int e = c->case_el0[k]; e < c->case_el0[k + 1]; ++e) {  // caller element order
+      const auto &g = c->groups[c->ext_group[e]];
+      const double *p = &c->host_part[(size_t)(g.e0 + c->ext_k[e]) * 5];
+      us += p[0];
+      vs += p[1];
+      ws += p[2];
+      s += p[3];
+      s2 += p[4];
+    }
+    // jacob(1,1,1) of the case's element 1
+    double j0 = 0.0;
+    {
+      const int e1 = c->case_el0[k];
+      const auto &g = c->groups[c->ext_group[e1]];
+      CK(cudaMemcpy(&j0, g.jac + (size_t)c->ext_k[e1] * g.G * g.G * g.G, sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    us /= j0;
+    vs /= j0;
+    ws /= j0;
+    const double tk = 0.5 * (us + vs + ws) / (8.0 * PI * PI * PI);
+    if (first) c->case_prestep[k] = 0.0;
+    if (ke) ke[k] = tk;
+    if (dkdt) dkdt[k] = (c->case_prestep[k] - tk) / dt[k];
+    c->case_prestep[k] = tk;
+    if (eps) eps[k] = (have && s2 > 0) ? 100.0 * (s / s2) * (1.0 / c->case_re[k]) : 0.0;
+  }
+  return DSEM_OK;
+}
+
+int check_case(dsem_ctx *c, int k) {
+  if (k < 0 || k >= c->ncase) return fail(c, DSEM_ERR_INVALID_ARG, "case index out of range");
+  return DSEM_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int dsem_stage(dsem_ctx *c, double time, double dt, int kk, double *Qt, int ldx) {
+  (void)time;
+  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (kk < 1 || kk > c->kord) return fail(c, DSEM_ERR_INVALID_ARG, "stage index outside 1..kord");
+  if (Qt) {
+    int r = check_ldx(c, ldx);
+    if (r) return r;
+  }
+  std::vector<double> dts(c->ncase, dt);
+  int r = set_dt(c, dts.data());
+  if (r) return r;
+  long long l = 0;
+  if (!c->traces_valid && (r = enqueue_traces(c, &l))) return r;
+  CK(cudaMemsetAsync(c->flag, 0, sizeof(int), c->st));
+  if (kk == 1 && c->shock && (r = enqueue_ev(c, &l))) return r;
+  r = enqueue_stage(c, kk, true, Qt ? c->Qt : nullptr, &l);
+  if (r) return r;
+  c->grad_valid = true;
+  c->ev_grad_valid = c->shock != 0;
+  if (Qt && (r = unpack_to_host(c, c->Qt, Qt, ldx, 5, state_offs(c)))) return r;
+  return check_flag(c);
+}
+
+int dsem_step(dsem_ctx *c, double time, double dt, int nsteps) {
+  (void)time;
+  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (nsteps < 0) return fail(c, DSEM_ERR_INVALID_ARG, "negative step count");
+  std::vector<double> dts(c->ncase, dt);
+  const int r = set_dt(c, dts.data());
+  if (r) return r;
+  return step_impl(c, nsteps);
+}
+
+int dsem_step_batch(dsem_ctx *c, const double *dt, int nsteps) {
+  if (!c || !dt) return fail(c, DSEM_ERR_INVALID_ARG, "null argument");
+  if (nsteps < 0) return fail(c, DSEM_ERR_INVALID_ARG, "negative step count");
+  const int r = set_dt(c, dt);
+  if (r) return r;
+  return step_impl(c, nsteps);
+}
+
+int dsem_diag(dsem_ctx *c, double dt, int first, double *ke, double *dkdt, double *eps) {
+  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (c->ncase != 1) return fail(c, DSEM_ERR_INVALID_ARG, "a batch reports per case: use dsem_diag_batch");
+  return diag_impl(c, &dt, first, ke, dkdt, eps);
+}
+
+int dsem_diag_batch(dsem_ctx *c, const double *dt, int first, double *ke, double *dkdt, double *eps) {
+  if (!c || !dt) return fail(c, DSEM_ERR_INVALID_ARG, "null argument");
+  return diag_impl(c, dt, first, ke, dkdt, eps);
+}
+
+int dsem_batch_size(const dsem_ctx *c) { return c ? c->ncase : DSEM_ERR_INVALID_ARG; }
+
+int dsem_upload_q_case(dsem_ctx *c, int k, const double *JQ, int ldx) {
+  if (!c || !JQ) return fail(c, DSEM_ERR_INVALID_ARG, "null argument");
+  int r = check_case(c, k);
+  if (r) return r;
+  for (auto &g : c->groups)
+    if (g.case_hi[k] > g.case_lo[k] && ldx < g.G) return fail(c, DSEM_ERR_INVALID_ARG, "ldx smaller than the number of Gauss points");
+  if ((r = ensure_stage_buf(c, ldx, 5))) return r;
+  const size_t n = (size_t)(c->case_el0[k + 1] - c->case_el0[k]) * 5 * ldx * ldx * ldx;
+  CK(cudaMemcpyAsync(c->stage, JQ, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  for (auto &g : c->groups) {
+    const int lo = g.case_lo[k], nk = g.case_hi[k] - lo;
+    if (nk <= 0) continue;
+    k_pack<<<nk, 256, 0, c->st>>>(c->stage, ldx, g.int2ext + lo, c->case_el0[k], g.G, 5,
+                                  c->JQ + g.q0 + (long long)lo * 5 * g.G * g.G * g.G, 1);
+    CK(cudaGetLastError());
+  }
+  long long l = 0;
+  if ((r = enqueue_traces(c, &l))) return r;
+  CK(cudaStreamSynchronize(c->st));
+  return DSEM_OK;
+}
+
+int dsem_download_q_case(dsem_ctx *c, int k, double *JQ, int ldx) {
+  if (!c || !JQ) return fail(c, DSEM_ERR_INVALID_ARG, "null argument");
+  int r = check_case(c, k);
+  if (r) return r;
+  for (auto &g : c->groups)
+    if (g.case_hi[k] > g.case_lo[k] && ldx < g.G) return fail(c, DSEM_ERR_INVALID_ARG, "ldx smaller than the number of Gauss points");
+  if ((r = ensure_stage_buf(c, ldx, 5))) return r;
+  const size_t n = (size_t)(c->case_el0[k + 1] - c->case_el0[k]) * 5 * ldx * ldx * ldx;
+  CK(cudaMemsetAsync(c->stage, 0, n * sizeof(double), c->st));
+  for (auto &g : c->groups) {
+    const int lo = g.case_lo[k], nk = g.case_hi[k] - lo;
+    if (nk <= 0) continue;
+    k_pack<<<nk, 256, 0, c->st>>>(c->JQ + g.q0 + (long long)lo * 5 * g.G * g.G * g.G, ldx, g.int2ext + lo,
+                                  c->case_el0[k], g.G, 5, c->stage, 0);
+    CK(cudaGetLastError());
+  }
+  CK(cudaMemcpyAsync(JQ, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
   return DSEM_OK;
 }
 
@@ -922,7 +1191,7 @@ int dsem_get_muhg(dsem_ctx *c, double *mu, int ldx) {
   const size_t n = (size_t)c->ngrid * ldx * ldx * ldx;
   CK(cudaMemsetAsync(c->stage, 0, n * sizeof(double), c->st));
   for (auto &g : c->groups) {
-    k_pack<<<g.nel, 256, 0, c->st>>>(g.muhg, ldx, g.int2ext, g.G, 1, c->stage, 0);
+    k_pack<<<g.nel, 256, 0, c->st>>>(g.muhg, ldx, g.int2ext, 0, g.G, 1, c->stage, 0);
     CK(cudaGetLastError());
   }
   CK(cudaMemcpyAsync(mu, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));

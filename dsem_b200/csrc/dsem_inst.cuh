@@ -2,6 +2,7 @@
 #pragma once
 #include "dsem_launch.h"
 #include "dsem_stage.cuh"
+#include "dsem_vol_diag.cuh"
 
 namespace dsem {
 
@@ -24,26 +25,40 @@ template <int G, bool DIAG, bool EV, int SAVE> static cudaError_t vol_one(const 
   return cudaGetLastError();
 }
 
+// diagonal metrics: k_vol_diag (two elements per SM at p = 8)
+template <int G, bool EV, int SAVE> static cudaError_t vol_diag_one(const VolArgs &a, int nel, cudaStream_t s) {
+  using C = VolDiagCfg<G, EV, SAVE>;
+  auto kern = k_vol_diag<G, EV, SAVE>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  if (nel <= 0) return cudaSuccess;
+  kern<<<nel, C::NT, C::SMEM, s>>>(a);
+  return cudaGetLastError();
+}
+
 template <int G> size_t Launch<G>::vol_smem(bool diag, int mode) {
   switch (mode) {
-    case VOL_SAVE: return diag ? VolCfg<G, true, false, 1>::SMEM : VolCfg<G, false, false, 1>::SMEM;
-    case VOL_EV: return diag ? VolCfg<G, true, true, 0>::SMEM : VolCfg<G, false, true, 0>::SMEM;
-    case VOL_EV_SAVE: return diag ? VolCfg<G, true, true, 2>::SMEM : VolCfg<G, false, true, 2>::SMEM;
-    default: return diag ? VolCfg<G, true, false, 0>::SMEM : VolCfg<G, false, false, 0>::SMEM;
+    case VOL_SAVE: return diag ? VolDiagCfg<G, false, 1>::SMEM : VolCfg<G, false, false, 1>::SMEM;
+    case VOL_EV: return diag ? VolDiagCfg<G, true, 0>::SMEM : VolCfg<G, false, true, 0>::SMEM;
+    case VOL_EV_SAVE: return diag ? VolDiagCfg<G, true, 2>::SMEM : VolCfg<G, false, true, 2>::SMEM;
+    default: return diag ? VolDiagCfg<G, false, 0>::SMEM : VolCfg<G, false, false, 0>::SMEM;
   }
 }
 template <int G> int Launch<G>::vol_threads(bool diag, int mode) {
-  (void)diag;
   (void)mode;
-  return VolCfg<G, true, false, 0>::NT;
+  return diag ? VolDiagCfg<G, false, 0>::NT : VolCfg<G, false, false, 0>::NT;
 }
 
 template <int G> cudaError_t Launch<G>::vol(const VolArgs &a, int nel, bool diag, int mode, cudaStream_t s) {
   switch (mode) {
-    case VOL_SAVE: return diag ? vol_one<G, true, false, 1>(a, nel, s) : vol_one<G, false, false, 1>(a, nel, s);
-    case VOL_EV: return diag ? vol_one<G, true, true, 0>(a, nel, s) : vol_one<G, false, true, 0>(a, nel, s);
-    case VOL_EV_SAVE: return diag ? vol_one<G, true, true, 2>(a, nel, s) : vol_one<G, false, true, 2>(a, nel, s);
-    default: return diag ? vol_one<G, true, false, 0>(a, nel, s) : vol_one<G, false, false, 0>(a, nel, s);
+    case VOL_SAVE: return diag ? vol_diag_one<G, false, 1>(a, nel, s) : vol_one<G, false, false, 1>(a, nel, s);
+    case VOL_EV: return diag ? vol_diag_one<G, true, 0>(a, nel, s) : vol_one<G, false, true, 0>(a, nel, s);
+    case VOL_EV_SAVE: return diag ? vol_diag_one<G, true, 2>(a, nel, s) : vol_one<G, false, true, 2>(a, nel, s);
+    default: return diag ? vol_diag_one<G, false, 0>(a, nel, s) : vol_one<G, false, false, 0>(a, nel, s);
   }
 }
 

@@ -479,6 +479,8 @@ struct VolArgs {
   double *QTI;                  // [elem][5][G^3]   out: interior divergence sum
   double *EVB;                  // [elem][15][G^3]  out: gradients kept for EV / diagnostics
   Phys P;
+  const int *ecase;             // optional: case of each element (ensembles)
+  const double *rec;            // optional: per case {re, 1/re}
 };
 
 template <int G, bool DIAG, bool EV, int SAVE> struct VolCfg {
@@ -567,7 +569,7 @@ __device__ __forceinline__ void deriv_task(int t, const double *LB, int NLS, con
 template <int G, bool DIAG, bool EV, int SAVE, int D>
 __device__ __forceinline__ void vol_dir(const VolArgs &A, const double *JQ, const double *jac, const double *QF,
                                         const double *gm, const double *muhg, const double *GR, double *LB, double *CH,
-                                        double *VF, double *QT, int tid, int nt, long long &t_ph_) {
+                                        double *VF, double *QT, const Phys &P, int tid, int nt, long long &t_ph_) {
   using C = VolCfg<G, DIAG, EV, SAVE>;
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
   constexpr int LX = C::LX, NLS = C::NLS, NCH = C::NCH;
@@ -591,7 +593,6 @@ __device__ __forceinline__ void vol_dir(const VolArgs &A, const double *JQ, cons
   }
   __syncthreads();
   PHASE_MARK(9 + 4 * D);
-  const Phys P = A.P;
   for (int qi = tid; qi < NL; qi += nt) {  // fluxes on grid D (Vis_Fluxes_new.f90:115-228, fluxesH_newa.f90:276-352)
     int s, a, b, p, pg;
     if (D == 0) {
@@ -715,6 +716,12 @@ __global__ void __launch_bounds__(VolCfg<G, DIAG, EV, SAVE>::NT, 1) k_vol(VolArg
   const double *gm = A.gm + (long long)k * 3 * NL * (DIAG ? 1 : 3);
   const double *muhg = EV ? A.muhg + (long long)k * NG : nullptr;
   const double gamma = A.P.gamma;
+  Phys P = A.P;
+  if (A.rec) {  // per-case Reynolds number
+    const int cs = A.ecase[k];
+    P.re = A.rec[2 * cs];
+    P.r_re = A.rec[2 * cs + 1];
+  }
   long long t_ph_ = 0;
 #ifdef DSEM_PHASE_TIMING
   t_ph_ = clock64();
@@ -753,9 +760,9 @@ __global__ void __launch_bounds__(VolCfg<G, DIAG, EV, SAVE>::NT, 1) k_vol(VolArg
     for (int i = tid; i < 12 * NG; i += nt) EVB[i] = GR[i];
   }
   // pass 2: z (reusing the last Lobatto array), y, x
-  vol_dir<G, DIAG, EV, SAVE, 2>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QT, tid, nt, t_ph_);
-  vol_dir<G, DIAG, EV, SAVE, 1>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QT, tid, nt, t_ph_);
-  vol_dir<G, DIAG, EV, SAVE, 0>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QT, tid, nt, t_ph_);
+  vol_dir<G, DIAG, EV, SAVE, 2>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QT, P, tid, nt, t_ph_);
+  vol_dir<G, DIAG, EV, SAVE, 1>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QT, P, tid, nt, t_ph_);
+  vol_dir<G, DIAG, EV, SAVE, 0>(A, JQ, jac, QF, gm, muhg, GR, LB, CH, VF, QT, P, tid, nt, t_ph_);
   if (C::QSM) {
     for (int i = tid; i < 5 * NG; i += nt) QTI[i] = QTS[i];
   }
@@ -773,6 +780,9 @@ struct UpdArgs {
   int *flag;       // bit 0: non-finite Qt
   double ark, cdt, re, r_re;  // r_re = 1/re
   int first, update;
+  const int *ecase;           // optional: case of each element (ensembles)
+  const double *rec, *dtc;    // optional: per case {re, 1/re} and dt; cdt = crk * dt
+  double crk;
 };
 
 template <int G> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
@@ -785,7 +795,16 @@ template <int G> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
   const int k = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
   const double *FF = A.FF + (long long)k * 30 * G2;
   const double *VF = A.VF + (long long)k * 30 * G2;
-  for (int i = tid; i < 30 * G2; i += nt) FB[i] = FF[i] - ddiv(VF[i], A.re, A.r_re);  // send_flux_to_faces_add
+  double re = A.re, rre = A.r_re, cdt = A.cdt;
+  if (A.ecase) {
+    const int cs = A.ecase[k];
+    if (A.rec) {
+      re = A.rec[2 * cs];
+      rre = A.rec[2 * cs + 1];
+    }
+    if (A.dtc) cdt = A.crk * A.dtc[cs];
+  }
+  for (int i = tid; i < 30 * G2; i += nt) FB[i] = FF[i] - ddiv(VF[i], re, rre);  // send_flux_to_faces_add
   for (int i = tid; i < G; i += nt) {
     Dlo[i] = Op<G>::D(i, 0);
     Dhi[i] = Op<G>::D(i, L - 1);
@@ -814,7 +833,7 @@ template <int G> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
     if (A.update) {  // updatea.f90:213-227
       const double g0 = A.first ? 0.0 : gQ[i];
       const double g = A.ark * g0 + Qt;
-      q = q + A.cdt * g;
+      q = q + cdt * g;
       gQ[i] = g;
       JQ[i] = q;
     }
@@ -833,6 +852,8 @@ struct EvArgs {
   double *muhg;
   int valid;
   Phys P;
+  const int *ecase;   // optional: case of each element (ensembles)
+  const double *rec;  // optional: per case {re, 1/re}
 };
 
 // RHS_ent_trans + Entropy_Viscosity at Gauss points (RHS.f90:21-278, EViscosity_GL.f90:19-101)
@@ -844,6 +865,12 @@ template <int G> __global__ void __launch_bounds__(256) k_ev(EvArgs A) {
   const double *hd = A.hd + (long long)k * NG;
   const double *EVB = A.EVB + (long long)k * 15 * NG;
   double *mu = A.muhg + (long long)k * NG;
+  Phys P = A.P;
+  if (A.rec) {
+    const int cs = A.ecase[k];
+    P.re = A.rec[2 * cs];
+    P.r_re = A.rec[2 * cs + 1];
+  }
   for (int p = threadIdx.x; p < NG; p += blockDim.x) {
     double out = 0.0;
     if (A.valid) {
@@ -861,13 +888,13 @@ template <int G> __global__ void __launch_bounds__(256) k_ev(EvArgs A) {
       T1[1] = EVB[13 * NG + p];
       T1[2] = EVB[14 * NG + p];
       double duc;
-      const double biS = ev_residual(A.P, Q, Qx, Qy, Qz, T1, duc);
+      const double biS = ev_residual(P, Q, Qx, Qy, Qz, T1, duc);
       const double rho = JQ[p] * jac[p];
       const double h = hd[p];
-      double mur = A.P.cmu * A.P.re * rho * (h * h) * fabs(biS);
-      if (A.P.ducros) mur = mur * duc;
+      double mur = P.cmu * P.re * rho * (h * h) * fabs(biS);
+      if (P.ducros) mur = mur * duc;
       const double mx = mur >= 0.0 ? mur : 0.0;
-      double m = mx <= A.P.mumax ? mx : A.P.mumax;
+      double m = mx <= P.mumax ? mx : P.mumax;
       if (!isfinite(m)) m = 0.0;
       out = m;
     }

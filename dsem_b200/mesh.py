@@ -346,6 +346,38 @@ def taylor_green(box, gamma=1.4, twall=100.0, v0=1.0):
     return jq.reshape(box.qshape())
 
 
+def _modes_separable(box, K, kmax, amp, a, phase):
+    """sum_m amp_m a_m cos(k_m.x + phase_m) at every point of box.xg, evaluated
+    as three 1-D sums per element when each element's Gauss points form a
+    tensor grid (x from n, y from m, z from l, to 1e-12); None otherwise."""
+    ldx = box.ldx
+    xg = box.xg.reshape(box.nel, ldx, ldx, ldx, 3)
+    nk = 2 * kmax + 1
+    C = np.zeros((nk, nk, nk, 3), dtype=complex)
+    idx = K.astype(int) + kmax
+    np.add.at(C, (idx[:, 0], idx[:, 1], idx[:, 2]), (amp * np.exp(1j * phase))[:, None] * a)
+    ks = np.arange(-kmax, kmax + 1, dtype=float)
+    u = np.zeros((box.nel, ldx, ldx, ldx, 3))
+    for G in np.unique(box.G):
+        G = int(G)
+        ids = np.where(box.G == G)[0]
+        x = xg[ids][:, :G, :G, :G]  # [e][l][m][n][c]
+        xe, ye, ze = x[:, 0, 0, :, 0], x[:, 0, :, 0, 1], x[:, :, 0, 0, 2]
+        tol = 1e-12 * max(1.0, float(np.abs(x).max()))
+        if not (np.abs(x[..., 0] - xe[:, None, None, :]).max() <= tol and
+                np.abs(x[..., 1] - ye[:, None, :, None]).max() <= tol and
+                np.abs(x[..., 2] - ze[:, :, None, None]).max() <= tol):
+            return None
+        Ex = np.exp(1j * xe[:, :, None] * ks)  # [e][n][kx]
+        Ey = np.exp(1j * ye[:, :, None] * ks)
+        Ez = np.exp(1j * ze[:, :, None] * ks)
+        t = np.einsum("abcv,elc->eablv", C, Ez, optimize=True)
+        t = np.einsum("eablv,emb->eamlv", t, Ey, optimize=True)
+        t = np.einsum("eamlv,ena->elmnv", t, Ex, optimize=True)
+        u[ids, :G, :G, :G] = t.real
+    return u.reshape(-1, 3)
+
+
 def random_isotropic(box, seed, k0=4.0, mach_t=0.3, gamma=1.4, twall=100.0):
     """Seeded divergence-free random-phase velocity with E(k) ~ k^4 exp(-2 (k/k0)^2),
     scaled to turbulent Mach number mach_t (u_rms = M_t c0 / sqrt(3)), uniform
@@ -363,11 +395,13 @@ def random_isotropic(box, seed, k0=4.0, mach_t=0.3, gamma=1.4, twall=100.0):
     a -= (np.sum(a * K, axis=1) / kk ** 2)[:, None] * K  # divergence free
     a /= np.linalg.norm(a, axis=1)[:, None] + 1e-300
     phase = rng.uniform(0, 2 * np.pi, len(K))
-    X = box.xg.reshape(-1, 3)
-    u = np.zeros((X.shape[0], 3))
-    for i in range(0, len(K), 256):
-        arg = X @ K[i:i + 256].T + phase[i:i + 256]
-        u += np.cos(arg) @ (amp[i:i + 256, None] * a[i:i + 256])
+    u = _modes_separable(box, K, kmax, amp, a, phase)
+    if u is None:  # rotated elements: direct sum over points and modes
+        X = box.xg.reshape(-1, 3)
+        u = np.zeros((X.shape[0], 3))
+        for i in range(0, len(K), 256):
+            arg = X @ K[i:i + 256].T + phase[i:i + 256]
+            u += np.cos(arg) @ (amp[i:i + 256, None] * a[i:i + 256])
     mask = (box.jacob != 0).reshape(-1)
     p0 = twall / gamma
     c0 = math.sqrt(gamma * p0 / 1.0)

@@ -16,7 +16,9 @@ LIB = os.path.join(HERE, "libdsem_b200.so")
 DSEM_OK = 0
 ERRORS = {-1: "INVALID_ARG", -2: "CUDA", -3: "NONFINITE", -4: "TIMEOUT", -5: "UNSUPPORTED", -6: "NOMEM"}
 EXPORTS = ("dsem_create", "dsem_destroy", "dsem_last_error", "dsem_upload_q", "dsem_download_q", "dsem_step",
-           "dsem_stage", "dsem_rhs", "dsem_diag", "dsem_get_muhg", "dsem_last_timing", "dsem_profile_rhs")
+           "dsem_stage", "dsem_rhs", "dsem_diag", "dsem_get_muhg", "dsem_last_timing", "dsem_profile_rhs",
+           "dsem_create_batch", "dsem_batch_size", "dsem_upload_q_case", "dsem_download_q_case", "dsem_step_batch",
+           "dsem_diag_batch")
 
 
 class DsemError(RuntimeError):
@@ -63,6 +65,12 @@ def lib(path=None):
         L.dsem_get_muhg.argtypes = [vp, dp, C.c_int]
         L.dsem_last_timing.argtypes = [vp, dp, C.POINTER(C.c_longlong)]
         L.dsem_profile_rhs.argtypes = [vp, C.c_int, dp]
+        L.dsem_create_batch.argtypes = [C.c_int, C.POINTER(MeshDesc), C.POINTER(Phys), C.POINTER(vp)]
+        L.dsem_batch_size.argtypes = [vp]
+        L.dsem_upload_q_case.argtypes = [vp, C.c_int, dp, C.c_int]
+        L.dsem_download_q_case.argtypes = [vp, C.c_int, dp, C.c_int]
+        L.dsem_step_batch.argtypes = [vp, dp, C.c_int]
+        L.dsem_diag_batch.argtypes = [vp, dp, C.c_int, dp, dp, dp]
         _lib = L
     return _lib
 
@@ -75,18 +83,22 @@ def _iptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_int))
 
 
+def _mesh_desc(desc):
+    """(MeshDesc, arrays kept alive while the descriptor is in use)."""
+    a = {k: np.ascontiguousarray(desc[k]) for k in ("ncg", "jacob", "gmetg", "gmet", "mortar", "n_hat", "norm")}
+    assert a["ncg"].dtype == np.int32 and a["mortar"].dtype == np.int32
+    md = MeshDesc(int(desc["ngrid"]), int(desc["nmort"]), int(desc["ldx"]), _iptr(a["ncg"]), _dptr(a["jacob"]),
+                  _dptr(a["gmetg"]), _dptr(a["gmet"]), _iptr(a["mortar"]), _dptr(a["n_hat"]), _dptr(a["norm"]))
+    return md, a
+
+
 class Solver:
     """One device context: geometry + state resident in HBM."""
 
     def __init__(self, desc, gamma=1.4, re=1600.0, pr=0.72, mach=1.0, cmu=0.0, mumax=0.0, shock=0, iord=4):
         L = lib()
-        self._arrays = {k: np.ascontiguousarray(desc[k]) for k in ("ncg", "jacob", "gmetg", "gmet", "mortar",
-                                                                  "n_hat", "norm")}
-        a = self._arrays
-        assert a["ncg"].dtype == np.int32 and a["mortar"].dtype == np.int32
+        md, self._arrays = _mesh_desc(desc)
         self.ngrid, self.nmort, self.ldx = int(desc["ngrid"]), int(desc["nmort"]), int(desc["ldx"])
-        md = MeshDesc(self.ngrid, self.nmort, self.ldx, _iptr(a["ncg"]), _dptr(a["jacob"]), _dptr(a["gmetg"]),
-                      _dptr(a["gmet"]), _iptr(a["mortar"]), _dptr(a["n_hat"]), _dptr(a["norm"]))
         ph = Phys(gamma, re, pr, mach, cmu, mumax, int(shock), int(iord))
         h = C.c_void_p()
         rc = L.dsem_create(C.byref(md), C.byref(ph), C.byref(h))
@@ -156,3 +168,56 @@ class Solver:
         ms, n = C.c_double(), C.c_longlong()
         self._check(lib().dsem_last_timing(self.h, C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+
+class Ensemble(Solver):
+    """Several independent cases advanced together (dsem_create_batch).
+
+    descs: mesh descriptors (each with its own order and padding); res: one
+    Reynolds number per case; the other physics parameters are shared.
+    """
+
+    def __init__(self, descs, res, gamma=1.4, pr=0.72, mach=1.0, cmu=0.0, mumax=0.0, shock=0, iord=4):
+        L = lib()
+        n = len(descs)
+        assert len(res) == n and n > 0
+        mds = (MeshDesc * n)()
+        phs = (Phys * n)()
+        self._keep = []
+        for k, d in enumerate(descs):
+            md, arrs = _mesh_desc(d)
+            self._keep.append(arrs)
+            mds[k] = md
+            phs[k] = Phys(gamma, float(res[k]), pr, mach, cmu, mumax, int(shock), int(iord))
+        h = C.c_void_p()
+        rc = L.dsem_create_batch(n, mds, phs, C.byref(h))
+        if rc != DSEM_OK:
+            raise DsemError(rc, L.dsem_last_error(None).decode())
+        self.h = h
+        self.ncase = n
+        self.case_ngrid = [int(d["ngrid"]) for d in descs]
+        self.case_ldx = [int(d["ldx"]) for d in descs]
+        self.ngrid = sum(self.case_ngrid)
+        self.ldx = max(self.case_ldx)
+        self.kord = 5 if iord == 4 else iord
+
+    def upload_case(self, k, JQ):
+        JQ = np.ascontiguousarray(JQ, dtype=np.float64)
+        self._check(lib().dsem_upload_q_case(self.h, int(k), _dptr(JQ), JQ.shape[-1]))
+
+    def download_case(self, k, ldx=None):
+        ldx = ldx or self.case_ldx[k]
+        out = np.zeros((self.case_ngrid[k], 5, ldx, ldx, ldx))
+        self._check(lib().dsem_download_q_case(self.h, int(k), _dptr(out), ldx))
+        return out
+
+    def step_batch(self, dts, nsteps=1):
+        dts = np.ascontiguousarray(dts, dtype=np.float64)
+        assert dts.shape == (self.ncase,)
+        self._check(lib().dsem_step_batch(self.h, _dptr(dts), int(nsteps)))
+
+    def diag_batch(self, dts, first=False):
+        dts = np.ascontiguousarray(dts, dtype=np.float64)
+        ke, dk, ep = (np.zeros(self.ncase) for _ in range(3))
+        self._check(lib().dsem_diag_batch(self.h, _dptr(dts), int(first), _dptr(ke), _dptr(dk), _dptr(ep)))
+        return ke, dk, ep

@@ -119,6 +119,30 @@ int dsem_last_timing(const dsem_ctx *ctx, double *ms, long long *launches);
  * volume, viscous face, divergence + update}.  The state is left unchanged. */
 int dsem_profile_rhs(dsem_ctx *ctx, int reps, double *ms);
 
+/* ---- Ensembles: ncase independent runs in one context ----
+ * No DSEM counterpart (DSEM runs one case per job; each would call tstep,
+ * tstep.f90:12, from its own time loop, 3DDriver_parfmdf.f90:466).  The
+ * cases' elements share the launches: one launch per kernel type and element
+ * order per stage for the whole ensemble, one CUDA graph per step, order
+ * groups as parallel graph branches.  Each case keeps its own mesh (with its
+ * own ldx), Reynolds number, time step, state and diagnostics; every case
+ * gives bit-for-bit the result of its own single-case context.
+ * meshes[ncase], phys[ncase]: all cases must share gamma, pr, mach, cmu,
+ * mumax, shock and iord (DSEM_ERR_UNSUPPORTED otherwise); re may differ.
+ * The descriptors' arrays are read only during the call.  Mortar ids are
+ * per case (1-based within the case).  dsem_step / dsem_stage on an
+ * ensemble use the same dt for every case; dsem_upload_q / dsem_download_q
+ * / dsem_rhs see the cases' elements concatenated in case order. */
+int dsem_create_batch(int ncase, const dsem_mesh_desc *meshes, const dsem_phys *phys, dsem_ctx **out);
+int dsem_batch_size(const dsem_ctx *ctx); /* number of cases (1 for dsem_create) */
+int dsem_upload_q_case(dsem_ctx *ctx, int icase, const double *JQ, int ldx);
+int dsem_download_q_case(dsem_ctx *ctx, int icase, double *JQ, int ldx);
+/* nsteps steps of every case, case k with time step dt[k] (tstep.f90:36-116). */
+int dsem_step_batch(dsem_ctx *ctx, const double *dt, int nsteps);
+/* dsem_diag per case: dt, ke, dkdt, eps are arrays of ncase (dsem_diag itself
+ * rejects contexts with more than one case). */
+int dsem_diag_batch(dsem_ctx *ctx, const double *dt, int first, double *ke, double *dkdt, double *eps);
+
 /* Size of the static device array that holds the working buffers of
  * dsem_rhs_noalloc: 2^20 doubles (8 MiB) on every GPU that loads the library. */
 #define DSEM_NOALLOC_SCRATCH_DOUBLES (1 << 20)
