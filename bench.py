@@ -9,6 +9,7 @@ the whole mesh.  Metric: DOF-RK-stages/s = unknowns x 5 x steps / seconds.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
     python bench.py --workload ensemble [--steps K] [--warmup W]
+    python bench.py --workload adjoint [--fd-check]
 
 value : device-resident throughput, CUDA events on the library's stream
         around exactly K steps (CUDA graph per step), max over ranks.
@@ -22,6 +23,13 @@ case, no data-path collective; value sums the ranks' unknowns.
 through the reference pressure, Taylor-Green or isotropic initial condition),
 advanced together by one ensemble context (dsem_create_batch) against the same
 64 cases run one after another through single-case contexts.
+
+--workload adjoint: 12^3 elements at p = 6 (2,963,520 unknowns), Taylor-Green
+with a seeded 5 % isotropic velocity perturbation (it removes the symmetries
+at which the Roe flux's branches meet), Re = 1600, 400 steps; J = sum of eps * dt over the last 100 steps and its
+exact discrete gradient with respect to the initial state and 1/Re
+(dsem_adjoint), with every stage state kept in HBM and with 20 binomial
+snapshots, timed against the 400 forward steps alone (dsem_step).
 """
 import argparse
 import json
@@ -51,7 +59,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nex", type=int, default=NEX)
     ap.add_argument("--p", type=int, default=P)
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "ensemble"])
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "ensemble", "adjoint"])
+    ap.add_argument("--fd-check", action="store_true")
     ap.add_argument("--cases", type=int, default=64)
     ap.add_argument("--seed", type=int, default=2024)
     return ap.parse_args()
@@ -312,6 +321,68 @@ def run_ensemble(args):
     print(json.dumps(out), flush=True)
 
 
+def run_adjoint(args):
+    import torch
+    from dsem_b200 import mesh
+    from dsem_b200.solver import Solver
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    nex, p, nsteps, window = 12, 6, 400, 100
+    box = mesh.Box(nex, nex, nex, p)
+    q = mesh.perturbed_taylor_green(box, seed=args.seed)
+    dt = CFL * mesh.dtcalc(box, q)
+    s = Solver(box.desc(), re=RE)
+    s.upload(q)
+    s.step(dt, 3)  # warm-up (graph capture), then back to the initial state
+    s.upload(q)
+    s.step(dt, nsteps)
+    fwd_ms, _ = s.last_timing()
+    s.upload(q)
+    out = {"metric": "adjoint / forward time, 400 steps", "unit": "ratio", "n_gpus": 1, "higher_is_better": False,
+           "dtype": "f64", "data": "synthetic (Taylor-Green + seeded 5% isotropic perturbation)",
+           "config": {"workload": f"perturbed taylor-green {nex}^3 hex p={p}, Re=1600, {nsteps} steps, J = sum eps dt "
+                                  f"over the last {window}", "unknowns": 5 * box.nel * (p + 1) ** 3},
+           "forward_ms": fwd_ms}
+    res = {}
+    for snaps in (0, 20):
+        J, g, lr, ms = s.adjoint(dt, nsteps, window, snapshots=snaps)
+        res[snaps] = (J, g, lr, ms)
+        out[f"adjoint_ms_snapshots_{snaps}"] = ms
+        out[f"ratio_snapshots_{snaps}"] = ms / fwd_ms
+    out["value"] = out["ratio_snapshots_0"]
+    J, g, lr, _ = res[0]
+    out["J"] = J
+    out["dJ_dinvRe"] = lr
+    out["gradients_identical_across_checkpointing"] = bool(np.array_equal(res[0][1], res[20][1]))
+    if args.fd_check:  # central differences on the GPU along 8 seeded directions
+        rng = np.random.default_rng(2024)
+        G = p + 1
+        rel = []
+        for _ in range(8):
+            d = rng.standard_normal(q.shape)
+            d[:, :, G:] = 0.0
+            d[:, :, :, G:] = 0.0
+            d[:, :, :, :, G:] = 0.0
+            h = 1e-6
+            Jpm = []
+            for sgn in (1.0, -1.0):
+                s.upload(q + sgn * h * d)
+                Jpm.append(s.adjoint(dt, nsteps, window, want_grad=False)[0])
+            fd = (Jpm[0] - Jpm[1]) / (2 * h)
+            rel.append(abs(float(np.sum(g * d)) - fd) / abs(fd))
+        r0 = 1.0 / RE
+        hr = 1e-4 * r0
+        Jr = []
+        for rr in (r0 + hr, r0 - hr):
+            sr = Solver(box.desc(), re=1.0 / rr)
+            sr.upload(q)
+            Jr.append(sr.adjoint(dt, nsteps, window, want_grad=False)[0])
+            sr.close()
+        fdr = (Jr[0] - Jr[1]) / (2 * hr)
+        out["fd_check"] = {"directions": 8, "max_rel_err_q0": max(rel), "rel_err_inv_re": abs(lr - fdr) / abs(fdr)}
+    s.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -320,6 +391,10 @@ def main():
     if args.workload == "ensemble":
         if int(os.environ.get("RANK", "0")) == 0:
             run_ensemble(args)
+        return
+    if args.workload == "adjoint":
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_adjoint(args)
         return
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -1,0 +1,341 @@
+// dsem_adjoint.cu -- dsem_adjoint: discrete adjoint of nsteps Runge-Kutta
+// steps for J = sum over the last `window` steps of eps_n * dt, eps_n being the
+// enstrophy dissipation dsem_diag reports after step n.  No DSEM counterpart.
+//
+// Forward sweep: the steps as dsem_step runs them; stage states are kept in
+// HBM (every stage of every step when snapshots == 0, else binomial
+// checkpoints of step states with the steps recomputed in the reverse sweep).
+// Reverse sweep, step n = N..1, stage k = kord..1 (2N-storage RK,
+// tstep.f90:66-114):  lg += crk_k dt lQ;  lQ += R'(Q_{k-1})^T lg;  lg *= ark_k,
+// with the enstrophy terms of eps_n added at stage kord of each window step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "../../include/dsem_gpu.h"
+#include "dsem_adjoint.cuh"
+#include "dsem_ctx.h"
+#include "dsem_host_math.h"
+
+using namespace dsem;
+
+namespace {
+
+#define CKA(call)                                                                                    \
+  do {                                                                                               \
+    cudaError_t e_ = (call);                                                                         \
+    if (e_ != cudaSuccess) return dsem_int::fail(c, DSEM_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+int upload_ops_here(dsem_ctx *c) {  // this translation unit's copy of the operator table
+  std::vector<double> table(OPS_TOTAL, 0.0);
+  for (int G = GMIN; G <= GMAX; ++G) hostmath::operators(G, &table[ops_off(G)], &table[ops_off(G) + G * (G + 1)]);
+  CKA(cudaMemcpyToSymbol(c_ops, table.data(), sizeof(double) * OPS_TOTAL));
+  return DSEM_OK;
+}
+
+struct AdjBuf {
+  double *lq = nullptr, *lg = nullptr, *ljq = nullptr, *ldir = nullptr;
+  double *qfr = nullptr, *lff = nullptr, *lvf = nullptr, *lqf = nullptr, *lqr = nullptr;
+  double *lrp = nullptr, *lr = nullptr;
+  double *q0 = nullptr;
+  std::vector<double *> slots;  // checkpoint slots (step states)
+  double *stages = nullptr;     // stage states: all steps (snapshots == 0) or one step
+  ~AdjBuf() {
+    for (double *p : {lq, lg, ljq, ldir, qfr, lff, lvf, lqf, lqr, lrp, lr, q0, stages}) cudaFree(p);
+    for (double *p : slots) cudaFree(p);
+  }
+};
+
+struct Adj {
+  dsem_ctx *c;
+  const Group *g;
+  const MList *ml;
+  AdjBuf b;
+  double dt = 0.0, s2 = 0.0;
+  int nsteps = 0, window = 0;
+  long long launches = 0;
+  bool in_window(int n) const { return n >= nsteps - window; }  // step n (0-based) ends inside the window
+  double eps_w() const { return dt * 100.0 * c->P.r_re / s2; }
+};
+
+template <int G> int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, bool direct_only) {
+  dsem_ctx *c = A.c;
+  const Group &g = *A.g;
+  const MList &ml = *A.ml;
+  if constexpr (G > 7) {
+    (void)Qs; (void)JQe; (void)eps_w; (void)direct_only; (void)g; (void)ml;
+    return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
+  } else {
+    constexpr int G2 = G * G;
+    // forward prerequisites: raw traces, Roe flux, averaged traces
+    TraceArgs ta{};
+    ta.JQ = Qs;
+    ta.sq = 5LL * G * G * G;
+    ta.jac = g.jac;
+    ta.QF = c->QF;
+    CKA(Launch<G>::trace(ta, g.nel, c->st));
+    CKA(cudaMemcpyAsync(A.b.qfr, c->QF, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    CKA(Launch<G>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st));
+    A.launches += 2;
+    using C = VolAdjCfg<G>;
+    static bool attr = false;
+    if (!attr) {
+      CKA(cudaFuncSetAttribute(k_vol_adj<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
+      attr = true;
+    }
+    VolAdjArgs va{};
+    va.JQ = Qs;
+    va.jac = g.jac;
+    va.gg = g.gg;
+    va.gm = g.gm;
+    va.QF = c->QF;
+    va.LQT = A.b.lg;
+    va.LVF = A.b.lvf;
+    va.LJQ = direct_only ? A.b.ldir : A.b.ljq;
+    va.LQF = A.b.lqf;
+    va.lr = A.b.lrp;
+    va.eps_w = eps_w;
+    va.JQe = JQe;
+    va.direct_only = direct_only ? 1 : 0;
+    va.P = c->P;
+    if (direct_only) {
+      k_vol_adj<G><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
+      CKA(cudaGetLastError());
+      ++A.launches;
+      return DSEM_OK;
+    }
+    const unsigned nb = (unsigned)(((long long)ml.n * G2 + 127) / 128);
+    k_upd_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lg, c->P.re, A.b.lff, A.b.lvf);
+    CKA(cudaGetLastError());
+    k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lvf, ml.nrm);
+    CKA(cudaGetLastError());
+    k_vol_adj<G><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
+    CKA(cudaGetLastError());
+    k_face_inv_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.qfr, A.b.lff, A.b.lqf, A.b.lqr, ml.nh, ml.nrm,
+                                             c->P.gamma);
+    CKA(cudaGetLastError());
+    k_trace_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq);
+    CKA(cudaGetLastError());
+    k_sum_into<<<1, 256, 0, c->st>>>(A.b.lrp, g.nel, A.b.lr);
+    CKA(cudaGetLastError());
+    A.launches += 6;
+    return DSEM_OK;
+  }
+}
+
+int stage_adjoint(Adj &A, const double *Qs, const double *JQe, double eps_w, bool direct_only) {
+  int r = DSEM_OK;
+  cudaError_t e = with_G(A.g->G, [&](auto gc) -> cudaError_t {
+    r = stage_adjoint_G<decltype(gc)::value>(A, Qs, JQe, eps_w, direct_only);
+    return cudaSuccess;
+  });
+  if (e != cudaSuccess) return dsem_int::fail(A.c, DSEM_ERR_UNSUPPORTED, "adjoint: element order not supported");
+  return r;
+}
+
+unsigned ew_blocks(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16); }
+
+// Reverse of step n, its stage input states at st[0..kord) and its end state at qend.
+int reverse_step(Adj &A, int n, double *const *st, const double *qend) {
+  dsem_ctx *c = A.c;
+  const long long nq = (long long)c->nq;
+  const bool win = A.in_window(n);
+  if (win) {  // d eps_n / d JQ_n through the JQ values of the enstrophy sum
+    int r = stage_adjoint(A, st[c->kord - 1], qend, A.eps_w(), true);
+    if (r) return r;
+    k_rk_adj_post<<<ew_blocks(nq), 256, 0, c->st>>>(nq, A.b.lq, A.b.ldir, A.b.lg, 1.0);
+    CKA(cudaGetLastError());
+    ++A.launches;
+  }
+  for (int kk = c->kord; kk >= 1; --kk) {
+    k_rk_adj_pre<<<ew_blocks(nq), 256, 0, c->st>>>(nq, A.b.lg, A.b.lq, c->crk[kk - 1] * A.dt);
+    CKA(cudaGetLastError());
+    const bool eps_here = win && kk == c->kord;
+    int r = stage_adjoint(A, st[kk - 1], qend, eps_here ? A.eps_w() : 0.0, false);
+    if (r) return r;
+    k_rk_adj_post<<<ew_blocks(nq), 256, 0, c->st>>>(nq, A.b.lq, A.b.ljq, A.b.lg, c->ark[kk - 1]);
+    CKA(cudaGetLastError());
+    A.launches += 2;
+  }
+  return DSEM_OK;
+}
+
+// One forward step from c->JQ; stage input states copied to st[0..kord) when st != nullptr.
+int forward_step(Adj &A, int n, double *const *st, std::vector<double> *s_win) {
+  dsem_ctx *c = A.c;
+  const bool win = A.in_window(n);
+  for (int kk = 1; kk <= c->kord; ++kk) {
+    if (st) CKA(cudaMemcpyAsync(st[kk - 1], c->JQ, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    int r = dsem_int::stage(c, kk, win && kk == c->kord);
+    if (r) return r;
+    A.launches += 2 * (long long)c->groups.size() + 2 * (long long)c->mlists.size();
+  }
+  if (win && s_win) {
+    double s = 0.0, s2 = 0.0;
+    int r = dsem_int::eps_sums(c, &s, &s2);
+    if (r) return r;
+    s_win->push_back(s);
+    A.s2 = s2;
+  }
+  return DSEM_OK;
+}
+
+int load_state(Adj &A, const double *src) {
+  dsem_ctx *c = A.c;
+  CKA(cudaMemcpyAsync(c->JQ, src, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  return dsem_int::traces(c);
+}
+
+// binomial checkpoint count beta(s, t) = C(s + t, s), saturated
+long long beta(int s, int t) {
+  long double v = 1.0L;
+  for (int i = 1; i <= s; ++i) {
+    v = v * (t + i) / i;
+    if (v > 4e18L) return (long long)4e18;
+  }
+  return (long long)(v + 0.5L);
+}
+
+// Reverse steps [i, j) whose start state is in slot si; slots [sfree, end) are free.
+int revolve(Adj &A, int i, int j, int si, int sfree) {
+  dsem_ctx *c = A.c;
+  const int nfree = (int)A.b.slots.size() - sfree;
+  std::vector<double *> st(c->kord);
+  for (int k = 0; k < c->kord; ++k) st[k] = A.b.stages + (size_t)k * c->nq;
+  if (j - i == 1) {
+    int r = load_state(A, A.b.slots[si]);
+    if (r) return r;
+    if ((r = forward_step(A, i, st.data(), nullptr))) return r;
+    return reverse_step(A, i, st.data(), c->JQ);
+  }
+  if (nfree == 0) {  // no free slot: re-advance from slot si for every step
+    for (int m = j - 1; m >= i; --m) {
+      int r = load_state(A, A.b.slots[si]);
+      if (r) return r;
+      for (int n = i; n < m; ++n)
+        if ((r = forward_step(A, n, nullptr, nullptr))) return r;
+      if ((r = forward_step(A, m, st.data(), nullptr))) return r;
+      if ((r = reverse_step(A, m, st.data(), c->JQ))) return r;
+    }
+    return DSEM_OK;
+  }
+  const long long l = j - i;
+  int t = 1;
+  while (beta(nfree, t) < l) ++t;
+  const long long left = std::max<long long>(1, std::min<long long>(l - 1, beta(nfree, t - 1)));
+  const int m = i + (int)left;
+  int r = load_state(A, A.b.slots[si]);
+  if (r) return r;
+  for (int n = i; n < m; ++n)
+    if ((r = forward_step(A, n, nullptr, nullptr))) return r;
+  CKA(cudaMemcpyAsync(A.b.slots[sfree], c->JQ, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  if ((r = revolve(A, m, j, sfree, sfree + 1))) return r;
+  return revolve(A, i, m, si, sfree);
+}
+
+}  // namespace
+
+extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int snapshots, double *J, double *dJdQ0,
+                            int ldx, double *dJdinvRe, double *ms) {
+  if (!c) return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (nsteps < 1 || window < 0 || window > nsteps || snapshots < 0 || !(dt > 0.0))
+    return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "adjoint: need nsteps >= 1, 0 <= window <= nsteps, snapshots >= 0, dt > 0");
+  if (c->ncase != 1 || c->groups.size() != 1 || c->mlists.size() != 1 || c->nnc > 0 || !c->groups[0].diag || c->shock)
+    return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED,
+                          "adjoint: one case, one element order, conforming mortars, axis-aligned elements, no entropy viscosity");
+  if (c->groups[0].G > 7) return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
+  if (dJdQ0 && ldx < c->groups[0].G) return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "ldx smaller than the number of Gauss points");
+  int r = upload_ops_here(c);
+  if (r) return r;
+  Adj A;
+  A.c = c;
+  A.g = &c->groups[0];
+  A.ml = &c->mlists[0];
+  A.dt = dt;
+  A.nsteps = nsteps;
+  A.window = window;
+  const size_t nq = c->nq, nf = c->nface, bq = nq * sizeof(double), bf = nf * sizeof(double);
+  const int kord = c->kord;
+  for (double **p : {&A.b.lq, &A.b.lg, &A.b.ljq, &A.b.ldir, &A.b.q0}) CKA(cudaMalloc(p, bq));
+  for (double **p : {&A.b.qfr, &A.b.lff, &A.b.lvf, &A.b.lqf, &A.b.lqr}) CKA(cudaMalloc(p, bf));
+  CKA(cudaMalloc(&A.b.lrp, (size_t)A.g->nel * sizeof(double)));
+  CKA(cudaMalloc(&A.b.lr, sizeof(double)));
+  const size_t nstage = snapshots == 0 ? (size_t)nsteps * kord : (size_t)kord;
+  if (cudaMalloc(&A.b.stages, nstage * bq) != cudaSuccess) {
+    cudaGetLastError();
+    return dsem_int::fail(c, DSEM_ERR_NOMEM, "adjoint: not enough device memory for the stage states (use snapshots > 0)");
+  }
+  for (int s = 0; s < snapshots; ++s) {
+    double *p = nullptr;
+    if (cudaMalloc(&p, bq) != cudaSuccess) {
+      cudaGetLastError();
+      return dsem_int::fail(c, DSEM_ERR_NOMEM, "adjoint: not enough device memory for the snapshots");
+    }
+    A.b.slots.push_back(p);
+  }
+  std::vector<double> tmp(1, dt);
+  if ((r = dsem_int::set_dt(c, tmp.data()))) return r;
+  cudaEvent_t e0, e1;
+  CKA(cudaEventCreate(&e0));
+  CKA(cudaEventCreate(&e1));
+  CKA(cudaEventRecord(e0, c->st));
+  CKA(cudaMemcpyAsync(A.b.q0, c->JQ, bq, cudaMemcpyDeviceToDevice, c->st));
+  CKA(cudaMemsetAsync(c->flag, 0, sizeof(int), c->st));
+  if ((r = dsem_int::traces(c))) return r;
+  // ---- forward sweep
+  std::vector<double> s_win;
+  for (int n = 0; n < nsteps; ++n) {
+    std::vector<double *> st;
+    if (snapshots == 0)
+      for (int k = 0; k < kord; ++k) st.push_back(A.b.stages + ((size_t)n * kord + k) * nq);
+    if ((r = forward_step(A, n, snapshots == 0 ? st.data() : nullptr, &s_win))) return r;
+  }
+  if ((r = dsem_int::check_flag(c))) return r;
+  double Jv = 0.0, lr_explicit = 0.0;
+  for (double s : s_win) {
+    Jv += dt * (A.s2 > 0 ? 100.0 * (s / A.s2) * (1.0 / c->P.re) : 0.0);
+    lr_explicit += dt * (A.s2 > 0 ? 100.0 * (s / A.s2) : 0.0);
+  }
+  // ---- reverse sweep
+  CKA(cudaMemsetAsync(A.b.lq, 0, bq, c->st));
+  CKA(cudaMemsetAsync(A.b.lg, 0, bq, c->st));
+  CKA(cudaMemsetAsync(A.b.lr, 0, sizeof(double), c->st));
+  if (window > 0) {
+    if (snapshots == 0) {
+      for (int n = nsteps - 1; n >= 0; --n) {
+        std::vector<double *> st;
+        for (int k = 0; k < kord; ++k) st.push_back(A.b.stages + ((size_t)n * kord + k) * nq);
+        const double *qend = n + 1 < nsteps ? A.b.stages + ((size_t)(n + 1) * kord) * nq : c->JQ;
+        if ((r = reverse_step(A, n, st.data(), qend))) return r;
+      }
+    } else {
+      CKA(cudaMemcpyAsync(A.b.slots[0], A.b.q0, bq, cudaMemcpyDeviceToDevice, c->st));
+      if ((r = revolve(A, 0, nsteps, 0, 1))) return r;
+    }
+  }
+  CKA(cudaEventRecord(e1, c->st));
+  CKA(cudaEventSynchronize(e1));
+  float t = 0.f;
+  CKA(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  double lr_dev = 0.0;
+  CKA(cudaMemcpy(&lr_dev, A.b.lr, sizeof(double), cudaMemcpyDeviceToHost));
+  if (J) *J = Jv;
+  if (dJdinvRe) *dJdinvRe = lr_dev + lr_explicit;
+  if (ms) *ms = t;
+  if (dJdQ0 && (r = dsem_int::unpack_state(c, A.b.lq, dJdQ0, ldx))) return r;
+  // restore the initial state
+  CKA(cudaMemcpyAsync(c->JQ, A.b.q0, bq, cudaMemcpyDeviceToDevice, c->st));
+  if ((r = dsem_int::traces(c))) return r;
+  c->grad_valid = false;
+  c->ev_grad_valid = false;
+  c->last_ms = t;
+  c->last_launches = A.launches;
+  CKA(cudaStreamSynchronize(c->st));
+  return DSEM_OK;
+}

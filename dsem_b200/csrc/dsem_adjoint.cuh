@@ -1,0 +1,705 @@
+// dsem_adjoint.cuh -- discrete adjoint of one right-hand side evaluation.
+//
+// Forward (one stage, dsem_stage.cuh / dsem_vol_diag.cuh):
+//   q = JQ jacob -> face traces QFR -> mortars: Roe flux FF, averaged state QF
+//   -> volume: Lobatto arrays, Gauss gradients, fluxes, interior divergence QTI,
+//      viscous face flux VF -> BR1 average of VF -> Qt = -(QTI + face terms(FF - VF/Re)).
+// Reverse, given lambda = dJ/dQt (LQT):
+//   k_upd_adj       face terms           -> dJ/dFF (LFF), dJ/dVF after averaging (LVF)
+//   k_face_vis_adj  BR1 average          -> dJ/dVF before averaging (LVF, in place)
+//   k_vol_adj       volume (recomputed)  -> dJ/dJQ (LJQ), dJ/dQF averaged (LQF), dJ/d(1/Re)
+//   k_face_inv_adj  Roe flux + average   -> dJ/dQFR (LQR)
+//   k_trace_adj     face traces          -> LJQ += jacob * trace^T LQR
+// The volume adjoint can also add the derivative of the enstrophy-dissipation
+// sum (energydissipation.f90:19-78) evaluated on the same gradients.
+// Derivatives are exact up to rounding; the Roe flux is differentiated in
+// forward mode (one tangent per input), the other pointwise functions by
+// hand-written reverse mode.  Diagonal metrics, conforming mortars, no
+// entropy viscosity.
+#pragma once
+#include "dsem_stage.cuh"
+
+namespace dsem {
+
+// ------------------------------------------------------------ dual numbers
+struct Dual {
+  double v, d;
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b) {
+  const double q = a.v / b.v;
+  return {q, (a.d - q * b.d) / b.v};
+}
+__device__ __forceinline__ Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
+__device__ __forceinline__ Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
+__device__ __forceinline__ Dual operator-(double a, Dual b) { return {a - b.v, -b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a) { return {-a.v, -a.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, double b) { return {a.v * b, a.d * b}; }
+__device__ __forceinline__ Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, double b) { return {a.v / b, a.d / b}; }
+__device__ __forceinline__ Dual operator/(double a, Dual b) {
+  const double q = a / b.v;
+  return {q, -q * b.d / b.v};
+}
+__device__ __forceinline__ Dual dsqrt(Dual a) {
+  const double s = sqrt(a.v);
+  return {s, a.d / (2.0 * s)};
+}
+__device__ __forceinline__ Dual dfabs(Dual a) { return a.v < 0.0 ? -a : a; }
+
+// The Roe flux of riemann() (PhysLib.f90:231-320) on dual numbers; branches
+// follow the values, as complex-step derivatives of the oracle do.
+__device__ __forceinline__ void riemann_dual(const double *nh, double ds, const Dual *Ql, const Dual *Qr, double gamma,
+                                             Dual *flux) {
+  const Dual rho = Ql[0], rhou = Ql[1], rhov = Ql[2], rhow = Ql[3], rhoe = Ql[4];
+  const Dual rhon = Qr[0], rhoun = Qr[1], rhovn = Qr[2], rhown = Qr[3], rhoen = Qr[4];
+  const Dual ul = rhou / rho, vl = rhov / rho, wl = rhow / rho;
+  const Dual pleft = (gamma - 1.0) * (rhoe - 0.5 / rho * (rhou * rhou + rhov * rhov + rhow * rhow));
+  const Dual ur = rhoun / rhon, vr = rhovn / rhon, wr = rhown / rhon;
+  const Dual pright = (gamma - 1.0) * (rhoen - 0.5 / rhon * (rhoun * rhoun + rhovn * rhovn + rhown * rhown));
+  const Dual ql = nh[0] * ul + nh[1] * vl + nh[2] * wl;
+  const Dual qr = nh[0] * ur + nh[1] * vr + nh[2] * wr;
+  const Dual hl = 0.5 * (ul * ul + vl * vl + wl * wl) + gamma / (gamma - 1.0) * pleft / rho;
+  const Dual hr = 0.5 * (ur * ur + vr * vr + wr * wr) + gamma / (gamma - 1.0) * pright / rhon;
+  const Dual rtd = dsqrt(rho * rhon);
+  const Dual betal = rho / (rho + rtd);
+  const Dual betar = 1.0 - betal;
+  const Dual utd = betal * ul + betar * ur;
+  const Dual vtd = betal * vl + betar * vr;
+  const Dual wtd = betal * wl + betar * wr;
+  const Dual htd = betal * hl + betar * hr;
+  const Dual atd2 = (gamma - 1.0) * (htd - 0.5 * (utd * utd + vtd * vtd + wtd * wtd));
+  const Dual atd = dsqrt(atd2);
+  const Dual qtd = utd * nh[0] + vtd * nh[1] + wtd * nh[2];
+  if (qtd.v >= 0.0) {
+    const Dual dw1 = 0.5 * ((pright - pleft) / atd2 - (qr - ql) * rtd / atd);
+    const Dual sp1 = qtd - atd;
+    const Dual sp1m = sp1.v <= 0.0 ? sp1 : Dual{0.0, 0.0};
+    const Dual hd1m = ((gamma + 1.0) / 4.0 * atd / rtd) * dw1;
+    const Dual e1 = -dfabs(sp1) - hd1m;
+    const Dual eta1 = e1.v >= 0.0 ? e1 : Dual{0.0, 0.0};
+    const Dual udw1 = dw1 * (sp1m - 0.5 * eta1);
+    const Dual rql = rho * ql;
+    flux[0] = ds * (rql + udw1);
+    flux[1] = ds * (rql * ul + pleft * nh[0] + udw1 * (utd - atd * nh[0]));
+    flux[2] = ds * (rql * vl + pleft * nh[1] + udw1 * (vtd - atd * nh[1]));
+    flux[3] = ds * (rql * wl + pleft * nh[2] + udw1 * (wtd - atd * nh[2]));
+    flux[4] = ds * (rql * hl + udw1 * (htd - qtd * atd));
+  } else {
+    const Dual dw4 = 0.5 * ((pright - pleft) / atd2 + (qr - ql) * rtd / atd);
+    const Dual sp4 = qtd + atd;
+    const Dual sp4p = sp4.v >= 0.0 ? sp4 : Dual{0.0, 0.0};
+    const Dual hd4 = ((gamma + 1.0) / 4.0 * atd / rtd) * dw4;
+    const Dual e4 = -dfabs(sp4) + hd4;
+    const Dual eta4 = e4.v >= 0.0 ? e4 : Dual{0.0, 0.0};
+    const Dual udw4 = dw4 * (sp4p + 0.5 * eta4);
+    const Dual rqr = rhon * qr;
+    flux[0] = ds * (rqr - udw4);
+    flux[1] = ds * (rqr * ur + pright * nh[0] - udw4 * (utd + atd * nh[0]));
+    flux[2] = ds * (rqr * vr + pright * nh[1] - udw4 * (vtd + atd * nh[1]));
+    flux[3] = ds * (rqr * wr + pright * nh[2] - udw4 * (wtd + atd * nh[2]));
+    flux[4] = ds * (rqr * hr - udw4 * (htd + qtd * atd));
+  }
+}
+
+// lQl += (dF/dQl)^T lf, lQr += (dF/dQr)^T lf: one forward-mode pass per input.
+__device__ __forceinline__ void roe_vjp(const double *nh, double ds, const double *Ql, const double *Qr, double gamma,
+                                        const double *lf, double *lQl, double *lQr) {
+#pragma unroll 1
+  for (int j = 0; j < 10; ++j) {
+    Dual L[NV], R[NV], F[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      L[v] = {Ql[v], j == v ? 1.0 : 0.0};
+      R[v] = {Qr[v], j == NV + v ? 1.0 : 0.0};
+    }
+    riemann_dual(nh, ds, L, R, gamma, F);
+    double s = 0.0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s += lf[v] * F[v].d;
+    if (j < NV)
+      lQl[j] += s;
+    else
+      lQr[j - NV] += s;
+  }
+}
+
+// ---------------------------------------------- hand-written reverse modes
+// Euler flux along D (PhysLib.f90:17-124): lQ += (dF/dQ)^T lf.
+template <int D> __device__ __forceinline__ void euler_vjp(const double *Q, double g, const double *lf, double *lQ) {
+  const double rho = Q[0], ri = 1.0 / rho;
+  const double vel[3] = {Q[1] * ri, Q[2] * ri, Q[3] * ri};
+  const double S = vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2];
+  const double p = (g - 1.0) * (Q[4] - 0.5 * rho * S);
+  double lvel[3] = {0.0, 0.0, 0.0}, lp = 0.0, lrho = 0.0;
+  lQ[1 + D] += lf[0];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {  // f_{1+i} = Q[1+D] vel_i + delta_{iD} p
+    lQ[1 + D] += vel[i] * lf[1 + i];
+    lvel[i] += Q[1 + D] * lf[1 + i];
+  }
+  lp += lf[1 + D];
+  lvel[D] += (Q[4] + p) * lf[4];  // f_4 = vel_D (rho e + p)
+  lQ[4] += vel[D] * lf[4];
+  lp += vel[D] * lf[4];
+  lQ[4] += (g - 1.0) * lp;
+  lrho += -(g - 1.0) * 0.5 * S * lp;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) lvel[i] += -(g - 1.0) * rho * vel[i] * lp;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    lQ[1 + i] += lvel[i] * ri;
+    lrho += -vel[i] * ri * lvel[i];
+  }
+  lQ[0] += lrho;
+}
+
+// Viscous flux along D (PhysLib.f90:419-583) with Gr[j][f] = d Q_f / d x_j:
+// fv = the flux, lQ += (dF/dQ)^T lf, lG += (dF/dGr)^T lf (amu held fixed).
+template <int D>
+__device__ __forceinline__ void vis_vjp(const double *Q, const double (&Gr)[3][NV], double amu, const Phys &P,
+                                        const double *lf, double *fv, double *lQ, double (&lG)[3][NV]) {
+  const double g = P.gamma, rho = Q[0], ri = 1.0 / rho;
+  const double vel[3] = {Q[1] * ri, Q[2] * ri, Q[3] * ri};
+  const double S = vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2];
+  const double p = (g - 1.0) * (Q[4] - 0.5 * rho * S);
+  double Gv[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) Gv[i][j] = (Gr[j][1 + i] - vel[i] * Gr[j][0]) * ri;
+  const double div = Gv[0][0] + Gv[1][1] + Gv[2][2];
+  const double vgD = vel[0] * Gv[0][D] + vel[1] * Gv[1][D] + vel[2] * Gv[2][D];
+  const double pD = (g - 1.0) * (Gr[D][4] - 0.5 * Gr[D][0] * S - rho * vgD);
+  const double K = P.mach * P.mach * g;
+  const double A = pD - p * Gr[D][0] * ri;
+  const double tD = A * K * ri;
+  const double kap = 1.0 + (amu - 1.0) * 0.2 / (g - 1.0);
+  const double den = P.pr * P.mach * P.mach * (g - 1.0);
+  double tau[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) tau[i] = amu * (Gv[i][D] + Gv[D][i]) - (i == D ? 2.0 / 3.0 * amu * div : 0.0);
+  fv[0] = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) fv[1 + i] = tau[i];
+  fv[4] = vel[0] * tau[0] + vel[1] * tau[1] + vel[2] * tau[2] + kap * tD / den;
+  // reverse
+  const double l4 = lf[4];
+  double lvel[3], ltau[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    lvel[i] = tau[i] * l4;
+    ltau[i] = lf[1 + i] + vel[i] * l4;
+  }
+  const double ltD = kap / den * l4;
+  double lGv[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    lGv[i][D] += amu * ltau[i];
+    lGv[D][i] += amu * ltau[i];
+  }
+  const double ldiv = -(2.0 / 3.0) * amu * ltau[D];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) lGv[i][i] += ldiv;
+  double lrho = 0.0, lp = 0.0, lS = 0.0;
+  const double lA = K * ri * ltD;  // tD = A K / rho
+  lrho += -tD * ri * ltD;
+  const double lpD = lA;  // A = pD - p Gr[D][0] / rho
+  lp += -Gr[D][0] * ri * lA;
+  lG[D][0] += -p * ri * lA;
+  lrho += p * Gr[D][0] * ri * ri * lA;
+  lG[D][4] += (g - 1.0) * lpD;  // pD
+  lG[D][0] += -(g - 1.0) * 0.5 * S * lpD;
+  lS += -(g - 1.0) * 0.5 * Gr[D][0] * lpD;
+  lrho += -(g - 1.0) * vgD * lpD;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    lvel[i] += -(g - 1.0) * rho * Gv[i][D] * lpD;
+    lGv[i][D] += -(g - 1.0) * rho * vel[i] * lpD;
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)  // Gv[i][j] = (Gr[j][1+i] - vel_i Gr[j][0]) / rho
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const double l = lGv[i][j];
+      lG[j][1 + i] += l * ri;
+      lvel[i] += -Gr[j][0] * ri * l;
+      lG[j][0] += -vel[i] * ri * l;
+      lrho += -Gv[i][j] * ri * l;
+    }
+  lQ[4] += (g - 1.0) * lp;  // p
+  lrho += -(g - 1.0) * 0.5 * S * lp;
+  lS += -(g - 1.0) * 0.5 * rho * lp;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) lvel[i] += 2.0 * vel[i] * lS;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    lQ[1 + i] += lvel[i] * ri;
+    lrho += -vel[i] * ri * lvel[i];
+  }
+  lQ[0] += lrho;
+}
+
+// Enstrophy term of one Gauss point (energydissipation.f90:19-78, as k_diag):
+// vort(JQ[0..3], gradients) ; lQ[0..3] += w dvort/dJQ, lgr[f*3+j] += w dvort/dgr.
+__device__ __forceinline__ void vort_vjp(const double *Qj, double jc, const double *gr, double w, double *lQ,
+                                         double *lgr) {
+  const double Q1 = Qj[0];
+  struct T3 {
+    int a, b, g0;  // gradient field of the numerator, variable index, gradient field of rho
+  };
+  // udery, uderz, vderx, vderz, wderx, wdery
+  const T3 t[6] = {{4, 1, 1}, {5, 1, 2}, {6, 2, 0}, {8, 2, 2}, {9, 3, 0}, {10, 3, 1}};
+  double d[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) d[k] = (gr[t[k].a] - (Qj[t[k].b] / Q1) * gr[t[k].g0]) / Q1;
+  const double c1 = (d[5] - d[3]) / jc, c2 = (d[1] - d[4]) / jc, c3 = (d[2] - d[0]) / jc;
+  const double kk = 2.0 * w / jc;
+  const double l1 = kk * c1 / jc, l2 = kk * c2 / jc, l3 = kk * c3 / jc;
+  const double ld[6] = {-l3, l2, l3, -l1, -l2, l1};
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const double Qb = Qj[t[k].b], G0 = gr[t[k].g0];
+    lgr[t[k].a] += ld[k] / Q1;
+    lgr[t[k].g0] += -Qb / (Q1 * Q1) * ld[k];
+    lQ[t[k].b] += -G0 / (Q1 * Q1) * ld[k];
+    lQ[0] += (Qb * G0 / (Q1 * Q1 * Q1) - d[k] / Q1) * ld[k];
+  }
+}
+
+// ---------------------------------------------------------------- kernels
+// Face terms of the divergence and the RK residual sign (k_update):
+// Qt = -(QTI + sum_faces D_edge FB), FB = FF - VF/Re.
+template <int G>
+__global__ void __launch_bounds__(256) k_upd_adj(const double *__restrict__ LQT, double re, double *__restrict__ LFF,
+                                                  double *__restrict__ LVF) {
+  constexpr int L = G + 1, G2 = G * G, NG = G * G * G;
+  const int k = blockIdx.x;
+  const double *lam = LQT + (long long)k * 5 * NG;
+  for (int t = threadIdx.x; t < 30 * G2; t += blockDim.x) {
+    const int f = t / (5 * G2), r = t - f * 5 * G2, v = r / G2, ln = r - v * G2, i = ln % G, j = ln / G;
+    const bool hi = (f == 1 || f == 3 || f == 4);
+    double acc = 0.0;
+#pragma unroll
+    for (int n = 0; n < G; ++n) {
+      int p;
+      if (f == 3 || f == 5)  // faces 4, 6: lines along x at (m, l) = (i, j)
+        p = n + G * (i + G * j);
+      else if (f == 0 || f == 1)  // faces 1, 2: along y at (n, l)
+        p = i + G * (n + G * j);
+      else  // faces 3, 5: along z at (n, m)
+        p = i + G * (j + G * n);
+      acc += Op<G>::D(n, hi ? L - 1 : 0) * lam[v * NG + p];
+    }
+    const double lfb = -acc;
+    LFF[(long long)k * 30 * G2 + t] = lfb;
+    LVF[(long long)k * 30 * G2 + t] = -lfb / re;
+  }
+}
+
+// BR1 average of the viscous normal flux (k_face_vis), transposed in place.
+template <int G>
+__global__ void __launch_bounds__(128) k_face_vis_adj(const MortarC *__restrict__ mc, int nm, double *__restrict__ LVF,
+                                                       const double *__restrict__ nrm) {
+  constexpr int G2 = G * G;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nm * G2) return;
+  const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
+  const MortarC M = mc[m];
+  int si, sj;
+  slave_index<G>(M.flags & 7, pt % G, pt / G, si, sj);
+  const int sp = si + G * sj;
+  const long long g0 = (long long)M.geo * G2;
+  const double nm_m = nrm[g0 + pt], nm_s = nrm[g0 + sp];
+  const bool neg_n = (M.flags >> 4) & 1, neg_s = (M.flags >> 3) & 1;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double lm = LVF[M.ms + v * G2 + pt], ls = LVF[M.ss + v * G2 + sp];
+    const double lqb = lm + (neg_s ? -ls : ls);
+    const double lh = 0.5 * nm_m * lqb;
+    LVF[M.ms + v * G2 + pt] = lh / nm_m;
+    LVF[M.ss + v * G2 + sp] = (neg_n ? -lh : lh) / nm_s;
+  }
+}
+
+// Roe flux and averaged state (k_face_inv), transposed: QFR = raw traces.
+template <int G>
+__global__ void __launch_bounds__(128) k_face_inv_adj(const MortarC *__restrict__ mc, int nm,
+                                                       const double *__restrict__ QFR, const double *__restrict__ LFF,
+                                                       const double *__restrict__ LQF, double *__restrict__ LQR,
+                                                       const double *__restrict__ nh, const double *__restrict__ nrm,
+                                                       double gamma) {
+  constexpr int G2 = G * G;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nm * G2) return;
+  const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
+  const MortarC M = mc[m];
+  int si, sj;
+  slave_index<G>(M.flags & 7, pt % G, pt / G, si, sj);
+  const int sp = si + G * sj;
+  double Q1[NV], Q2[NV], lf[NV], l1[NV], l2[NV];
+  const double sgn = ((M.flags >> 3) & 1) ? -1.0 : 1.0;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    Q1[v] = QFR[M.ms + v * G2 + pt];
+    Q2[v] = QFR[M.ss + v * G2 + sp];
+    lf[v] = LFF[M.ms + v * G2 + pt] + sgn * LFF[M.ss + v * G2 + sp];
+    const double la = 0.5 * (LQF[M.ms + v * G2 + pt] + LQF[M.ss + v * G2 + sp]);
+    l1[v] = la;
+    l2[v] = la;
+  }
+  const long long gp = (long long)M.geo * G2 + pt;
+  const double n3[3] = {nh[gp * 3], nh[gp * 3 + 1], nh[gp * 3 + 2]};
+  const bool low = (M.flags >> 5) & 1;
+  if (low)
+    roe_vjp(n3, nrm[gp], Q2, Q1, gamma, lf, l2, l1);
+  else
+    roe_vjp(n3, nrm[gp], Q1, Q2, gamma, lf, l1, l2);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    LQR[M.ms + v * G2 + pt] = l1[v];
+    LQR[M.ss + v * G2 + sp] = l2[v];
+  }
+}
+
+// Face traces (write_traces), transposed: LJQ += jacob * trace^T LQR.
+template <int G>
+__global__ void __launch_bounds__(256) k_trace_adj(const double *__restrict__ LQR, const double *__restrict__ jac,
+                                                    double *__restrict__ LJQ) {
+  constexpr int L = G + 1, G2 = G * G, NG = G * G * G;
+  const int k = blockIdx.x;
+  const double *F = LQR + (long long)k * 30 * G2;
+  for (int i = threadIdx.x; i < 5 * NG; i += blockDim.x) {
+    const int v = i / NG, p = i - v * NG, n = p % G, m = (p / G) % G, l = p / G2;
+    const double *Fv = F + v * G2;
+    double s = Op<G>::B(0, n) * Fv[5 * 5 * G2 + m + G * l];    // face 6 (x = 0)
+    s += Op<G>::B(L - 1, n) * Fv[3 * 5 * G2 + m + G * l];      // face 4
+    s += Op<G>::B(0, m) * Fv[0 * 5 * G2 + n + G * l];          // face 1 (y = 0)
+    s += Op<G>::B(L - 1, m) * Fv[1 * 5 * G2 + n + G * l];      // face 2
+    s += Op<G>::B(0, l) * Fv[2 * 5 * G2 + n + G * m];          // face 3 (z = 0)
+    s += Op<G>::B(L - 1, l) * Fv[4 * 5 * G2 + n + G * m];      // face 5
+    LJQ[(long long)k * 5 * NG + i] += jac[(long long)k * NG + p] * s;
+  }
+}
+
+struct VolAdjArgs {
+  const double *JQ;
+  const double *jac, *gg, *gm;  // diagonal metric layout
+  const double *QF;             // averaged face state
+  const double *LQT;            // dJ/dQt
+  const double *LVF;            // dJ/dVF before averaging
+  double *LJQ;                  // out: dJ/dJQ (volume part)
+  double *LQF;                  // out: dJ/dQF (averaged face state)
+  double *lr;                   // out: per element dJ/d(1/Re)
+  double eps_w;                 // weight of the enstrophy sum (0: none)
+  const double *JQe;            // state whose JQ values the enstrophy sum uses (end of the step)
+  int direct_only;              // 1: only dJ/dJQe of the enstrophy sum, into LJQ
+  Phys P;
+};
+
+template <int G> struct VolAdjCfg {
+  static constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
+  static constexpr int NT = 256;
+  static constexpr size_t NDBL = 5 * NG + 15 * NG + 15 * NG + 5 * NL + 5 * NL + 11 * NL + 5 * NG + 5 * NG + 30 * G2 +
+                                 2 * G * L + NT;
+  static constexpr size_t SMEM = sizeof(double) * NDBL;
+};
+
+// Volume adjoint of one element (diagonal metrics): recomputes the Lobatto
+// arrays and Gauss gradients, then runs the volume operations in reverse.
+template <int G> __global__ void __launch_bounds__(256, 1) k_vol_adj(VolAdjArgs A) {
+  using C = VolAdjCfg<G>;
+  constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G, NT = C::NT;
+  extern __shared__ double sm[];
+  double *q = sm;               // [5][NG] physical state
+  double *GR = q + 5 * NG;      // [15][NG] Gauss gradients, field f*3 + direction
+  double *LGR = GR + 15 * NG;   // [15][NG] their adjoints
+  double *LB = LGR + 15 * NG;   // [5][NL] Lobatto arrays of the current grid
+  double *LL = LB + 5 * NL;     // [5][NL] their adjoints
+  double *LG = LL + 5 * NL;     // [11][NL] adjoints of the interpolated gradient fields
+  double *LQ = LG + 11 * NL;    // [5][NG] dJ/dq
+  double *LAM = LQ + 5 * NG;    // [5][NG] dJ/dQt
+  double *LQFs = LAM + 5 * NG;  // [30][G2] dJ/dQF
+  double *Bm = LQFs + 30 * G2;  // bx [L][G]
+  double *Dm = Bm + L * G;      // dmx [G][L]
+  double *red = Dm + G * L;     // [NT]
+  const int k = blockIdx.x, tid = threadIdx.x;
+  const double *JQ = A.JQ + (long long)k * 5 * NG;
+  const double *jac = A.jac + (long long)k * NG;
+  const double *gg = A.gg + (long long)k * 3 * NG;
+  const double *gm = A.gm + (long long)k * 3 * NL;
+  const double *QF = A.QF + (long long)k * 30 * G2;
+  const double *LVF = A.LVF + (long long)k * 30 * G2;
+  double *LJQ = A.LJQ + (long long)k * 5 * NG;
+  const Phys P = A.P;
+  const double gamma = P.gamma;
+  double lr = 0.0;
+
+  for (int i = tid; i < L * G; i += NT) {
+    Bm[i] = Op<G>::B(i / G, i % G);
+    Dm[i] = Op<G>::D(i / L, i % L);
+  }
+  for (int i = tid; i < 5 * NG; i += NT) {
+    q[i] = JQ[i] * jac[i % NG];
+    LAM[i] = A.LQT[(long long)k * 5 * NG + i];
+    LQ[i] = 0.0;
+  }
+  for (int i = tid; i < 15 * NG; i += NT) LGR[i] = 0.0;
+  for (int i = tid; i < 30 * G2; i += NT) LQFs[i] = 0.0;
+  __syncthreads();
+
+  // Lobatto arrays of grid D into LB (interior from q, faces from QF)
+  auto build = [&](int D) {
+    const int xs = D == 0 ? 1 : (D == 1 ? G : G2);
+    for (int t = tid; t < 5 * G2; t += NT) {
+      const int v = t / G2, ln = t - v * G2, a = ln % G, b = ln / G;
+      const int p0 = gbase<G>(D, a, b), l0 = lbase<G>(D, a, b);
+      double x[G];
+#pragma unroll
+      for (int kk = 0; kk < G; ++kk) x[kk] = q[v * NG + p0 + kk * xs];
+      LB[v * NL + l0] = QF[(face_lo(D) - 1) * 5 * G2 + v * G2 + ln];
+      LB[v * NL + l0 + (L - 1) * xs] = QF[(face_hi(D) - 1) * 5 * G2 + v * G2 + ln];
+#pragma unroll
+      for (int s = 1; s < L - 1; ++s) {
+        double acc = Op<G>::B(s, 0) * x[0];
+#pragma unroll
+        for (int kk = 1; kk < G; ++kk) acc = __fma_rn(Op<G>::B(s, kk), x[kk], acc);
+        LB[v * NL + l0 + s * xs] = acc;
+      }
+    }
+  };
+
+  // ---- forward: Gauss gradients of the five fields
+  for (int D = 0; D < 3; ++D) {
+    build(D);
+    __syncthreads();
+    const int xs = D == 0 ? 1 : (D == 1 ? G : G2);
+    for (int t = tid; t < 5 * G2; t += NT) {
+      const int f = t / G2, ln = t - f * G2, a = ln % G, b = ln / G;
+      const int p0 = gbase<G>(D, a, b), l0 = lbase<G>(D, a, b);
+      double y[L];
+#pragma unroll
+      for (int s = 0; s < L; ++s) y[s] = LB[f * NL + l0 + s * xs];
+#pragma unroll
+      for (int kk = 0; kk < G; ++kk) {
+        double acc = Op<G>::D(kk, 0) * y[0];
+#pragma unroll
+        for (int s = 1; s < L; ++s) acc = __fma_rn(Op<G>::D(kk, s), y[s], acc);
+        GR[(f * 3 + D) * NG + p0 + kk * xs] = gg[D * NG + p0 + kk * xs] * acc;
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- enstrophy term (energydissipation.f90:19-78) on these gradients and the
+  // JQ values of JQe: the gradient part goes to LGR; with direct_only the JQe
+  // part is the whole output
+  if (A.eps_w != 0.0) {
+    const double *JQe = A.JQe + (long long)k * 5 * NG;
+    for (int p = tid; p < NG; p += NT) {
+      double Qj[4], gr[12], lgr[12], lq4[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int v = 0; v < 4; ++v) Qj[v] = JQe[v * NG + p];
+#pragma unroll
+      for (int f = 0; f < 12; ++f) {
+        gr[f] = GR[f * NG + p];
+        lgr[f] = 0.0;
+      }
+      vort_vjp(Qj, jac[p], gr, A.eps_w, lq4, lgr);
+      if (A.direct_only) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) LJQ[v * NG + p] = lq4[v];
+        LJQ[4 * NG + p] = 0.0;
+      } else {
+#pragma unroll
+        for (int f = 0; f < 12; ++f) LGR[f * NG + p] += lgr[f];
+      }
+    }
+    __syncthreads();
+  }
+  if (A.direct_only) return;
+
+  // ---- reverse of pass 2: fluxes and interior divergence, grid by grid
+  for (int D = 0; D < 3; ++D) {
+    build(D);
+    __syncthreads();
+    const int xs = D == 0 ? 1 : (D == 1 ? G : G2);
+    for (int qi = tid; qi < NL; qi += NT) {
+      int s, a, b;
+      ldecode<G>(D, qi, s, a, b);
+      const int g0 = gbase<G>(D, a, b);
+      double Q[NV], Gr[3][NV], lG[3][NV], lQ[NV], lfv[NV], fv[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        Q[v] = LB[v * NL + qi];
+        lQ[v] = 0.0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          Gr[j][v] = 0.0;
+          lG[j][v] = 0.0;
+        }
+      }
+#pragma unroll
+      for (int jf = 0; jf < 11; ++jf) {
+        const int fi = diag_field(D, jf);
+        double acc = Bm[s * G] * GR[fi * NG + g0];
+#pragma unroll
+        for (int kk = 1; kk < G; ++kk) acc = __fma_rn(Bm[s * G + kk], GR[fi * NG + g0 + kk * xs], acc);
+        Gr[fi % 3][fi / 3] = acc;
+      }
+      const double gd = gm[D * NL + qi];
+      if (s == 0 || s == L - 1) {  // face point: VF = gd * fv
+        const int fc = s == 0 ? face_lo(D) : face_hi(D);
+        double lvf[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          lvf[v] = LVF[(fc - 1) * 5 * G2 + v * G2 + a + G * b];
+          lfv[v] = gd * lvf[v];
+        }
+        if (D == 0) vis_vjp<0>(Q, Gr, 1.0, P, lfv, fv, lQ, lG);
+        else if (D == 1) vis_vjp<1>(Q, Gr, 1.0, P, lfv, fv, lQ, lG);
+        else vis_vjp<2>(Q, Gr, 1.0, P, lfv, fv, lQ, lG);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) lr += P.re * lvf[v] * (gd * fv[v]);
+      } else {  // interior: F = gd fe - gd fv / Re, QTI += Dm F, Qt = -(QTI + ...)
+        double lF[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          double acc = 0.0;
+#pragma unroll
+          for (int kk = 0; kk < G; ++kk) acc += Dm[kk * L + s] * LAM[v * NG + g0 + kk * xs];
+          lF[v] = -acc;
+          lfv[v] = -gd * P.r_re * lF[v];
+        }
+        double lfe[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) lfe[v] = gd * lF[v];
+        if (D == 0) {
+          vis_vjp<0>(Q, Gr, 1.0, P, lfv, fv, lQ, lG);
+          euler_vjp<0>(Q, gamma, lfe, lQ);
+        } else if (D == 1) {
+          vis_vjp<1>(Q, Gr, 1.0, P, lfv, fv, lQ, lG);
+          euler_vjp<1>(Q, gamma, lfe, lQ);
+        } else {
+          vis_vjp<2>(Q, Gr, 1.0, P, lfv, fv, lQ, lG);
+          euler_vjp<2>(Q, gamma, lfe, lQ);
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) lr += -gd * fv[v] * lF[v];
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) LL[v * NL + qi] = lQ[v];
+#pragma unroll
+      for (int jf = 0; jf < 11; ++jf) {
+        const int fi = diag_field(D, jf);
+        LG[jf * NL + qi] = lG[fi % 3][fi / 3];
+      }
+    }
+    __syncthreads();
+    // transposed interpolations along the lines of D
+    for (int t = tid; t < 16 * G2; t += NT) {
+      const int j = t / G2, ln = t - j * G2, a = ln % G, b = ln / G;
+      const int p0 = gbase<G>(D, a, b), l0 = lbase<G>(D, a, b);
+      if (j < 11) {  // gradient field j of grid D -> its Gauss line
+        const int fi = diag_field(D, j);
+        double y[L];
+#pragma unroll
+        for (int s = 0; s < L; ++s) y[s] = LG[j * NL + l0 + s * xs];
+#pragma unroll
+        for (int kk = 0; kk < G; ++kk) {
+          double acc = 0.0;
+#pragma unroll
+          for (int s = 0; s < L; ++s) acc += Op<G>::B(s, kk) * y[s];
+          LGR[fi * NG + p0 + kk * xs] += acc;
+        }
+      } else {  // state field v: interior Lobatto points -> q, end points -> QF
+        const int v = j - 11;
+        double y[L];
+#pragma unroll
+        for (int s = 0; s < L; ++s) y[s] = LL[v * NL + l0 + s * xs];
+#pragma unroll
+        for (int kk = 0; kk < G; ++kk) {
+          double acc = 0.0;
+#pragma unroll
+          for (int s = 1; s < L - 1; ++s) acc += Op<G>::B(s, kk) * y[s];
+          LQ[v * NG + p0 + kk * xs] += acc;
+        }
+        LQFs[(face_lo(D) - 1) * 5 * G2 + v * G2 + ln] += y[0];
+        LQFs[(face_hi(D) - 1) * 5 * G2 + v * G2 + ln] += y[L - 1];
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- reverse of pass 1: gradients -> Lobatto arrays -> q and QF
+  for (int D = 0; D < 3; ++D) {
+    const int xs = D == 0 ? 1 : (D == 1 ? G : G2);
+    for (int t = tid; t < 5 * G2; t += NT) {
+      const int f = t / G2, ln = t - f * G2, a = ln % G, b = ln / G;
+      const int p0 = gbase<G>(D, a, b);
+      double lg[G];
+#pragma unroll
+      for (int kk = 0; kk < G; ++kk) lg[kk] = gg[D * NG + p0 + kk * xs] * LGR[(f * 3 + D) * NG + p0 + kk * xs];
+      double y[L];
+#pragma unroll
+      for (int s = 0; s < L; ++s) {
+        double acc = 0.0;
+#pragma unroll
+        for (int kk = 0; kk < G; ++kk) acc += Op<G>::D(kk, s) * lg[kk];
+        y[s] = acc;
+      }
+#pragma unroll
+      for (int kk = 0; kk < G; ++kk) {
+        double acc = 0.0;
+#pragma unroll
+        for (int s = 1; s < L - 1; ++s) acc += Op<G>::B(s, kk) * y[s];
+        LQ[f * NG + p0 + kk * xs] += acc;
+      }
+      LQFs[(face_lo(D) - 1) * 5 * G2 + f * G2 + ln] += y[0];
+      LQFs[(face_hi(D) - 1) * 5 * G2 + f * G2 + ln] += y[L - 1];
+    }
+    __syncthreads();
+  }
+
+  // ---- outputs
+  for (int i = tid; i < 5 * NG; i += NT) LJQ[i] = jac[i % NG] * LQ[i];
+  for (int i = tid; i < 30 * G2; i += NT) A.LQF[(long long)k * 30 * G2 + i] = LQFs[i];
+  red[tid] = lr;
+  __syncthreads();
+  for (int w = NT / 2; w > 0; w >>= 1) {
+    if (tid < w) red[tid] += red[tid + w];
+    __syncthreads();
+  }
+  if (tid == 0) A.lr[k] = red[0];
+}
+
+// RK bookkeeping of the reverse sweep
+__global__ void k_rk_adj_pre(long long n, double *__restrict__ lg, const double *__restrict__ lq, double cdt) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    lg[i] += cdt * lq[i];
+}
+__global__ void k_rk_adj_post(long long n, double *__restrict__ lq, const double *__restrict__ ljq,
+                              double *__restrict__ lg, double a) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    lq[i] += ljq[i];
+    lg[i] *= a;
+  }
+}
+// out[0] += sum of part[0..n) (one block, fixed order)
+__global__ void k_sum_into(const double *__restrict__ part, int n, double *__restrict__ out) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) s += part[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] += red[0];
+}
+
+}  // namespace dsem

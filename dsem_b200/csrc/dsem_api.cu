@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/dsem_gpu.h"
+#include "dsem_ctx.h"
 #include "dsem_host_math.h"
 #include "dsem_launch.h"
 #include "dsem_stage.cuh"
@@ -22,39 +23,6 @@ using namespace dsem;
 namespace {
 
 thread_local std::string g_create_err;
-
-template <class F> cudaError_t with_G(int G, F &&f) {
-  switch (G) {
-    case 2: return f(std::integral_constant<int, 2>{});
-    case 3: return f(std::integral_constant<int, 3>{});
-    case 4: return f(std::integral_constant<int, 4>{});
-    case 5: return f(std::integral_constant<int, 5>{});
-    case 6: return f(std::integral_constant<int, 6>{});
-    case 7: return f(std::integral_constant<int, 7>{});
-    case 8: return f(std::integral_constant<int, 8>{});
-    case 9: return f(std::integral_constant<int, 9>{});
-    default: return cudaErrorInvalidValue;
-  }
-}
-
-struct Group {
-  int G = 0, nel = 0;
-  bool diag = true;
-  long long e0 = 0;  // first internal element
-  long long q0 = 0;  // offset of the group's state (doubles)
-  long long f0 = 0;  // offset of the group's face slots (doubles)
-  double *jac = nullptr, *gg = nullptr, *gm = nullptr, *hd = nullptr;
-  double *muhg = nullptr, *EVB = nullptr, *kew = nullptr;
-  int *int2ext = nullptr;  // device: caller element id of each group element
-  int *ecase = nullptr;    // device: case of each group element
-  std::vector<int> case_lo, case_hi;  // group elements [lo, hi) of each case
-};
-
-struct MList {  // conforming mortars of one order
-  int G = 0, n = 0;
-  MortarC *mc = nullptr;
-  double *nh = nullptr, *nrm = nullptr;
-};
 
 // ---------------------------------------------------------- layout kernels
 __global__ void k_pack(const double *__restrict__ src, int ldx, const int *__restrict__ ext, int ext0, int G, int nf,
@@ -133,47 +101,6 @@ __global__ void k_diag(const double *__restrict__ JQ, const double *__restrict__
 
 }  // namespace
 
-struct dsem_ctx {
-  int dev = 0;
-  cudaStream_t st = nullptr;
-  int ngrid = 0, nmort = 0;
-  Phys P{};
-  int shock = 0, iord = 4, kord = 5;
-  double ark[5] = {}, brk[5] = {}, crk[5] = {};
-  std::vector<Group> groups;
-  std::vector<MList> mlists;
-  MortarNC *nc = nullptr;  // p-nonconforming mortars
-  int nnc = 0;
-  double *nc_nh = nullptr, *nc_nrm = nullptr, *nc_mats = nullptr;
-  std::vector<int> ext_group, ext_k;  // caller element -> (group, index in group)
-  double *JQ = nullptr, *gQ = nullptr, *QTI = nullptr, *QF = nullptr, *FF = nullptr, *VF = nullptr;
-  double *Qt = nullptr, *stage = nullptr, *part = nullptr;
-  size_t nq = 0, nface = 0, nstage = 0;
-  int stage_ldx = 0;
-  int *flag = nullptr;
-  bool traces_valid = false;
-  bool grad_valid = false;     // EVB holds the Q gradients of the last Fluxes call
-  bool ev_grad_valid = false;  // ... and the temperature gradients (EV)
-  int keep_grad = 0;
-  cudaGraphExec_t gexec = nullptr;
-  int graph_key = -1;
-  long long graph_launches = 0;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  double last_ms = 0.0;
-  long long last_launches = 0;
-  std::string err;
-  std::vector<double> host_part;
-  // ensemble: independent cases sharing the launches (a single case is an ensemble of one)
-  int ncase = 1;
-  std::vector<int> case_el0;         // first caller element of each case (+ total)
-  std::vector<double> case_re, case_dt, case_prestep;
-  double *d_rec = nullptr;           // device: per case {re, 1/re}
-  double *d_dtc = nullptr;           // device: per case dt of the current call
-  // order groups run as parallel branches of the stream (and of the captured graph)
-  std::vector<cudaStream_t> aux;
-  std::vector<cudaEvent_t> ev_join;
-  cudaEvent_t ev_fork = nullptr;
-};
 
 namespace {
 
@@ -1271,3 +1198,42 @@ int dsem_last_timing(const dsem_ctx *c, double *ms, long long *launches) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------- hooks for the adjoint unit
+namespace dsem_int {
+int fail(dsem_ctx *c, int code, const std::string &msg) { return ::fail(c, code, msg); }
+int stage(dsem_ctx *c, int kk, bool save) {
+  long long l = 0;
+  return enqueue_stage(c, kk, save, nullptr, &l);
+}
+int traces(dsem_ctx *c) {
+  long long l = 0;
+  return enqueue_traces(c, &l);
+}
+int set_dt(dsem_ctx *c, const double *dt) { return ::set_dt(c, dt); }
+int unpack_state(dsem_ctx *c, const double *dev, double *host, int ldx) {
+  return unpack_to_host(c, dev, host, ldx, 5, state_offs(c));
+}
+int check_flag(dsem_ctx *c) { return ::check_flag(c); }
+// enstrophy sums of the last stage's gradients, in the caller's element order
+int eps_sums(dsem_ctx *c, double *s, double *s2) {
+  for (auto &g : c->groups) {
+    k_diag<<<(g.nel + 127) / 128, 128, 0, c->st>>>(c->JQ + g.q0, g.jac, g.EVB, g.kew, g.G, g.nel, 1,
+                                                    c->part + g.e0 * 5);
+    CK(cudaGetLastError());
+  }
+  c->host_part.resize((size_t)c->ngrid * 5);
+  CK(cudaMemcpyAsync(c->host_part.data(), c->part, c->host_part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double a = 0.0, b = 0.0;
+  for (int e = 0; e < c->ngrid; ++e) {
+    const auto &g = c->groups[c->ext_group[e]];
+    const double *pp = &c->host_part[(size_t)(g.e0 + c->ext_k[e]) * 5];
+    a += pp[3];
+    b += pp[4];
+  }
+  *s = a;
+  *s2 = b;
+  return DSEM_OK;
+}
+}  // namespace dsem_int

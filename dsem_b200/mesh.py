@@ -378,10 +378,9 @@ def _modes_separable(box, K, kmax, amp, a, phase):
     return u.reshape(-1, 3)
 
 
-def random_isotropic(box, seed, k0=4.0, mach_t=0.3, gamma=1.4, twall=100.0):
-    """Seeded divergence-free random-phase velocity with E(k) ~ k^4 exp(-2 (k/k0)^2),
-    scaled to turbulent Mach number mach_t (u_rms = M_t c0 / sqrt(3)), uniform
-    density and pressure; evaluated at the Gauss points, returned as J*Q."""
+def _isotropic_velocity(box, seed, k0):
+    """Seeded divergence-free random-phase velocity with E(k) ~ k^4 exp(-2 (k/k0)^2)
+    at every point of box.xg ([nel * ldx^3][3]) and its rms per component."""
     rng = np.random.default_rng(seed)
     kmax = int(3 * k0)
     ks = np.arange(-kmax, kmax + 1)
@@ -403,19 +402,43 @@ def random_isotropic(box, seed, k0=4.0, mach_t=0.3, gamma=1.4, twall=100.0):
             arg = X @ K[i:i + 256].T + phase[i:i + 256]
             u += np.cos(arg) @ (amp[i:i + 256, None] * a[i:i + 256])
     mask = (box.jacob != 0).reshape(-1)
-    p0 = twall / gamma
-    c0 = math.sqrt(gamma * p0 / 1.0)
     urms = math.sqrt(np.mean(np.sum(u[mask] ** 2, axis=1)) / 3.0)
-    u *= (mach_t * c0 / math.sqrt(3.0)) / urms
-    u = u.reshape(box.nel, -1, 3)
-    rho = 1.0
+    return u, urms
+
+
+def _jq(box, rho, u, p, gamma):
     jq = np.zeros((box.nel, NV, box.ldx ** 3))
     m2 = box.jacob != 0
-    q = [np.full(u.shape[:2], rho), rho * u[..., 0], rho * u[..., 1], rho * u[..., 2],
-         p0 / (gamma - 1.0) + 0.5 * rho * np.sum(u * u, axis=-1)]
+    q = [rho, rho * u[..., 0], rho * u[..., 1], rho * u[..., 2],
+         p / (gamma - 1.0) + 0.5 * rho * np.sum(u * u, axis=-1)]
     for v in range(NV):
         jq[:, v][m2] = q[v][m2] / box.jacob[m2]
     return jq.reshape(box.qshape())
+
+
+def random_isotropic(box, seed, k0=4.0, mach_t=0.3, gamma=1.4, twall=100.0):
+    """Seeded divergence-free random-phase velocity with E(k) ~ k^4 exp(-2 (k/k0)^2),
+    scaled to turbulent Mach number mach_t (u_rms = M_t c0 / sqrt(3)), uniform
+    density and pressure; evaluated at the Gauss points, returned as J*Q."""
+    u, urms = _isotropic_velocity(box, seed, k0)
+    p0 = twall / gamma
+    c0 = math.sqrt(gamma * p0 / 1.0)
+    u = (u * ((mach_t * c0 / math.sqrt(3.0)) / urms)).reshape(box.nel, -1, 3)
+    return _jq(box, np.ones(u.shape[:2]), u, np.full(u.shape[:2], p0), gamma)
+
+
+def perturbed_taylor_green(box, seed, amp=0.05, k0=2.0, gamma=1.4, twall=100.0):
+    """Taylor-Green initial condition plus a seeded isotropic velocity of rms
+    amp (same density and pressure).  The perturbation removes the exact
+    symmetries of the Taylor-Green field (w = 0, zero normal velocity on
+    symmetry planes) at which the Roe flux's branches meet, so derivatives of
+    the flow with respect to its initial state are smooth."""
+    x, y, z = (box.xg[..., k] for k in range(3))
+    ut, urms = _isotropic_velocity(box, seed, k0)
+    ut = ut.reshape(box.nel, -1, 3) * (amp / urms)
+    u = np.stack([np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z), np.zeros_like(x)], -1) + ut
+    p = twall * 1.0 / gamma + (np.cos(2.0 * x) + np.cos(2.0 * y)) * (np.cos(2.0 * z) + 2.0) / 16.0
+    return _jq(box, np.ones_like(x), u, p, gamma)
 
 
 def dtcalc(box, JQ, gamma=1.4):

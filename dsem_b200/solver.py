@@ -18,7 +18,7 @@ ERRORS = {-1: "INVALID_ARG", -2: "CUDA", -3: "NONFINITE", -4: "TIMEOUT", -5: "UN
 EXPORTS = ("dsem_create", "dsem_destroy", "dsem_last_error", "dsem_upload_q", "dsem_download_q", "dsem_step",
            "dsem_stage", "dsem_rhs", "dsem_diag", "dsem_get_muhg", "dsem_last_timing", "dsem_profile_rhs",
            "dsem_create_batch", "dsem_batch_size", "dsem_upload_q_case", "dsem_download_q_case", "dsem_step_batch",
-           "dsem_diag_batch")
+           "dsem_diag_batch", "dsem_adjoint")
 
 
 class DsemError(RuntimeError):
@@ -71,6 +71,7 @@ def lib(path=None):
         L.dsem_download_q_case.argtypes = [vp, C.c_int, dp, C.c_int]
         L.dsem_step_batch.argtypes = [vp, dp, C.c_int]
         L.dsem_diag_batch.argtypes = [vp, dp, C.c_int, dp, dp, dp]
+        L.dsem_adjoint.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.c_int, dp, dp, C.c_int, dp, dp]
         _lib = L
     return _lib
 
@@ -163,6 +164,15 @@ class Solver:
         ms = np.zeros(4)
         self._check(lib().dsem_profile_rhs(self.h, int(reps), _dptr(ms)))
         return ms
+
+    def adjoint(self, dt, nsteps, window, snapshots=0, want_grad=True):
+        """J = sum of eps*dt over the last `window` of `nsteps` steps and its
+        gradient: returns (J, dJ/dJQ0 in the upload layout or None, dJ/d(1/Re), ms)."""
+        J, lr, ms = C.c_double(), C.c_double(), C.c_double()
+        g = np.zeros(self.qshape()) if want_grad else None
+        self._check(lib().dsem_adjoint(self.h, float(dt), int(nsteps), int(window), int(snapshots), C.byref(J),
+                                       _dptr(g) if want_grad else None, self.ldx, C.byref(lr), C.byref(ms)))
+        return J.value, g, lr.value, ms.value
 
     def last_timing(self):
         ms, n = C.c_double(), C.c_longlong()

@@ -143,6 +143,24 @@ int dsem_step_batch(dsem_ctx *ctx, const double *dt, int nsteps);
  * rejects contexts with more than one case). */
 int dsem_diag_batch(dsem_ctx *ctx, const double *dt, int first, double *ke, double *dkdt, double *eps);
 
+/* ---- Discrete adjoint ----
+ * No DSEM counterpart (DSEM has no adjoint solver).  Objective:
+ *   J = sum over the last `window` of `nsteps` steps of eps_n * dt,
+ * eps_n being the enstrophy dissipation dsem_diag reports after step n
+ * (100 <|w|^2>/Re from the JQ values after the step and the gradients of its
+ * last stage, energydissipation.f90:2-89).  Advances nsteps steps of size dt
+ * from the current state (tstep.f90:36-116), then runs the exact discrete
+ * adjoint of those steps backwards.  snapshots == 0 keeps every stage state
+ * in device memory (nsteps * kord states); snapshots = s > 0 keeps s step
+ * states and recomputes steps in binomial checkpointing order.  Outputs (each
+ * may be NULL): J; dJ/d(JQ at the start) in the ldx layout of dsem_upload_q;
+ * dJ/d(1/Re); the device milliseconds of the whole call.  The state is
+ * restored on return.  Supported: one case, one element order with p <= 6,
+ * axis-aligned elements, conforming mortars, shock = 0
+ * (DSEM_ERR_UNSUPPORTED otherwise). */
+int dsem_adjoint(dsem_ctx *ctx, double dt, int nsteps, int window, int snapshots, double *J, double *dJdQ0,
+                 int ldx, double *dJdinvRe, double *ms);
+
 /* Size of the static device array that holds the working buffers of
  * dsem_rhs_noalloc: 2^20 doubles (8 MiB) on every GPU that loads the library. */
 #define DSEM_NOALLOC_SCRATCH_DOUBLES (1 << 20)

@@ -1632,6 +1632,122 @@ template <class T> void diag(Case<T> &c, double dt, int first, double *turbk, do
   *enst = sum2 > 0 ? 100.0 * (sum / sum2) * (1.0 / c.re) : 0.0;
 }
 
+// Enstrophy dissipation of energydissipation (energydissipation.f90:19-78), the
+// eps of diag() in the case's scalar type (complex-step derivatives).
+template <class T> T enst_t(Case<T> &c) {
+  T sum = T(0.0);
+  double sum2 = 0.0;
+  for (auto &E : c.el) {
+    const Ops &o = ops_for(E.G);
+    const int G = E.G;
+    const size_t ng = E.ng();
+    if (!c.ql_valid) continue;
+    const T *w3[3] = {E.QL[0].data(), E.QL[1].data(), E.QL[2].data()};
+    std::vector<T> gq;
+    gauss_deriv(E, o, w3, 4, gq);
+    T se = T(0.0);
+    double sj = 0.0;
+    for (int l = 0; l < G; ++l)
+      for (int m = 0; m < G; ++m)
+        for (int n = 0; n < G; ++n) {
+          size_t p = gidx(G, l, m, n);
+          auto Qx = [&](int v) { return gq[(v * 3 + 0) * ng + p]; };
+          auto Qy = [&](int v) { return gq[(v * 3 + 1) * ng + p]; };
+          auto Qz = [&](int v) { return gq[(v * 3 + 2) * ng + p]; };
+          T Q1 = E.Q[p], Q2 = E.Q[ng + p], Q3 = E.Q[2 * ng + p], Q4 = E.Q[3 * ng + p];
+          double jac = E.jacob[p];
+          T udery = ((Qy(1) - (Q2 / Q1) * Qy(0))) / Q1;
+          T uderz = ((Qz(1) - (Q2 / Q1) * Qz(0))) / Q1;
+          T vderx = ((Qx(2) - (Q3 / Q1) * Qx(0))) / Q1;
+          T vderz = ((Qz(2) - (Q3 / Q1) * Qz(0))) / Q1;
+          T wderx = ((Qx(3) - (Q4 / Q1) * Qx(0))) / Q1;
+          T wdery = ((Qy(3) - (Q4 / Q1) * Qy(0))) / Q1;
+          T c1 = (wdery - vderz) / jac, c2 = (uderz - wderx) / jac, c3 = (vderx - udery) / jac;
+          T vort = c1 * c1 + c2 * c2 + c3 * c3;
+          vort = vort / jac;
+          sj = sj + 1.0 / jac;
+          se = se + vort;
+        }
+    sum += se;
+    sum2 += sj;
+  }
+  return sum2 > 0 ? 100.0 * (sum / sum2) * (1.0 / c.re) : T(0.0);
+}
+
+// The case with its state in another scalar type (geometry and parameters copied).
+template <class T> Case<T> *convert_case(const Case<double> &c) {
+  auto *o = new Case<T>();
+  auto cv = [](const std::vector<double> &a) { return std::vector<T>(a.begin(), a.end()); };
+  o->el.resize(c.el.size());
+  for (size_t e = 0; e < c.el.size(); ++e) {
+    const auto &A = c.el[e];
+    auto &B = o->el[e];
+    B.G = A.G;
+    B.L = A.L;
+    std::memcpy(B.corner, A.corner, sizeof(A.corner));
+    std::memcpy(B.node, A.node, sizeof(A.node));
+    std::memcpy(B.mort, A.mort, sizeof(A.mort));
+    std::memcpy(B.mside, A.mside, sizeof(A.mside));
+    std::memcpy(B.orientation, A.orientation, sizeof(A.orientation));
+    std::memcpy(B.boundary, A.boundary, sizeof(A.boundary));
+    B.jacob = A.jacob;
+    B.gmetg = A.gmetg;
+    for (int d = 0; d < 3; ++d) B.gmet[d] = A.gmet[d];
+    B.xg = A.xg;
+    B.hdelta = A.hdelta;
+    B.Q = cv(A.Q);
+    B.gQ = cv(A.gQ);
+    for (int d = 0; d < 3; ++d) {
+      B.QL[d] = cv(A.QL[d]);
+      B.F[d] = cv(A.F[d]);
+      B.R[d] = cv(A.R[d]);
+      B.muh[d] = cv(A.muh[d]);
+    }
+    B.muhg = cv(A.muhg);
+  }
+  o->mo.resize(c.mo.size());
+  for (size_t j = 0; j < c.mo.size(); ++j) {
+    const auto &A = c.mo[j];
+    auto &B = o->mo[j];
+    std::memcpy(B.id, A.id, sizeof(A.id));
+    std::memcpy(B.iface, A.iface, sizeof(A.iface));
+    std::memcpy(B.len, A.len, sizeof(A.len));
+    std::memcpy(B.lenm, A.lenm, sizeof(A.lenm));
+    B.orient = A.orient;
+    B.sign = A.sign;
+    B.nsign = A.nsign;
+    std::memcpy(B.conf, A.conf, sizeof(A.conf));
+    B.n_hat = A.n_hat;
+    B.norm = A.norm;
+    for (int a = 0; a < 2; ++a)
+      for (int d = 0; d < 2; ++d) {
+        B.P[a][d] = A.P[a][d];
+        B.Rm[a][d] = A.Rm[a][d];
+        B.pin[a][d] = A.pin[a][d];
+      }
+    for (int a = 0; a < 2; ++a) {
+      B.Qm[a] = cv(A.Qm[a]);
+      B.fv[a] = cv(A.fv[a]);
+    }
+  }
+  o->gamma = c.gamma;
+  o->re = c.re;
+  o->pr = c.pr;
+  o->mach = c.mach;
+  o->cmu = c.cmu;
+  o->mumax = c.mumax;
+  o->shock = c.shock;
+  o->ducros = c.ducros;
+  o->iord = c.iord;
+  o->kord = c.kord;
+  std::memcpy(o->ark, c.ark, sizeof(c.ark));
+  std::memcpy(o->brk, c.brk, sizeof(c.brk));
+  std::memcpy(o->crk, c.crk, sizeof(c.crk));
+  o->ql_valid = c.ql_valid;
+  o->prestep = c.prestep;
+  return o;
+}
+
 }  // namespace
 
 // ====================================================================== C API
@@ -1776,6 +1892,37 @@ void orc_euler(const double *Q, double gamma, double *f, double *g, double *h) {
 void orc_vis(const double *Q, const double *Qx, const double *Qy, const double *Qz, double amu, double gamma,
              double pr, double mach, double *f, double *g, double *h) {
   vis_fluxes(Q, Qx, Qy, Qz, amu, gamma, pr, mach, f, g, h);
+}
+// J = sum over the last `window` of `nsteps` steps of dt * eps_n (eps_n = the
+// enstrophy dissipation of orc_diag after step n), from the current state
+// plus i*hstep*dq (complex step): *J = Re J, *dJ = Im J / hstep = dJ/dJQ . dq.
+// The case itself is left unchanged.  dq uses the ldx layout of orc_set_q.
+void orc_objective_cs(const orc_case *h, double dt, int nsteps, int window, const double *dq, double hstep, int ldx,
+                      double *J, double *dJ) {
+  using CT = std::complex<double>;
+  Case<CT> *cc = convert_case<CT>(*h->c);
+  const size_t L3 = (size_t)ldx * ldx * ldx;
+  if (dq)
+    for (size_t e = 0; e < cc->el.size(); ++e) {
+      auto &E = cc->el[e];
+      const int G = E.G;
+      const size_t ng = E.ng();
+      for (int v = 0; v < NV; ++v)
+        for (int l = 0; l < G; ++l)
+          for (int m = 0; m < G; ++m)
+            for (int n = 0; n < G; ++n) {
+              CT &q = E.Q[v * ng + gidx(G, n, m, l)];
+              q = CT(q.real(), hstep * dq[e * NV * L3 + n + (size_t)ldx * (m + (size_t)ldx * (l + (size_t)ldx * v))]);
+            }
+    }
+  CT Jc = 0.0;
+  for (int s = 0; s < nsteps; ++s) {
+    for (int kk = 1; kk <= cc->kord; ++kk) stage(*cc, 0.0, dt, kk, nullptr, 0);
+    if (s >= nsteps - window) Jc += dt * enst_t(*cc);
+  }
+  *J = Jc.real();
+  *dJ = hstep != 0.0 ? Jc.imag() / hstep : 0.0;
+  delete cc;
 }
 void orc_rk(const orc_case *h, double *a, double *b, double *c) {
   for (int i = 0; i < 5; ++i) {

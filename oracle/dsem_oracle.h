@@ -86,6 +86,13 @@ void orc_euler(const double *Q, double gamma, double *f, double *g, double *h);
 void orc_vis(const double *Q, const double *Qx, const double *Qy, const double *Qz, double amu, double gamma,
              double pr, double mach, double *f, double *g, double *h);
 void orc_rk(const orc_case *c, double *ark, double *brk, double *crk);
+/* Objective of the adjoint, J = sum over the last `window` of `nsteps` steps of
+ * dt * enst (orc_diag's enstrophy dissipation after each step), evaluated from
+ * the current state + i*hstep*dq in complex arithmetic: *J = Re J and
+ * *dJ = Im J / hstep (the directional derivative along dq).  The case is not
+ * modified. */
+void orc_objective_cs(const orc_case *c, double dt, int nsteps, int window, const double *dq, double hstep, int ldx,
+                      double *J, double *dJ);
 
 #ifdef __cplusplus
 }

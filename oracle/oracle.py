@@ -59,6 +59,8 @@ def lib():
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_set_threads.restype = C.c_int
         L.orc_rk.argtypes = [vp, _dp, _dp, _dp]
+        L.orc_objective_cs.argtypes = [vp, C.c_double, C.c_int, C.c_int, vp, C.c_double, C.c_int,
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_riemann.argtypes = [_dp, C.c_double, _dp, _dp, C.c_double, _dp]
         L.orc_euler.argtypes = [_dp, C.c_double, _dp, _dp, _dp]
         L.orc_vis.argtypes = [_dp] * 4 + [C.c_double] * 4 + [_dp] * 3
@@ -199,6 +201,16 @@ class Case:
 
     def kord(self):
         return lib().orc_kord(self.h)
+
+    def objective_cs(self, dt, nsteps, window, dq=None, h=1e-30):
+        """(J, dJ/dJQ . dq) of J = sum over the last `window` steps of dt * eps,
+        by complex step from the current state; the case is not modified."""
+        J, dJ = C.c_double(), C.c_double()
+        dqa = None if dq is None else np.ascontiguousarray(dq, dtype=np.float64)
+        lib().orc_objective_cs(self.h, float(dt), int(nsteps), int(window),
+                               None if dqa is None else dqa.ctypes.data_as(C.c_void_p), float(h), self.ldx,
+                               C.byref(J), C.byref(dJ))
+        return J.value, dJ.value
 
     def rk(self):
         a, b, c = np.zeros(5), np.zeros(5), np.zeros(5)
