@@ -12,11 +12,13 @@
 //   k_trace_adj     face traces          -> LJQ += jacob * trace^T LQR
 // The volume adjoint can also add the derivative of the enstrophy-dissipation
 // sum (energydissipation.f90:19-78) evaluated on the same gradients.
-// Derivatives are exact up to rounding; the Roe flux is differentiated in
-// forward mode (one tangent per input), the other pointwise functions by
-// hand-written reverse mode.  Diagonal metrics, conforming mortars, no
+// Derivatives are exact up to rounding; every pointwise function is
+// differentiated by hand-written reverse mode (riemann_dual / roe_vjp, the
+// forward-mode derivative of the Roe flux, is kept as its independent check).  Diagonal metrics, conforming mortars, no
 // entropy viscosity.
 #pragma once
+#include <type_traits>
+
 #include "dsem_stage.cuh"
 
 namespace dsem {
@@ -125,6 +127,196 @@ __device__ __forceinline__ void roe_vjp(const double *nh, double ds, const doubl
     else
       lQr[j - NV] += s;
   }
+}
+
+// Reverse mode of riemann(): lQl += (dF/dQl)^T lf, lQr += (dF/dQr)^T lf, the
+// adjoint statements of each forward statement in reverse order; branches and
+// kinks as riemann_dual (value of the forward quantity decides).
+__device__ __forceinline__ void roe_vjp_rev(const double *nh, double ds, const double *Ql, const double *Qr,
+                                            double gamma, const double *lfin, double *lQl, double *lQr) {
+  const double g1 = gamma - 1.0, gg = gamma / (gamma - 1.0), K = (gamma + 1.0) / 4.0;
+  const double rho = Ql[0], rhou = Ql[1], rhov = Ql[2], rhow = Ql[3], rhoe = Ql[4];
+  const double rhon = Qr[0], rhoun = Qr[1], rhovn = Qr[2], rhown = Qr[3], rhoen = Qr[4];
+  const double ul = rhou / rho, vl = rhov / rho, wl = rhow / rho;
+  const double M2l = rhou * rhou + rhov * rhov + rhow * rhow;
+  const double pleft = g1 * (rhoe - 0.5 / rho * M2l);
+  const double ur = rhoun / rhon, vr = rhovn / rhon, wr = rhown / rhon;
+  const double M2r = rhoun * rhoun + rhovn * rhovn + rhown * rhown;
+  const double pright = g1 * (rhoen - 0.5 / rhon * M2r);
+  const double ql = nh[0] * ul + nh[1] * vl + nh[2] * wl;
+  const double qr = nh[0] * ur + nh[1] * vr + nh[2] * wr;
+  const double hl = 0.5 * (ul * ul + vl * vl + wl * wl) + gg * pleft / rho;
+  const double hr = 0.5 * (ur * ur + vr * vr + wr * wr) + gg * pright / rhon;
+  const double rtd = sqrt(rho * rhon);
+  const double sb = rho + rtd;
+  const double betal = rho / sb, betar = 1.0 - betal;
+  const double utd = betal * ul + betar * ur, vtd = betal * vl + betar * vr, wtd = betal * wl + betar * wr;
+  const double htd = betal * hl + betar * hr;
+  const double atd2 = g1 * (htd - 0.5 * (utd * utd + vtd * vtd + wtd * wtd));
+  const double atd = sqrt(atd2);
+  const double qtd = utd * nh[0] + vtd * nh[1] + wtd * nh[2];
+  double lf[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) lf[v] = ds * lfin[v];
+  const double lpn = lf[1] * nh[0] + lf[2] * nh[1] + lf[3] * nh[2];
+  double lul = 0, lvl = 0, lwl = 0, lur = 0, lvr = 0, lwr = 0, lhl = 0, lhr = 0, lpl = 0, lpr = 0;
+  double lutd = 0, lvtd = 0, lwtd = 0, lhtd = 0, latd = 0, lqtd = 0, lrho = 0, lrhon = 0, lql = 0, lqr = 0;
+  double lrtd = 0, latd2 = 0, ldw = 0;
+  const double X = (qr - ql) * rtd / atd;
+  double lX = 0.0;
+  if (qtd >= 0.0) {
+    const double dw1 = 0.5 * ((pright - pleft) / atd2 - X);
+    const double sp1 = qtd - atd;
+    const double sp1m = sp1 <= 0.0 ? sp1 : 0.0;
+    const double hd1m = (K * atd / rtd) * dw1;
+    const double e1 = -fabs(sp1) - hd1m;
+    const double eta1 = e1 >= 0.0 ? e1 : 0.0;
+    const double udw1 = dw1 * (sp1m - 0.5 * eta1);
+    const double rql = rho * ql;
+    const double lrql = lf[0] + lf[1] * ul + lf[2] * vl + lf[3] * wl + lf[4] * hl;
+    const double ludw = lf[0] + lf[1] * (utd - atd * nh[0]) + lf[2] * (vtd - atd * nh[1]) +
+                        lf[3] * (wtd - atd * nh[2]) + lf[4] * (htd - qtd * atd);
+    lul += lf[1] * rql;
+    lvl += lf[2] * rql;
+    lwl += lf[3] * rql;
+    lhl += lf[4] * rql;
+    lpl += lpn;
+    lutd += lf[1] * udw1;
+    lvtd += lf[2] * udw1;
+    lwtd += lf[3] * udw1;
+    lhtd += lf[4] * udw1;
+    latd += -udw1 * lpn - lf[4] * udw1 * qtd;
+    lqtd += -lf[4] * udw1 * atd;
+    lrho += lrql * ql;
+    lql += lrql * rho;
+    ldw += ludw * (sp1m - 0.5 * eta1);
+    const double lsp1m = ludw * dw1;
+    const double leta = -0.5 * ludw * dw1;
+    const double le = e1 >= 0.0 ? leta : 0.0;
+    double lsp1 = -(sp1 < 0.0 ? -1.0 : 1.0) * le;
+    const double lhd = -le;
+    latd += K / rtd * dw1 * lhd;
+    lrtd += -K * atd / (rtd * rtd) * dw1 * lhd;
+    ldw += K * atd / rtd * lhd;
+    lsp1 += sp1 <= 0.0 ? lsp1m : 0.0;
+    lqtd += lsp1;
+    latd -= lsp1;
+    lpr += 0.5 / atd2 * ldw;
+    lpl -= 0.5 / atd2 * ldw;
+    latd2 += -0.5 * (pright - pleft) / (atd2 * atd2) * ldw;
+    lX = -0.5 * ldw;
+  } else {
+    const double dw4 = 0.5 * ((pright - pleft) / atd2 + X);
+    const double sp4 = qtd + atd;
+    const double sp4p = sp4 >= 0.0 ? sp4 : 0.0;
+    const double hd4 = (K * atd / rtd) * dw4;
+    const double e4 = -fabs(sp4) + hd4;
+    const double eta4 = e4 >= 0.0 ? e4 : 0.0;
+    const double udw4 = dw4 * (sp4p + 0.5 * eta4);
+    const double rqr = rhon * qr;
+    const double lrqr = lf[0] + lf[1] * ur + lf[2] * vr + lf[3] * wr + lf[4] * hr;
+    const double ludw = -(lf[0] + lf[1] * (utd + atd * nh[0]) + lf[2] * (vtd + atd * nh[1]) +
+                          lf[3] * (wtd + atd * nh[2]) + lf[4] * (htd + qtd * atd));
+    lur += lf[1] * rqr;
+    lvr += lf[2] * rqr;
+    lwr += lf[3] * rqr;
+    lhr += lf[4] * rqr;
+    lpr += lpn;
+    lutd += -lf[1] * udw4;
+    lvtd += -lf[2] * udw4;
+    lwtd += -lf[3] * udw4;
+    lhtd += -lf[4] * udw4;
+    latd += -udw4 * lpn - lf[4] * udw4 * qtd;
+    lqtd += -lf[4] * udw4 * atd;
+    lrhon += lrqr * qr;
+    lqr += lrqr * rhon;
+    ldw += ludw * (sp4p + 0.5 * eta4);
+    const double lsp4p = ludw * dw4;
+    const double leta = 0.5 * ludw * dw4;
+    const double le = e4 >= 0.0 ? leta : 0.0;
+    double lsp4 = -(sp4 < 0.0 ? -1.0 : 1.0) * le;
+    const double lhd = le;
+    latd += K / rtd * dw4 * lhd;
+    lrtd += -K * atd / (rtd * rtd) * dw4 * lhd;
+    ldw += K * atd / rtd * lhd;
+    lsp4 += sp4 >= 0.0 ? lsp4p : 0.0;
+    lqtd += lsp4;
+    latd += lsp4;
+    lpr += 0.5 / atd2 * ldw;
+    lpl -= 0.5 / atd2 * ldw;
+    latd2 += -0.5 * (pright - pleft) / (atd2 * atd2) * ldw;
+    lX = 0.5 * ldw;
+  }
+  // X = (qr - ql) rtd / atd
+  lqr += lX * rtd / atd;
+  lql -= lX * rtd / atd;
+  lrtd += lX * (qr - ql) / atd;
+  latd += -lX * X / atd;
+  // qtd, atd, atd2
+  lutd += nh[0] * lqtd;
+  lvtd += nh[1] * lqtd;
+  lwtd += nh[2] * lqtd;
+  latd2 += latd / (2.0 * atd);
+  lhtd += g1 * latd2;
+  lutd += -g1 * utd * latd2;
+  lvtd += -g1 * vtd * latd2;
+  lwtd += -g1 * wtd * latd2;
+  // Roe averages
+  double lbl = hl * lhtd + ul * lutd + vl * lvtd + wl * lwtd;
+  const double lbr = hr * lhtd + ur * lutd + vr * lvtd + wr * lwtd;
+  lhl += betal * lhtd;
+  lhr += betar * lhtd;
+  lul += betal * lutd;
+  lvl += betal * lvtd;
+  lwl += betal * lwtd;
+  lur += betar * lutd;
+  lvr += betar * lvtd;
+  lwr += betar * lwtd;
+  lbl -= lbr;
+  lrho += lbl * rtd / (sb * sb);
+  lrtd += -lbl * rho / (sb * sb);
+  lrho += lrtd * rhon / (2.0 * rtd);
+  lrhon += lrtd * rho / (2.0 * rtd);
+  // enthalpies
+  lul += ul * lhl;
+  lvl += vl * lhl;
+  lwl += wl * lhl;
+  lpl += gg / rho * lhl;
+  lrho += -gg * pleft / (rho * rho) * lhl;
+  lur += ur * lhr;
+  lvr += vr * lhr;
+  lwr += wr * lhr;
+  lpr += gg / rhon * lhr;
+  lrhon += -gg * pright / (rhon * rhon) * lhr;
+  // normal velocities
+  lul += nh[0] * lql;
+  lvl += nh[1] * lql;
+  lwl += nh[2] * lql;
+  lur += nh[0] * lqr;
+  lvr += nh[1] * lqr;
+  lwr += nh[2] * lqr;
+  // pressures
+  lQl[4] += g1 * lpl;
+  lrho += g1 * 0.5 * M2l / (rho * rho) * lpl;
+  lQl[1] += -g1 * rhou / rho * lpl;
+  lQl[2] += -g1 * rhov / rho * lpl;
+  lQl[3] += -g1 * rhow / rho * lpl;
+  lQr[4] += g1 * lpr;
+  lrhon += g1 * 0.5 * M2r / (rhon * rhon) * lpr;
+  lQr[1] += -g1 * rhoun / rhon * lpr;
+  lQr[2] += -g1 * rhovn / rhon * lpr;
+  lQr[3] += -g1 * rhown / rhon * lpr;
+  // velocities
+  lQl[1] += lul / rho;
+  lQl[2] += lvl / rho;
+  lQl[3] += lwl / rho;
+  lrho += -(ul * lul + vl * lvl + wl * lwl) / rho;
+  lQr[1] += lur / rhon;
+  lQr[2] += lvr / rhon;
+  lQr[3] += lwr / rhon;
+  lrhon += -(ur * lur + vr * lvr + wr * lwr) / rhon;
+  lQl[0] += lrho;
+  lQr[0] += lrhon;
 }
 
 // ---------------------------------------------- hand-written reverse modes
@@ -355,9 +547,9 @@ __global__ void __launch_bounds__(128) k_face_inv_adj(const MortarC *__restrict_
   const double n3[3] = {nh[gp * 3], nh[gp * 3 + 1], nh[gp * 3 + 2]};
   const bool low = (M.flags >> 5) & 1;
   if (low)
-    roe_vjp(n3, nrm[gp], Q2, Q1, gamma, lf, l2, l1);
+    roe_vjp_rev(n3, nrm[gp], Q2, Q1, gamma, lf, l2, l1);
   else
-    roe_vjp(n3, nrm[gp], Q1, Q2, gamma, lf, l1, l2);
+    roe_vjp_rev(n3, nrm[gp], Q1, Q2, gamma, lf, l1, l2);
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
     LQR[M.ms + v * G2 + pt] = l1[v];
@@ -402,7 +594,7 @@ struct VolAdjArgs {
 
 template <int G> struct VolAdjCfg {
   static constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
-  static constexpr int NT = 256;
+  static constexpr int NT = G >= 6 ? 384 : 256;  // one element per SM (shared memory); 12 warps at p >= 5
   static constexpr size_t NDBL = 5 * NG + 15 * NG + 15 * NG + 5 * NL + 5 * NL + 11 * NL + 5 * NG + 5 * NG + 30 * G2 +
                                  2 * G * L + NT;
   static constexpr size_t SMEM = sizeof(double) * NDBL;
@@ -410,7 +602,7 @@ template <int G> struct VolAdjCfg {
 
 // Volume adjoint of one element (diagonal metrics): recomputes the Lobatto
 // arrays and Gauss gradients, then runs the volume operations in reverse.
-template <int G> __global__ void __launch_bounds__(256, 1) k_vol_adj(VolAdjArgs A) {
+template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_adj(VolAdjArgs A) {
   using C = VolAdjCfg<G>;
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G, NT = C::NT;
   extern __shared__ double sm[];
@@ -452,8 +644,9 @@ template <int G> __global__ void __launch_bounds__(256, 1) k_vol_adj(VolAdjArgs 
   __syncthreads();
 
   // Lobatto arrays of grid D into LB (interior from q, faces from QF)
-  auto build = [&](int D) {
-    const int xs = D == 0 ? 1 : (D == 1 ? G : G2);
+  auto build = [&](auto Dc) {
+    constexpr int D = decltype(Dc)::value;
+    constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
     for (int t = tid; t < 5 * G2; t += NT) {
       const int v = t / G2, ln = t - v * G2, a = ln % G, b = ln / G;
       const int p0 = gbase<G>(D, a, b), l0 = lbase<G>(D, a, b);
@@ -473,10 +666,11 @@ template <int G> __global__ void __launch_bounds__(256, 1) k_vol_adj(VolAdjArgs 
   };
 
   // ---- forward: Gauss gradients of the five fields
-  for (int D = 0; D < 3; ++D) {
-    build(D);
+  auto grad_dir = [&](auto Dc) {
+    constexpr int D = decltype(Dc)::value;
+    build(Dc);
     __syncthreads();
-    const int xs = D == 0 ? 1 : (D == 1 ? G : G2);
+    constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
     for (int t = tid; t < 5 * G2; t += NT) {
       const int f = t / G2, ln = t - f * G2, a = ln % G, b = ln / G;
       const int p0 = gbase<G>(D, a, b), l0 = lbase<G>(D, a, b);
@@ -492,7 +686,10 @@ template <int G> __global__ void __launch_bounds__(256, 1) k_vol_adj(VolAdjArgs 
       }
     }
     __syncthreads();
-  }
+  };
+  grad_dir(std::integral_constant<int, 0>{});
+  grad_dir(std::integral_constant<int, 1>{});
+  grad_dir(std::integral_constant<int, 2>{});
 
   // ---- enstrophy term (energydissipation.f90:19-78) on these gradients and the
   // JQ values of JQe: the gradient part goes to LGR; with direct_only the JQe
@@ -523,10 +720,11 @@ template <int G> __global__ void __launch_bounds__(256, 1) k_vol_adj(VolAdjArgs 
   if (A.direct_only) return;
 
   // ---- reverse of pass 2: fluxes and interior divergence, grid by grid
-  for (int D = 0; D < 3; ++D) {
-    build(D);
+  auto flux_dir = [&](auto Dc) {
+    constexpr int D = decltype(Dc)::value;
+    build(Dc);
     __syncthreads();
-    const int xs = D == 0 ? 1 : (D == 1 ? G : G2);
+    constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
     for (int qi = tid; qi < NL; qi += NT) {
       int s, a, b;
       ldecode<G>(D, qi, s, a, b);
@@ -632,11 +830,15 @@ template <int G> __global__ void __launch_bounds__(256, 1) k_vol_adj(VolAdjArgs 
       }
     }
     __syncthreads();
-  }
+  };
+  flux_dir(std::integral_constant<int, 0>{});
+  flux_dir(std::integral_constant<int, 1>{});
+  flux_dir(std::integral_constant<int, 2>{});
 
   // ---- reverse of pass 1: gradients -> Lobatto arrays -> q and QF
-  for (int D = 0; D < 3; ++D) {
-    const int xs = D == 0 ? 1 : (D == 1 ? G : G2);
+  auto lob_dir = [&](auto Dc) {
+    constexpr int D = decltype(Dc)::value;
+    constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
     for (int t = tid; t < 5 * G2; t += NT) {
       const int f = t / G2, ln = t - f * G2, a = ln % G, b = ln / G;
       const int p0 = gbase<G>(D, a, b);
@@ -662,16 +864,21 @@ template <int G> __global__ void __launch_bounds__(256, 1) k_vol_adj(VolAdjArgs 
       LQFs[(face_hi(D) - 1) * 5 * G2 + f * G2 + ln] += y[L - 1];
     }
     __syncthreads();
-  }
+  };
+  lob_dir(std::integral_constant<int, 0>{});
+  lob_dir(std::integral_constant<int, 1>{});
+  lob_dir(std::integral_constant<int, 2>{});
 
   // ---- outputs
   for (int i = tid; i < 5 * NG; i += NT) LJQ[i] = jac[i % NG] * LQ[i];
   for (int i = tid; i < 30 * G2; i += NT) A.LQF[(long long)k * 30 * G2 + i] = LQFs[i];
   red[tid] = lr;
   __syncthreads();
-  for (int w = NT / 2; w > 0; w >>= 1) {
-    if (tid < w) red[tid] += red[tid + w];
+  for (int n = NT; n > 1;) {  // pairwise halving, any NT
+    const int h = (n + 1) / 2;
+    if (tid < n - h) red[tid] += red[tid + h];
     __syncthreads();
+    n = h;
   }
   if (tid == 0) A.lr[k] = red[0];
 }

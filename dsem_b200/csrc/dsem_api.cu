@@ -44,59 +44,63 @@ __global__ void k_pack(const double *__restrict__ src, int ldx, const int *__res
   }
 }
 
-// Per-element partial sums for the diagnostics, one thread per element, in the
+// Per-element partial sums for the diagnostics, one block per element: the
+// point terms in parallel, then each sum accumulated by one thread in the
 // oracle's loop order: [0..2] sum u^2 w, v^2 w, w^2 w; [3] sum |w|^2 J; [4] sum J.
 __global__ void k_diag(const double *__restrict__ JQ, const double *__restrict__ jac, const double *__restrict__ EVB,
                        const double *__restrict__ kew, int G, int nel, int have_grad, double *__restrict__ part) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nel) return;
+  extern __shared__ double sm[];
+  const int k = blockIdx.x;
   const int NG = G * G * G;
+  double *T = sm;  // [5][NG]
   const double *Q = JQ + (long long)k * 5 * NG;
   const double *J = jac + (long long)k * NG;
-  double su = 0, sv = 0, sw = 0;
-  for (int i = 0; i < G; ++i)
-    for (int j = 0; j < G; ++j)
-      for (int l = 0; l < G; ++l) {
-        const int p = i + G * (j + G * l);
-        const double q1 = Q[p];
-        const double u = Q[NG + p] / q1, v = Q[2 * NG + p] / q1, w = Q[3 * NG + p] / q1;
-        const double b = kew[p];
-        su = su + (u * u) * b;
-        sv = sv + (v * v) * b;
-        sw = sw + (w * w) * b;
-      }
-  double s = 0.0, s2 = 0.0;
-  if (have_grad) {  // energydissipation.f90:19-78
-    const double *E = EVB + (long long)k * 15 * NG;
-    for (int l = 0; l < G; ++l)
-      for (int m = 0; m < G; ++m)
-        for (int n = 0; n < G; ++n) {
-          const int p = l + G * (m + G * n);
-          const double Q1 = Q[p], Q2 = Q[NG + p], Q3 = Q[2 * NG + p], Q4 = Q[3 * NG + p];
-          const double jc = J[p];
-          const double Qx0 = E[0 * NG + p], Qy0 = E[1 * NG + p], Qz0 = E[2 * NG + p];
-          const double Qy1 = E[4 * NG + p], Qz1 = E[5 * NG + p];
-          const double Qx2 = E[6 * NG + p], Qz2 = E[8 * NG + p];
-          const double Qx3 = E[9 * NG + p], Qy3 = E[10 * NG + p];
-          const double udery = ((Qy1 - (Q2 / Q1) * Qy0)) / Q1;
-          const double uderz = ((Qz1 - (Q2 / Q1) * Qz0)) / Q1;
-          const double vderx = ((Qx2 - (Q3 / Q1) * Qx0)) / Q1;
-          const double vderz = ((Qz2 - (Q3 / Q1) * Qz0)) / Q1;
-          const double wderx = ((Qx3 - (Q4 / Q1) * Qx0)) / Q1;
-          const double wdery = ((Qy3 - (Q4 / Q1) * Qy0)) / Q1;
-          const double c1 = (wdery - vderz) / jc, c2 = (uderz - wderx) / jc, c3 = (vderx - udery) / jc;
-          double vort = c1 * c1 + c2 * c2 + c3 * c3;
-          vort = vort / jc;
-          s2 = s2 + 1.0 / jc;
-          s = s + vort;
-        }
+  const double *E = EVB + (long long)k * 15 * NG;
+  for (int p = threadIdx.x; p < NG; p += blockDim.x) {
+    const double q1 = Q[p];
+    const double u = Q[NG + p] / q1, v = Q[2 * NG + p] / q1, w = Q[3 * NG + p] / q1;
+    const double b = kew[p];
+    T[p] = (u * u) * b;
+    T[NG + p] = (v * v) * b;
+    T[2 * NG + p] = (w * w) * b;
+    if (have_grad) {  // energydissipation.f90:19-78
+      const double Q1 = Q[p], Q2 = Q[NG + p], Q3 = Q[2 * NG + p], Q4 = Q[3 * NG + p];
+      const double jc = J[p];
+      const double Qx0 = E[0 * NG + p], Qy0 = E[1 * NG + p], Qz0 = E[2 * NG + p];
+      const double Qy1 = E[4 * NG + p], Qz1 = E[5 * NG + p];
+      const double Qx2 = E[6 * NG + p], Qz2 = E[8 * NG + p];
+      const double Qx3 = E[9 * NG + p], Qy3 = E[10 * NG + p];
+      const double udery = ((Qy1 - (Q2 / Q1) * Qy0)) / Q1;
+      const double uderz = ((Qz1 - (Q2 / Q1) * Qz0)) / Q1;
+      const double vderx = ((Qx2 - (Q3 / Q1) * Qx0)) / Q1;
+      const double vderz = ((Qz2 - (Q3 / Q1) * Qz0)) / Q1;
+      const double wderx = ((Qx3 - (Q4 / Q1) * Qx0)) / Q1;
+      const double wdery = ((Qy3 - (Q4 / Q1) * Qy0)) / Q1;
+      const double c1 = (wdery - vderz) / jc, c2 = (uderz - wderx) / jc, c3 = (vderx - udery) / jc;
+      double vort = c1 * c1 + c2 * c2 + c3 * c3;
+      vort = vort / jc;
+      T[3 * NG + p] = vort;
+      T[4 * NG + p] = 1.0 / jc;
+    }
   }
-  double *o = part + (long long)k * 5;
-  o[0] = su;
-  o[1] = sv;
-  o[2] = sw;
-  o[3] = s;
-  o[4] = s2;
+  __syncthreads();
+  const int f = threadIdx.x;
+  if (f < 3 || (f < 5 && have_grad)) {
+    const double *t = T + f * NG;
+    double acc = 0.0;
+    if (f < 3) {
+      for (int i = 0; i < G; ++i)
+        for (int j = 0; j < G; ++j)
+          for (int l = 0; l < G; ++l) acc = acc + t[i + G * (j + G * l)];
+    } else {
+      for (int l = 0; l < G; ++l)
+        for (int m = 0; m < G; ++m)
+          for (int n = 0; n < G; ++n) acc = acc + t[l + G * (m + G * n)];
+    }
+    part[(long long)k * 5 + f] = acc;
+  } else if (f < 5) {
+    part[(long long)k * 5 + f] = 0.0;
+  }
 }
 
 }  // namespace
@@ -963,8 +967,8 @@ int diag_impl(dsem_ctx *c, const double *dt, int first, double *ke, double *dkdt
   c->keep_grad = 1;
   const bool have = c->grad_valid;
   for (auto &g : c->groups) {
-    k_diag<<<(g.nel + 127) / 128, 128, 0, c->st>>>(c->JQ + g.q0, g.jac, g.EVB, g.kew, g.G, g.nel, have ? 1 : 0,
-                                                    c->part + g.e0 * 5);
+    k_diag<<<g.nel, 128, sizeof(double) * 5 * g.G * g.G * g.G, c->st>>>(c->JQ + g.q0, g.jac, g.EVB, g.kew, g.G, g.nel,
+                                                                         have ? 1 : 0, c->part + g.e0 * 5);
     CK(cudaGetLastError());
   }
   c->host_part.resize((size_t)c->ngrid * 5);
@@ -1218,8 +1222,8 @@ int check_flag(dsem_ctx *c) { return ::check_flag(c); }
 // enstrophy sums of the last stage's gradients, in the caller's element order
 int eps_sums(dsem_ctx *c, double *s, double *s2) {
   for (auto &g : c->groups) {
-    k_diag<<<(g.nel + 127) / 128, 128, 0, c->st>>>(c->JQ + g.q0, g.jac, g.EVB, g.kew, g.G, g.nel, 1,
-                                                    c->part + g.e0 * 5);
+    k_diag<<<g.nel, 128, sizeof(double) * 5 * g.G * g.G * g.G, c->st>>>(c->JQ + g.q0, g.jac, g.EVB, g.kew, g.G, g.nel, 1,
+                                                                         c->part + g.e0 * 5);
     CK(cudaGetLastError());
   }
   c->host_part.resize((size_t)c->ngrid * 5);
