@@ -467,7 +467,7 @@ def main():
         hbm_ach = vol_bytes(G) * box.nel / t_vol / 1e9
         tr = profiled_traffic()
         roof = {"bound": "tensor", "pipe": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": achieved / fp64_peak, "kernel": "k_vol",
+                "frac": achieved / fp64_peak, "kernel": "k_vol_diag (volume kernel, diagonal metrics)",
                 "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                 "traffic": (tr["bytes_per_launch"] if tr else None),
                 "hbm": {"achieved": hbm_ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
