@@ -131,6 +131,49 @@ __device__ __forceinline__ void vol_diag_tgrad(int ln, const double *WK, const d
   }
 }
 
+// Fluxes at Lobatto point qi = (s; a, b) of grid D from its 11 interpolated
+// gradient fields c (diag_field order; c[4] = energy gradient along D): the
+// viscous flux times gmet at face points goes to VF, the inviscid minus viscous
+// flux over Re overwrites the point's state slot in LB.
+template <int G, int D>
+__device__ __forceinline__ void vol_diag_point(int qi, int s, int a, int b, const double *c, double amu, const Phys &P,
+                                               const double *gm, double *LB, double *VF) {
+  constexpr int L = G + 1, G2 = G * G, NL = L * G * G;
+  double Q[NV], Qx[NV], Qy[NV], Qz[NV], r[NV], fl[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) Q[v] = LB[v * NL + qi];
+  const double rr = 1.0 / Q[0];
+  const double gdiag = gm[D * NL + qi];
+  if (D == 0) {
+    Qx[0] = c[0]; Qx[1] = c[1]; Qx[2] = c[2]; Qx[3] = c[3]; Qx[4] = c[4];
+    Qy[0] = c[5]; Qy[1] = c[6]; Qy[2] = c[7]; Qy[3] = 0.0; Qy[4] = 0.0;
+    Qz[0] = c[8]; Qz[1] = c[9]; Qz[3] = c[10]; Qz[2] = 0.0; Qz[4] = 0.0;
+    vis_flux_x(Q, rr, Qx, Qy, Qz, amu, P, fl);
+  } else if (D == 1) {
+    Qy[0] = c[0]; Qy[1] = c[1]; Qy[2] = c[2]; Qy[3] = c[3]; Qy[4] = c[4];
+    Qx[0] = c[5]; Qx[1] = c[6]; Qx[2] = c[7]; Qx[3] = 0.0; Qx[4] = 0.0;
+    Qz[0] = c[8]; Qz[2] = c[9]; Qz[3] = c[10]; Qz[1] = 0.0; Qz[4] = 0.0;
+    vis_flux_y(Q, rr, Qx, Qy, Qz, amu, P, fl);
+  } else {
+    Qz[0] = c[0]; Qz[1] = c[1]; Qz[2] = c[2]; Qz[3] = c[3]; Qz[4] = c[4];
+    Qx[0] = c[5]; Qx[1] = c[6]; Qx[3] = c[7]; Qx[2] = 0.0; Qx[4] = 0.0;
+    Qy[0] = c[8]; Qy[2] = c[9]; Qy[3] = c[10]; Qy[1] = 0.0; Qy[4] = 0.0;
+    vis_flux_z(Q, rr, Qx, Qy, Qz, amu, P, fl);
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) r[v] = gdiag * fl[v];
+  if (s == 0 || s == L - 1) {
+    const int fc = s == 0 ? face_lo(D) : face_hi(D);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) VF[(fc - 1) * 5 * G2 + v * G2 + a + G * b] = r[v];
+  } else {
+    double fi[NV];
+    euler_flux(D, Q, rr, P.gamma, fi);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) LB[v * NL + qi] = gdiag * fi[v] - ddiv(r[v], P.re, P.r_re);
+  }
+}
+
 // Pass 2 along direction D: Lobatto arrays of grid D, fluxes at its points,
 // interior divergence accumulated into acc (the thread's Gauss points).
 template <int G, bool EV, int SAVE, int D>
@@ -180,57 +223,49 @@ __device__ __forceinline__ void vol_diag_dir(const VolArgs &A, const Phys &P, co
   }
   __syncthreads();
   PHASE_MARK(2 + 3 * (2 - D));
-  // (b) fluxes at the Lobatto points of grid D (Vis_Fluxes_new.f90:115-228, fluxesH_newa.f90:276-352)
-  for (int qi = tid; qi < NL; qi += NT) {
-    int s, a, b;
-    ldecode<G>(D, qi, s, a, b);
-    const int g0 = gbase<G>(D, a, b);
-    double br[G];
+  // (b) fluxes at the Lobatto points of grid D (Vis_Fluxes_new.f90:115-228, fluxesH_newa.f90:276-352),
+  // two points (s, s + NH) of one line per task so that both share the gradient loads
+  constexpr int NH = (L + 1) / 2;
+  for (int t = tid; t < NH * G2; t += NT) {
+    const int h = t / G2, ln = t - h * G2, a = ln % G, b = ln / G;
+    const int g0 = gbase<G>(D, a, b), l0 = lbase<G>(D, a, b);
+    const int s0 = h, s1 = h + NH;
+    const bool two = s1 < L;
+    const int s1c = two ? s1 : s0;
+    double br0[G], br1[G];
 #pragma unroll
-    for (int kk = 0; kk < G; ++kk) br[kk] = Bm[s * G + kk];
-    double c[11];
+    for (int kk = 0; kk < G; ++kk) {
+      br0[kk] = Bm[s0 * G + kk];
+      br1[kk] = Bm[s1c * G + kk];
+    }
+    double c0[11], c1[11];
 #pragma unroll
     for (int jf = 0; jf < 11; ++jf) {
-      if (jf == 4)
-        c[jf] = T4[qi];
-      else
-        c[jf] = chain<G>(br, GR + diag_field(D, jf) * NG + g0, xs);
+      if (jf == 4) {
+        c0[jf] = T4[l0 + s0 * ls];
+        c1[jf] = T4[l0 + s1c * ls];
+      } else {
+        const double *x = GR + diag_field(D, jf) * NG + g0;
+        double xv[G];
+#pragma unroll
+        for (int kk = 0; kk < G; ++kk) xv[kk] = x[kk * xs];
+        double a0 = br0[0] * xv[0], a1 = br1[0] * xv[0];
+#pragma unroll
+        for (int kk = 1; kk < G; ++kk) {
+          a0 = __fma_rn(br0[kk], xv[kk], a0);
+          a1 = __fma_rn(br1[kk], xv[kk], a1);
+        }
+        c0[jf] = a0;
+        c1[jf] = a1;
+      }
     }
-    double Q[NV], Qx[NV], Qy[NV], Qz[NV], r[NV], fl[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) Q[v] = LB[v * NL + qi];
-    const double rr = 1.0 / Q[0];
-    double amu = 1.0;
-    if (EV) amu = amu + chain<G>(br, muhg + g0, xs);  // EV_Prolong (Prolong_gtol.f90:7-51)
-    const double gdiag = gm[D * NL + qi];
-    if (D == 0) {
-      Qx[0] = c[0]; Qx[1] = c[1]; Qx[2] = c[2]; Qx[3] = c[3]; Qx[4] = c[4];
-      Qy[0] = c[5]; Qy[1] = c[6]; Qy[2] = c[7]; Qy[3] = 0.0; Qy[4] = 0.0;
-      Qz[0] = c[8]; Qz[1] = c[9]; Qz[3] = c[10]; Qz[2] = 0.0; Qz[4] = 0.0;
-      vis_flux_x(Q, rr, Qx, Qy, Qz, amu, P, fl);
-    } else if (D == 1) {
-      Qy[0] = c[0]; Qy[1] = c[1]; Qy[2] = c[2]; Qy[3] = c[3]; Qy[4] = c[4];
-      Qx[0] = c[5]; Qx[1] = c[6]; Qx[2] = c[7]; Qx[3] = 0.0; Qx[4] = 0.0;
-      Qz[0] = c[8]; Qz[2] = c[9]; Qz[3] = c[10]; Qz[1] = 0.0; Qz[4] = 0.0;
-      vis_flux_y(Q, rr, Qx, Qy, Qz, amu, P, fl);
-    } else {
-      Qz[0] = c[0]; Qz[1] = c[1]; Qz[2] = c[2]; Qz[3] = c[3]; Qz[4] = c[4];
-      Qx[0] = c[5]; Qx[1] = c[6]; Qx[3] = c[7]; Qx[2] = 0.0; Qx[4] = 0.0;
-      Qy[0] = c[8]; Qy[2] = c[9]; Qy[3] = c[10]; Qy[1] = 0.0; Qy[4] = 0.0;
-      vis_flux_z(Q, rr, Qx, Qy, Qz, amu, P, fl);
+    double mu0 = 0.0, mu1 = 0.0;
+    if (EV) {  // EV_Prolong (Prolong_gtol.f90:7-51)
+      mu0 = chain<G>(br0, muhg + g0, xs);
+      mu1 = chain<G>(br1, muhg + g0, xs);
     }
-#pragma unroll
-    for (int v = 0; v < NV; ++v) r[v] = gdiag * fl[v];
-    if (s == 0 || s == L - 1) {
-      const int fc = s == 0 ? face_lo(D) : face_hi(D);
-#pragma unroll
-      for (int v = 0; v < NV; ++v) VF[(fc - 1) * 5 * G2 + v * G2 + a + G * b] = r[v];
-    } else {
-      double fi[NV];
-      euler_flux(D, Q, rr, gamma, fi);
-#pragma unroll
-      for (int v = 0; v < NV; ++v) LB[v * NL + qi] = gdiag * fi[v] - ddiv(r[v], P.re, P.r_re);
-    }
+    vol_diag_point<G, D>(l0 + s0 * ls, s0, a, b, c0, EV ? 1.0 + mu0 : 1.0, P, gm, LB, VF);
+    if (two) vol_diag_point<G, D>(l0 + s1 * ls, s1, a, b, c1, EV ? 1.0 + mu1 : 1.0, P, gm, LB, VF);
   }
   __syncthreads();
   PHASE_MARK(3 + 3 * (2 - D));
