@@ -239,6 +239,17 @@ int revolve(Adj &A, int i, int j, int si, int sfree) {
 
 }  // namespace
 
+#ifdef DSEM_PHASE_TIMING
+extern "C" int dsem_debug_phase_cycles_adj(unsigned long long *out, int reset) {
+  cudaError_t e = cudaMemcpyFromSymbol(out, ::g_phase_cycles, sizeof(unsigned long long) * 32);
+  if (reset) {
+    unsigned long long z[32] = {};
+    cudaMemcpyToSymbol(::g_phase_cycles, z, sizeof(z));
+  }
+  return (int)e;
+}
+#endif
+
 extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int snapshots, double *J, double *dJdQ0,
                             int ldx, double *dJdinvRe, double *ms) {
   if (!c) return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "null context");

@@ -594,7 +594,8 @@ struct VolAdjArgs {
 
 template <int G> struct VolAdjCfg {
   static constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
-  static constexpr int NT = G >= 6 ? 384 : 256;  // one element per SM (shared memory); 12 warps at p >= 5
+  // one element per SM (shared memory); at least one thread per Lobatto point of a grid
+  static constexpr int NT = NL <= 256 ? 256 : ((NL + 31) / 32) * 32;
   static constexpr size_t NDBL = 5 * NG + 15 * NG + 15 * NG + 5 * NL + 5 * NL + 11 * NL + 5 * NG + 5 * NG + 30 * G2 +
                                  2 * G * L + NT;
   static constexpr size_t SMEM = sizeof(double) * NDBL;
@@ -629,19 +630,42 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
   const Phys P = A.P;
   const double gamma = P.gamma;
   double lr = 0.0;
+  long long t_ph_ = 0;
+#ifdef DSEM_PHASE_TIMING
+  t_ph_ = clock64();
+#endif
 
   for (int i = tid; i < L * G; i += NT) {
     Bm[i] = Op<G>::B(i / G, i % G);
     Dm[i] = Op<G>::D(i / L, i % L);
   }
-  for (int i = tid; i < 5 * NG; i += NT) {
-    q[i] = JQ[i] * jac[i % NG];
-    LAM[i] = A.LQT[(long long)k * 5 * NG + i];
-    LQ[i] = 0.0;
+  {  // state and dJ/dQt: all of a thread's loads in flight at once
+    constexpr int NQ = (5 * NG + NT - 1) / NT;
+    const double *lqt = A.LQT + (long long)k * 5 * NG;
+    double qv[NQ], jv[NQ], lv[NQ];
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) {
+      const int i = tid + j * NT;
+      if (i < 5 * NG) {
+        qv[j] = JQ[i];
+        jv[j] = jac[i % NG];
+        lv[j] = lqt[i];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) {
+      const int i = tid + j * NT;
+      if (i < 5 * NG) {
+        q[i] = qv[j] * jv[j];
+        LAM[i] = lv[j];
+        LQ[i] = 0.0;
+      }
+    }
   }
   for (int i = tid; i < 15 * NG; i += NT) LGR[i] = 0.0;
   for (int i = tid; i < 30 * G2; i += NT) LQFs[i] = 0.0;
   __syncthreads();
+  PHASE_MARK(21);
 
   // Lobatto arrays of grid D into LB (interior from q, faces from QF)
   auto build = [&](auto Dc) {
@@ -665,31 +689,44 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
     }
   };
 
-  // ---- forward: Gauss gradients of the five fields
-  auto grad_dir = [&](auto Dc) {
+  // ---- forward: Gauss gradients of the five fields, one task per (direction, field, line):
+  // the Lobatto line is built and differentiated in registers
+  auto grad_task = [&](auto Dc, int f, int ln) {
     constexpr int D = decltype(Dc)::value;
-    build(Dc);
-    __syncthreads();
     constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
-    for (int t = tid; t < 5 * G2; t += NT) {
-      const int f = t / G2, ln = t - f * G2, a = ln % G, b = ln / G;
-      const int p0 = gbase<G>(D, a, b), l0 = lbase<G>(D, a, b);
-      double y[L];
+    const int a = ln % G, b = ln / G;
+    const int p0 = gbase<G>(D, a, b);
+    double x[G], y[L];
 #pragma unroll
-      for (int s = 0; s < L; ++s) y[s] = LB[f * NL + l0 + s * xs];
+    for (int kk = 0; kk < G; ++kk) x[kk] = q[f * NG + p0 + kk * xs];
+    y[0] = QF[(face_lo(D) - 1) * 5 * G2 + f * G2 + ln];
+    y[L - 1] = QF[(face_hi(D) - 1) * 5 * G2 + f * G2 + ln];
 #pragma unroll
-      for (int kk = 0; kk < G; ++kk) {
-        double acc = Op<G>::D(kk, 0) * y[0];
+    for (int s = 1; s < L - 1; ++s) {
+      double acc = Op<G>::B(s, 0) * x[0];
 #pragma unroll
-        for (int s = 1; s < L; ++s) acc = __fma_rn(Op<G>::D(kk, s), y[s], acc);
-        GR[(f * 3 + D) * NG + p0 + kk * xs] = gg[D * NG + p0 + kk * xs] * acc;
-      }
+      for (int kk = 1; kk < G; ++kk) acc = __fma_rn(Op<G>::B(s, kk), x[kk], acc);
+      y[s] = acc;
     }
-    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < G; ++kk) {
+      double acc = Op<G>::D(kk, 0) * y[0];
+#pragma unroll
+      for (int s = 1; s < L; ++s) acc = __fma_rn(Op<G>::D(kk, s), y[s], acc);
+      GR[(f * 3 + D) * NG + p0 + kk * xs] = gg[D * NG + p0 + kk * xs] * acc;
+    }
   };
-  grad_dir(std::integral_constant<int, 0>{});
-  grad_dir(std::integral_constant<int, 1>{});
-  grad_dir(std::integral_constant<int, 2>{});
+  for (int t = tid; t < 15 * G2; t += NT) {
+    const int df = t / G2, ln = t - df * G2, D = df / 5, f = df - D * 5;
+    if (D == 0)
+      grad_task(std::integral_constant<int, 0>{}, f, ln);
+    else if (D == 1)
+      grad_task(std::integral_constant<int, 1>{}, f, ln);
+    else
+      grad_task(std::integral_constant<int, 2>{}, f, ln);
+  }
+  __syncthreads();
+  PHASE_MARK(22);
 
   // ---- enstrophy term (energydissipation.f90:19-78) on these gradients and the
   // JQ values of JQe: the gradient part goes to LGR; with direct_only the JQe
@@ -717,6 +754,7 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
     }
     __syncthreads();
   }
+  PHASE_MARK(23);
   if (A.direct_only) return;
 
   // ---- reverse of pass 2: fluxes and interior divergence, grid by grid
@@ -724,6 +762,7 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
     constexpr int D = decltype(Dc)::value;
     build(Dc);
     __syncthreads();
+    PHASE_MARK(26);
     constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
     for (int qi = tid; qi < NL; qi += NT) {
       int s, a, b;
@@ -797,6 +836,7 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
       }
     }
     __syncthreads();
+    PHASE_MARK(27);
     // transposed interpolations along the lines of D
     for (int t = tid; t < 16 * G2; t += NT) {
       const int j = t / G2, ln = t - j * G2, a = ln % G, b = ln / G;
@@ -834,6 +874,7 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
   flux_dir(std::integral_constant<int, 0>{});
   flux_dir(std::integral_constant<int, 1>{});
   flux_dir(std::integral_constant<int, 2>{});
+  PHASE_MARK(24);
 
   // ---- reverse of pass 1: gradients -> Lobatto arrays -> q and QF
   auto lob_dir = [&](auto Dc) {
@@ -868,6 +909,7 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
   lob_dir(std::integral_constant<int, 0>{});
   lob_dir(std::integral_constant<int, 1>{});
   lob_dir(std::integral_constant<int, 2>{});
+  PHASE_MARK(25);
 
   // ---- outputs
   for (int i = tid; i < 5 * NG; i += NT) LJQ[i] = jac[i % NG] * LQ[i];
