@@ -166,14 +166,16 @@ __device__ __forceinline__ void riemann(const double *nh, double ds, const doubl
                                         double *flux) {
   double rho = Ql[0], rhou = Ql[1], rhov = Ql[2], rhow = Ql[3], rhoe = Ql[4];
   double rhon = Qr[0], rhoun = Qr[1], rhovn = Qr[2], rhown = Qr[3], rhoen = Qr[4];
-  double ul = rhou / rho, vl = rhov / rho, wl = rhow / rho;
-  double pleft = (gamma - 1.0) * (rhoe - 0.5 / rho * (rhou * rhou + rhov * rhov + rhow * rhow));
-  double ur = rhoun / rhon, vr = rhovn / rhon, wr = rhown / rhon;
-  double pright = (gamma - 1.0) * (rhoen - 0.5 / rhon * (rhoun * rhoun + rhovn * rhovn + rhown * rhown));
+  const double rl = 1.0 / rho, rn = 1.0 / rhon;  // divisions by the densities: ddiv (correctly rounded)
+  double ul = ddiv(rhou, rho, rl), vl = ddiv(rhov, rho, rl), wl = ddiv(rhow, rho, rl);
+  double pleft = (gamma - 1.0) * (rhoe - ddiv(0.5, rho, rl) * (rhou * rhou + rhov * rhov + rhow * rhow));
+  double ur = ddiv(rhoun, rhon, rn), vr = ddiv(rhovn, rhon, rn), wr = ddiv(rhown, rhon, rn);
+  double pright = (gamma - 1.0) * (rhoen - ddiv(0.5, rhon, rn) * (rhoun * rhoun + rhovn * rhovn + rhown * rhown));
   double ql = nh[0] * ul + nh[1] * vl + nh[2] * wl;
   double qr = nh[0] * ur + nh[1] * vr + nh[2] * wr;
-  double hl = 0.5 * (ul * ul + vl * vl + wl * wl) + gamma / (gamma - 1.0) * pleft / rho;
-  double hr = 0.5 * (ur * ur + vr * vr + wr * wr) + gamma / (gamma - 1.0) * pright / rhon;
+  const double gg1 = gamma / (gamma - 1.0);
+  double hl = 0.5 * (ul * ul + vl * vl + wl * wl) + ddiv(gg1 * pleft, rho, rl);
+  double hr = 0.5 * (ur * ur + vr * vr + wr * wr) + ddiv(gg1 * pright, rhon, rn);
   double rtd = sqrt(rho * rhon);
   double betal = rho / (rho + rtd);
   double betar = 1.0 - betal;

@@ -159,11 +159,12 @@ __global__ void __launch_bounds__(128) k_face_vis(const MortarC *__restrict__ mc
   const int sp = si + G * sj;
   const long long g0 = (long long)M.geo * G2;
   const double nm_m = nrm[g0 + pt], nm_s = nrm[g0 + sp];
+  const double rm = 1.0 / nm_m, rs = 1.0 / nm_s;
   const bool neg_n = (M.flags >> 4) & 1, neg_s = (M.flags >> 3) & 1;
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
-    const double fv1 = VF[M.ms + v * G2 + pt] / nm_m;
-    const double fv2 = VF[M.ss + v * G2 + sp] / nm_s;
+    const double fv1 = ddiv(VF[M.ms + v * G2 + pt], nm_m, rm);
+    const double fv2 = ddiv(VF[M.ss + v * G2 + sp], nm_s, rs);
     const double Qs = neg_n ? -fv2 : fv2;
     const double qb = 0.5 * (fv1 + Qs) * nm_m;
     VF[M.ms + v * G2 + pt] = qb;
@@ -804,7 +805,23 @@ template <int G> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
     }
     if (A.dtc) cdt = A.crk * A.dtc[cs];
   }
-  for (int i = tid; i < 30 * G2; i += nt) FB[i] = FF[i] - ddiv(VF[i], re, rre);  // send_flux_to_faces_add
+  // send_flux_to_faces_add; four items per thread in flight (HBM latency)
+  for (int i0 = tid; i0 < 30 * G2; i0 += 4 * nt) {
+    double ff[4], vf[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * nt;
+      if (i < 30 * G2) {
+        ff[u] = FF[i];
+        vf[u] = VF[i];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * nt;
+      if (i < 30 * G2) FB[i] = ff[u] - ddiv(vf[u], re, rre);
+    }
+  }
   for (int i = tid; i < G; i += nt) {
     Dlo[i] = Op<G>::D(i, 0);
     Dhi[i] = Op<G>::D(i, L - 1);
@@ -815,11 +832,27 @@ template <int G> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
   const double *QTI = A.QTI + (long long)k * 5 * NG;
   const double *jac = A.jac + (long long)k * NG;
   bool bad = false;
-  for (int i = tid; i < 5 * NG; i += nt) {
+  constexpr int U = 2;  // items per thread with their loads in flight together
+  for (int i0 = tid; i0 < 5 * NG; i0 += U * nt) {
+    double qti[U], jq[U], gq[U], jc[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * nt;
+      if (i < 5 * NG) {
+        qti[u] = QTI[i];
+        jq[u] = JQ[i];
+        gq[u] = (A.update && !A.first) ? gQ[i] : 0.0;
+        jc[u] = jac[i % NG];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+    const int i = i0 + u * nt;
+    if (i >= 5 * NG) break;
     const int v = i / NG, p = i - v * NG;
     const int n = p % G, m = (p / G) % G, l = p / G2;
     const double *F = FB + v * G2;
-    double acc = QTI[i];
+    double acc = qti[u];
     acc = __fma_rn(Dlo[n], F[5 * 5 * G2 + m + G * l], acc);  // face 6 (x = 0)
     acc = __fma_rn(Dhi[n], F[3 * 5 * G2 + m + G * l], acc);  // face 4 (x = 1)
     acc = __fma_rn(Dlo[m], F[0 * 5 * G2 + n + G * l], acc);  // face 1 (y = 0)
@@ -829,15 +862,16 @@ template <int G> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
     const double Qt = -acc;
     if (!isfinite(Qt)) bad = true;
     if (A.Qt_out) A.Qt_out[(long long)k * 5 * NG + i] = Qt;
-    double q = JQ[i];
+    double q = jq[u];
     if (A.update) {  // updatea.f90:213-227
-      const double g0 = A.first ? 0.0 : gQ[i];
+      const double g0 = A.first ? 0.0 : gq[u];
       const double g = A.ark * g0 + Qt;
       q = q + cdt * g;
       gQ[i] = g;
       JQ[i] = q;
     }
-    QN[i] = q * jac[p];
+    QN[i] = q * jc[u];
+    }
   }
   if (bad) atomicOr(A.flag, 1);
   __syncthreads();
