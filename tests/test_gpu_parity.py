@@ -188,3 +188,31 @@ def test_cfg3_layout_small(oracle_mod):
     s.step(dt, 3)
     c.step(0.0, dt, 3)
     assert relmax(s.download(), c.get_q()) <= 1e-12
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 5, 6, 7, 8])
+def test_rhs_every_order(oracle_mod, p):
+    """Every supported order (ncg = 2..9), isotropic state."""
+    box = mesh.Box(2, 2, 2, p)
+    q = mesh.random_isotropic(box, seed=p, k0=2.0, mach_t=0.2)
+    s, c = _pair(oracle_mod, box, q, re=900.0)
+    g, o = s.rhs(), c.rhs()
+    assert np.isfinite(g).all()
+    assert np.array_equal(g, o)
+
+
+@pytest.mark.parametrize("dims,p", [((1, 1, 1), 4), ((3, 2, 1), 4), ((1, 4, 2), 3), ((5, 1, 1), 8)])
+def test_rhs_degenerate_and_anisotropic_boxes(oracle_mod, dims, p):
+    """One-element periodic box (every face its own neighbour) and boxes one
+    element thick in some directions."""
+    box = mesh.Box(*dims, p)
+    q = mesh.random_isotropic(box, seed=7, k0=1.0, mach_t=0.2)
+    s, c = _pair(oracle_mod, box, q, re=700.0)
+    g, o = s.rhs(), c.rhs()
+    assert np.isfinite(g).all()
+    assert np.array_equal(g, o)
+    # one step too
+    dt = 0.5 * mesh.dtcalc(box, q)
+    s.step(dt, 1)
+    c.step(0.0, dt, 1)
+    assert np.array_equal(s.download(), c.get_q())
