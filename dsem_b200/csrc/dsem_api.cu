@@ -244,6 +244,7 @@ int enqueue_stage(dsem_ctx *c, int kk, bool save, double *qt_out, long long *lau
     a.P = c->P;
     a.ecase = g.ecase;
     a.rec = c->d_rec;
+    a.nuhg = c->les ? g.nuhg : nullptr;
     CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::vol(a, g.nel, g.diag, mode, st); }));
     return DSEM_OK;
   });
@@ -313,6 +314,31 @@ int enqueue_ev(dsem_ctx *c, long long *launches) {
   return DSEM_OK;
 }
 
+// Smagorinsky viscosity from the last Fluxes call's gradients (tstep.f90:40-43)
+int enqueue_les(dsem_ctx *c, long long *launches) {
+  const int r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
+    auto &g = c->groups[j];
+    LesArgs a{};
+    a.JQ = c->JQ + g.q0;
+    a.sq = 5LL * g.G * g.G * g.G;
+    a.jac = g.jac;
+    a.hd = g.hd;
+    a.EVB = g.EVB;
+    a.nuhg = g.nuhg;
+    a.valid = c->grad_valid ? 1 : 0;
+    a.re = c->P.re;
+    a.cs = c->les_cs;
+    a.numax = c->les_numax;
+    a.ecase = g.ecase;
+    a.rec = c->d_rec;
+    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::les(a, g.nel, st); }));
+    return DSEM_OK;
+  });
+  if (r) return r;
+  *launches += (long long)c->groups.size();
+  return DSEM_OK;
+}
+
 int enqueue_traces(dsem_ctx *c, long long *launches) {
   const int r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
     auto &g = c->groups[j];
@@ -334,6 +360,10 @@ int enqueue_traces(dsem_ctx *c, long long *launches) {
 int enqueue_step(dsem_ctx *c, bool save_last, long long *launches) {
   if (c->shock) {
     int r = enqueue_ev(c, launches);
+    if (r) return r;
+  }
+  if (c->les) {
+    int r = enqueue_les(c, launches);
     if (r) return r;
   }
   for (int kk = 1; kk <= c->kord; ++kk) {
@@ -824,6 +854,7 @@ void dsem_destroy(dsem_ctx *c) {
     cudaFree(g.kew);
     cudaFree(g.int2ext);
     cudaFree(g.ecase);
+    cudaFree(g.nuhg);
   }
   cudaFree(c->d_rec);
   cudaFree(c->d_dtc);
@@ -918,11 +949,11 @@ int step_impl(dsem_ctx *c, int nsteps) {
   int r;
   if (!c->traces_valid && (r = enqueue_traces(c, &l))) return r;
   CK(cudaMemsetAsync(c->flag, 0, sizeof(int), c->st));
-  const bool save = c->shock || c->keep_grad;
+  const bool save = c->shock || c->keep_grad || c->les;
   long long per_step = 0;
-  // the first step of a run may need EV without valid gradients: run it eagerly
+  // the first step of a run may need EV / LES without valid gradients: run it eagerly
   CK(cudaEventRecord(c->e0, c->st));
-  if (nsteps > 0 && c->shock && !c->ev_grad_valid) {
+  if (nsteps > 0 && ((c->shock && !c->ev_grad_valid) || (c->les && !c->grad_valid))) {
     if ((r = enqueue_step(c, save, &per_step))) return r;
     c->ev_grad_valid = true;
     c->grad_valid = true;
@@ -930,7 +961,7 @@ int step_impl(dsem_ctx *c, int nsteps) {
   }
   long long launches = per_step;
   if (nsteps > 0) {
-    const int key = (save ? 1 : 0) | (c->ev_grad_valid ? 2 : 0);
+    const int key = (save ? 1 : 0) | (c->ev_grad_valid ? 2 : 0) | (c->grad_valid ? 4 : 0) | (c->les ? 8 : 0);
     if (!c->gexec || c->graph_key != key) {
       if (c->gexec) cudaGraphExecDestroy(c->gexec);
       c->gexec = nullptr;
@@ -1029,6 +1060,7 @@ int dsem_stage(dsem_ctx *c, double time, double dt, int kk, double *Qt, int ldx)
   if (!c->traces_valid && (r = enqueue_traces(c, &l))) return r;
   CK(cudaMemsetAsync(c->flag, 0, sizeof(int), c->st));
   if (kk == 1 && c->shock && (r = enqueue_ev(c, &l))) return r;
+  if (kk == 1 && c->les && (r = enqueue_les(c, &l))) return r;
   r = enqueue_stage(c, kk, true, Qt ? c->Qt : nullptr, &l);
   if (r) return r;
   c->grad_valid = true;
@@ -1126,6 +1158,48 @@ int dsem_get_muhg(dsem_ctx *c, double *mu, int ldx) {
     CK(cudaGetLastError());
   }
   CK(cudaMemcpyAsync(mu, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return DSEM_OK;
+}
+
+int dsem_set_les(dsem_ctx *c, double cs, double numax) {
+  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (!(cs >= 0.0) || !(numax >= 0.0)) return fail(c, DSEM_ERR_INVALID_ARG, "cs and numax must be >= 0");
+  if (cs > 0.0) {
+    for (auto &g : c->groups)
+      if (!g.diag) return fail(c, DSEM_ERR_UNSUPPORTED, "LES needs axis-aligned (diagonal-metric) elements");
+    for (auto &g : c->groups) {
+      if (!g.nuhg) {
+        const size_t n = (size_t)g.nel * g.G * g.G * g.G;
+        CK(cudaMalloc(&g.nuhg, n * sizeof(double)));
+        CK(cudaMemset(g.nuhg, 0, n * sizeof(double)));
+      }
+    }
+  }
+  c->les = cs > 0.0 ? 1 : 0;
+  c->les_cs = cs;
+  c->les_numax = numax;
+  if (c->gexec) {  // the captured step changes
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  return DSEM_OK;
+}
+
+int dsem_get_nut(dsem_ctx *c, double *nu, int ldx) {
+  if (!c || !nu) return fail(c, DSEM_ERR_INVALID_ARG, "null argument");
+  if (!c->les) return fail(c, DSEM_ERR_INVALID_ARG, "LES is off (dsem_set_les)");
+  int r = check_ldx(c, ldx);
+  if (r) return r;
+  r = ensure_stage_buf(c, ldx, 1);
+  if (r) return r;
+  const size_t n = (size_t)c->ngrid * ldx * ldx * ldx;
+  CK(cudaMemsetAsync(c->stage, 0, n * sizeof(double), c->st));
+  for (auto &g : c->groups) {
+    k_pack<<<g.nel, 256, 0, c->st>>>(g.nuhg, ldx, g.int2ext, 0, g.G, 1, c->stage, 0);
+    CK(cudaGetLastError());
+  }
+  CK(cudaMemcpyAsync(nu, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   return DSEM_OK;
 }

@@ -34,6 +34,7 @@ struct Group {
   long long f0 = 0;  // offset of the group's face slots (doubles)
   double *jac = nullptr, *gg = nullptr, *gm = nullptr, *hd = nullptr;
   double *muhg = nullptr, *EVB = nullptr, *kew = nullptr;
+  double *nuhg = nullptr;  // Smagorinsky viscosity at Gauss points (LES on)
   int *int2ext = nullptr;  // device: caller element id of each group element
   int *ecase = nullptr;    // device: case of each group element
   std::vector<int> case_lo, case_hi;  // group elements [lo, hi) of each case
@@ -58,6 +59,8 @@ struct dsem_ctx {
   int ngrid = 0, nmort = 0;
   Phys P{};
   int shock = 0, iord = 4, kord = 5;
+  int les = 0;                     // static Smagorinsky model (dsem_set_les)
+  double les_cs = 0.0, les_numax = 0.0;
   double ark[5] = {}, brk[5] = {}, crk[5] = {};
   std::vector<Group> groups;
   std::vector<MList> mlists;

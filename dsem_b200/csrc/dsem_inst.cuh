@@ -81,6 +81,12 @@ template <int G> cudaError_t Launch<G>::ev(const EvArgs &a, int nel, cudaStream_
   return cudaGetLastError();
 }
 
+template <int G> cudaError_t Launch<G>::les(const LesArgs &a, int nel, cudaStream_t s) {
+  if (nel <= 0) return cudaSuccess;
+  k_les<G><<<nel, 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
 template <int G>
 cudaError_t Launch<G>::face_inv(const MortarC *mc, int nm, double *QF, double *FF, const double *nh, const double *nrm,
                                 double gamma, cudaStream_t s) {

@@ -10,6 +10,7 @@ struct VolArgs;
 struct UpdArgs;
 struct TraceArgs;
 struct EvArgs;
+struct LesArgs;
 struct MortarC;
 
 // volume kernel variants: metric layout x entropy viscosity x saved gradients
@@ -23,6 +24,7 @@ template <int G> struct Launch {
   static cudaError_t update(const UpdArgs &a, int nel, cudaStream_t s);
   static cudaError_t trace(const TraceArgs &a, int nel, cudaStream_t s);
   static cudaError_t ev(const EvArgs &a, int nel, cudaStream_t s);
+  static cudaError_t les(const LesArgs &a, int nel, cudaStream_t s);
   static cudaError_t face_inv(const MortarC *mc, int nm, double *QF, double *FF, const double *nh, const double *nrm,
                               double gamma, cudaStream_t s);
   static cudaError_t face_vis(const MortarC *mc, int nm, double *VF, const double *nrm, cudaStream_t s);

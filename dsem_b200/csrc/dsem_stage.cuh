@@ -475,6 +475,7 @@ struct VolArgs {
   long long sq;
   const double *jac, *gg, *gm;  // metrics, layout per DIAG
   const double *muhg;           // [elem][G^3] entropy viscosity (EV)
+  const double *nuhg;           // [elem][G^3] Smagorinsky viscosity (LES; null: off)
   const double *QF;             // [elem][6][5][G^2] averaged face state
   double *VF;                   // [elem][6][5][G^2] out: viscous normal flux at faces
   double *QTI;                  // [elem][5][G^3]   out: interior divergence sum
@@ -933,6 +934,59 @@ template <int G> __global__ void __launch_bounds__(256) k_ev(EvArgs A) {
       out = m;
     }
     mu[p] = out;
+  }
+}
+
+// ------------------------------------------------------------------- LES
+struct LesArgs {
+  const double *JQ;
+  long long sq;
+  const double *jac, *hd, *EVB;
+  double *nuhg;
+  int valid;  // EVB holds the gradients of the last Fluxes call
+  double re, cs, numax;
+  const int *ecase;   // optional: case of each element (ensembles)
+  const double *rec;  // optional: per case {re, 1/re}
+};
+
+// Static Smagorinsky viscosity at Gauss points (simpleSmag and filteredStrain,
+// turbulence/staticSmago/staticSmag.f90:32-183): DSEM's rho = Q jacob(1,1,1)
+// and velocities Q(2..4)/rho are kept as written.
+template <int G> __global__ void __launch_bounds__(128) k_les(LesArgs A) {
+  constexpr int NG = G * G * G;
+  const int k = blockIdx.x;
+  const double *JQ = A.JQ + (long long)k * A.sq;
+  const double *jac = A.jac + (long long)k * NG;
+  const double *hd = A.hd + (long long)k * NG;
+  const double *E = A.EVB + (long long)k * 15 * NG;
+  double re = A.re;
+  if (A.rec) re = A.rec[2 * A.ecase[k]];
+  const double jac0 = jac[0];
+  for (int p = threadIdx.x; p < NG; p += blockDim.x) {
+    double gx[4] = {0.0, 0.0, 0.0, 0.0}, gy[4] = {0.0, 0.0, 0.0, 0.0}, gz[4] = {0.0, 0.0, 0.0, 0.0};
+    if (A.valid) {
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        gx[v] = E[(v * 3 + 0) * NG + p];
+        gy[v] = E[(v * 3 + 1) * NG + p];
+        gz[v] = E[(v * 3 + 2) * NG + p];
+      }
+    }
+    const double rho = JQ[p] * jac0;
+    const double u = JQ[NG + p] / rho, v = JQ[2 * NG + p] / rho, w = JQ[3 * NG + p] / rho;
+    const double rho_x = gx[0], rho_y = gy[0], rho_z = gz[0];
+    const double u_x = (gx[1] - rho_x * u) / rho, u_y = (gy[1] - rho_y * u) / rho, u_z = (gz[1] - rho_z * u) / rho;
+    const double v_x = (gx[2] - rho_x * v) / rho, v_y = (gy[2] - rho_y * v) / rho, v_z = (gz[2] - rho_z * v) / rho;
+    const double w_x = (gx[3] - rho_x * w) / rho, w_y = (gy[3] - rho_y * w) / rho, w_z = (gz[3] - rho_z * w) / rho;
+    const double S11 = u_x, S12 = 0.5 * (u_y + v_x), S13 = 0.5 * (u_z + w_x);
+    const double S21 = 0.5 * (v_x + u_y), S22 = v_y, S23 = 0.5 * (v_z + w_y);
+    const double S31 = 0.5 * (w_x + u_z), S32 = 0.5 * (w_y + v_z), S33 = w_z;
+    const double S = sqrt(2.0 * S11 * S11 + 2.0 * S12 * S12 + 2.0 * S13 * S13 + 2.0 * S21 * S21 + 2.0 * S22 * S22 +
+                          2.0 * S23 * S23 + 2.0 * S31 * S31 + 2.0 * S32 * S32 + 2.0 * S33 * S33);
+    const double dg = hd[p];
+    const double nu = re * (A.cs * dg) * (A.cs * dg) * S;
+    const double mx = nu >= 0.0 ? nu : 0.0;
+    A.nuhg[(long long)k * NG + p] = mx <= A.numax ? mx : A.numax;
   }
 }
 

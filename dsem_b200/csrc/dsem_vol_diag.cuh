@@ -136,12 +136,16 @@ __device__ __forceinline__ void vol_diag_tgrad(int ln, const double *WK, const d
 // viscous flux times gmet at face points goes to VF, the inviscid minus viscous
 // flux over Re overwrites the point's state slot in LB.
 template <int G, int D>
-__device__ __forceinline__ void vol_diag_point(int qi, int s, int a, int b, const double *c, double amu, const Phys &P,
-                                               const double *gm, double *LB, double *VF) {
+__device__ __forceinline__ void vol_diag_point(int qi, int s, int a, int b, const double *c, bool les, double nu,
+                                               bool ev, double mu, const Phys &P, const double *gm, double *LB,
+                                               double *VF) {
   constexpr int L = G + 1, G2 = G * G, NL = L * G * G;
   double Q[NV], Qx[NV], Qy[NV], Qz[NV], r[NV], fl[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) Q[v] = LB[v * NL + qi];
+  double amu = 1.0;  // Vis_Fluxes_new.f90:123-125
+  if (les) amu = amu + nu * Q[0];
+  if (ev) amu = amu + mu;
   const double rr = 1.0 / Q[0];
   const double gdiag = gm[D * NL + qi];
   if (D == 0) {
@@ -179,6 +183,7 @@ __device__ __forceinline__ void vol_diag_point(int qi, int s, int a, int b, cons
 template <int G, bool EV, int SAVE, int D>
 __device__ __forceinline__ void vol_diag_dir(const VolArgs &A, const Phys &P, const double *JQ, const double *jac,
                                              const double *QF, const double *gg, const double *gm, const double *muhg,
+                                             const double *nuhg,
                                              const double *GR, double *LB, double *T4, const double *Bm,
                                              const double *Dm, double *VF, double *QTI, int tid, long long &t_ph_) {
   using C = VolDiagCfg<G, EV, SAVE>;
@@ -259,13 +264,20 @@ __device__ __forceinline__ void vol_diag_dir(const VolArgs &A, const Phys &P, co
         c1[jf] = a1;
       }
     }
-    double mu0 = 0.0, mu1 = 0.0;
+    double mu0 = 0.0, mu1 = 0.0, nu0 = 0.0, nu1 = 0.0;
     if (EV) {  // EV_Prolong (Prolong_gtol.f90:7-51)
       mu0 = chain<G>(br0, muhg + g0, xs);
       mu1 = chain<G>(br1, muhg + g0, xs);
     }
-    vol_diag_point<G, D>(l0 + s0 * ls, s0, a, b, c0, EV ? 1.0 + mu0 : 1.0, P, gm, LB, VF);
-    if (two) vol_diag_point<G, D>(l0 + s1 * ls, s1, a, b, c1, EV ? 1.0 + mu1 : 1.0, P, gm, LB, VF);
+    const bool les = nuhg != nullptr;
+    if (les) {  // nut_prolong (staticSmag.f90:206-261): negative values clipped to 0
+      nu0 = chain<G>(br0, nuhg + g0, xs);
+      nu1 = chain<G>(br1, nuhg + g0, xs);
+      if (nu0 < 0.0) nu0 = 0.0;
+      if (nu1 < 0.0) nu1 = 0.0;
+    }
+    vol_diag_point<G, D>(l0 + s0 * ls, s0, a, b, c0, les, nu0, EV, mu0, P, gm, LB, VF);
+    if (two) vol_diag_point<G, D>(l0 + s1 * ls, s1, a, b, c1, les, nu1, EV, mu1, P, gm, LB, VF);
   }
   __syncthreads();
   PHASE_MARK(3 + 3 * (2 - D));
@@ -322,6 +334,7 @@ __global__ void __launch_bounds__(VolDiagCfg<G, EV, SAVE>::NT, VolDiagCfg<G, EV,
   const double *gg = A.gg + (long long)k * 3 * NG;
   const double *gm = A.gm + (long long)k * 3 * NL;
   const double *muhg = EV ? A.muhg + (long long)k * NG : nullptr;
+  const double *nuhg = A.nuhg ? A.nuhg + (long long)k * NG : nullptr;
   double *EVB = SAVE ? A.EVB + (long long)k * 15 * NG : nullptr;
   const double gamma = A.P.gamma;
   Phys P = A.P;
@@ -390,9 +403,9 @@ __global__ void __launch_bounds__(VolDiagCfg<G, EV, SAVE>::NT, VolDiagCfg<G, EV,
 
   // ---- pass 2: z, y, x
   double *QTI = A.QTI + (long long)k * 5 * NG;
-  vol_diag_dir<G, EV, SAVE, 2>(A, P, JQ, jac, QF, gg, gm, muhg, GR, LB, T4, Bm, Dm, VF, QTI, tid, t_ph_);
-  vol_diag_dir<G, EV, SAVE, 1>(A, P, JQ, jac, QF, gg, gm, muhg, GR, LB, T4, Bm, Dm, VF, QTI, tid, t_ph_);
-  vol_diag_dir<G, EV, SAVE, 0>(A, P, JQ, jac, QF, gg, gm, muhg, GR, LB, T4, Bm, Dm, VF, QTI, tid, t_ph_);
+  vol_diag_dir<G, EV, SAVE, 2>(A, P, JQ, jac, QF, gg, gm, muhg, nuhg, GR, LB, T4, Bm, Dm, VF, QTI, tid, t_ph_);
+  vol_diag_dir<G, EV, SAVE, 1>(A, P, JQ, jac, QF, gg, gm, muhg, nuhg, GR, LB, T4, Bm, Dm, VF, QTI, tid, t_ph_);
+  vol_diag_dir<G, EV, SAVE, 0>(A, P, JQ, jac, QF, gg, gm, muhg, nuhg, GR, LB, T4, Bm, Dm, VF, QTI, tid, t_ph_);
   PHASE_MARK(20);
 }
 

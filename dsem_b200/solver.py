@@ -18,7 +18,7 @@ ERRORS = {-1: "INVALID_ARG", -2: "CUDA", -3: "NONFINITE", -4: "TIMEOUT", -5: "UN
 EXPORTS = ("dsem_create", "dsem_destroy", "dsem_last_error", "dsem_upload_q", "dsem_download_q", "dsem_step",
            "dsem_stage", "dsem_rhs", "dsem_diag", "dsem_get_muhg", "dsem_last_timing", "dsem_profile_rhs",
            "dsem_create_batch", "dsem_batch_size", "dsem_upload_q_case", "dsem_download_q_case", "dsem_step_batch",
-           "dsem_diag_batch", "dsem_adjoint")
+           "dsem_diag_batch", "dsem_adjoint", "dsem_set_les", "dsem_get_nut")
 
 
 class DsemError(RuntimeError):
@@ -71,6 +71,8 @@ def lib(path=None):
         L.dsem_download_q_case.argtypes = [vp, C.c_int, dp, C.c_int]
         L.dsem_step_batch.argtypes = [vp, dp, C.c_int]
         L.dsem_diag_batch.argtypes = [vp, dp, C.c_int, dp, dp, dp]
+        L.dsem_set_les.argtypes = [vp, C.c_double, C.c_double]
+        L.dsem_get_nut.argtypes = [vp, dp, C.c_int]
         L.dsem_adjoint.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.c_int, dp, dp, C.c_int, dp, dp]
         _lib = L
     return _lib
@@ -164,6 +166,15 @@ class Solver:
         ms = np.zeros(4)
         self._check(lib().dsem_profile_rhs(self.h, int(reps), _dptr(ms)))
         return ms
+
+    def set_les(self, cs, numax):
+        """Static Smagorinsky model (cs = 0: off)."""
+        self._check(lib().dsem_set_les(self.h, float(cs), float(numax)))
+
+    def nut(self):
+        m = np.zeros((self.ngrid, self.ldx, self.ldx, self.ldx))
+        self._check(lib().dsem_get_nut(self.h, _dptr(m), self.ldx))
+        return m
 
     def adjoint(self, dt, nsteps, window, snapshots=0, want_grad=True):
         """J = sum of eps*dt over the last `window` of `nsteps` steps and its

@@ -119,6 +119,19 @@ int dsem_last_timing(const dsem_ctx *ctx, double *ms, long long *launches);
  * volume, viscous face, divergence + update}.  The state is left unchanged. */
 int dsem_profile_rhs(dsem_ctx *ctx, int reps, double *ms);
 
+/* Static Smagorinsky LES (tstep.f90:40-43, turbulence/staticSmago/staticSmag.f90):
+ * at the start of every step the subgrid viscosity
+ *   nu_t = Re (C_s delta_g)^2 |S|, clipped to [0, numax],
+ * is formed at Gauss points from the gradients of the previous step's last
+ * stage (zero before the first), prolonged to the Lobatto grids (negatives
+ * set to 0) and added to the viscosity as amu = 1 + nu_t rho (+ mu_EV)
+ * (Vis_Fluxes_new.f90:123-125).  cs = 0 turns it off.  DSEM's input keywords:
+ * `smagorinsky`, C_s, numax; its shock and density sensors are not supported.
+ * Axis-aligned elements only (DSEM_ERR_UNSUPPORTED otherwise). */
+int dsem_set_les(dsem_ctx *ctx, double cs, double numax);
+/* nu_t at Gauss points after the last evaluation (ldx layout, one field). */
+int dsem_get_nut(dsem_ctx *ctx, double *nu, int ldx);
+
 /* ---- Ensembles: ncase independent runs in one context ----
  * No DSEM counterpart (DSEM runs one case per job; each would call tstep,
  * tstep.f90:12, from its own time loop, 3DDriver_parfmdf.f90:466).  The

@@ -279,7 +279,7 @@ template <class T> struct Elem {
   int orientation[6] = {};
   bool boundary[6] = {};
   std::vector<double> jacob, gmetg, gmet[3], xg, hdelta;
-  std::vector<T> Q, gQ, QL[3], F[3], R[3], muhg, muh[3];
+  std::vector<T> Q, gQ, QL[3], F[3], R[3], muhg, muh[3], nutg, nut[3];
   size_t ng() const { return (size_t)G * G * G; }
   size_t nl() const { return (size_t)L * G * G; }
 };
@@ -301,6 +301,8 @@ template <class T> struct Case {
   std::vector<Mortar<T>> mo;
   double gamma = 1.4, re = 1600.0, pr = 0.72, mach = 1.0, cmu = 0.0, mumax = 0.0;
   bool shock = false, ducros = false;
+  bool les = false;               // static Smagorinsky (staticSmag.f90)
+  double cs = 0.0, numax = 0.0;  // C_s, numax
   int iord = 4, kord = 5;
   double ark[5] = {}, brk[5] = {}, crk[5] = {};
   bool ql_valid = false;
@@ -763,7 +765,8 @@ template <class T> void vis_element(Case<T> &c, Elem<T> &E) {
             Qy[v] = gi[(v * 3 + 1) * nl + p];
             Qz[v] = gi[(v * 3 + 2) * nl + p];
           }
-          T amu = T(1.0);
+          T amu = T(1.0);  // Vis_Fluxes_new.f90:123-125
+          if (c.les) amu = amu + E.nut[d][p] * Qv[0];
           if (c.shock) amu = amu + E.muh[d][p];
           vis_fluxes(Qv, Qx, Qy, Qz, amu, c.gamma, c.pr, c.mach, f, g, h);
           const double *gm = &E.gmet[d][p * 3];
@@ -977,6 +980,55 @@ template <class T> void entropy(Case<T> &c) {
   }
 }
 
+// Static Smagorinsky viscosity (simpleSmag, turbulence/staticSmago/staticSmag.f90:32-118,
+// filteredStrain :126-183, delta_g :191-201) from the last Fluxes call's Lobatto
+// arrays, and nut_prolong (:206-261).  DSEM forms rho from jacob(1,1,1) of the
+// element and the velocities from d%Q without the Jacobian; both kept.
+template <class T> void smagorinsky(Case<T> &c) {
+  const int ne = (int)c.el.size();
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int e = 0; e < ne; ++e) {
+    Elem<T> &E = c.el[e];
+    const Ops &o = ops_for(E.G);
+    const int G = E.G, L = E.L;
+    const size_t ng = E.ng(), nl = E.nl();
+    std::vector<T> gq((size_t)4 * 3 * ng, T(0.0));
+    if (c.ql_valid) {
+      const T *w3[3] = {E.QL[0].data(), E.QL[1].data(), E.QL[2].data()};
+      gauss_deriv(E, o, w3, 4, gq);
+    }
+    E.nutg.assign(ng, T(0.0));
+    for (size_t p = 0; p < ng; ++p) {
+      auto Qx = [&](int v) { return gq[(v * 3 + 0) * ng + p]; };
+      auto Qy = [&](int v) { return gq[(v * 3 + 1) * ng + p]; };
+      auto Qz = [&](int v) { return gq[(v * 3 + 2) * ng + p]; };
+      T rho = E.Q[p] * E.jacob[0];
+      T u = E.Q[ng + p] / rho, v = E.Q[2 * ng + p] / rho, w = E.Q[3 * ng + p] / rho;
+      T rho_x = Qx(0), rho_y = Qy(0), rho_z = Qz(0);
+      T u_x = (Qx(1) - rho_x * u) / rho, u_y = (Qy(1) - rho_y * u) / rho, u_z = (Qz(1) - rho_z * u) / rho;
+      T v_x = (Qx(2) - rho_x * v) / rho, v_y = (Qy(2) - rho_y * v) / rho, v_z = (Qz(2) - rho_z * v) / rho;
+      T w_x = (Qx(3) - rho_x * w) / rho, w_y = (Qy(3) - rho_y * w) / rho, w_z = (Qz(3) - rho_z * w) / rho;
+      T S11 = u_x, S12 = 0.5 * (u_y + v_x), S13 = 0.5 * (u_z + w_x);
+      T S21 = 0.5 * (v_x + u_y), S22 = v_y, S23 = 0.5 * (v_z + w_y);
+      T S31 = 0.5 * (w_x + u_z), S32 = 0.5 * (w_y + v_z), S33 = w_z;
+      T S = std::sqrt(2.0 * S11 * S11 + 2.0 * S12 * S12 + 2.0 * S13 * S13 + 2.0 * S21 * S21 + 2.0 * S22 * S22 +
+                      2.0 * S23 * S23 + 2.0 * S31 * S31 + 2.0 * S32 * S32 + 2.0 * S33 * S33);
+      const double dg = E.hdelta[p];
+      T nu = c.re * (c.cs * dg) * (c.cs * dg) * S;
+      E.nutg[p] = rmin(rmax(nu, T(0.0)), T(c.numax));
+    }
+    const int eg[3] = {G, G, G};
+    for (int d = 0; d < 3; ++d) {
+      int el[3];
+      grid_ext(d, G, L, el);
+      E.nut[d].resize(nl);
+      contract(d, o.bx.data(), L, G, E.nutg.data(), eg, E.nut[d].data(), el);
+      for (auto &x : E.nut[d])
+        if (re_(x) < 0.0) x = T(0.0);
+    }
+  }
+}
+
 // ----------------------------------------------------------------- stage
 template <class T> double update_all(Case<T> &c, double dt, int kk, double *Qt_out, int ldx) {
   const int ne = (int)c.el.size();
@@ -1016,6 +1068,7 @@ template <class T> double update_all(Case<T> &c, double dt, int kk, double *Qt_o
 template <class T> int stage(Case<T> &c, double time, double dt, int kk, double *Qt, int ldx) {
   if (kk == 1) {
     if (c.shock) entropy(c);
+    if (c.les) smagorinsky(c);
     for (auto &E : c.el) std::fill(E.gQ.begin(), E.gQ.end(), T(0.0));
   }
   (void)time;
@@ -1702,8 +1755,10 @@ template <class T> Case<T> *convert_case(const Case<double> &c) {
       B.F[d] = cv(A.F[d]);
       B.R[d] = cv(A.R[d]);
       B.muh[d] = cv(A.muh[d]);
+      B.nut[d] = cv(A.nut[d]);
     }
     B.muhg = cv(A.muhg);
+    B.nutg = cv(A.nutg);
   }
   o->mo.resize(c.mo.size());
   for (size_t j = 0; j < c.mo.size(); ++j) {
@@ -1738,6 +1793,9 @@ template <class T> Case<T> *convert_case(const Case<double> &c) {
   o->mumax = c.mumax;
   o->shock = c.shock;
   o->ducros = c.ducros;
+  o->les = c.les;
+  o->cs = c.cs;
+  o->numax = c.numax;
   o->iord = c.iord;
   o->kord = c.kord;
   std::memcpy(o->ark, c.ark, sizeof(c.ark));
@@ -1923,6 +1981,27 @@ void orc_objective_cs(const orc_case *h, double dt, int nsteps, int window, cons
   *J = Jc.real();
   *dJ = hstep != 0.0 ? Jc.imag() / hstep : 0.0;
   delete cc;
+}
+void orc_set_les(orc_case *h, double cs, double numax) {
+  auto &c = *h->c;
+  c.les = cs > 0.0;
+  c.cs = cs;
+  c.numax = numax;
+  for (auto &E : c.el) {
+    E.nutg.assign(E.ng(), 0.0);
+    for (int d = 0; d < 3; ++d) E.nut[d].assign(E.nl(), 0.0);
+  }
+}
+void orc_get_nut(const orc_case *h, double *nu, int ldx) {
+  for (size_t e = 0; e < h->c->el.size(); ++e) {
+    const auto &E = h->c->el[e];
+    const int G = E.G;
+    for (int l = 0; l < G; ++l)
+      for (int m = 0; m < G; ++m)
+        for (int n = 0; n < G; ++n)
+          nu[e * (size_t)ldx * ldx * ldx + n + (size_t)ldx * (m + (size_t)ldx * l)] =
+              E.nutg.empty() ? 0.0 : E.nutg[gidx(G, n, m, l)];
+  }
 }
 void orc_rk(const orc_case *h, double *a, double *b, double *c) {
   for (int i = 0; i < 5; ++i) {

@@ -86,6 +86,11 @@ void orc_euler(const double *Q, double gamma, double *f, double *g, double *h);
 void orc_vis(const double *Q, const double *Qx, const double *Qy, const double *Qz, double amu, double gamma,
              double pr, double mach, double *f, double *g, double *h);
 void orc_rk(const orc_case *c, double *ark, double *brk, double *crk);
+/* Static Smagorinsky LES (staticSmag.f90) with coefficient cs (0: off) and
+ * clip numax; evaluated at the start of each step like the entropy viscosity.
+ * orc_get_nut: its Gauss-point viscosity after the last evaluation. */
+void orc_set_les(orc_case *c, double cs, double numax);
+void orc_get_nut(const orc_case *c, double *nu, int ldx);
 /* Objective of the adjoint, J = sum over the last `window` of `nsteps` steps of
  * dt * enst (orc_diag's enstrophy dissipation after each step), evaluated from
  * the current state + i*hstep*dq in complex arithmetic: *J = Re J and

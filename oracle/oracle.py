@@ -59,6 +59,8 @@ def lib():
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_set_threads.restype = C.c_int
         L.orc_rk.argtypes = [vp, _dp, _dp, _dp]
+        L.orc_set_les.argtypes = [vp, C.c_double, C.c_double]
+        L.orc_get_nut.argtypes = [vp, _dp, C.c_int]
         L.orc_objective_cs.argtypes = [vp, C.c_double, C.c_int, C.c_int, vp, C.c_double, C.c_int,
                                        C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_riemann.argtypes = [_dp, C.c_double, _dp, _dp, C.c_double, _dp]
@@ -201,6 +203,14 @@ class Case:
 
     def kord(self):
         return lib().orc_kord(self.h)
+
+    def set_les(self, cs, numax):
+        lib().orc_set_les(self.h, float(cs), float(numax))
+
+    def nut(self):
+        m = np.zeros((self.nel, self.ldx, self.ldx, self.ldx))
+        lib().orc_get_nut(self.h, m.ravel(), self.ldx)
+        return m
 
     def objective_cs(self, dt, nsteps, window, dq=None, h=1e-30):
         """(J, dJ/dJQ . dq) of J = sum over the last `window` steps of dt * eps,
