@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 #include <algorithm>
 #include <map>
@@ -1200,6 +1201,112 @@ int dsem_get_nut(dsem_ctx *c, double *nu, int ldx) {
     CK(cudaGetLastError());
   }
   CK(cudaMemcpyAsync(nu, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return DSEM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+// Snapshot layout: header, then JQ (internal order), then the saved gradients
+// of every group when they are valid.  The header pins the mesh layout.
+struct StateHeader {
+  char magic[8];
+  long long version, ngrid, nmort, ncase, ngroups, nq, nevb, flags;
+  long long layout;  // hash of the groups' (order, element count)
+  double prestep[1];  // ncase values follow in the blob (prestep[0] is the first)
+};
+long long layout_hash(const dsem_ctx *c) {
+  unsigned long long h = 1469598103934665603ULL;
+  auto mix = [&](long long v) {
+    h ^= (unsigned long long)v;
+    h *= 1099511628211ULL;
+  };
+  for (const auto &g : c->groups) {
+    mix(g.G);
+    mix(g.nel);
+    mix(g.diag);
+  }
+  mix(c->nmort);
+  return (long long)h;
+}
+long long evb_doubles(const dsem_ctx *c) {
+  long long n = 0;
+  for (const auto &g : c->groups) n += 15LL * g.nel * g.G * g.G * g.G;
+  return n;
+}
+long long state_bytes(const dsem_ctx *c) {
+  return (long long)sizeof(StateHeader) + (long long)sizeof(double) * (c->ncase - 1) +
+         (long long)sizeof(double) * ((long long)c->nq + evb_doubles(c));
+}
+}  // namespace
+
+extern "C" {
+
+int dsem_state_size(const dsem_ctx *c, long long *nbytes) {
+  if (!c || !nbytes) return DSEM_ERR_INVALID_ARG;
+  *nbytes = state_bytes(c);
+  return DSEM_OK;
+}
+
+int dsem_save_state(dsem_ctx *c, void *buf, long long nbytes) {
+  if (!c || !buf) return fail(c, DSEM_ERR_INVALID_ARG, "null argument");
+  if (nbytes < state_bytes(c)) return fail(c, DSEM_ERR_INVALID_ARG, "buffer smaller than dsem_state_size");
+  StateHeader h{};
+  std::memcpy(h.magic, "DSEMSTAT", 8);
+  h.version = 1;
+  h.ngrid = c->ngrid;
+  h.nmort = c->nmort;
+  h.ncase = c->ncase;
+  h.ngroups = (long long)c->groups.size();
+  h.nq = (long long)c->nq;
+  h.nevb = evb_doubles(c);
+  h.flags = (c->grad_valid ? 1 : 0) | (c->ev_grad_valid ? 2 : 0) | (c->keep_grad ? 4 : 0);
+  h.layout = layout_hash(c);
+  char *out = (char *)buf;
+  std::memcpy(out, &h, sizeof(h) - sizeof(double));
+  double *pre = (double *)(out + offsetof(StateHeader, prestep));
+  for (int k = 0; k < c->ncase; ++k) pre[k] = c->case_prestep[k];
+  double *data = pre + c->ncase;
+  CK(cudaMemcpyAsync(data, c->JQ, c->nq * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  data += c->nq;
+  for (auto &g : c->groups) {
+    const size_t n = 15ULL * g.nel * g.G * g.G * g.G;
+    CK(cudaMemcpyAsync(data, g.EVB, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    data += n;
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return DSEM_OK;
+}
+
+int dsem_load_state(dsem_ctx *c, const void *buf, long long nbytes) {
+  if (!c || !buf) return fail(c, DSEM_ERR_INVALID_ARG, "null argument");
+  if (nbytes < (long long)sizeof(StateHeader)) return fail(c, DSEM_ERR_INVALID_ARG, "snapshot too short");
+  StateHeader h{};
+  std::memcpy(&h, buf, sizeof(h) - sizeof(double));
+  if (std::memcmp(h.magic, "DSEMSTAT", 8) != 0 || h.version != 1)
+    return fail(c, DSEM_ERR_INVALID_ARG, "not a dsem state snapshot (version 1)");
+  if (h.ngrid != c->ngrid || h.nmort != c->nmort || h.ncase != c->ncase || h.nq != (long long)c->nq ||
+      h.ngroups != (long long)c->groups.size() || h.nevb != evb_doubles(c) || h.layout != layout_hash(c))
+    return fail(c, DSEM_ERR_INVALID_ARG, "snapshot was taken on a different mesh");
+  if (nbytes < state_bytes(c)) return fail(c, DSEM_ERR_INVALID_ARG, "snapshot truncated");
+  const char *in = (const char *)buf;
+  const double *pre = (const double *)(in + offsetof(StateHeader, prestep));
+  for (int k = 0; k < c->ncase; ++k) c->case_prestep[k] = pre[k];
+  const double *data = pre + c->ncase;
+  CK(cudaMemcpyAsync(c->JQ, data, c->nq * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  data += c->nq;
+  for (auto &g : c->groups) {
+    const size_t n = 15ULL * g.nel * g.G * g.G * g.G;
+    CK(cudaMemcpyAsync(g.EVB, data, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    data += n;
+  }
+  c->grad_valid = (h.flags & 1) != 0;
+  c->ev_grad_valid = (h.flags & 2) != 0;
+  c->keep_grad = (h.flags & 4) ? 1 : 0;
+  long long l = 0;
+  int r = enqueue_traces(c, &l);
+  if (r) return r;
   CK(cudaStreamSynchronize(c->st));
   return DSEM_OK;
 }

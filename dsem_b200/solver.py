@@ -18,7 +18,8 @@ ERRORS = {-1: "INVALID_ARG", -2: "CUDA", -3: "NONFINITE", -4: "TIMEOUT", -5: "UN
 EXPORTS = ("dsem_create", "dsem_destroy", "dsem_last_error", "dsem_upload_q", "dsem_download_q", "dsem_step",
            "dsem_stage", "dsem_rhs", "dsem_diag", "dsem_get_muhg", "dsem_last_timing", "dsem_profile_rhs",
            "dsem_create_batch", "dsem_batch_size", "dsem_upload_q_case", "dsem_download_q_case", "dsem_step_batch",
-           "dsem_diag_batch", "dsem_adjoint", "dsem_set_les", "dsem_get_nut")
+           "dsem_diag_batch", "dsem_adjoint", "dsem_set_les", "dsem_get_nut", "dsem_state_size",
+           "dsem_save_state", "dsem_load_state")
 
 
 class DsemError(RuntimeError):
@@ -72,6 +73,9 @@ def lib(path=None):
         L.dsem_step_batch.argtypes = [vp, dp, C.c_int]
         L.dsem_diag_batch.argtypes = [vp, dp, C.c_int, dp, dp, dp]
         L.dsem_set_les.argtypes = [vp, C.c_double, C.c_double]
+        L.dsem_state_size.argtypes = [vp, C.POINTER(C.c_longlong)]
+        L.dsem_save_state.argtypes = [vp, C.c_void_p, C.c_longlong]
+        L.dsem_load_state.argtypes = [vp, C.c_void_p, C.c_longlong]
         L.dsem_get_nut.argtypes = [vp, dp, C.c_int]
         L.dsem_adjoint.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.c_int, dp, dp, C.c_int, dp, dp]
         _lib = L
@@ -166,6 +170,18 @@ class Solver:
         ms = np.zeros(4)
         self._check(lib().dsem_profile_rhs(self.h, int(reps), _dptr(ms)))
         return ms
+
+    def save_state(self):
+        """Snapshot of the device state (bytes) for dsem_load_state."""
+        n = C.c_longlong()
+        self._check(lib().dsem_state_size(self.h, C.byref(n)))
+        buf = np.zeros(n.value, dtype=np.uint8)
+        self._check(lib().dsem_save_state(self.h, buf.ctypes.data_as(C.c_void_p), n.value))
+        return buf
+
+    def load_state(self, buf):
+        buf = np.ascontiguousarray(buf, dtype=np.uint8)
+        self._check(lib().dsem_load_state(self.h, buf.ctypes.data_as(C.c_void_p), buf.size))
 
     def set_les(self, cs, numax):
         """Static Smagorinsky model (cs = 0: off)."""

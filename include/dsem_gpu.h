@@ -132,6 +132,17 @@ int dsem_set_les(dsem_ctx *ctx, double cs, double numax);
 /* nu_t at Gauss points after the last evaluation (ldx layout, one field). */
 int dsem_get_nut(dsem_ctx *ctx, double *nu, int ldx);
 
+/* Checkpoint / resume of the device state (the solver-side part of DSEM's
+ * write_restart / read_restart, Statistics/dongru/restart.f90:14-310, which
+ * store d%Q and the Lobatto arrays d%Qlgg.. that entropy viscosity reads on
+ * the next step).  The snapshot holds JQ, the last stage's gradients and the
+ * diagnostics' previous kinetic energy, in the library's own versioned
+ * layout; it loads only into a context built on the same mesh, and a run
+ * resumed from it continues bit for bit. */
+int dsem_state_size(const dsem_ctx *ctx, long long *nbytes);
+int dsem_save_state(dsem_ctx *ctx, void *buf, long long nbytes);
+int dsem_load_state(dsem_ctx *ctx, const void *buf, long long nbytes);
+
 /* ---- Ensembles: ncase independent runs in one context ----
  * No DSEM counterpart (DSEM runs one case per job; each would call tstep,
  * tstep.f90:12, from its own time loop, 3DDriver_parfmdf.f90:466).  The
