@@ -208,10 +208,10 @@ int vol_mode(const dsem_ctx *c, bool save) {
   return save ? VOL_SAVE : VOL_PLAIN;
 }
 
-// One evaluation of Fluxes and the flux divergence, plus the update when kk > 0.
-// The update reads dt per case from d_dtc (written before the stage is enqueued
-// or the graph replayed).
-int enqueue_stage(dsem_ctx *c, int kk, bool save, double *qt_out, long long *launches) {
+// The four parts of one evaluation of Fluxes + the flux divergence (+ the
+// update when kk > 0).  The update reads dt per case from d_dtc (written before
+// the stage is enqueued or the graph replayed).
+int enqueue_face_inv(dsem_ctx *c, long long *launches) {
   const double gamma = c->P.gamma;
   const size_t nml = c->mlists.size(), nfj = nml + (c->nnc > 0 ? 1 : 0);
   int r = fork_jobs(c, nfj, [&](size_t j, cudaStream_t st) -> int {
@@ -228,8 +228,19 @@ int enqueue_stage(dsem_ctx *c, int kk, bool save, double *qt_out, long long *lau
   });
   if (r) return r;
   *launches += (long long)nfj;
+  if (c->ncut > 0) {
+    CK(with_G(c->cut_G, [&](auto g) {
+      return Launch<decltype(g)::value>::face_inv_cut(c->cut, c->ncut, c->QF, c->FF, c->ghost, c->cut_nh, c->cut_nrm,
+                                                      gamma, c->st);
+    }));
+    ++*launches;
+  }
+  return DSEM_OK;
+}
+
+int enqueue_vol(dsem_ctx *c, bool save, long long *launches) {
   const int mode = vol_mode(c, save);
-  r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
+  int r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
     auto &g = c->groups[j];
     VolArgs a{};
     a.JQ = c->JQ + g.q0;
@@ -251,7 +262,12 @@ int enqueue_stage(dsem_ctx *c, int kk, bool save, double *qt_out, long long *lau
   });
   if (r) return r;
   *launches += (long long)c->groups.size();
-  r = fork_jobs(c, nfj, [&](size_t j, cudaStream_t st) -> int {
+  return DSEM_OK;
+}
+
+int enqueue_face_vis(dsem_ctx *c, long long *launches) {
+  const size_t nml = c->mlists.size(), nfj = nml + (c->nnc > 0 ? 1 : 0);
+  int r = fork_jobs(c, nfj, [&](size_t j, cudaStream_t st) -> int {
     if (j < nml) {
       auto &ml = c->mlists[j];
       CK(with_G(ml.G, [&](auto g) { return Launch<decltype(g)::value>::face_vis(ml.mc, ml.n, c->VF, ml.nrm, st); }));
@@ -263,7 +279,17 @@ int enqueue_stage(dsem_ctx *c, int kk, bool save, double *qt_out, long long *lau
   });
   if (r) return r;
   *launches += (long long)nfj;
-  r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
+  if (c->ncut > 0) {
+    CK(with_G(c->cut_G, [&](auto g) {
+      return Launch<decltype(g)::value>::face_vis_cut(c->cut, c->ncut, c->VF, c->ghost, c->cut_nrm, c->st);
+    }));
+    ++*launches;
+  }
+  return DSEM_OK;
+}
+
+int enqueue_update(dsem_ctx *c, int kk, double *qt_out, long long *launches) {
+  int r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
     auto &g = c->groups[j];
     UpdArgs u{};
     u.JQ = c->JQ + g.q0;
@@ -291,6 +317,14 @@ int enqueue_stage(dsem_ctx *c, int kk, bool save, double *qt_out, long long *lau
   if (r) return r;
   *launches += (long long)c->groups.size();
   return DSEM_OK;
+}
+
+int enqueue_stage(dsem_ctx *c, int kk, bool save, double *qt_out, long long *launches) {
+  int r;
+  if ((r = enqueue_face_inv(c, launches))) return r;
+  if ((r = enqueue_vol(c, save, launches))) return r;
+  if ((r = enqueue_face_vis(c, launches))) return r;
+  return enqueue_update(c, kk, qt_out, launches);
 }
 
 int enqueue_ev(dsem_ctx *c, long long *launches) {
@@ -676,6 +710,10 @@ int setup_ctx(dsem_ctx *c, const MeshSet &ms) {
   c->nface = (size_t)f0;
 
   // ---- mortars
+  std::vector<MortarCut> cuts;
+  std::vector<int> cut_ghost;
+  std::vector<double> cut_nh, cut_nrm;
+  int cut_G = 0;
   std::vector<std::vector<MortarC>> mcs(GMAX + 1);
   std::vector<MortarNC> ncs;
   std::vector<double> nc_nh, nc_nrm, mats;
@@ -686,6 +724,38 @@ int setup_ctx(dsem_ctx *c, const MeshSet &ms) {
   const int ldx = m->ldx;
   for (int j = 0; j < m->nmort; ++j) {
     const int *t = m->mortar + (size_t)DSEM_MORTAR_INTS * j;
+    if (t[0] < 0 || t[1] < 0) {  // cut mortar: the side with id -(g+1) is ghost face g (another shard)
+      if (c->ncase != 1) return fail(c, DSEM_ERR_UNSUPPORTED, "cut mortars are not supported in an ensemble");
+      if (t[0] < 0 && t[1] < 0) return fail(c, DSEM_ERR_INVALID_ARG, "a cut mortar needs one local side");
+      const bool lm = t[0] > 0;
+      const int lid = (lm ? t[0] : t[1]) - 1, g = -(lm ? t[1] : t[0]) - 1;
+      if (lid < 0 || lid >= m->ngrid) return fail(c, DSEM_ERR_INVALID_ARG, "mortar id out of range");
+      const int f1 = t[2], f2 = t[3], orient = t[10];
+      if (f1 < 1 || f1 > 6 || f2 < 1 || f2 > 6 || orient < 0 || orient > 7)
+        return fail(c, DSEM_ERR_INVALID_ARG, "bad mortar face or orientation");
+      const int G = ms.G(lid), G2 = G * G;
+      if (!(t[13] && t[14] && t[15] && t[16]) || t[4] != G || t[5] != G || t[6] != G || t[7] != G || t[8] != G ||
+          t[9] != G)
+        return fail(c, DSEM_ERR_UNSUPPORTED, "cut mortars must be conforming");
+      if (cut_G && cut_G != G) return fail(c, DSEM_ERR_UNSUPPORTED, "cut mortars of one order only");
+      cut_G = G;
+      const int lf = lm ? f1 : f2;
+      MortarCut mc;
+      mc.ls = c->groups[c->ext_group[lid]].f0 + (long long)c->ext_k[lid] * 30 * G2 + (long long)(lf - 1) * 5 * G2;
+      mc.go = (long long)g * 5 * G2;
+      mc.geo = (int)cuts.size();
+      const bool low = (f1 == 1 || f1 == 3 || f1 == 6);
+      mc.flags = orient | ((t[11] < 0) << 3) | ((t[12] < 0) << 4) | (low << 5) | ((lm ? 1 : 0) << 6);
+      cuts.push_back(mc);
+      cut_ghost.push_back(g);
+      for (int jj = 0; jj < G; ++jj)
+        for (int i = 0; i < G; ++i) {
+          const size_t q = (size_t)j * ldx * ldx + i + (size_t)ldx * jj;
+          cut_nrm.push_back(m->norm[q]);
+          for (int k = 0; k < 3; ++k) cut_nh.push_back(m->n_hat[q * 3 + k]);
+        }
+      continue;
+    }
     if (t[0] - 1 < 0 || t[0] - 1 >= m->ngrid) return fail(c, DSEM_ERR_INVALID_ARG, "mortar master id out of range");
     if (t[1] - 1 < 0) return fail(c, DSEM_ERR_UNSUPPORTED, "boundary mortars (id(2)=0) are not supported: the implemented path is fully periodic");
     if (t[1] - 1 >= m->ngrid) return fail(c, DSEM_ERR_INVALID_ARG, "mortar slave id out of range");
@@ -775,6 +845,31 @@ int setup_ctx(dsem_ctx *c, const MeshSet &ms) {
     c->mlists.push_back(ml);
   }
 
+  if (!cuts.empty()) {  // ghost g must appear on exactly one cut mortar
+    const int n = (int)cuts.size();
+    std::vector<long long> src(n, -1);
+    for (int i = 0; i < n; ++i) {
+      const int g = cut_ghost[i];
+      if (g >= n || src[g] >= 0) return fail(c, DSEM_ERR_INVALID_ARG, "ghost faces must be numbered 1..ncut, each once");
+      src[g] = cuts[i].ls;
+    }
+    c->ncut = n;
+    c->cut_G = cut_G;
+    CK(cudaMalloc(&c->cut, n * sizeof(MortarCut)));
+    CK(cudaMemcpy(c->cut, cuts.data(), n * sizeof(MortarCut), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->cut_nh, cut_nh.size() * sizeof(double)));
+    CK(cudaMemcpy(c->cut_nh, cut_nh.data(), cut_nh.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->cut_nrm, cut_nrm.size() * sizeof(double)));
+    CK(cudaMemcpy(c->cut_nrm, cut_nrm.data(), cut_nrm.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->pack_src, n * sizeof(long long)));
+    CK(cudaMemcpy(c->pack_src, src.data(), n * sizeof(long long), cudaMemcpyHostToDevice));
+    const size_t nb = (size_t)n * 5 * cut_G * cut_G * sizeof(double);
+    CK(cudaMalloc(&c->send, nb));
+    CK(cudaMalloc(&c->ghost, nb));
+    CK(cudaMemset(c->send, 0, nb));
+    CK(cudaMemset(c->ghost, 0, nb));
+  }
+
   if (!ncs.empty()) {
     c->nnc = (int)ncs.size();
     CK(cudaMalloc(&c->nc, ncs.size() * sizeof(MortarNC)));
@@ -859,6 +954,12 @@ void dsem_destroy(dsem_ctx *c) {
   }
   cudaFree(c->d_rec);
   cudaFree(c->d_dtc);
+  cudaFree(c->cut);
+  cudaFree(c->cut_nh);
+  cudaFree(c->cut_nrm);
+  cudaFree(c->pack_src);
+  cudaFree(c->send);
+  cudaFree(c->ghost);
   for (auto s : c->aux) cudaStreamDestroy(s);
   for (auto e : c->ev_join) cudaEventDestroy(e);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -916,6 +1017,7 @@ int dsem_download_q(dsem_ctx *c, double *JQ, int ldx) {
 int dsem_rhs(dsem_ctx *c, double tk, double *Qt, int ldx) {
   (void)tk;
   if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (c->ncut) return fail(c, DSEM_ERR_INVALID_ARG, "a shard advances with dsem_shard_stage");
   if (Qt) {
     int r = check_ldx(c, ldx);
     if (r) return r;
@@ -1049,6 +1151,7 @@ extern "C" {
 int dsem_stage(dsem_ctx *c, double time, double dt, int kk, double *Qt, int ldx) {
   (void)time;
   if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (c->ncut) return fail(c, DSEM_ERR_INVALID_ARG, "a shard advances with dsem_shard_stage");
   if (kk < 1 || kk > c->kord) return fail(c, DSEM_ERR_INVALID_ARG, "stage index outside 1..kord");
   if (Qt) {
     int r = check_ldx(c, ldx);
@@ -1073,6 +1176,7 @@ int dsem_stage(dsem_ctx *c, double time, double dt, int kk, double *Qt, int ldx)
 int dsem_step(dsem_ctx *c, double time, double dt, int nsteps) {
   (void)time;
   if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (c->ncut) return fail(c, DSEM_ERR_INVALID_ARG, "a shard advances with dsem_shard_stage");
   if (nsteps < 0) return fail(c, DSEM_ERR_INVALID_ARG, "negative step count");
   std::vector<double> dts(c->ncase, dt);
   const int r = set_dt(c, dts.data());
@@ -1082,6 +1186,7 @@ int dsem_step(dsem_ctx *c, double time, double dt, int nsteps) {
 
 int dsem_step_batch(dsem_ctx *c, const double *dt, int nsteps) {
   if (!c || !dt) return fail(c, DSEM_ERR_INVALID_ARG, "null argument");
+  if (c->ncut) return fail(c, DSEM_ERR_INVALID_ARG, "a shard advances with dsem_shard_stage");
   if (nsteps < 0) return fail(c, DSEM_ERR_INVALID_ARG, "negative step count");
   const int r = set_dt(c, dt);
   if (r) return r;
@@ -1160,6 +1265,80 @@ int dsem_get_muhg(dsem_ctx *c, double *mu, int ldx) {
   }
   CK(cudaMemcpyAsync(mu, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  return DSEM_OK;
+}
+
+int dsem_shard_info(const dsem_ctx *c, int *nghost, int *doubles_per_face, double **send, double **ghost) {
+  if (!c) return DSEM_ERR_INVALID_ARG;
+  if (nghost) *nghost = c->ncut;
+  if (doubles_per_face) *doubles_per_face = 5 * c->cut_G * c->cut_G;
+  if (send) *send = c->send;
+  if (ghost) *ghost = c->ghost;
+  return DSEM_OK;
+}
+
+int dsem_shard_stage(dsem_ctx *c, double dt, int kk, int phase) {
+  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (kk < 1 || kk > c->kord || phase < 0 || phase > 2)
+    return fail(c, DSEM_ERR_INVALID_ARG, "stage index outside 1..kord or phase outside 0..2");
+  long long l = 0;
+  int r;
+  const unsigned nb = (unsigned)std::min<long long>(((long long)c->ncut * 5 * c->cut_G * c->cut_G + 255) / 256, 148LL * 8);
+  if (phase == 0) {  // stage start; local cut-face traces -> send
+    if (!c->traces_valid && (r = enqueue_traces(c, &l))) return r;
+    if (kk == 1) {
+      CK(cudaMemsetAsync(c->flag, 0, sizeof(int), c->st));
+      if (c->shock && (r = enqueue_ev(c, &l))) return r;
+      if (c->les && (r = enqueue_les(c, &l))) return r;
+    }
+    std::vector<double> dts(c->ncase, dt);
+    if ((r = set_dt(c, dts.data()))) return r;
+    if (c->ncut) {
+      k_pack_cut<<<std::max(nb, 1u), 256, 0, c->st>>>(c->pack_src, c->ncut, 5 * c->cut_G * c->cut_G, c->QF, c->send);
+      CK(cudaGetLastError());
+    }
+  } else if (phase == 1) {  // ghost traces in; inviscid mortars, volume; local cut-face VF -> send
+    const bool save = kk == c->kord && (c->shock || c->keep_grad || c->les);
+    if ((r = enqueue_face_inv(c, &l)) || (r = enqueue_vol(c, save, &l))) return r;
+    if (c->ncut) {
+      k_pack_cut<<<std::max(nb, 1u), 256, 0, c->st>>>(c->pack_src, c->ncut, 5 * c->cut_G * c->cut_G, c->VF, c->send);
+      CK(cudaGetLastError());
+    }
+  } else {  // ghost VF in; viscous mortars, update
+    if ((r = enqueue_face_vis(c, &l)) || (r = enqueue_update(c, kk, nullptr, &l))) return r;
+    if (kk == c->kord) {
+      const bool save = c->shock || c->keep_grad || c->les;
+      c->grad_valid = c->grad_valid || save;
+      c->ev_grad_valid = c->ev_grad_valid || c->shock;
+      CK(cudaStreamSynchronize(c->st));
+      return check_flag(c);
+    }
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return DSEM_OK;
+}
+
+int dsem_diag_sums(dsem_ctx *c, double *sums) {
+  if (!c || !sums) return fail(c, DSEM_ERR_INVALID_ARG, "null argument");
+  c->keep_grad = 1;
+  const bool have = c->grad_valid;
+  for (auto &g : c->groups) {
+    k_diag<<<g.nel, 128, sizeof(double) * 5 * g.G * g.G * g.G, c->st>>>(c->JQ + g.q0, g.jac, g.EVB, g.kew, g.G, g.nel,
+                                                                         have ? 1 : 0, c->part + g.e0 * 5);
+    CK(cudaGetLastError());
+  }
+  c->host_part.resize((size_t)c->ngrid * 5);
+  CK(cudaMemcpyAsync(c->host_part.data(), c->part, c->host_part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  for (int k = 0; k < 5; ++k) sums[k] = 0.0;
+  for (int e = 0; e < c->ngrid; ++e) {
+    const auto &g = c->groups[c->ext_group[e]];
+    const double *p = &c->host_part[(size_t)(g.e0 + c->ext_k[e]) * 5];
+    for (int k = 0; k < 5; ++k) sums[k] += p[k];
+  }
+  const auto &g = c->groups[c->ext_group[0]];
+  CK(cudaMemcpy(&sums[5], g.jac + (size_t)c->ext_k[0] * g.G * g.G * g.G, sizeof(double), cudaMemcpyDeviceToHost));
+  sums[6] = have ? 1.0 : 0.0;
   return DSEM_OK;
 }
 
@@ -1313,6 +1492,7 @@ int dsem_load_state(dsem_ctx *c, const void *buf, long long nbytes) {
 
 int dsem_profile_rhs(dsem_ctx *c, int reps, double *ms) {
   if (!c || !ms || reps <= 0) return fail(c, DSEM_ERR_INVALID_ARG, "bad argument");
+  if (c->ncut) return fail(c, DSEM_ERR_INVALID_ARG, "a shard advances with dsem_shard_stage");
   long long l = 0;
   int r;
   if (!c->traces_valid && (r = enqueue_traces(c, &l))) return r;

@@ -51,6 +51,7 @@ struct MList {  // conforming mortars of one order
 using dsem::Group;
 using dsem::MList;
 using dsem::MortarNC;
+using dsem::MortarCut;
 using dsem::Phys;
 
 struct dsem_ctx {
@@ -95,6 +96,14 @@ struct dsem_ctx {
   std::vector<cudaStream_t> aux;
   std::vector<cudaEvent_t> ev_join;
   cudaEvent_t ev_fork = nullptr;
+  // sharding: mortars whose other side lives on another shard; the remote
+  // face data arrive in `ghost` (one 5 x G^2 block per cut mortar), the local
+  // faces leave through `send` (same order)
+  int ncut = 0, cut_G = 0;
+  dsem::MortarCut *cut = nullptr;
+  double *cut_nh = nullptr, *cut_nrm = nullptr;
+  long long *pack_src = nullptr;
+  double *send = nullptr, *ghost = nullptr;
 };
 
 // error text of calls made without a context (read by dsem_last_error(NULL))

@@ -103,6 +103,24 @@ template <int G> cudaError_t Launch<G>::face_vis(const MortarC *mc, int nm, doub
   return cudaGetLastError();
 }
 
+template <int G>
+cudaError_t Launch<G>::face_inv_cut(const MortarCut *mc, int nm, double *QF, double *FF, const double *ghost,
+                                    const double *nh, const double *nrm, double gamma, cudaStream_t s) {
+  if (nm <= 0) return cudaSuccess;
+  const long long n = (long long)nm * G * G;
+  k_face_inv_cut<G><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(mc, nm, QF, FF, ghost, nh, nrm, gamma);
+  return cudaGetLastError();
+}
+
+template <int G>
+cudaError_t Launch<G>::face_vis_cut(const MortarCut *mc, int nm, double *VF, const double *ghost, const double *nrm,
+                                    cudaStream_t s) {
+  if (nm <= 0) return cudaSuccess;
+  const long long n = (long long)nm * G * G;
+  k_face_vis_cut<G><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(mc, nm, VF, ghost, nrm);
+  return cudaGetLastError();
+}
+
 }  // namespace dsem
 
 #define DSEM_INSTANTIATE(GG) template struct dsem::Launch<GG>;

@@ -12,6 +12,7 @@ struct TraceArgs;
 struct EvArgs;
 struct LesArgs;
 struct MortarC;
+struct MortarCut;
 
 // volume kernel variants: metric layout x entropy viscosity x saved gradients
 enum VolMode { VOL_PLAIN = 0, VOL_SAVE = 1, VOL_EV = 2, VOL_EV_SAVE = 3 };
@@ -28,6 +29,10 @@ template <int G> struct Launch {
   static cudaError_t face_inv(const MortarC *mc, int nm, double *QF, double *FF, const double *nh, const double *nrm,
                               double gamma, cudaStream_t s);
   static cudaError_t face_vis(const MortarC *mc, int nm, double *VF, const double *nrm, cudaStream_t s);
+  static cudaError_t face_inv_cut(const MortarCut *mc, int nm, double *QF, double *FF, const double *ghost,
+                                  const double *nh, const double *nrm, double gamma, cudaStream_t s);
+  static cudaError_t face_vis_cut(const MortarCut *mc, int nm, double *VF, const double *ghost, const double *nrm,
+                                  cudaStream_t s);
 };
 
 }  // namespace dsem

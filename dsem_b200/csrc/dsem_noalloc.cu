@@ -95,15 +95,27 @@ int setup_device(int dev, double **out) {
 
 // Mortar kernels reading the caller's DSEM_MORTAR_INTS rows directly
 // (1-based element ids; elements of one order, slots [elem][face][var][G^2]).
+// The rows live in device memory, so they are range-checked here: a row with
+// an element outside 1..nel, a face outside 1..6 or an orientation outside
+// 0..7 is skipped and sets bit 2 of the flag.
+__device__ __forceinline__ bool row_ok(const int *r, int nel, int *flag, int pt) {
+  const bool ok = r[0] >= 1 && r[0] <= nel && r[1] >= 1 && r[1] <= nel && r[2] >= 1 && r[2] <= 6 && r[3] >= 1 &&
+                  r[3] <= 6 && r[10] >= 0 && r[10] <= 7;
+  if (!ok && pt == 0) atomicOr(flag, 4);
+  return ok;
+}
+
 template <int G>
-__global__ void __launch_bounds__(128) k_face_inv_rows(const int *__restrict__ rows, int nm, double *__restrict__ QF,
-                                                        double *__restrict__ FF, const double *__restrict__ nh,
-                                                        const double *__restrict__ nrm, double gamma) {
+__global__ void __launch_bounds__(128) k_face_inv_rows(const int *__restrict__ rows, int nm, int nel, int *flag,
+                                                        double *__restrict__ QF, double *__restrict__ FF,
+                                                        const double *__restrict__ nh, const double *__restrict__ nrm,
+                                                        double gamma) {
   constexpr int G2 = G * G;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)nm * G2) return;
   const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
   const int *r = rows + (long long)DSEM_MORTAR_INTS * m;
+  if (!row_ok(r, nel, flag, pt)) return;
   const long long ms = (long long)(r[0] - 1) * 30 * G2 + (long long)(r[2] - 1) * 5 * G2;
   const long long ss = (long long)(r[1] - 1) * 30 * G2 + (long long)(r[3] - 1) * 5 * G2;
   int si, sj;
@@ -129,13 +141,14 @@ __global__ void __launch_bounds__(128) k_face_inv_rows(const int *__restrict__ r
 }
 
 template <int G>
-__global__ void __launch_bounds__(128) k_face_vis_rows(const int *__restrict__ rows, int nm, double *__restrict__ VF,
-                                                        const double *__restrict__ nrm) {
+__global__ void __launch_bounds__(128) k_face_vis_rows(const int *__restrict__ rows, int nm, int nel, int *flag,
+                                                        double *__restrict__ VF, const double *__restrict__ nrm) {
   constexpr int G2 = G * G;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)nm * G2) return;
   const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
   const int *r = rows + (long long)DSEM_MORTAR_INTS * m;
+  if (!row_ok(r, nel, flag, pt)) return;
   const long long ms = (long long)(r[0] - 1) * 30 * G2 + (long long)(r[2] - 1) * 5 * G2;
   const long long ss = (long long)(r[1] - 1) * 30 * G2 + (long long)(r[3] - 1) * 5 * G2;
   int si, sj;
@@ -173,7 +186,7 @@ int run(double *scratch, int nel, int nmort, const int *rows, const double *nh, 
   NK(Launch<G>::trace(ta, nel, st));
   const unsigned nb = (unsigned)(((long long)nmort * G2 + 127) / 128);
   if (nmort > 0) {
-    k_face_inv_rows<G><<<nb, 128, 0, st>>>(rows, nmort, QF, FF, nh, nrm, gamma);
+    k_face_inv_rows<G><<<nb, 128, 0, st>>>(rows, nmort, nel, flag, QF, FF, nh, nrm, gamma);
     NK(cudaGetLastError());
   }
   VolArgs va{};
@@ -192,7 +205,7 @@ int run(double *scratch, int nel, int nmort, const int *rows, const double *nh, 
   phys_recips(va.P);
   NK(Launch<G>::vol(va, nel, true, VOL_PLAIN, st));
   if (nmort > 0) {
-    k_face_vis_rows<G><<<nb, 128, 0, st>>>(rows, nmort, VF, nrm);
+    k_face_vis_rows<G><<<nb, 128, 0, st>>>(rows, nmort, nel, flag, VF, nrm);
     NK(cudaGetLastError());
   }
   UpdArgs ua{};
@@ -214,6 +227,7 @@ int run(double *scratch, int nel, int nmort, const int *rows, const double *nh, 
   NK(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
   NK(cudaStreamSynchronize(st));
 #undef NK
+  if (h & 4) return nfail(DSEM_ERR_INVALID_ARG, "dsem_rhs_noalloc: mortar row with an element, face or orientation out of range");
   if (h & 1) return nfail(DSEM_ERR_NONFINITE, "NaN or Inf in the right-hand side");
   return DSEM_OK;
 }

@@ -172,6 +172,96 @@ __global__ void __launch_bounds__(128) k_face_vis(const MortarC *__restrict__ mc
   }
 }
 
+// --------------------------------------------------------- cut mortars
+// A conforming mortar whose other side lives on another shard (another GPU):
+// the local face slot ls, the remote face's data (its own face layout) at ghost
+// offset go of the ghost buffer, flags as MortarC plus (local side is master)<<6.
+// Both shards evaluate the same point with the same operands and each writes
+// only its own side, so the result equals the unsharded kernels' bit for bit.
+struct MortarCut {
+  long long ls, go;
+  int geo, flags;
+};
+
+template <int G>
+__global__ void __launch_bounds__(128) k_face_inv_cut(const MortarCut *__restrict__ mc, int nm, double *__restrict__ QF,
+                                                       double *__restrict__ FF, const double *__restrict__ ghost,
+                                                       const double *__restrict__ nh, const double *__restrict__ nrm,
+                                                       double gamma) {
+  constexpr int G2 = G * G;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nm * G2) return;
+  const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
+  const MortarCut M = mc[m];
+  int si, sj;
+  slave_index<G>(M.flags & 7, pt % G, pt / G, si, sj);
+  const int sp = si + G * sj;
+  const bool lm = (M.flags >> 6) & 1;
+  double Q1[NV], Q2[NV], f[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    Q1[v] = lm ? QF[M.ls + v * G2 + pt] : ghost[M.go + v * G2 + pt];
+    Q2[v] = lm ? ghost[M.go + v * G2 + sp] : QF[M.ls + v * G2 + sp];
+  }
+  const long long gp = (long long)M.geo * G2 + pt;
+  const double n3[3] = {nh[gp * 3], nh[gp * 3 + 1], nh[gp * 3 + 2]};
+  const bool low = (M.flags >> 5) & 1;
+  riemann(n3, nrm[gp], low ? Q2 : Q1, low ? Q1 : Q2, gamma, f);
+  const double sgn = ((M.flags >> 3) & 1) ? -1.0 : 1.0;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double avg = (Q1[v] + Q2[v]) * 0.5;
+    if (lm) {
+      FF[M.ls + v * G2 + pt] = f[v];
+      QF[M.ls + v * G2 + pt] = avg;
+    } else {
+      FF[M.ls + v * G2 + sp] = sgn * f[v];
+      QF[M.ls + v * G2 + sp] = avg;
+    }
+  }
+}
+
+template <int G>
+__global__ void __launch_bounds__(128) k_face_vis_cut(const MortarCut *__restrict__ mc, int nm, double *__restrict__ VF,
+                                                       const double *__restrict__ ghost, const double *__restrict__ nrm) {
+  constexpr int G2 = G * G;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nm * G2) return;
+  const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
+  const MortarCut M = mc[m];
+  int si, sj;
+  slave_index<G>(M.flags & 7, pt % G, pt / G, si, sj);
+  const int sp = si + G * sj;
+  const bool lm = (M.flags >> 6) & 1;
+  const long long g0 = (long long)M.geo * G2;
+  const double nm_m = nrm[g0 + pt], nm_s = nrm[g0 + sp];
+  const double rm = 1.0 / nm_m, rs = 1.0 / nm_s;
+  const bool neg_n = (M.flags >> 4) & 1, neg_s = (M.flags >> 3) & 1;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double vm = lm ? VF[M.ls + v * G2 + pt] : ghost[M.go + v * G2 + pt];
+    const double vs = lm ? ghost[M.go + v * G2 + sp] : VF[M.ls + v * G2 + sp];
+    const double fv1 = ddiv(vm, nm_m, rm);
+    const double fv2 = ddiv(vs, nm_s, rs);
+    const double Qs = neg_n ? -fv2 : fv2;
+    const double qb = 0.5 * (fv1 + Qs) * nm_m;
+    if (lm)
+      VF[M.ls + v * G2 + pt] = qb;
+    else
+      VF[M.ls + v * G2 + sp] = neg_s ? -qb : qb;
+  }
+}
+
+// send[g] = the local face slot src[g] (5 fields of G^2 points) of field array F
+static __global__ void k_pack_cut(const long long *__restrict__ src, int nghost, int nper, const double *__restrict__ F,
+                           double *__restrict__ send) {
+  const long long n = (long long)nghost * nper;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long g = i / nper, r = i - g * nper;
+    send[i] = F[src[g] + r];
+  }
+}
+
 // ------------------------------------------------------- nonconforming faces
 // One CTA per p-nonconforming mortar (lenmortar > len on at least one side).
 // Mirrors interface_flux / map_to_mortar_space / map_to_face_space /

@@ -19,7 +19,7 @@ EXPORTS = ("dsem_create", "dsem_destroy", "dsem_last_error", "dsem_upload_q", "d
            "dsem_stage", "dsem_rhs", "dsem_diag", "dsem_get_muhg", "dsem_last_timing", "dsem_profile_rhs",
            "dsem_create_batch", "dsem_batch_size", "dsem_upload_q_case", "dsem_download_q_case", "dsem_step_batch",
            "dsem_diag_batch", "dsem_adjoint", "dsem_set_les", "dsem_get_nut", "dsem_state_size",
-           "dsem_save_state", "dsem_load_state")
+           "dsem_save_state", "dsem_load_state", "dsem_shard_info", "dsem_shard_stage", "dsem_diag_sums")
 
 
 class DsemError(RuntimeError):
@@ -73,6 +73,9 @@ def lib(path=None):
         L.dsem_step_batch.argtypes = [vp, dp, C.c_int]
         L.dsem_diag_batch.argtypes = [vp, dp, C.c_int, dp, dp, dp]
         L.dsem_set_les.argtypes = [vp, C.c_double, C.c_double]
+        L.dsem_shard_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(dp), C.POINTER(dp)]
+        L.dsem_shard_stage.argtypes = [vp, C.c_double, C.c_int, C.c_int]
+        L.dsem_diag_sums.argtypes = [vp, dp]
         L.dsem_state_size.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.dsem_save_state.argtypes = [vp, C.c_void_p, C.c_longlong]
         L.dsem_load_state.argtypes = [vp, C.c_void_p, C.c_longlong]

@@ -143,6 +143,32 @@ int dsem_state_size(const dsem_ctx *ctx, long long *nbytes);
 int dsem_save_state(dsem_ctx *ctx, void *buf, long long nbytes);
 int dsem_load_state(dsem_ctx *ctx, const void *buf, long long nbytes);
 
+/* ---- One case sharded over several GPUs (one context per GPU) ----
+ * The replacement for DSEM's MPI face exchange (send_q_to_mortars_mpi,
+ * send_flux_to_mortars_mpi, add_flux_mpi: send_q.f90:771-895,
+ * send_flux.f90:464-692, 1109-1206).  Each shard's descriptor holds its own
+ * elements; a mortar whose other side is on another shard is "cut": that
+ * side's element id is -(g+1), g (0-based) numbering the shard's ghost faces
+ * 0..ncut-1.  A stage runs in three phases with two exchanges between them:
+ *   phase 0: stage start; the local faces of the cut mortars (their face
+ *            traces) are packed into `send`, block g for ghost g;
+ *   exchange: the caller makes `ghost` block g the remote shard's `send`
+ *            block of the same mortar (NCCL send/recv over NVLink, or any copy);
+ *   phase 1: inviscid mortars (cut ones read the ghost traces), volume; the
+ *            viscous face fluxes of the cut faces are packed into `send`;
+ *   exchange again;
+ *   phase 2: viscous mortars, update.
+ * Both shards evaluate a cut mortar's points with the same operands, so a
+ * sharded run reproduces the single-context run bit for bit.  Conforming cut
+ * mortars of one element order; dsem_step / dsem_stage / dsem_rhs reject
+ * sharded contexts.  dsem_diag_sums returns this shard's diagnostic sums
+ * {sum u^2 w, v^2 w, w^2 w, |w|^2 J, J, jacob(1,1,1) of its element 1,
+ * gradients valid}: the caller adds them over shards (an all-reduce) and
+ * forms KE and eps as dsem_diag does. */
+int dsem_shard_info(const dsem_ctx *ctx, int *nghost, int *doubles_per_face, double **send, double **ghost);
+int dsem_shard_stage(dsem_ctx *ctx, double dt, int kk, int phase);
+int dsem_diag_sums(dsem_ctx *ctx, double *sums);
+
 /* ---- Ensembles: ncase independent runs in one context ----
  * No DSEM counterpart (DSEM runs one case per job; each would call tstep,
  * tstep.f90:12, from its own time loop, 3DDriver_parfmdf.f90:466).  The

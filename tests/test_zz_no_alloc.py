@@ -86,3 +86,20 @@ def test_noalloc_rejects_oversized_mesh(lib):
                               C.c_void_p(1), None)
     assert rc == -1
     assert b"too large" in lib.dsem_last_error(None)
+
+
+@pytest.mark.parametrize("field,value", [(0, 0), (1, 9), (2, 7), (10, 8)])
+def test_noalloc_rejects_out_of_range_mortar_rows(lib, field, value):
+    """A mortar row naming an element outside 1..nel, a face outside 1..6 or an
+    orientation outside 0..7 is skipped by the face kernels and reported."""
+    import torch
+    box = mesh.Box(2, 2, 2, 3)
+    arrs = internal_arrays(box, mesh.taylor_green(box))
+    rows = arrs["mortar"].reshape(box.nmort, -1).copy()
+    rows[1, field] = value
+    arrs["mortar"] = rows
+    rc, _ = call_noalloc(lib, box, arrs, torch, 3)
+    assert rc == -1
+    assert b"out of range" in lib.dsem_last_error(None)
+    rc, _ = call_noalloc(lib, box, internal_arrays(box, mesh.taylor_green(box)), torch, 3)
+    assert rc == 0
