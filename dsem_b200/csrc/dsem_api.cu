@@ -211,14 +211,34 @@ int vol_mode(const dsem_ctx *c, bool save) {
 // The four parts of one evaluation of Fluxes + the flux divergence (+ the
 // update when kk > 0).  The update reads dt per case from d_dtc (written before
 // the stage is enqueued or the graph replayed).
+// physical constants of the boundary kernels
+static dsem::BndPhys bnd_phys(const dsem_ctx *c) {
+  dsem::BndPhys P;
+  P.gamma = c->P.gamma;
+  P.twall = c->twall;
+  P.cv = c->P.mach * c->P.mach * c->P.gamma * (c->P.gamma - 1.0);
+  P.r_cv = 1.0 / P.cv;
+  return P;
+}
+
 int enqueue_face_inv(dsem_ctx *c, long long *launches) {
+  if ((c->bnd_need_twall && !c->bnd_twall_set) || (c->bnd_need_ext && !c->bnd_ext_set))
+    return fail(c, DSEM_ERR_INVALID_ARG,
+                "boundary faces need dsem_set_boundary first (twall for isothermal walls, external states for "
+                "inflow/outflow)");
   const double gamma = c->P.gamma;
-  const size_t nml = c->mlists.size(), nfj = nml + (c->nnc > 0 ? 1 : 0);
+  const size_t nml = c->mlists.size(), nnj = nml + (c->nnc > 0 ? 1 : 0), nfj = nnj + c->blists.size();
+  const dsem::BndPhys BP = bnd_phys(c);
   int r = fork_jobs(c, nfj, [&](size_t j, cudaStream_t st) -> int {
     if (j < nml) {
       auto &ml = c->mlists[j];
       CK(with_G(ml.G, [&](auto g) {
         return Launch<decltype(g)::value>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, gamma, st);
+      }));
+    } else if (j >= nnj) {  // boundary faces: their master face slots only
+      auto &bl = c->blists[j - nnj];
+      CK(with_G(bl.G, [&](auto g) {
+        return Launch<decltype(g)::value>::face_bnd_inv(bl.mb, bl.n, c->QF, c->FF, bl.nh, bl.nrm, bl.qext, BP, st);
       }));
     } else {
       k_face_nc_inv<<<c->nnc, 128, 0, st>>>(c->nc, c->QF, c->FF, c->nc_nh, c->nc_nrm, c->nc_mats, gamma);
@@ -266,11 +286,16 @@ int enqueue_vol(dsem_ctx *c, bool save, long long *launches) {
 }
 
 int enqueue_face_vis(dsem_ctx *c, long long *launches) {
-  const size_t nml = c->mlists.size(), nfj = nml + (c->nnc > 0 ? 1 : 0);
+  const size_t nml = c->mlists.size(), nnj = nml + (c->nnc > 0 ? 1 : 0), nfj = nnj + c->blists.size();
   int r = fork_jobs(c, nfj, [&](size_t j, cudaStream_t st) -> int {
     if (j < nml) {
       auto &ml = c->mlists[j];
       CK(with_G(ml.G, [&](auto g) { return Launch<decltype(g)::value>::face_vis(ml.mc, ml.n, c->VF, ml.nrm, st); }));
+    } else if (j >= nnj) {
+      auto &bl = c->blists[j - nnj];
+      CK(with_G(bl.G, [&](auto g) {
+        return Launch<decltype(g)::value>::face_bnd_vis(bl.mb, bl.n, c->VF, bl.nrm, bl.fvext, st);
+      }));
     } else {
       k_face_nc_vis<<<c->nnc, 128, 0, st>>>(c->nc, c->VF, c->nc_nrm, c->nc_mats);
       CK(cudaGetLastError());
@@ -719,6 +744,9 @@ int setup_ctx(dsem_ctx *c, const MeshSet &ms) {
   std::vector<double> nc_nh, nc_nrm, mats;
   std::map<long long, std::pair<int, int>> mat_off;
   std::vector<std::vector<double>> nhs(GMAX + 1), nrs(GMAX + 1);
+  std::vector<std::vector<dsem::MortarB>> bms(GMAX + 1);
+  std::vector<std::vector<double>> bnhs(GMAX + 1), bnrs(GMAX + 1);
+  std::vector<std::vector<int>> bids(GMAX + 1);
   for (int cs = 0; cs < c->ncase; ++cs) {
   const dsem_mesh_desc *m = ms.m[cs];
   const int ldx = m->ldx;
@@ -757,7 +785,35 @@ int setup_ctx(dsem_ctx *c, const MeshSet &ms) {
       continue;
     }
     if (t[0] - 1 < 0 || t[0] - 1 >= m->ngrid) return fail(c, DSEM_ERR_INVALID_ARG, "mortar master id out of range");
-    if (t[1] - 1 < 0) return fail(c, DSEM_ERR_UNSUPPORTED, "boundary mortars (id(2)=0) are not supported: the implemented path is fully periodic");
+    if (t[1] == 0) {  // boundary mortar: the master face's d%bcond selects the condition
+      if (c->ncase != 1) return fail(c, DSEM_ERR_UNSUPPORTED, "boundary faces are not supported in an ensemble");
+      if (!m->bcond) return fail(c, DSEM_ERR_INVALID_ARG, "boundary mortars (id(2)=0) need dsem_mesh_desc.bcond");
+      const int id1 = t[0] - 1, f1 = t[2];
+      if (f1 < 1 || f1 > 6) return fail(c, DSEM_ERR_INVALID_ARG, "bad mortar face or orientation");
+      const int bc = m->bcond[6 * id1 + f1 - 1];
+      if (bc < DSEM_BC_WALLADIAB || bc > DSEM_BC_OUTFLOW)
+        return fail(c, DSEM_ERR_INVALID_ARG, "the master face of a boundary mortar has no boundary condition in bcond");
+      const int G = ms.G(id1), G2 = G * G;
+      if (t[4] != G || t[5] != G || t[8] != G || t[9] != G || t[10] != 0)
+        return fail(c, DSEM_ERR_UNSUPPORTED, "boundary mortars must match their face's order, with orient 0");
+      dsem::MortarB mb;
+      mb.ms = c->groups[c->ext_group[id1]].f0 + (long long)c->ext_k[id1] * 30 * G2 + (long long)(f1 - 1) * 5 * G2;
+      mb.geo = (int)bms[G].size();
+      const bool low = (f1 == 1 || f1 == 3 || f1 == 6);
+      mb.flags = bc | (low << 3) | ((t[12] < 0) << 4);
+      bms[G].push_back(mb);
+      bids[G].push_back(j);
+      for (int jj = 0; jj < G; ++jj)
+        for (int i = 0; i < G; ++i) {
+          const size_t q = (size_t)j * ldx * ldx + i + (size_t)ldx * jj;
+          bnrs[G].push_back(m->norm[q]);
+          for (int k = 0; k < 3; ++k) bnhs[G].push_back(m->n_hat[q * 3 + k]);
+        }
+      if (bc == DSEM_BC_WALLISOTH) c->bnd_need_twall = true;
+      if (bc == DSEM_BC_INFLOW || bc == DSEM_BC_OUTFLOW) c->bnd_need_ext = true;
+      continue;
+    }
+    if (t[1] - 1 < 0) return fail(c, DSEM_ERR_INVALID_ARG, "mortar slave id out of range");
     if (t[1] - 1 >= m->ngrid) return fail(c, DSEM_ERR_INVALID_ARG, "mortar slave id out of range");
     const int id1 = t[0] - 1 + ms.el0[cs], id2 = t[1] - 1 + ms.el0[cs];
     const int f1 = t[2], f2 = t[3], orient = t[10];
@@ -844,6 +900,26 @@ int setup_ctx(dsem_ctx *c, const MeshSet &ms) {
     CK(cudaMemcpy(ml.nrm, nrs[G].data(), nrs[G].size() * sizeof(double), cudaMemcpyHostToDevice));
     c->mlists.push_back(ml);
   }
+  for (int G = GMIN; G <= GMAX; ++G) {
+    if (bms[G].empty()) continue;
+    BList bl;
+    bl.G = G;
+    bl.n = (int)bms[G].size();
+    bl.mortar = bids[G];
+    const size_t next = (size_t)bl.n * 5 * G * G;
+    CK(cudaMalloc(&bl.mb, bms[G].size() * sizeof(dsem::MortarB)));
+    CK(cudaMemcpy(bl.mb, bms[G].data(), bms[G].size() * sizeof(dsem::MortarB), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&bl.nh, bnhs[G].size() * sizeof(double)));
+    CK(cudaMemcpy(bl.nh, bnhs[G].data(), bnhs[G].size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&bl.nrm, bnrs[G].size() * sizeof(double)));
+    CK(cudaMemcpy(bl.nrm, bnrs[G].data(), bnrs[G].size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&bl.qext, next * sizeof(double)));
+    CK(cudaMemset(bl.qext, 0, next * sizeof(double)));
+    CK(cudaMalloc(&bl.fvext, next * sizeof(double)));
+    CK(cudaMemset(bl.fvext, 0, next * sizeof(double)));
+    c->nbnd += bl.n;
+    c->blists.push_back(bl);
+  }
 
   if (!cuts.empty()) {  // ghost g must appear on exactly one cut mortar
     const int n = (int)cuts.size();
@@ -911,7 +987,7 @@ int setup_ctx(dsem_ctx *c, const MeshSet &ms) {
   }
   // streams for the parallel branches of a stage
   {
-    const size_t nj = std::max(c->groups.size(), c->mlists.size() + (c->nnc > 0 ? 1 : 0));
+    const size_t nj = std::max(c->groups.size(), c->mlists.size() + (c->nnc > 0 ? 1 : 0) + c->blists.size());
     if (nj > 1) {
       CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
       for (size_t j = 0; j < nj; ++j) {
@@ -971,6 +1047,13 @@ void dsem_destroy(dsem_ctx *c) {
     cudaFree(ml.mc);
     cudaFree(ml.nh);
     cudaFree(ml.nrm);
+  }
+  for (auto &bl : c->blists) {
+    cudaFree(bl.mb);
+    cudaFree(bl.nh);
+    cudaFree(bl.nrm);
+    cudaFree(bl.qext);
+    cudaFree(bl.fvext);
   }
   cudaFree(c->JQ);
   cudaFree(c->gQ);
@@ -1342,6 +1425,40 @@ int dsem_diag_sums(dsem_ctx *c, double *sums) {
   return DSEM_OK;
 }
 
+int dsem_set_boundary(dsem_ctx *c, double twall, const double *Qext, const double *fvext, int ldx) {
+  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (!std::isfinite(twall)) return fail(c, DSEM_ERR_INVALID_ARG, "twall is not finite");
+  if ((Qext || fvext) && !c->nbnd) return fail(c, DSEM_ERR_INVALID_ARG, "the mesh has no boundary faces");
+  for (auto &bl : c->blists)
+    if ((Qext || fvext) && ldx < bl.G) return fail(c, DSEM_ERR_INVALID_ARG, "ldx smaller than the number of Gauss points");
+  if (twall != c->twall && c->gexec) {  // twall is a kernel parameter of the captured step
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  c->twall = twall;
+  c->bnd_twall_set = true;
+  // caller layout [nmort][5][ldx][ldx] (mrtr(:)%Q(:,:,:,2), i fastest) -> [entry][5][G^2]
+  for (auto &bl : c->blists) {
+    const int G = bl.G, G2 = G * G;
+    std::vector<double> h((size_t)bl.n * 5 * G2);
+    for (int which = 0; which < 2; ++which) {
+      const double *src = which ? fvext : Qext;
+      if (!src) continue;
+      for (int k = 0; k < bl.n; ++k)
+        for (int v = 0; v < 5; ++v)
+          for (int j = 0; j < G; ++j)
+            for (int i = 0; i < G; ++i)
+              h[((size_t)k * 5 + v) * G2 + i + G * j] =
+                  src[((((size_t)bl.mortar[k] * 5 + v) * ldx + j) * ldx) + i];
+      CK(cudaMemcpyAsync(which ? bl.fvext : bl.qext, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice,
+                         c->st));
+      CK(cudaStreamSynchronize(c->st));
+    }
+  }
+  if (Qext) c->bnd_ext_set = true;
+  return DSEM_OK;
+}
+
 int dsem_set_les(dsem_ctx *c, double cs, double numax) {
   if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
   if (!(cs >= 0.0) || !(numax >= 0.0)) return fail(c, DSEM_ERR_INVALID_ARG, "cs and numax must be >= 0");
@@ -1506,6 +1623,11 @@ int dsem_profile_rhs(dsem_ctx *c, int reps, double *ms) {
       CK(with_G(ml.G, [&](auto g) {
         return Launch<decltype(g)::value>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st);
       }));
+    for (auto &bl : c->blists)
+      CK(with_G(bl.G, [&](auto g) {
+        return Launch<decltype(g)::value>::face_bnd_inv(bl.mb, bl.n, c->QF, c->FF, bl.nh, bl.nrm, bl.qext,
+                                                        bnd_phys(c), c->st);
+      }));
     CK(cudaEventRecord(ev[1], c->st));
     for (auto &g : c->groups) {
       VolArgs a{};
@@ -1525,6 +1647,10 @@ int dsem_profile_rhs(dsem_ctx *c, int reps, double *ms) {
     CK(cudaEventRecord(ev[2], c->st));
     for (auto &ml : c->mlists)
       CK(with_G(ml.G, [&](auto g) { return Launch<decltype(g)::value>::face_vis(ml.mc, ml.n, c->VF, ml.nrm, c->st); }));
+    for (auto &bl : c->blists)
+      CK(with_G(bl.G, [&](auto g) {
+        return Launch<decltype(g)::value>::face_bnd_vis(bl.mb, bl.n, c->VF, bl.nrm, bl.fvext, c->st);
+      }));
     CK(cudaEventRecord(ev[3], c->st));
     for (auto &g : c->groups) {
       UpdArgs u{};

@@ -46,10 +46,19 @@ struct MList {  // conforming mortars of one order
   double *nh = nullptr, *nrm = nullptr;
 };
 
+struct BList {  // boundary mortars (id(2) = 0) of one order
+  int G = 0, n = 0;
+  MortarB *mb = nullptr;
+  double *nh = nullptr, *nrm = nullptr;
+  double *qext = nullptr, *fvext = nullptr;  // external mrtr%Q / mrtr%fv (side 2), [n][5][G^2]
+  std::vector<int> mortar;                   // caller mortar index of each entry
+};
+
 }  // namespace dsem
 
 using dsem::Group;
 using dsem::MList;
+using dsem::BList;
 using dsem::MortarNC;
 using dsem::MortarCut;
 using dsem::Phys;
@@ -65,6 +74,10 @@ struct dsem_ctx {
   double ark[5] = {}, brk[5] = {}, crk[5] = {};
   std::vector<Group> groups;
   std::vector<MList> mlists;
+  std::vector<BList> blists;  // boundary faces; their conditions need dsem_set_boundary first
+  int nbnd = 0;
+  bool bnd_need_twall = false, bnd_need_ext = false, bnd_twall_set = false, bnd_ext_set = false;
+  double twall = 0.0;
   MortarNC *nc = nullptr;  // p-nonconforming mortars
   int nnc = 0;
   double *nc_nh = nullptr, *nc_nrm = nullptr, *nc_mats = nullptr;

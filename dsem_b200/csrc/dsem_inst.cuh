@@ -121,6 +121,24 @@ cudaError_t Launch<G>::face_vis_cut(const MortarCut *mc, int nm, double *VF, con
   return cudaGetLastError();
 }
 
+template <int G>
+cudaError_t Launch<G>::face_bnd_inv(const MortarB *mb, int nm, double *QF, double *FF, const double *nh,
+                                    const double *nrm, const double *qext, const BndPhys &P, cudaStream_t s) {
+  if (nm <= 0) return cudaSuccess;
+  const long long n = (long long)nm * G * G;
+  k_face_bnd_inv<G><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(mb, nm, QF, FF, nh, nrm, qext, P);
+  return cudaGetLastError();
+}
+
+template <int G>
+cudaError_t Launch<G>::face_bnd_vis(const MortarB *mb, int nm, double *VF, const double *nrm, const double *fvext,
+                                    cudaStream_t s) {
+  if (nm <= 0) return cudaSuccess;
+  const long long n = (long long)nm * G * G;
+  k_face_bnd_vis<G><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(mb, nm, VF, nrm, fvext);
+  return cudaGetLastError();
+}
+
 }  // namespace dsem
 
 #define DSEM_INSTANTIATE(GG) template struct dsem::Launch<GG>;

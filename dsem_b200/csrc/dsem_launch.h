@@ -13,6 +13,8 @@ struct EvArgs;
 struct LesArgs;
 struct MortarC;
 struct MortarCut;
+struct MortarB;
+struct BndPhys;
 
 // volume kernel variants: metric layout x entropy viscosity x saved gradients
 enum VolMode { VOL_PLAIN = 0, VOL_SAVE = 1, VOL_EV = 2, VOL_EV_SAVE = 3 };
@@ -32,6 +34,10 @@ template <int G> struct Launch {
   static cudaError_t face_inv_cut(const MortarCut *mc, int nm, double *QF, double *FF, const double *ghost,
                                   const double *nh, const double *nrm, double gamma, cudaStream_t s);
   static cudaError_t face_vis_cut(const MortarCut *mc, int nm, double *VF, const double *ghost, const double *nrm,
+                                  cudaStream_t s);
+  static cudaError_t face_bnd_inv(const MortarB *mb, int nm, double *QF, double *FF, const double *nh,
+                                  const double *nrm, const double *qext, const BndPhys &P, cudaStream_t s);
+  static cudaError_t face_bnd_vis(const MortarB *mb, int nm, double *VF, const double *nrm, const double *fvext,
                                   cudaStream_t s);
 };
 

@@ -262,6 +262,208 @@ static __global__ void k_pack_cut(const long long *__restrict__ src, int nghost,
   }
 }
 
+// ------------------------------------------------------- boundary faces
+// Mortars without a neighbour (id(2) = 0), conforming with orient 0: the master
+// face only.  boundary_flux, DirichletBC and Vis_Neumann of the problem file
+// (caseFiles/tgv/BackstepProblem-stoch.f90:1602-1729) dispatch on the master
+// face's d%bcond to the routines of NS/BCs/stac3m restated below.
+enum { BC_WALLADIAB = 1, BC_WALLISOTH = 2, BC_INFLOW = 3, BC_OUTFLOW = 4 };
+struct MortarB {
+  long long ms;  // master face slot
+  int geo;       // index in the order's boundary list (geometry, external state)
+  int flags;     // condition (bits 0-2) | master face 1, 3 or 6 (bit 3) | nsign < 0 (bit 4)
+};
+struct BndPhys {
+  double gamma, twall, r_cv;  // r_cv = 1 / (mach^2 gamma (gamma-1)), correctly rounded
+  double cv;                  // mach^2 gamma (gamma-1)
+};
+
+// External state of a wall: density and energy kept, normal momentum reversed
+// (wallbc_inv.f90:32-50, wallbc_isoth2.f90:31-54).
+__device__ __forceinline__ void wall_mirror(const double *nh, const double *Q1, double *Q2) {
+  const double qnorm = nh[0] * Q1[1] + nh[1] * Q1[2] + nh[2] * Q1[3];
+  const double tx = Q1[1] - qnorm * nh[0], ty = Q1[2] - qnorm * nh[1], tz = Q1[3] - qnorm * nh[2];
+  Q2[0] = Q1[0];
+  Q2[1] = tx - qnorm * nh[0];
+  Q2[2] = ty - qnorm * nh[1];
+  Q2[3] = tz - qnorm * nh[2];
+  Q2[4] = Q1[4];
+}
+
+// osher (PhysLib.f90:698-790): the state between the normal Riemann
+// invariants of Ql and Qr, then its Euler flux (fflux/gflux/hflux :17-124)
+// along n scaled by ds.
+static __device__ __noinline__ void osher_flux(const double *nh, double ds, const double *Ql, const double *Qr, double gamma,
+                                        double *flux) {
+  const double en1 = nh[0], en2 = nh[1], en3 = nh[2];
+  const double rho = Ql[0], rhou = Ql[1], rhov = Ql[2], rhow = Ql[3], rhoe = Ql[4];
+  const double rhon = Qr[0], rhoun = Qr[1], rhovn = Qr[2], rhown = Qr[3], rhoen = Qr[4];
+  const double qdotn = (en1 * rhou + en2 * rhov + en3 * rhow) / rho;
+  const double qdotnn = (en1 * rhoun + en2 * rhovn + en3 * rhown) / rhon;
+  const double p = (gamma - 1.0) * (rhoe - 0.5 / rho * (rhou * rhou + rhov * rhov + rhow * rhow));
+  const double a = sqrt(gamma * p / rho);
+  double pn = (gamma - 1.0) * (rhoen - 0.5 / rhon * (rhoun * rhoun + rhovn * rhovn + rhown * rhown));
+  const double an = sqrt(gamma * pn / rhon);
+  const double q_tanx = rhoun / rhon - qdotnn * en1;
+  const double q_tany = rhovn / rhon - qdotnn * en2;
+  const double q_tanz = rhown / rhon - qdotnn * en3;
+  const double z = (gamma - 1.0) / (2.0 * gamma);
+  double Ha = -qdotnn / an + 2.0 / (gamma - 1.0);
+  Ha = Ha / (qdotn / a + 2.0 / (gamma - 1.0));
+  pn = p / pow(Ha, 1.0 / z);
+  double pstar = a + an - (qdotnn - qdotn) * (gamma - 1.0) / 2.0;
+  pstar = pstar / (a / pow(p, z) + an / pow(pn, z));
+  pstar = pow(pstar, 1.0 / z);
+  double ustar = Ha * qdotn / a + qdotnn / an + 2.0 * (Ha - 1.0) / (gamma - 1.0);
+  ustar = ustar / (Ha / a + 1.0 / an);
+  const double rs = pstar * gamma / (an * an);
+  const double u = q_tanx + en1 * ustar, v = q_tany + en2 * ustar, w = q_tanz + en3 * ustar;
+  const double Q0 = rs, Q1 = rs * u, Q2 = rs * v, Q3 = rs * w;
+  const double Q4 = pstar / (gamma - 1.0) + 0.5 * rs * (u * u + v * v + w * w);
+  // fflux / gflux / hflux of Q
+  const double uu = Q1 / Q0, vv = Q2 / Q0, ww = Q3 / Q0;
+  const double pp = (gamma - 1.0) * (Q4 - 0.5 * Q0 * (uu * uu + vv * vv + ww * ww));
+  const double f[NV] = {Q1, pp + Q1 * uu, Q1 * vv, Q1 * ww, uu * (Q4 + pp)};
+  const double g[NV] = {Q2, Q1 * vv, pp + Q2 * vv, Q3 * vv, vv * (Q4 + pp)};
+  const double h[NV] = {Q3, Q1 * ww, Q2 * ww, pp + Q3 * ww, ww * (Q4 + pp)};
+#pragma unroll
+  for (int k = 0; k < NV; ++k) flux[k] = ds * (en1 * f[k] + en2 * g[k] + en3 * h[k]);
+}
+
+// riemann_solution (PhysLib.f90:326-412): the interface state from the normal
+// Riemann invariants (Dirichlet values of inflow and outflow faces).
+static __device__ __noinline__ void riemann_state(const double *nh, const double *Ql, const double *Qr, double gamma,
+                                           double *Q) {
+  const double en1 = nh[0], en2 = nh[1], en3 = nh[2];
+  const double rho = Ql[0], rhou = Ql[1], rhov = Ql[2], rhow = Ql[3], rhoe = Ql[4];
+  const double rhon = Qr[0], rhoun = Qr[1], rhovn = Qr[2], rhown = Qr[3], rhoen = Qr[4];
+  const double qdotn = (en1 * rhou + en2 * rhov + en3 * rhow) / rho;
+  const double qdotnn = (en1 * rhoun + en2 * rhovn + en3 * rhown) / rhon;
+  const double p = (gamma - 1.0) * (rhoe - 0.5 / rho * (rhou * rhou + rhov * rhov + rhow * rhow));
+  const double a = sqrt(gamma * p / rho);
+  const double pn = (gamma - 1.0) * (rhoen - 0.5 / rhon * (rhoun * rhoun + rhovn * rhovn + rhown * rhown));
+  const double an = sqrt(gamma * pn / rhon);
+  const double e0 = 0.5 * (qdotn + qdotnn);
+  const double eplus = e0 + 0.5 * (a + an);
+  const double eminus = e0 - 0.5 * (a + an);
+  double etos, q_tanx, q_tany, q_tanz;
+  if (e0 > 0.0) {
+    etos = p / pow(rho, gamma);
+    q_tanx = rhou / rho - qdotn * en1;
+    q_tany = rhov / rho - qdotn * en2;
+    q_tanz = rhow / rho - qdotn * en3;
+  } else {
+    etos = pn / pow(rhon, gamma);
+    q_tanx = rhoun / rhon - qdotnn * en1;
+    q_tany = rhovn / rhon - qdotnn * en2;
+    q_tanz = rhown / rhon - qdotnn * en3;
+  }
+  const double rplus = eplus >= 0.0 ? qdotn + 2.0 / (gamma - 1.0) * a : qdotnn + 2.0 / (gamma - 1.0) * an;
+  const double rminus = eminus >= 0.0 ? qdotn - 2.0 / (gamma - 1.0) * a : qdotnn - 2.0 / (gamma - 1.0) * an;
+  const double qn = 0.5 * (rplus + rminus);
+  const double as = 0.25 * (gamma - 1.0) * (rplus - rminus);
+  const double rs = pow(as * as / (gamma * etos), 1.0 / (gamma - 1.0));
+  const double ps = pow(rs, gamma) * etos;
+  const double u = q_tanx + en1 * qn, v = q_tany + en2 * qn, w = q_tanz + en3 * qn;
+  Q[0] = rs;
+  Q[1] = rs * u;
+  Q[2] = rs * v;
+  Q[3] = rs * w;
+  Q[4] = ps / (gamma - 1.0) + 0.5 * rs * (u * u + v * v + w * w);
+}
+
+// Inviscid boundary faces (fluxesH_newa.f90:116-139): boundary_flux, then
+// DirichletBC into the face's Q trace.  One thread per mortar point.
+//  walladiab: Roe flux against the mirror state; Q trace (rho, 0, 0, 0, rhoE)
+//             (wallbc_Inv; set_adiabatic_wall, ViscousBC_slide.f90:111-175)
+//  wallisoth: the mirror state at the wall temperature, osher flux (normal
+//             reversed on faces 1, 3, 6); Q trace (rho, 0, 0, 0, rho twall/cv)
+//             (wallbc_isoth2.f90; set_isothermal_wall, ViscousBC_slide.f90:356-420)
+//  inflow, outflow: Roe flux against the external state; Q trace from
+//             riemann_solution (inflow_specAll / outflow_specAll; boundary_values
+//             ViscousBC_slide.f90:9-102)
+template <int G>
+__global__ void __launch_bounds__(128) k_face_bnd_inv(const MortarB *__restrict__ mb, int nm, double *__restrict__ QF,
+                                                       double *__restrict__ FF, const double *__restrict__ nh,
+                                                       const double *__restrict__ nrm, const double *__restrict__ qext,
+                                                       BndPhys P) {
+  constexpr int G2 = G * G;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nm * G2) return;
+  const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
+  const MortarB M = mb[m];
+  const int bc = M.flags & 7;
+  const bool low = (M.flags >> 3) & 1;
+  double Q1[NV], Q2[NV], f[NV], qb[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) Q1[v] = QF[M.ms + v * G2 + pt];
+  const long long gp = (long long)M.geo * G2 + pt;
+  const double n3[3] = {nh[gp * 3], nh[gp * 3 + 1], nh[gp * 3 + 2]};
+  const double ds = nrm[gp];
+  if (bc == BC_WALLADIAB || bc == BC_WALLISOTH) {
+    wall_mirror(n3, Q1, Q2);
+    if (bc == BC_WALLADIAB) {
+      riemann(n3, ds, low ? Q2 : Q1, low ? Q1 : Q2, P.gamma, f);
+      qb[4] = Q1[4];
+    } else {
+      const double rho = Q2[0];
+      const double u = Q2[1] / rho, v = Q2[2] / rho, w = Q2[3] / rho;
+      Q2[4] = ddiv(rho * P.twall, P.cv, P.r_cv) + 0.5 * rho * (u * u + v * v + w * w);
+      if (low) {
+        const double mn[3] = {-n3[0], -n3[1], -n3[2]};
+        osher_flux(mn, -ds, Q1, Q2, P.gamma, f);
+      } else {
+        osher_flux(n3, ds, Q1, Q2, P.gamma, f);
+      }
+      qb[4] = ddiv(Q1[0] * P.twall, P.cv, P.r_cv);
+    }
+    qb[0] = Q1[0];
+    qb[1] = qb[2] = qb[3] = 0.0;
+  } else {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Q2[v] = qext[(long long)M.geo * NV * G2 + v * G2 + pt];
+    riemann(n3, ds, low ? Q2 : Q1, low ? Q1 : Q2, P.gamma, f);
+    riemann_state(n3, low ? Q2 : Q1, low ? Q1 : Q2, P.gamma, qb);
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    FF[M.ms + v * G2 + pt] = f[v];
+    QF[M.ms + v * G2 + pt] = qb[v];
+  }
+}
+
+// Viscous boundary faces: Vis_Neumann (Vis_Fluxes_new.f90:337-343).  Walls
+// keep the face's own viscous flux, with a zero energy flux on adiabatic walls
+// (wall_vis_flux, ViscousBC_slide.f90:279-348); inflow and outflow average it
+// with the external one (boundary_vis_flux, :183-225).
+template <int G>
+__global__ void __launch_bounds__(128) k_face_bnd_vis(const MortarB *__restrict__ mb, int nm, double *__restrict__ VF,
+                                                       const double *__restrict__ nrm,
+                                                       const double *__restrict__ fvext) {
+  constexpr int G2 = G * G;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nm * G2) return;
+  const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
+  const MortarB M = mb[m];
+  const int bc = M.flags & 7;
+  const bool neg_n = (M.flags >> 4) & 1;
+  const long long gp = (long long)M.geo * G2 + pt;
+  const double nm_m = nrm[gp], rm = 1.0 / nm_m;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double fv1 = ddiv(VF[M.ms + v * G2 + pt], nm_m, rm);
+    double qb;
+    if (bc == BC_WALLADIAB || bc == BC_WALLISOTH) {
+      qb = (v == 4 && bc == BC_WALLADIAB) ? 0.0 : fv1 * nm_m;
+    } else {
+      const double fx = fvext[(long long)M.geo * NV * G2 + v * G2 + pt];
+      const double Qs = neg_n ? -fx : fx;
+      qb = 0.5 * (fv1 + Qs) * nm_m;
+    }
+    VF[M.ms + v * G2 + pt] = qb;
+  }
+}
+
 // ------------------------------------------------------- nonconforming faces
 // One CTA per p-nonconforming mortar (lenmortar > len on at least one side).
 // Mirrors interface_flux / map_to_mortar_space / map_to_face_space /

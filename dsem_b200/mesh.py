@@ -116,11 +116,25 @@ def invert_metric(gx):
     return gc, J
 
 
-class Box:
-    """Periodic box of nex*ney*nez hex8 elements with per-element orders."""
+# d%bcond codes of faces without a neighbour (the C-ABI's DSEM_BC_*)
+BC_CODES = {"interface": 0, "walladiab": 1, "wallisoth": 2, "inflow": 3, "outflow": 4}
 
-    def __init__(self, nex, ney, nez, orders, length=2 * np.pi, rot=None, ldx=None):
+
+class Box:
+    """Box of nex*ney*nez hex8 elements with per-element orders, periodic in
+    every direction that `bc` does not name.  bc maps an axis ("x", "y", "z")
+    to the conditions of its low and high faces, e.g. {"y": ("walladiab",
+    "wallisoth")}; those faces become boundary mortars (id(2) = 0)."""
+
+    def __init__(self, nex, ney, nez, orders, length=2 * np.pi, rot=None, ldx=None, bc=None):
         self.nex, self.ney, self.nez = nex, ney, nez
+        self.length = float(length)
+        self.bc = {}
+        for ax, pair in (bc or {}).items():
+            codes = tuple(BC_CODES.get(x, -1) if isinstance(x, str) else int(x) for x in pair)
+            if len(codes) != 2 or not all(1 <= x <= 4 for x in codes):
+                raise ValueError("bc: two boundary conditions (low, high) per axis")
+            self.bc["xyz".index(ax)] = codes
         ne = nex * ney * nez
         self.nel = ne
         self.orders = np.broadcast_to(np.asarray(orders, dtype=np.int32), (ne,)).copy()
@@ -201,19 +215,36 @@ class Box:
                     if ids is not None and self.boundary[ids, fs - 1]:
                         yield idm, ids
 
-        for idm, ids in list(first_match(3, 5, 0, 4, [0, 1])):
-            pair(idm, 3, ids, 5, True)
-        for idm, ids in list(first_match(1, 2, 0, 3, [0, 2])):
-            pair(idm, 1, ids, 2, True)
-        for idm, ids in list(first_match(6, 4, 0, 1, [2, 1])):
-            pair(idm, 6, ids, 4, False)
+        if 2 not in self.bc:
+            for idm, ids in list(first_match(3, 5, 0, 4, [0, 1])):
+                pair(idm, 3, ids, 5, True)
+        if 1 not in self.bc:
+            for idm, ids in list(first_match(1, 2, 0, 3, [0, 2])):
+                pair(idm, 1, ids, 2, True)
+        if 0 not in self.bc:
+            for idm, ids in list(first_match(6, 4, 0, 1, [2, 1])):
+                pair(idm, 6, ids, 4, False)
         keep = [j for j in range(len(mort)) if j not in removed]
         newid = {j: i for i, j in enumerate(keep)}
         self.mort_raw = [mort[j] for j in keep]
         self.mort_geo_src = keep
         self.emort = np.vectorize(lambda j: newid.get(j, -1))(self.emort)
-        if any(m[1] < 0 for m in self.mort_raw):
-            raise ValueError("unpaired boundary faces remain")
+        # faces left without a neighbour lie on a non-periodic side: d%bcond
+        self.bcond = np.zeros((ne, 6), dtype=np.int32)
+        tol = 1e-9 * self.length
+        for m in self.mort_raw:
+            if m[1] >= 0:
+                continue
+            ctr = C[m[0], list(FACE_MAP[m[2] - 1])].mean(axis=0)
+            code = 0
+            for a, (lo, hi) in self.bc.items():
+                if abs(ctr[a]) < tol:
+                    code = lo
+                elif abs(ctr[a] - self.length) < tol:
+                    code = hi
+            if code == 0:
+                raise ValueError("unpaired boundary faces remain")
+            self.bcond[m[0], m[2] - 1] = code
 
     # ------------------------------------------------------------ geometry
     def _geometry(self):
@@ -266,6 +297,11 @@ class Box:
         self.n_hat = np.zeros((nm, ldx, ldx, 3))
         self.norm = np.zeros((nm, ldx, ldx))
         for j, (id1, id2, f1, f2, orient, sign) in enumerate(self.mort_raw):
+            if id2 < 0:  # boundary mortar: master face only, nsign = 1 (set_mortars.f90:361)
+                Gm = int(self.G[id1])
+                self.mortar[j] = [id1 + 1, 0, f1, 0, Gm, Gm, Gm, Gm, Gm, Gm, 0, 1, 1, 1, 1, 1, 1]
+                self._mortar_geometry(j, id1, f1, [Gm, Gm])
+                continue
             Gm, Gs = int(self.G[id1]), int(self.G[id2])
             j1, j2 = (1, 0) if orient >= 4 else (0, 1)
             lens = [[Gm, Gs], [Gm, Gs]]
@@ -319,7 +355,26 @@ class Box:
                     gmet=np.ascontiguousarray(self.gmet.ravel()),
                     mortar=np.ascontiguousarray(self.mortar.ravel()),
                     n_hat=np.ascontiguousarray(self.n_hat.ravel()),
-                    norm=np.ascontiguousarray(self.norm.ravel()))
+                    norm=np.ascontiguousarray(self.norm.ravel()),
+                    bcond=np.ascontiguousarray(self.bcond.ravel()) if self.bc else None)
+
+    def boundary_mortars(self):
+        """Indices of the boundary mortars (id(2) = 0)."""
+        return np.where(self.mortar[:, 1] == 0)[0]
+
+    def mortar_xyz(self):
+        """Physical coordinates of the mortar Gauss points [nmort][ldx][ldx][3]
+        (j, i order as mrtr%xg; zero in the padding)."""
+        out = np.zeros((self.nmort, self.ldx, self.ldx, 3))
+        for j in range(self.nmort):
+            e, face, G = int(self.mortar[j, 0]) - 1, int(self.mortar[j, 2]), int(self.mortar[j, 8])
+            d = FACE_DIR[face]
+            c1 = gauss_points(G)
+            A, B = c1[None, :], c1[:, None]
+            end = np.full_like(A * B, END_VALS[face - 1])
+            X, Y, Z = {1: (A + 0 * B, end, B + 0 * A), 2: (A + 0 * B, B + 0 * A, end), 0: (end, A + 0 * B, B + 0 * A)}[d]
+            out[j, :G, :G] = hex8(self.corner[e], X, Y, Z)
+        return out
 
     def gauss_xyz(self):
         """Physical Gauss-point coordinates [nel][ldx^3][3] (zero in the padding)."""
@@ -439,6 +494,24 @@ def perturbed_taylor_green(box, seed, amp=0.05, k0=2.0, gamma=1.4, twall=100.0):
     u = np.stack([np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z), np.zeros_like(x)], -1) + ut
     p = twall * 1.0 / gamma + (np.cos(2.0 * x) + np.cos(2.0 * y)) * (np.cos(2.0 * z) + 2.0) / 16.0
     return _jq(box, np.ones_like(x), u, p, gamma)
+
+
+def boundary_state(box, rho, vel, p, gamma=1.4, seed=None, amp=0.0):
+    """External states of the boundary mortars ([nmort][5][ldx][ldx], the
+    mrtr%Q(:,:,:,2) that initc / inflow_time_bc fill): a uniform stream of
+    density rho, velocity vel and pressure p, optionally with a seeded relative
+    perturbation of size amp on every conserved variable."""
+    out = np.zeros((box.nmort, NV, box.ldx, box.ldx))
+    u, v, w = (float(x) for x in vel)
+    q = np.array([rho, rho * u, rho * v, rho * w, p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)])
+    rng = np.random.default_rng(seed) if seed is not None else None
+    for j in box.boundary_mortars():
+        G = int(box.mortar[j, 8])
+        blk = np.broadcast_to(q[:, None, None], (NV, G, G)).copy()
+        if rng is not None and amp:
+            blk *= 1.0 + amp * rng.standard_normal(blk.shape)
+        out[j, :, :G, :G] = blk
+    return out
 
 
 def dtcalc(box, JQ, gamma=1.4):

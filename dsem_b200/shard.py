@@ -42,8 +42,10 @@ def slab_partition(box, nparts, axis=0):
 def partition(desc, part):
     """Per-part descriptors and exchange plans.
 
-    Returns a list over parts of dicts {desc, elements (global ids),
-    plan: [(neighbour, ghost_start, count)], ghosts: [global mortar ids]}."""
+    Returns a list over parts of dicts {desc, elements (global ids), mortars
+    (global ids of the part's mortar rows), plan: [(neighbour, ghost_start,
+    count)], ghosts: [global mortar ids]}.  Boundary mortars (id(2) = 0) go
+    with their element."""
     part = np.asarray(part, dtype=np.int64)
     ne, nm, ldx = int(desc["ngrid"]), int(desc["nmort"]), int(desc["ldx"])
     nparts = int(part.max()) + 1
@@ -55,6 +57,7 @@ def partition(desc, part):
     gg = np.asarray(desc["gmetg"]).reshape(ne, L3 * 9)
     gm = np.asarray(desc["gmet"]).reshape(ne, L3 * 9)
     ncg = np.asarray(desc["ncg"]).reshape(ne, 3)
+    bcond = None if desc.get("bcond") is None else np.asarray(desc["bcond"], dtype=np.int32).reshape(ne, 6)
     out = []
     for r in range(nparts):
         els = np.where(part == r)[0]
@@ -64,6 +67,12 @@ def partition(desc, part):
         cut = []
         for j in range(nm):
             e1, e2 = int(mort[j, 0]) - 1, int(mort[j, 1]) - 1
+            if e2 < 0:  # boundary face: stays with its element
+                if part[e1] == r:
+                    t = mort[j].copy()
+                    t[0] = local[e1] + 1
+                    rows.append((j, t))
+                continue
             p1, p2 = part[e1], part[e2]
             if p1 != r and p2 != r:
                 continue
@@ -98,8 +107,10 @@ def partition(desc, part):
                  gmet=np.ascontiguousarray(gm[els].ravel()),
                  mortar=np.ascontiguousarray(np.array([t for _, t in rows], dtype=np.int32).ravel()),
                  n_hat=np.ascontiguousarray(nh[js].ravel()),
-                 norm=np.ascontiguousarray(nr[js].ravel()))
-        out.append(dict(desc=d, elements=els, plan=[tuple(p) for p in plan], ghosts=ghosts))
+                 norm=np.ascontiguousarray(nr[js].ravel()),
+                 bcond=None if bcond is None else np.ascontiguousarray(bcond[els].ravel()))
+        out.append(dict(desc=d, elements=els, mortars=np.asarray(js, dtype=np.int64), plan=[tuple(p) for p in plan],
+                        ghosts=ghosts))
     return out
 
 
@@ -141,6 +152,12 @@ class ShardedRun:
     def set_les(self, cs, numax):
         for s in self.shards:
             s.set_les(cs, numax)
+
+    def set_boundary(self, twall, Qext=None, fvext=None):
+        """As Solver.set_boundary, with the unsharded mesh's [nmort][5][ldx][ldx] arrays."""
+        for p, s in zip(self.parts, self.shards):
+            s.set_boundary(twall, None if Qext is None else Qext[p["mortars"]],
+                           None if fvext is None else fvext[p["mortars"]])
 
     def upload(self, JQ):
         for p, s in zip(self.parts, self.shards):

@@ -19,7 +19,8 @@ EXPORTS = ("dsem_create", "dsem_destroy", "dsem_last_error", "dsem_upload_q", "d
            "dsem_stage", "dsem_rhs", "dsem_diag", "dsem_get_muhg", "dsem_last_timing", "dsem_profile_rhs",
            "dsem_create_batch", "dsem_batch_size", "dsem_upload_q_case", "dsem_download_q_case", "dsem_step_batch",
            "dsem_diag_batch", "dsem_adjoint", "dsem_set_les", "dsem_get_nut", "dsem_state_size",
-           "dsem_save_state", "dsem_load_state", "dsem_shard_info", "dsem_shard_stage", "dsem_diag_sums")
+           "dsem_save_state", "dsem_load_state", "dsem_shard_info", "dsem_shard_stage", "dsem_diag_sums",
+           "dsem_set_boundary")
 
 
 class DsemError(RuntimeError):
@@ -31,7 +32,8 @@ class DsemError(RuntimeError):
 class MeshDesc(C.Structure):
     _fields_ = [("ngrid", C.c_int), ("nmort", C.c_int), ("ldx", C.c_int), ("ncg", C.POINTER(C.c_int)),
                 ("jacob", C.POINTER(C.c_double)), ("gmetg", C.POINTER(C.c_double)), ("gmet", C.POINTER(C.c_double)),
-                ("mortar", C.POINTER(C.c_int)), ("n_hat", C.POINTER(C.c_double)), ("norm", C.POINTER(C.c_double))]
+                ("mortar", C.POINTER(C.c_int)), ("n_hat", C.POINTER(C.c_double)), ("norm", C.POINTER(C.c_double)),
+                ("bcond", C.POINTER(C.c_int))]
 
 
 class Phys(C.Structure):
@@ -73,6 +75,7 @@ def lib(path=None):
         L.dsem_step_batch.argtypes = [vp, dp, C.c_int]
         L.dsem_diag_batch.argtypes = [vp, dp, C.c_int, dp, dp, dp]
         L.dsem_set_les.argtypes = [vp, C.c_double, C.c_double]
+        L.dsem_set_boundary.argtypes = [vp, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]
         L.dsem_shard_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(dp), C.POINTER(dp)]
         L.dsem_shard_stage.argtypes = [vp, C.c_double, C.c_int, C.c_int]
         L.dsem_diag_sums.argtypes = [vp, dp]
@@ -97,8 +100,12 @@ def _mesh_desc(desc):
     """(MeshDesc, arrays kept alive while the descriptor is in use)."""
     a = {k: np.ascontiguousarray(desc[k]) for k in ("ncg", "jacob", "gmetg", "gmet", "mortar", "n_hat", "norm")}
     assert a["ncg"].dtype == np.int32 and a["mortar"].dtype == np.int32
+    bc = desc.get("bcond")
+    if bc is not None:
+        a["bcond"] = np.ascontiguousarray(bc, dtype=np.int32)
     md = MeshDesc(int(desc["ngrid"]), int(desc["nmort"]), int(desc["ldx"]), _iptr(a["ncg"]), _dptr(a["jacob"]),
-                  _dptr(a["gmetg"]), _dptr(a["gmet"]), _iptr(a["mortar"]), _dptr(a["n_hat"]), _dptr(a["norm"]))
+                  _dptr(a["gmetg"]), _dptr(a["gmet"]), _iptr(a["mortar"]), _dptr(a["n_hat"]), _dptr(a["norm"]),
+                  _iptr(a["bcond"]) if bc is not None else None)
     return md, a
 
 
@@ -185,6 +192,17 @@ class Solver:
     def load_state(self, buf):
         buf = np.ascontiguousarray(buf, dtype=np.uint8)
         self._check(lib().dsem_load_state(self.h, buf.ctypes.data_as(C.c_void_p), buf.size))
+
+    def set_boundary(self, twall, Qext=None, fvext=None):
+        """Wall temperature and external states of the boundary mortars
+        ([nmort][5][ldx][ldx] each, or None)."""
+        keep = [None if x is None else np.ascontiguousarray(x, dtype=np.float64) for x in (Qext, fvext)]
+        ldx = next((x.shape[-1] for x in keep if x is not None), self.ldx)
+        for x in keep:
+            if x is not None and x.shape != (self.nmort, 5, ldx, ldx):
+                raise ValueError("external states are [nmort][5][ldx][ldx]")
+        self._check(lib().dsem_set_boundary(self.h, float(twall), None if keep[0] is None else _dptr(keep[0]),
+                                            None if keep[1] is None else _dptr(keep[1]), int(ldx)))
 
     def set_les(self, cs, numax):
         """Static Smagorinsky model (cs = 0: off)."""

@@ -62,7 +62,17 @@ typedef struct {
   const int *mortar;     /* [nmort][DSEM_MORTAR_INTS]                                   */
   const double *n_hat;   /* [nmort][ldx][ldx][3]  mrtr%n_hat(3,nmax,nmax)               */
   const double *norm;    /* [nmort][ldx][ldx]     mrtr%norm(nmax,nmax)                  */
+  const int *bcond;      /* [ngrid][6] d%bcond as DSEM_BC_* codes; read for the master
+                            faces of boundary mortars (id(2) = 0). NULL: no boundary   */
 } dsem_mesh_desc;
+
+/* d%bcond values of faces without a neighbour (boundary_flux / DirichletBC /
+ * Vis_Neumann in caseFiles/tgv/BackstepProblem-stoch.f90:1602-1729). */
+#define DSEM_BC_INTERFACE 0
+#define DSEM_BC_WALLADIAB 1 /* 'walladiab': wallbc_Inv, set_adiabatic_wall, wall_vis_flux   */
+#define DSEM_BC_WALLISOTH 2 /* 'wallisoth': wallbc_isoth (osher), set_isothermal_wall        */
+#define DSEM_BC_INFLOW 3    /* 'inflow':  inflow_specAll, boundary_values, boundary_vis_flux */
+#define DSEM_BC_OUTFLOW 4   /* 'outflow': outflow_specAll, boundary_values, boundary_vis_flux */
 
 /* Physics and time-integration parameters (MODULE physics, input_data, rk_coefs). */
 typedef struct {
@@ -142,6 +152,19 @@ int dsem_get_nut(dsem_ctx *ctx, double *nu, int ldx);
 int dsem_state_size(const dsem_ctx *ctx, long long *nbytes);
 int dsem_save_state(dsem_ctx *ctx, void *buf, long long nbytes);
 int dsem_load_state(dsem_ctx *ctx, const void *buf, long long nbytes);
+
+/* ---- Boundary faces (mortars with id(2) = 0) ----
+ * Sets the wall temperature of isothermal walls (MODULE physics twall) and,
+ * for inflow and outflow faces, the external state and viscous flux that DSEM
+ * keeps in mrtr%Q(:,:,:,2) and mrtr%fv(:,:,:,2) (set by initc / exactsol and
+ * updated between steps by inflow_time_bc, BackstepProblem-stoch.f90:1275-1443,
+ * 2077-2165).  Qext and fvext are [nmort][5][ldx][ldx] over all mortars of the
+ * descriptor, point (i,j) of variable v of mortar k at i + ldx*(j + ldx*(v +
+ * 5*k)); only boundary mortars are read.  Either may be NULL (fvext starts at
+ * zero).  Call it before the first stage when the mesh has isothermal walls
+ * (twall) or inflow/outflow faces (Qext); stepping fails otherwise.  It may be
+ * called again between steps. */
+int dsem_set_boundary(dsem_ctx *ctx, double twall, const double *Qext, const double *fvext, int ldx);
 
 /* ---- One case sharded over several GPUs (one context per GPU) ----
  * The replacement for DSEM's MPI face exchange (send_q_to_mortars_mpi,

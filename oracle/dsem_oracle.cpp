@@ -278,6 +278,7 @@ template <class T> struct Elem {
   int mside[6] = {0, 0, 0, 0, 0, 0};  // 1 master, 2 slave
   int orientation[6] = {};
   bool boundary[6] = {};
+  int bcond[6] = {};  // d%bcond as BC_* codes (faces without a neighbour)
   std::vector<double> jacob, gmetg, gmet[3], xg, hdelta;
   std::vector<T> Q, gQ, QL[3], F[3], R[3], muhg, muh[3], nutg, nut[3];
   size_t ng() const { return (size_t)G * G * G; }
@@ -294,7 +295,12 @@ template <class T> struct Mortar {
   std::vector<double> P[2][2], Rm[2][2];           // [side][dir]
   int pin[2][2] = {};                              // input extent of P[side][dir]
   std::vector<T> Qm[2], fv[2];                     // [v][j*NMX+i]
+  int bc = 0;                                      // boundary mortar (id(2) = 0): bcond of the master face
+  std::vector<double> Qx, fvx;                     // external mrtr%Q(:,:,:,2), mrtr%fv(:,:,:,2): [v][j*NMX+i]
 };
+
+// boundary condition codes (the CHARACTER d%bcond values of the problem file)
+enum { BC_INTERFACE = 0, BC_WALLADIAB = 1, BC_WALLISOTH = 2, BC_INFLOW = 3, BC_OUTFLOW = 4 };
 
 template <class T> struct Case {
   std::vector<Elem<T>> el;
@@ -307,6 +313,7 @@ template <class T> struct Case {
   double ark[5] = {}, brk[5] = {}, crk[5] = {};
   bool ql_valid = false;
   double prestep = 0.0;
+  double twall = 0.0;  // wall temperature of isothermal walls (MODULE physics)
 };
 
 // -------------------------------------------------- rkcoefs (baselib.f90:86-160)
@@ -660,12 +667,179 @@ template <class T> void map_to_face(const Mortar<T> &M, int side, const std::vec
   }
 }
 
+// ------------------------------------------ boundary mortars (NS/BCs/stac3m)
+// The external state of a wall: equal density and energy, normal momentum
+// reversed (wallbc_Inv, wallbc_inv.f90:32-50; wallbc_isoth, wallbc_isoth2.f90:31-54).
+template <class T> void wall_mirror(const double *nh, const T *Q1, T *Q2) {
+  T qnorm = nh[0] * Q1[1] + nh[1] * Q1[2] + nh[2] * Q1[3];
+  T q_tanx = Q1[1] - qnorm * nh[0];
+  T q_tany = Q1[2] - qnorm * nh[1];
+  T q_tanz = Q1[3] - qnorm * nh[2];
+  Q2[0] = Q1[0];
+  Q2[1] = q_tanx - qnorm * nh[0];
+  Q2[2] = q_tany - qnorm * nh[1];
+  Q2[3] = q_tanz - qnorm * nh[2];
+  Q2[4] = Q1[4];
+}
+
+// osher (PhysLib.f90:698-790): the state between the two normal Riemann
+// invariants and its Euler flux (fflux/gflux/hflux, PhysLib.f90:17-124).
+template <class T> void osher(const double *nh, double ds, const T *Ql, const T *Qr, double gamma, T *flux) {
+  const double en1 = nh[0], en2 = nh[1], en3 = nh[2];
+  T rho = Ql[0], rhou = Ql[1], rhov = Ql[2], rhow = Ql[3], rhoe = Ql[4];
+  T rhon = Qr[0], rhoun = Qr[1], rhovn = Qr[2], rhown = Qr[3], rhoen = Qr[4];
+  T qdotn = (en1 * rhou + en2 * rhov + en3 * rhow) / rho;
+  T qdotnn = (en1 * rhoun + en2 * rhovn + en3 * rhown) / rhon;
+  T p = (gamma - 1.0) * (rhoe - 0.5 / rho * (rhou * rhou + rhov * rhov + rhow * rhow));
+  T a = std::sqrt(gamma * p / rho);
+  T pn = (gamma - 1.0) * (rhoen - 0.5 / rhon * (rhoun * rhoun + rhovn * rhovn + rhown * rhown));
+  T an = std::sqrt(gamma * pn / rhon);
+  T q_tanx = rhoun / rhon - qdotnn * en1;
+  T q_tany = rhovn / rhon - qdotnn * en2;
+  T q_tanz = rhown / rhon - qdotnn * en3;
+  const double z = (gamma - 1.0) / (2.0 * gamma);
+  T Ha = -qdotnn / an + 2.0 / (gamma - 1.0);
+  Ha = Ha / (qdotn / a + 2.0 / (gamma - 1.0));
+  pn = p / std::pow(Ha, 1.0 / z);
+  T pstar = a + an - (qdotnn - qdotn) * (gamma - 1.0) / 2.0;
+  pstar = pstar / (a / std::pow(p, z) + an / std::pow(pn, z));
+  pstar = std::pow(pstar, 1.0 / z);
+  T ustar = Ha * qdotn / a + qdotnn / an + 2.0 * (Ha - 1.0) / (gamma - 1.0);
+  ustar = ustar / (Ha / a + 1.0 / an);
+  T rho23 = pstar * gamma / (an * an);
+  rho = rho23;
+  p = pstar;
+  qdotn = ustar;
+  T u = q_tanx + en1 * qdotn, v = q_tany + en2 * qdotn, w = q_tanz + en3 * qdotn;
+  T Q[NV] = {rho, rho * u, rho * v, rho * w, p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)};
+  T f[NV], g[NV], h[NV];
+  euler_fluxes(Q, gamma, f, g, h);
+  for (int k = 0; k < NV; ++k) flux[k] = ds * (en1 * f[k] + en2 * g[k] + en3 * h[k]);
+}
+
+// riemann_solution (PhysLib.f90:326-412): the interface state from the normal
+// Riemann invariants (used for the Dirichlet values of inflow and outflow).
+template <class T> void riemann_solution(const double *nh, const T *Ql, const T *Qr, double gamma, T *Q) {
+  const double en1 = nh[0], en2 = nh[1], en3 = nh[2];
+  T rho = Ql[0], rhou = Ql[1], rhov = Ql[2], rhow = Ql[3], rhoe = Ql[4];
+  T rhon = Qr[0], rhoun = Qr[1], rhovn = Qr[2], rhown = Qr[3], rhoen = Qr[4];
+  T qdotn = (en1 * rhou + en2 * rhov + en3 * rhow) / rho;
+  T qdotnn = (en1 * rhoun + en2 * rhovn + en3 * rhown) / rhon;
+  T p = (gamma - 1.0) * (rhoe - 0.5 / rho * (rhou * rhou + rhov * rhov + rhow * rhow));
+  T a = std::sqrt(gamma * p / rho);
+  T pn = (gamma - 1.0) * (rhoen - 0.5 / rhon * (rhoun * rhoun + rhovn * rhovn + rhown * rhown));
+  T an = std::sqrt(gamma * pn / rhon);
+  T e0 = 0.5 * (qdotn + qdotnn);
+  T eplus = e0 + 0.5 * (a + an);
+  T eminus = e0 - 0.5 * (a + an);
+  T etos, q_tanx, q_tany, q_tanz;
+  if (re_(e0) > 0.0) {
+    etos = p / std::pow(rho, gamma);
+    q_tanx = rhou / rho - qdotn * en1;
+    q_tany = rhov / rho - qdotn * en2;
+    q_tanz = rhow / rho - qdotn * en3;
+  } else {
+    etos = pn / std::pow(rhon, gamma);
+    q_tanx = rhoun / rhon - qdotnn * en1;
+    q_tany = rhovn / rhon - qdotnn * en2;
+    q_tanz = rhown / rhon - qdotnn * en3;
+  }
+  T rplus = re_(eplus) >= 0.0 ? qdotn + 2.0 / (gamma - 1.0) * a : qdotnn + 2.0 / (gamma - 1.0) * an;
+  T rminus = re_(eminus) >= 0.0 ? qdotn - 2.0 / (gamma - 1.0) * a : qdotnn - 2.0 / (gamma - 1.0) * an;
+  qdotn = 0.5 * (rplus + rminus);
+  a = 0.25 * (gamma - 1.0) * (rplus - rminus);
+  rho = std::pow(a * a / (gamma * etos), 1.0 / (gamma - 1.0));
+  p = std::pow(rho, gamma) * etos;
+  T u = q_tanx + en1 * qdotn, v = q_tany + en2 * qdotn, w = q_tanz + en3 * qdotn;
+  Q[0] = rho;
+  Q[1] = rho * u;
+  Q[2] = rho * v;
+  Q[3] = rho * w;
+  Q[4] = p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w);
+}
+
+// Inviscid boundary mortar: boundary_flux, then DirichletBC and send_q_to_faces
+// (fluxesH_newa.f90:116-139; BackstepProblem-stoch.f90:1602-1689;
+// wallbc_inv.f90, wallbc_isoth2.f90, inflow_specAll.f90, outflow_specAll.f90,
+// set_adiabatic_wall / set_isothermal_wall / boundary_values in ViscousBC_slide.f90).
+// Boundary mortars are conforming with orient 0: the master face only.
+template <class T> void boundary_inviscid(Case<T> &c, Mortar<T> &M) {
+  std::vector<T> Q1;
+  gather_face(c, M, 0, c.el[M.id[0]].QL, Q1);
+  Elem<T> &Em = c.el[M.id[0]];
+  const bool low = (M.iface[0] == 1 || M.iface[0] == 3 || M.iface[0] == 6);
+  const double cv = c.mach * c.mach * c.gamma * (c.gamma - 1.0);
+  for (int j = 0; j < M.lenm[1]; ++j)
+    for (int i = 0; i < M.lenm[0]; ++i) {
+      const int pt = j * NMX + i;
+      const double *nh = &M.n_hat[pt * 3];
+      const double ds = M.norm[pt];
+      T q1[NV], q2[NV], f[NV], qb[NV];
+      for (int v = 0; v < NV; ++v) q1[v] = Q1[v * NMX * NMX + pt];
+      if (M.bc == BC_WALLADIAB || M.bc == BC_WALLISOTH) {
+        wall_mirror(nh, q1, q2);
+        if (M.bc == BC_WALLADIAB) {
+          riemann(nh, ds, low ? q2 : q1, low ? q1 : q2, c.gamma, f);
+          qb[4] = q1[4];
+        } else {
+          T rho = q2[0], u = q2[1] / rho, v = q2[2] / rho, w = q2[3] / rho;
+          q2[4] = rho * c.twall / cv + 0.5 * rho * (u * u + v * v + w * w);
+          if (low) {
+            const double mn[3] = {-nh[0], -nh[1], -nh[2]};
+            osher(mn, -ds, q1, q2, c.gamma, f);
+          } else {
+            osher(nh, ds, q1, q2, c.gamma, f);
+          }
+          qb[4] = q1[0] * c.twall / cv;
+        }
+        qb[0] = q1[0];
+        qb[1] = qb[2] = qb[3] = T(0.0);
+      } else {  // inflow, outflow: the external state is the neighbour
+        for (int v = 0; v < NV; ++v) q2[v] = T(M.Qx[v * NMX * NMX + pt]);
+        riemann(nh, ds, low ? q2 : q1, low ? q1 : q2, c.gamma, f);
+        riemann_solution(nh, low ? q2 : q1, low ? q1 : q2, c.gamma, qb);
+      }
+      for (int v = 0; v < NV; ++v) {
+        face_ref(Em.F, Em, M.iface[0], i, j, v) = f[v];
+        face_ref(Em.QL, Em, M.iface[0], i, j, v) = qb[v];
+      }
+    }
+}
+
+// Viscous boundary mortar: Vis_Neumann (BackstepProblem-stoch.f90:1693-1729)
+// with wall_vis_flux / boundary_vis_flux (ViscousBC_slide.f90:183-348), then
+// send_flux_to_faces_add on the master face.
+template <class T> void boundary_viscous(Case<T> &c, Mortar<T> &M) {
+  std::vector<T> r1;
+  gather_face(c, M, 0, c.el[M.id[0]].R, r1);
+  Elem<T> &Em = c.el[M.id[0]];
+  for (int j = 0; j < M.lenm[1]; ++j)
+    for (int i = 0; i < M.lenm[0]; ++i) {
+      const int pt = j * NMX + i;
+      const double nrm = M.norm[pt];
+      for (int v = 0; v < NV; ++v) {
+        T fv1 = r1[v * NMX * NMX + pt] / nrm;
+        T qb;
+        if (M.bc == BC_WALLADIAB || M.bc == BC_WALLISOTH) {
+          qb = (v == 4 && M.bc == BC_WALLADIAB) ? T(0.0) : fv1 * nrm;
+        } else {
+          T Qs = T(M.fvx[v * NMX * NMX + pt]);
+          if (M.nsign == -1) Qs = -Qs;
+          qb = 0.5 * (fv1 + Qs) * nrm;
+        }
+        T &F = face_ref(Em.F, Em, M.iface[0], i, j, v);
+        F = F - qb / c.re;
+      }
+    }
+}
+
 // Inviscid mortar: interface_flux + send_flux_to_faces + V_Avg_Soln + send_q_to_faces
 // (mortar_operations.f90:151-238, 781-837; send_flux.f90:22-236; send_q.f90:21-280).
 // Nonconforming faces use the consistent prolong -> flux/average -> restrict
 // sequence (DSEM maps the averaged state twice and writes mortar-space data
 // into face slots; those are documented deviations).
 template <class T> void mortar_inviscid(Case<T> &c, Mortar<T> &M) {
+  if (M.id[1] < 0) return boundary_inviscid(c, M);
   std::vector<T> Q1, Q2;
   gather_face(c, M, 0, c.el[M.id[0]].QL, Q1);
   gather_face(c, M, 1, c.el[M.id[1]].QL, Q2);
@@ -787,6 +961,7 @@ template <class T> void vis_element(Case<T> &c, Elem<T> &E) {
 // slave's fv is divided by the mortar norm at the slave's face index before
 // rotation); nonconforming faces use the consistent prolong/restrict path.
 template <class T> void mortar_viscous(Case<T> &c, Mortar<T> &M) {
+  if (M.id[1] < 0) return boundary_viscous(c, M);
   std::vector<T> r1, r2;
   gather_face(c, M, 0, c.el[M.id[0]].R, r1);
   gather_face(c, M, 1, c.el[M.id[1]].R, r2);
@@ -1848,6 +2023,39 @@ void orc_set_phys(orc_case *h, double gamma, double re, double pr, double mach, 
       E.muhg.assign(E.ng(), 0.0);
       for (int d = 0; d < 3; ++d) E.muh[d].assign(E.nl(), 0.0);
     }
+}
+// d%bcond of every element face ([ngrid][6], BC_* codes); boundary mortars
+// (id(2) = 0) take the code of their master face
+int orc_set_bcond(orc_case *h, const int *bcond) {
+  auto &c = *h->c;
+  for (size_t e = 0; e < c.el.size(); ++e)
+    for (int f = 0; f < 6; ++f) c.el[e].bcond[f] = bcond[6 * e + f];
+  for (auto &M : c.mo) {
+    if (M.id[1] >= 0) continue;
+    M.bc = c.el[M.id[0]].bcond[M.iface[0] - 1];
+    if (M.bc < BC_WALLADIAB || M.bc > BC_OUTFLOW) return -1;
+  }
+  return 0;
+}
+// twall and the external mrtr%Q(:,:,:,2) / mrtr%fv(:,:,:,2) of the boundary
+// mortars ([nmort][5][ldx][ldx], i fastest; a null array keeps the previous
+// values, zero initially)
+void orc_set_boundary(orc_case *h, double twall, const double *Qx, const double *fvx, int ldx) {
+  auto &c = *h->c;
+  c.twall = twall;
+  for (size_t j = 0; j < c.mo.size(); ++j) {
+    auto &M = c.mo[j];
+    if (M.id[1] >= 0) continue;
+    if (M.Qx.empty()) M.Qx.assign(NV * NMX * NMX, 0.0);  // a null array keeps the previous state
+    if (M.fvx.empty()) M.fvx.assign(NV * NMX * NMX, 0.0);
+    for (int v = 0; v < NV; ++v)
+      for (int jj = 0; jj < M.lenm[1]; ++jj)
+        for (int i = 0; i < M.lenm[0]; ++i) {
+          const size_t q = (((size_t)j * NV + v) * ldx + jj) * ldx + i;
+          if (Qx) M.Qx[v * NMX * NMX + jj * NMX + i] = Qx[q];
+          if (fvx) M.fvx[v * NMX * NMX + jj * NMX + i] = fvx[q];
+        }
+  }
 }
 int orc_nel(const orc_case *h) { return (int)h->c->el.size(); }
 int orc_nmort(const orc_case *h) { return (int)h->c->mo.size(); }

@@ -90,6 +90,11 @@ void orc_rk(const orc_case *c, double *ark, double *brk, double *crk);
  * clip numax; evaluated at the start of each step like the entropy viscosity.
  * orc_get_nut: its Gauss-point viscosity after the last evaluation. */
 void orc_set_les(orc_case *c, double cs, double numax);
+/* boundary faces: d%bcond per element face ([ngrid][6]: 1 walladiab, 2 wallisoth,
+ * 3 inflow, 4 outflow), then twall and the external mortar states
+ * ([nmort][5][ldx][ldx], i fastest; null without inflow/outflow faces) */
+int orc_set_bcond(orc_case *c, const int *bcond);
+void orc_set_boundary(orc_case *c, double twall, const double *Qx, const double *fvx, int ldx);
 void orc_get_nut(const orc_case *c, double *nu, int ldx);
 /* Objective of the adjoint, J = sum over the last `window` of `nsteps` steps of
  * dt * enst (orc_diag's enstrophy dissipation after each step), evaluated from

@@ -60,6 +60,9 @@ def lib():
         L.orc_set_threads.restype = C.c_int
         L.orc_rk.argtypes = [vp, _dp, _dp, _dp]
         L.orc_set_les.argtypes = [vp, C.c_double, C.c_double]
+        L.orc_set_bcond.argtypes = [vp, _ip]
+        L.orc_set_bcond.restype = C.c_int
+        L.orc_set_boundary.argtypes = [vp, C.c_double, vp, vp, C.c_int]
         L.orc_get_nut.argtypes = [vp, _dp, C.c_int]
         L.orc_objective_cs.argtypes = [vp, C.c_double, C.c_int, C.c_int, vp, C.c_double, C.c_int,
                                        C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -136,7 +139,26 @@ class Case:
     def from_desc(cls, d):
         h = lib().orc_from_desc(d["ngrid"], d["nmort"], d["ldx"], d["ncg"], d["jacob"], d["gmetg"], d["gmet"],
                                 d["mortar"], d["n_hat"], d["norm"])
-        return cls(h)
+        c = cls(h)
+        if d.get("bcond") is not None:
+            c.set_bcond(d["bcond"])
+        return c
+
+    def set_bcond(self, bcond):
+        """d%bcond per element face ([ngrid][6] codes: 1 walladiab, 2 wallisoth, 3 inflow, 4 outflow)."""
+        b = np.ascontiguousarray(bcond, dtype=np.int32).ravel()
+        if lib().orc_set_bcond(self.h, b) != 0:
+            raise ValueError("a boundary mortar's master face has no boundary condition")
+
+    def set_boundary(self, twall, Qx=None, fvx=None):
+        """twall and the external states of the boundary mortars ([nmort][5][ldx][ldx])."""
+        keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (Qx, fvx)]
+        ldx = next((a.shape[-1] for a in keep if a is not None), self.ldx)
+        for a in keep:
+            if a is not None and a.shape != (self.nmort, 5, ldx, ldx):
+                raise ValueError("external states are [nmort][5][ldx][ldx]")
+        ptr = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+        lib().orc_set_boundary(self.h, float(twall), ptr(keep[0]), ptr(keep[1]), ldx)
 
     def __del__(self):
         try:

@@ -1,0 +1,118 @@
+"""Boundary faces (mortars with id(2) = 0) on the CPU: the mesh builder's
+boundary mortars, and properties of the oracle's restatement of DSEM's wall,
+inflow and outflow conditions (caseFiles/tgv/BackstepProblem-stoch.f90:1602-1729
+with NS/BCs/stac3m) that hold for the reference algorithm itself:
+
+* free-stream preservation: a uniform state at rest between walls (adiabatic,
+  or isothermal at the state's own temperature), and a uniform stream through
+  inflow/outflow faces whose external state is that stream, has a zero
+  right-hand side up to rounding;
+* a wall without normal velocity passes no mass: the Roe flux of two equal
+  states has a zero mass component, so the domain's mass changes only by
+  rounding."""
+import numpy as np
+import pytest
+
+from dsem_b200 import mesh
+
+TWALL = 100.0
+GAMMA = 1.4
+
+
+def _weights(G):
+    """Interpolatory quadrature weights on [0, 1] at the Gauss points (exact to degree G-1)."""
+    x = mesh.gauss_points(G)
+    V = np.array([np.polynomial.legendre.Legendre.basis(k)(2.0 * x - 1.0) for k in range(G)])
+    rhs = np.zeros(G)
+    rhs[0] = 1.0
+    return np.linalg.solve(V, rhs)
+
+
+def _uniform(box, rho, vel, p):
+    q = np.zeros(box.qshape())
+    u, v, w = vel
+    cons = [rho, rho * u, rho * v, rho * w, p / (GAMMA - 1.0) + 0.5 * rho * (u * u + v * v + w * w)]
+    jac = box.jacob.reshape(box.nel, box.ldx, box.ldx, box.ldx)
+    for e in range(box.nel):
+        G = int(box.G[e])
+        for k in range(5):
+            q[e, k, :G, :G, :G] = cons[k] / jac[e, :G, :G, :G]
+    return q
+
+
+def test_box_boundary_mortars():
+    box = mesh.Box(2, 3, 2, 3, bc={"y": ("walladiab", "wallisoth")})
+    b = box.boundary_mortars()
+    assert len(b) == 2 * 2 * 2  # nex * nez faces on each of the two y sides
+    rows = box.mortar[b]
+    assert np.all(rows[:, 1] == 0) and np.all(rows[:, 10] == 0) and np.all(rows[:, 12] == 1)
+    bc = box.bcond
+    for r in rows:
+        e, f = r[0] - 1, r[2]
+        assert f in (1, 2)  # y faces of unrotated elements
+        assert bc[e, f - 1] == (1 if f == 1 else 2)
+    assert int((bc > 0).sum()) == len(b)
+    # x and z stay periodic (12 + 12 mortars), y has 8 interior and 8 boundary mortars
+    assert box.nmort == 12 + 12 + 8 + 8
+    with pytest.raises(ValueError):
+        mesh.Box(2, 2, 2, 3, bc={"y": ("walladiab", "slip")})
+    assert mesh.Box(2, 2, 2, 3).desc()["bcond"] is None
+
+
+@pytest.mark.parametrize("bc", [{"y": ("walladiab", "walladiab")}, {"y": ("wallisoth", "walladiab")},
+                                {"x": ("inflow", "outflow"), "z": ("wallisoth", "wallisoth")}])
+def test_free_stream_preserved(oracle_mod, bc):
+    box = mesh.Box(2, 3, 2, 4, bc=bc)
+    rho, p = 1.0, TWALL / GAMMA  # T = twall with mach = 1: E = rho twall / (gamma (gamma-1))
+    q = _uniform(box, rho, (0.0, 0.0, 0.0), p)
+    c = oracle_mod.Case.from_desc(box.desc())
+    c.set_phys(re=400.0)
+    c.set_q(q)
+    c.set_boundary(TWALL, mesh.boundary_state(box, rho, (0.0, 0.0, 0.0), p),
+                   np.zeros((box.nmort, 5, box.ldx, box.ldx)))
+    qt = c.rhs()
+    assert np.abs(qt).max() <= 1e-10 * p
+
+
+def test_free_stream_through_inflow_outflow(oracle_mod):
+    box = mesh.Box(3, 2, 2, 3, bc={"x": ("inflow", "outflow")})
+    rho, vel, p = 1.2, (0.3, 0.05, -0.1), TWALL / GAMMA
+    q = _uniform(box, rho, vel, p)
+    c = oracle_mod.Case.from_desc(box.desc())
+    c.set_phys(re=400.0)
+    c.set_q(q)
+    c.set_boundary(TWALL, mesh.boundary_state(box, rho, vel, p), None)
+    assert np.abs(c.rhs()).max() <= 1e-10 * p
+
+
+def test_wall_without_normal_velocity_passes_no_mass(oracle_mod):
+    box = mesh.Box(2, 3, 2, 4, bc={"y": ("walladiab", "wallisoth")})
+    x, y, z = (box.xg[..., k].reshape(box.nel, box.ldx, box.ldx, box.ldx) for k in range(3))
+    G = 5
+    q = np.zeros(box.qshape())
+    jac = box.jacob.reshape(box.nel, box.ldx, box.ldx, box.ldx)
+    s = np.s_[:, :G, :G, :G]
+    rho = 1.0 + 0.1 * np.sin(x[s]) * np.cos(z[s]) + 0.05 * np.cos(y[s])
+    u, w = 0.4 * np.sin(z[s]), 0.2 * np.cos(x[s])
+    pr = TWALL / GAMMA * (1.0 + 0.02 * np.cos(y[s] + x[s]))
+    for k, val in enumerate([rho, rho * u, 0.0 * rho, rho * w, pr / (GAMMA - 1.0) + 0.5 * rho * (u * u + w * w)]):
+        q[:, k, :G, :G, :G] = val / jac[s]
+    c = oracle_mod.Case.from_desc(box.desc())
+    c.set_phys(re=300.0)
+    c.set_q(q)
+    c.set_boundary(TWALL)
+    qt = c.rhs()[:, 0, :G, :G, :G]
+    w1 = _weights(G)
+    W = w1[:, None, None] * w1[None, :, None] * w1[None, None, :]
+    total = float((qt * W).sum())
+    scale = float((np.abs(qt) * W).sum())
+    assert scale > 1.0
+    assert abs(total) <= 1e-13 * scale, (total, scale)
+
+
+def test_boundary_needs_its_condition(oracle_mod):
+    box = mesh.Box(2, 2, 2, 3, bc={"z": ("walladiab", "outflow")})
+    d = box.desc()
+    d["bcond"] = np.zeros_like(d["bcond"])
+    with pytest.raises(ValueError):
+        oracle_mod.Case.from_desc(d)
