@@ -62,12 +62,16 @@ struct Adj {
   double eps_w() const { return dt * 100.0 * c->P.r_re / s2; }
 };
 
-template <int G> int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, bool direct_only) {
+// Adjoint of one stage.  Unless direct_only, the RK steps around it are fused in:
+// dJ/dQt += cdt dJ/dQ before, dJ/dQ += R'^T dJ/dQt and dJ/dQt *= ark after.
+template <int G>
+int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, bool direct_only, double cdt,
+                    double ark) {
   dsem_ctx *c = A.c;
   const Group &g = *A.g;
   const MList &ml = *A.ml;
   if constexpr (G > 7) {
-    (void)Qs; (void)JQe; (void)eps_w; (void)direct_only; (void)g; (void)ml;
+    (void)Qs; (void)JQe; (void)eps_w; (void)direct_only; (void)g; (void)ml; (void)cdt; (void)ark;
     return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
   } else {
     constexpr int G2 = G * G;
@@ -109,7 +113,7 @@ template <int G> int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe
       return DSEM_OK;
     }
     const unsigned nb = (unsigned)(((long long)ml.n * G2 + 127) / 128);
-    k_upd_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lg, c->P.re, A.b.lff, A.b.lvf);
+    k_upd_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lg, A.b.lq, cdt, c->P.re, A.b.lff, A.b.lvf);
     CKA(cudaGetLastError());
     k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lvf, ml.nrm);
     CKA(cudaGetLastError());
@@ -118,7 +122,7 @@ template <int G> int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe
     k_face_inv_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.qfr, A.b.lff, A.b.lqf, A.b.lqr, ml.nh, ml.nrm,
                                              c->P.gamma);
     CKA(cudaGetLastError());
-    k_trace_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq);
+    k_trace_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq, A.b.lq, A.b.lg, ark);
     CKA(cudaGetLastError());
     k_sum_into<<<1, 256, 0, c->st>>>(A.b.lrp, g.nel, A.b.lr);
     CKA(cudaGetLastError());
@@ -127,10 +131,11 @@ template <int G> int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe
   }
 }
 
-int stage_adjoint(Adj &A, const double *Qs, const double *JQe, double eps_w, bool direct_only) {
+int stage_adjoint(Adj &A, const double *Qs, const double *JQe, double eps_w, bool direct_only, double cdt = 0.0,
+                  double ark = 1.0) {
   int r = DSEM_OK;
   cudaError_t e = with_G(A.g->G, [&](auto gc) -> cudaError_t {
-    r = stage_adjoint_G<decltype(gc)::value>(A, Qs, JQe, eps_w, direct_only);
+    r = stage_adjoint_G<decltype(gc)::value>(A, Qs, JQe, eps_w, direct_only, cdt, ark);
     return cudaSuccess;
   });
   if (e != cudaSuccess) return dsem_int::fail(A.c, DSEM_ERR_UNSUPPORTED, "adjoint: element order not supported");
@@ -152,14 +157,10 @@ int reverse_step(Adj &A, int n, double *const *st, const double *qend) {
     ++A.launches;
   }
   for (int kk = c->kord; kk >= 1; --kk) {
-    k_rk_adj_pre<<<ew_blocks(nq), 256, 0, c->st>>>(nq, A.b.lg, A.b.lq, c->crk[kk - 1] * A.dt);
-    CKA(cudaGetLastError());
     const bool eps_here = win && kk == c->kord;
-    int r = stage_adjoint(A, st[kk - 1], qend, eps_here ? A.eps_w() : 0.0, false);
+    int r = stage_adjoint(A, st[kk - 1], qend, eps_here ? A.eps_w() : 0.0, false, c->crk[kk - 1] * A.dt,
+                          c->ark[kk - 1]);
     if (r) return r;
-    k_rk_adj_post<<<ew_blocks(nq), 256, 0, c->st>>>(nq, A.b.lq, A.b.ljq, A.b.lg, c->ark[kk - 1]);
-    CKA(cudaGetLastError());
-    A.launches += 2;
   }
   return DSEM_OK;
 }

@@ -369,15 +369,15 @@ __device__ __forceinline__ void vis_vjp(const double *Q, const double (&Gr)[3][N
   const double K = P.mach * P.mach * g;
   const double A = pD - p * Gr[D][0] * ri;
   const double tD = A * K * ri;
-  const double kap = 1.0 + (amu - 1.0) * 0.2 / (g - 1.0);
-  const double den = P.pr * P.mach * P.mach * (g - 1.0);
+  const double kap = 1.0 + (amu - 1.0) * 0.2 * P.r_gm1;
+  const double rden = P.r_den;  // 1 / (pr mach^2 (gamma-1))
   double tau[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) tau[i] = amu * (Gv[i][D] + Gv[D][i]) - (i == D ? 2.0 / 3.0 * amu * div : 0.0);
   fv[0] = 0.0;
 #pragma unroll
   for (int i = 0; i < 3; ++i) fv[1 + i] = tau[i];
-  fv[4] = vel[0] * tau[0] + vel[1] * tau[1] + vel[2] * tau[2] + kap * tD / den;
+  fv[4] = vel[0] * tau[0] + vel[1] * tau[1] + vel[2] * tau[2] + kap * tD * rden;
   // reverse
   const double l4 = lf[4];
   double lvel[3], ltau[3];
@@ -386,7 +386,7 @@ __device__ __forceinline__ void vis_vjp(const double *Q, const double (&Gr)[3][N
     lvel[i] = tau[i] * l4;
     ltau[i] = lf[1 + i] + vel[i] * l4;
   }
-  const double ltD = kap / den * l4;
+  const double ltD = kap * rden * l4;
   double lGv[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
@@ -464,13 +464,17 @@ __device__ __forceinline__ void vort_vjp(const double *Qj, double jc, const doub
 
 // ---------------------------------------------------------------- kernels
 // Face terms of the divergence and the RK residual sign (k_update):
-// Qt = -(QTI + sum_faces D_edge FB), FB = FF - VF/Re.
+// Qt = -(QTI + sum_faces D_edge FB), FB = FF - VF/Re.  First the RK step of
+// the reverse sweep for this element's entries: dJ/dQt += cdt dJ/dQ.
 template <int G>
-__global__ void __launch_bounds__(256) k_upd_adj(const double *__restrict__ LQT, double re, double *__restrict__ LFF,
-                                                  double *__restrict__ LVF) {
+__global__ void __launch_bounds__(256) k_upd_adj(double *__restrict__ LQT, const double *__restrict__ LQ, double cdt,
+                                                  double re, double *__restrict__ LFF, double *__restrict__ LVF) {
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G;
   const int k = blockIdx.x;
-  const double *lam = LQT + (long long)k * 5 * NG;
+  double *lam = LQT + (long long)k * 5 * NG;
+  const double *lq = LQ + (long long)k * 5 * NG;
+  for (int i = threadIdx.x; i < 5 * NG; i += blockDim.x) lam[i] += cdt * lq[i];
+  __syncthreads();
   for (int t = threadIdx.x; t < 30 * G2; t += blockDim.x) {
     const int f = t / (5 * G2), r = t - f * 5 * G2, v = r / G2, ln = r - v * G2, i = ln % G, j = ln / G;
     const bool hi = (f == 1 || f == 3 || f == 4);
@@ -557,10 +561,12 @@ __global__ void __launch_bounds__(128) k_face_inv_adj(const MortarC *__restrict_
   }
 }
 
-// Face traces (write_traces), transposed: LJQ += jacob * trace^T LQR.
+// Face traces (write_traces), transposed: LJQ += jacob * trace^T LQR; then the
+// RK step of the reverse sweep: dJ/dQ += LJQ, dJ/dQt *= ark.
 template <int G>
 __global__ void __launch_bounds__(256) k_trace_adj(const double *__restrict__ LQR, const double *__restrict__ jac,
-                                                    double *__restrict__ LJQ) {
+                                                    const double *__restrict__ LJQ, double *__restrict__ LQ,
+                                                    double *__restrict__ LQT, double ark) {
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G;
   const int k = blockIdx.x;
   const double *F = LQR + (long long)k * 30 * G2;
@@ -573,7 +579,9 @@ __global__ void __launch_bounds__(256) k_trace_adj(const double *__restrict__ LQ
     s += Op<G>::B(L - 1, m) * Fv[1 * 5 * G2 + n + G * l];      // face 2
     s += Op<G>::B(0, l) * Fv[2 * 5 * G2 + n + G * m];          // face 3 (z = 0)
     s += Op<G>::B(L - 1, l) * Fv[4 * 5 * G2 + n + G * m];      // face 5
-    LJQ[(long long)k * 5 * NG + i] += jac[(long long)k * NG + p] * s;
+    const long long o = (long long)k * 5 * NG + i;
+    LQ[o] += LJQ[o] + jac[(long long)k * NG + p] * s;
+    LQT[o] *= ark;
   }
 }
 
@@ -597,7 +605,7 @@ template <int G> struct VolAdjCfg {
   // one element per SM (shared memory); at least one thread per Lobatto point of a grid
   static constexpr int NT = NL <= 256 ? 256 : ((NL + 31) / 32) * 32;
   static constexpr size_t NDBL = 5 * NG + 15 * NG + 15 * NG + 5 * NL + 5 * NL + 11 * NL + 5 * NG + 5 * NG + 30 * G2 +
-                                 2 * G * L + NT;
+                                 NT + 3 * NG + 30 * G2;
   static constexpr size_t SMEM = sizeof(double) * NDBL;
 };
 
@@ -616,15 +624,15 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
   double *LQ = LG + 11 * NL;    // [5][NG] dJ/dq
   double *LAM = LQ + 5 * NG;    // [5][NG] dJ/dQt
   double *LQFs = LAM + 5 * NG;  // [30][G2] dJ/dQF
-  double *Bm = LQFs + 30 * G2;  // bx [L][G]
-  double *Dm = Bm + L * G;      // dmx [G][L]
-  double *red = Dm + G * L;     // [NT]
+  double *red = LQFs + 30 * G2;  // [NT]
+  double *gg = red + NT;         // [3][NG] metric diagonal at the Gauss points
+  double *QF = gg + 3 * NG;      // [30][G2] averaged face states
   const int k = blockIdx.x, tid = threadIdx.x;
   const double *JQ = A.JQ + (long long)k * 5 * NG;
   const double *jac = A.jac + (long long)k * NG;
-  const double *gg = A.gg + (long long)k * 3 * NG;
+  const double *ggk = A.gg + (long long)k * 3 * NG;
   const double *gm = A.gm + (long long)k * 3 * NL;
-  const double *QF = A.QF + (long long)k * 30 * G2;
+  const double *QFk = A.QF + (long long)k * 30 * G2;
   const double *LVF = A.LVF + (long long)k * 30 * G2;
   double *LJQ = A.LJQ + (long long)k * 5 * NG;
   const Phys P = A.P;
@@ -635,14 +643,10 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
   t_ph_ = clock64();
 #endif
 
-  for (int i = tid; i < L * G; i += NT) {
-    Bm[i] = Op<G>::B(i / G, i % G);
-    Dm[i] = Op<G>::D(i / L, i % L);
-  }
-  {  // state and dJ/dQt: all of a thread's loads in flight at once
-    constexpr int NQ = (5 * NG + NT - 1) / NT;
+  {  // state, dJ/dQt, metrics and face states: all of a thread's loads in flight at once
+    constexpr int NQ = (5 * NG + NT - 1) / NT, NM = (3 * NG + NT - 1) / NT, NF = (30 * G2 + NT - 1) / NT;
     const double *lqt = A.LQT + (long long)k * 5 * NG;
-    double qv[NQ], jv[NQ], lv[NQ];
+    double qv[NQ], jv[NQ], lv[NQ], mv[NM], fv[NF];
 #pragma unroll
     for (int j = 0; j < NQ; ++j) {
       const int i = tid + j * NT;
@@ -653,6 +657,12 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
       }
     }
 #pragma unroll
+    for (int j = 0; j < NM; ++j)
+      if (tid + j * NT < 3 * NG) mv[j] = ggk[tid + j * NT];
+#pragma unroll
+    for (int j = 0; j < NF; ++j)
+      if (tid + j * NT < 30 * G2) fv[j] = QFk[tid + j * NT];
+#pragma unroll
     for (int j = 0; j < NQ; ++j) {
       const int i = tid + j * NT;
       if (i < 5 * NG) {
@@ -661,33 +671,17 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
         LQ[i] = 0.0;
       }
     }
+#pragma unroll
+    for (int j = 0; j < NM; ++j)
+      if (tid + j * NT < 3 * NG) gg[tid + j * NT] = mv[j];
+#pragma unroll
+    for (int j = 0; j < NF; ++j)
+      if (tid + j * NT < 30 * G2) QF[tid + j * NT] = fv[j];
   }
   for (int i = tid; i < 15 * NG; i += NT) LGR[i] = 0.0;
   for (int i = tid; i < 30 * G2; i += NT) LQFs[i] = 0.0;
   __syncthreads();
   PHASE_MARK(21);
-
-  // Lobatto arrays of grid D into LB (interior from q, faces from QF)
-  auto build = [&](auto Dc) {
-    constexpr int D = decltype(Dc)::value;
-    constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
-    for (int t = tid; t < 5 * G2; t += NT) {
-      const int v = t / G2, ln = t - v * G2, a = ln % G, b = ln / G;
-      const int p0 = gbase<G>(D, a, b), l0 = lbase<G>(D, a, b);
-      double x[G];
-#pragma unroll
-      for (int kk = 0; kk < G; ++kk) x[kk] = q[v * NG + p0 + kk * xs];
-      LB[v * NL + l0] = QF[(face_lo(D) - 1) * 5 * G2 + v * G2 + ln];
-      LB[v * NL + l0 + (L - 1) * xs] = QF[(face_hi(D) - 1) * 5 * G2 + v * G2 + ln];
-#pragma unroll
-      for (int s = 1; s < L - 1; ++s) {
-        double acc = Op<G>::B(s, 0) * x[0];
-#pragma unroll
-        for (int kk = 1; kk < G; ++kk) acc = __fma_rn(Op<G>::B(s, kk), x[kk], acc);
-        LB[v * NL + l0 + s * xs] = acc;
-      }
-    }
-  };
 
   // ---- forward: Gauss gradients of the five fields, one task per (direction, field, line):
   // the Lobatto line is built and differentiated in registers
@@ -760,18 +754,69 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
   // ---- reverse of pass 2: fluxes and interior divergence, grid by grid
   auto flux_dir = [&](auto Dc) {
     constexpr int D = decltype(Dc)::value;
-    build(Dc);
+    constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
+    // LB, LL and LG hold grid D's points.  The lines of grid 0 are contiguous
+    // runs of L doubles; when L is a power of two the 16 lines of a half-warp
+    // would meet in two bank pairs, so point s of grid-0 line r is stored at
+    // r*L + (s ^ ((r >> 1) & (L-1))) (a permutation within the line).
+    auto sw = [](int i) -> int {
+      if constexpr (D == 0 && (L & (L - 1)) == 0) return i ^ (((i / L) >> 1) & (L - 1));
+      else return i;
+    };
+    // line phase: per line of grid D, the Lobatto state (LB), the 11 gradient
+    // fields interpolated to the Lobatto points (into LG) and the transposed
+    // derivative of dJ/dQt at the interior points (into LL), so that the point
+    // phase reads each operand once
+    for (int t = tid; t < 21 * G2; t += NT) {
+      const int j = t / G2, ln = t - j * G2, a = ln % G, b = ln / G;
+      const int p0 = gbase<G>(D, a, b), l0 = lbase<G>(D, a, b);
+      double x[G];
+      if (j < 5) {  // state field j
+#pragma unroll
+        for (int kk = 0; kk < G; ++kk) x[kk] = q[j * NG + p0 + kk * xs];
+        LB[j * NL + sw(l0)] = QF[(face_lo(D) - 1) * 5 * G2 + j * G2 + ln];
+        LB[j * NL + sw(l0 + (L - 1) * xs)] = QF[(face_hi(D) - 1) * 5 * G2 + j * G2 + ln];
+#pragma unroll
+        for (int s = 1; s < L - 1; ++s) {
+          double acc = Op<G>::B(s, 0) * x[0];
+#pragma unroll
+          for (int kk = 1; kk < G; ++kk) acc = __fma_rn(Op<G>::B(s, kk), x[kk], acc);
+          LB[j * NL + sw(l0 + s * xs)] = acc;
+        }
+      } else if (j < 16) {  // gradient field j-5 of grid D
+        const int fi = diag_field(D, j - 5);
+#pragma unroll
+        for (int kk = 0; kk < G; ++kk) x[kk] = GR[fi * NG + p0 + kk * xs];
+#pragma unroll
+        for (int s = 0; s < L; ++s) {
+          double acc = Op<G>::B(s, 0) * x[0];
+#pragma unroll
+          for (int kk = 1; kk < G; ++kk) acc = __fma_rn(Op<G>::B(s, kk), x[kk], acc);
+          LG[(j - 5) * NL + sw(l0 + s * xs)] = acc;
+        }
+      } else {  // dJ/dQt of field j-16: -D^T along the line, interior points
+        const int v = j - 16;
+#pragma unroll
+        for (int kk = 0; kk < G; ++kk) x[kk] = LAM[v * NG + p0 + kk * xs];
+#pragma unroll
+        for (int s = 1; s < L - 1; ++s) {
+          double acc = 0.0;
+#pragma unroll
+          for (int kk = 0; kk < G; ++kk) acc += Op<G>::D(kk, s) * x[kk];
+          LL[v * NL + sw(l0 + s * xs)] = -acc;
+        }
+      }
+    }
     __syncthreads();
     PHASE_MARK(26);
-    constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
     for (int qi = tid; qi < NL; qi += NT) {
       int s, a, b;
       ldecode<G>(D, qi, s, a, b);
-      const int g0 = gbase<G>(D, a, b);
+      const int qs = sw(qi);
       double Q[NV], Gr[3][NV], lG[3][NV], lQ[NV], lfv[NV], fv[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        Q[v] = LB[v * NL + qi];
+        Q[v] = LB[v * NL + qs];
         lQ[v] = 0.0;
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
@@ -782,10 +827,7 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
 #pragma unroll
       for (int jf = 0; jf < 11; ++jf) {
         const int fi = diag_field(D, jf);
-        double acc = Bm[s * G] * GR[fi * NG + g0];
-#pragma unroll
-        for (int kk = 1; kk < G; ++kk) acc = __fma_rn(Bm[s * G + kk], GR[fi * NG + g0 + kk * xs], acc);
-        Gr[fi % 3][fi / 3] = acc;
+        Gr[fi % 3][fi / 3] = LG[jf * NL + qs];
       }
       const double gd = gm[D * NL + qi];
       if (s == 0 || s == L - 1) {  // face point: VF = gd * fv
@@ -805,10 +847,7 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
         double lF[NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-          double acc = 0.0;
-#pragma unroll
-          for (int kk = 0; kk < G; ++kk) acc += Dm[kk * L + s] * LAM[v * NG + g0 + kk * xs];
-          lF[v] = -acc;
+          lF[v] = LL[v * NL + qs];
           lfv[v] = -gd * P.r_re * lF[v];
         }
         double lfe[NV];
@@ -828,11 +867,11 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
         for (int v = 0; v < NV; ++v) lr += -gd * fv[v] * lF[v];
       }
 #pragma unroll
-      for (int v = 0; v < NV; ++v) LL[v * NL + qi] = lQ[v];
+      for (int v = 0; v < NV; ++v) LL[v * NL + qs] = lQ[v];
 #pragma unroll
       for (int jf = 0; jf < 11; ++jf) {
         const int fi = diag_field(D, jf);
-        LG[jf * NL + qi] = lG[fi % 3][fi / 3];
+        LG[jf * NL + qs] = lG[fi % 3][fi / 3];
       }
     }
     __syncthreads();
@@ -845,7 +884,7 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
         const int fi = diag_field(D, j);
         double y[L];
 #pragma unroll
-        for (int s = 0; s < L; ++s) y[s] = LG[j * NL + l0 + s * xs];
+        for (int s = 0; s < L; ++s) y[s] = LG[j * NL + sw(l0 + s * xs)];
 #pragma unroll
         for (int kk = 0; kk < G; ++kk) {
           double acc = 0.0;
@@ -857,7 +896,7 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
         const int v = j - 11;
         double y[L];
 #pragma unroll
-        for (int s = 0; s < L; ++s) y[s] = LL[v * NL + l0 + s * xs];
+        for (int s = 0; s < L; ++s) y[s] = LL[v * NL + sw(l0 + s * xs)];
 #pragma unroll
         for (int kk = 0; kk < G; ++kk) {
           double acc = 0.0;
@@ -926,10 +965,6 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
 }
 
 // RK bookkeeping of the reverse sweep
-__global__ void k_rk_adj_pre(long long n, double *__restrict__ lg, const double *__restrict__ lq, double cdt) {
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    lg[i] += cdt * lq[i];
-}
 __global__ void k_rk_adj_post(long long n, double *__restrict__ lq, const double *__restrict__ ljq,
                               double *__restrict__ lg, double a) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
