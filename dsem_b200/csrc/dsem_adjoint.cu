@@ -320,12 +320,49 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   CKA(cudaMemsetAsync(A.b.lr, 0, sizeof(double), c->st));
   if (window > 0) {
     if (snapshots == 0) {
+      // Every reverse step launches the same kernels with other stage pointers:
+      // after the first (eager) step, each step is captured and replayed as a
+      // CUDA graph, one executable graph per kind of step (inside or outside
+      // the objective's window) updated in place with the new pointers.
+      cudaGraphExec_t gx[2] = {nullptr, nullptr};
+      auto drop = [&]() {
+        for (auto &x : gx)
+          if (x) cudaGraphExecDestroy(x);
+      };
       for (int n = nsteps - 1; n >= 0; --n) {
         std::vector<double *> st;
         for (int k = 0; k < kord; ++k) st.push_back(A.b.stages + ((size_t)n * kord + k) * nq);
         const double *qend = n + 1 < nsteps ? A.b.stages + ((size_t)(n + 1) * kord) * nq : c->JQ;
-        if ((r = reverse_step(A, n, st.data(), qend))) return r;
+        if (n == nsteps - 1) {
+          if ((r = reverse_step(A, n, st.data(), qend))) return drop(), r;
+          continue;
+        }
+        const int kind = A.in_window(n) ? 1 : 0;
+        cudaGraph_t graph = nullptr;
+        cudaError_t ec = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
+        if (ec != cudaSuccess) return drop(), dsem_int::fail(c, DSEM_ERR_CUDA, "adjoint: cudaStreamBeginCapture failed");
+        r = reverse_step(A, n, st.data(), qend);
+        ec = cudaStreamEndCapture(c->st, &graph);
+        if (r) {
+          if (graph) cudaGraphDestroy(graph);
+          return drop(), r;
+        }
+        if (ec != cudaSuccess) return drop(), dsem_int::fail(c, DSEM_ERR_CUDA, "adjoint: cudaStreamEndCapture failed");
+        if (gx[kind]) {
+          cudaGraphExecUpdateResultInfo info;
+          if (cudaGraphExecUpdate(gx[kind], graph, &info) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(gx[kind]);
+            gx[kind] = nullptr;
+          }
+        }
+        if (!gx[kind]) ec = cudaGraphInstantiate(&gx[kind], graph, 0);
+        cudaGraphDestroy(graph);
+        if (ec != cudaSuccess) return drop(), dsem_int::fail(c, DSEM_ERR_CUDA, "adjoint: cudaGraphInstantiate failed");
+        ec = cudaGraphLaunch(gx[kind], c->st);
+        if (ec != cudaSuccess) return drop(), dsem_int::fail(c, DSEM_ERR_CUDA, "adjoint: cudaGraphLaunch failed");
       }
+      drop();
     } else {
       CKA(cudaMemcpyAsync(A.b.slots[0], A.b.q0, bq, cudaMemcpyDeviceToDevice, c->st));
       if ((r = revolve(A, 0, nsteps, 0, 1))) return r;
