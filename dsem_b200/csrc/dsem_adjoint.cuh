@@ -470,10 +470,15 @@ template <int G>
 __global__ void __launch_bounds__(256) k_upd_adj(double *__restrict__ LQT, const double *__restrict__ LQ, double cdt,
                                                   double re, double *__restrict__ LFF, double *__restrict__ LVF) {
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G;
+  __shared__ double lam[5 * NG];  // this element's dJ/dQt after the RK step
   const int k = blockIdx.x;
-  double *lam = LQT + (long long)k * 5 * NG;
+  double *lamg = LQT + (long long)k * 5 * NG;
   const double *lq = LQ + (long long)k * 5 * NG;
-  for (int i = threadIdx.x; i < 5 * NG; i += blockDim.x) lam[i] += cdt * lq[i];
+  for (int i = threadIdx.x; i < 5 * NG; i += blockDim.x) {
+    const double x = lamg[i] + cdt * lq[i];
+    lamg[i] = x;
+    lam[i] = x;
+  }
   __syncthreads();
   for (int t = threadIdx.x; t < 30 * G2; t += blockDim.x) {
     const int f = t / (5 * G2), r = t - f * 5 * G2, v = r / G2, ln = r - v * G2, i = ln % G, j = ln / G;
@@ -488,7 +493,8 @@ __global__ void __launch_bounds__(256) k_upd_adj(double *__restrict__ LQT, const
         p = i + G * (n + G * j);
       else  // faces 3, 5: along z at (n, m)
         p = i + G * (j + G * n);
-      acc += Op<G>::D(n, hi ? L - 1 : 0) * lam[v * NG + p];
+      const double dlo = Op<G>::D(n, 0), dhi = Op<G>::D(n, L - 1);
+      acc += (hi ? dhi : dlo) * lam[v * NG + p];
     }
     const double lfb = -acc;
     LFF[(long long)k * 30 * G2 + t] = lfb;
@@ -549,15 +555,21 @@ __global__ void __launch_bounds__(128) k_face_inv_adj(const MortarC *__restrict_
   }
   const long long gp = (long long)M.geo * G2 + pt;
   const double n3[3] = {nh[gp * 3], nh[gp * 3 + 1], nh[gp * 3 + 2]};
+  // one call with the operands ordered by the master face (no divergent copies)
   const bool low = (M.flags >> 5) & 1;
-  if (low)
-    roe_vjp_rev(n3, nrm[gp], Q2, Q1, gamma, lf, l2, l1);
-  else
-    roe_vjp_rev(n3, nrm[gp], Q1, Q2, gamma, lf, l1, l2);
+  double Ql[NV], Qr[NV], ll[NV], lr_[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
-    LQR[M.ms + v * G2 + pt] = l1[v];
-    LQR[M.ss + v * G2 + sp] = l2[v];
+    Ql[v] = low ? Q2[v] : Q1[v];
+    Qr[v] = low ? Q1[v] : Q2[v];
+    ll[v] = low ? l2[v] : l1[v];
+    lr_[v] = low ? l1[v] : l2[v];
+  }
+  roe_vjp_rev(n3, nrm[gp], Ql, Qr, gamma, lf, ll, lr_);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    LQR[M.ms + v * G2 + pt] = low ? lr_[v] : ll[v];
+    LQR[M.ss + v * G2 + sp] = low ? ll[v] : lr_[v];
   }
 }
 
@@ -568,17 +580,24 @@ __global__ void __launch_bounds__(256) k_trace_adj(const double *__restrict__ LQ
                                                     const double *__restrict__ LJQ, double *__restrict__ LQ,
                                                     double *__restrict__ LQT, double ark) {
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G;
+  __shared__ double F[30 * G2];  // this element's face adjoints
+  __shared__ double b0[G], b1[G];  // end rows of the interpolation (thread-dependent index)
   const int k = blockIdx.x;
-  const double *F = LQR + (long long)k * 30 * G2;
+  for (int i = threadIdx.x; i < 30 * G2; i += blockDim.x) F[i] = LQR[(long long)k * 30 * G2 + i];
+  if (threadIdx.x < G) {
+    b0[threadIdx.x] = Op<G>::B(0, threadIdx.x);
+    b1[threadIdx.x] = Op<G>::B(L - 1, threadIdx.x);
+  }
+  __syncthreads();
   for (int i = threadIdx.x; i < 5 * NG; i += blockDim.x) {
     const int v = i / NG, p = i - v * NG, n = p % G, m = (p / G) % G, l = p / G2;
     const double *Fv = F + v * G2;
-    double s = Op<G>::B(0, n) * Fv[5 * 5 * G2 + m + G * l];    // face 6 (x = 0)
-    s += Op<G>::B(L - 1, n) * Fv[3 * 5 * G2 + m + G * l];      // face 4
-    s += Op<G>::B(0, m) * Fv[0 * 5 * G2 + n + G * l];          // face 1 (y = 0)
-    s += Op<G>::B(L - 1, m) * Fv[1 * 5 * G2 + n + G * l];      // face 2
-    s += Op<G>::B(0, l) * Fv[2 * 5 * G2 + n + G * m];          // face 3 (z = 0)
-    s += Op<G>::B(L - 1, l) * Fv[4 * 5 * G2 + n + G * m];      // face 5
+    double s = b0[n] * Fv[5 * 5 * G2 + m + G * l];    // face 6 (x = 0)
+    s += b1[n] * Fv[3 * 5 * G2 + m + G * l];          // face 4
+    s += b0[m] * Fv[0 * 5 * G2 + n + G * l];          // face 1 (y = 0)
+    s += b1[m] * Fv[1 * 5 * G2 + n + G * l];          // face 2
+    s += b0[l] * Fv[2 * 5 * G2 + n + G * m];          // face 3 (z = 0)
+    s += b1[l] * Fv[4 * 5 * G2 + n + G * m];          // face 5
     const long long o = (long long)k * 5 * NG + i;
     LQ[o] += LJQ[o] + jac[(long long)k * NG + p] * s;
     LQT[o] *= ark;
