@@ -44,8 +44,9 @@ struct AdjBuf {
   double *q0 = nullptr;
   std::vector<double *> slots;  // checkpoint slots (step states)
   double *stages = nullptr;     // stage states: all steps (snapshots == 0) or one step
+  double *traces = nullptr;     // raw face traces of every stage state (snapshots == 0, when memory allows)
   ~AdjBuf() {
-    for (double *p : {lq, lg, ljq, ldir, qfr, lff, lvf, lqf, lqr, lrp, lr, q0, stages}) cudaFree(p);
+    for (double *p : {lq, lg, ljq, ldir, qfr, lff, lvf, lqf, lqr, lrp, lr, q0, stages, traces}) cudaFree(p);
     for (double *p : slots) cudaFree(p);
   }
 };
@@ -64,27 +65,37 @@ struct Adj {
 
 // Adjoint of one stage.  Unless direct_only, the RK steps around it are fused in:
 // dJ/dQt += cdt dJ/dQ before, dJ/dQ += R'^T dJ/dQt and dJ/dQt *= ark after.
+// qraw: the raw face traces of Qs kept by the forward sweep, or null to recompute them.
 template <int G>
 int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, bool direct_only, double cdt,
-                    double ark) {
+                    double ark, const double *qraw) {
   dsem_ctx *c = A.c;
   const Group &g = *A.g;
   const MList &ml = *A.ml;
   if constexpr (G > 7) {
-    (void)Qs; (void)JQe; (void)eps_w; (void)direct_only; (void)g; (void)ml; (void)cdt; (void)ark;
+    (void)Qs; (void)JQe; (void)eps_w; (void)direct_only; (void)g; (void)ml; (void)cdt; (void)ark; (void)qraw;
     return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
   } else {
     constexpr int G2 = G * G;
-    // forward prerequisites: raw traces, Roe flux, averaged traces
-    TraceArgs ta{};
-    ta.JQ = Qs;
-    ta.sq = 5LL * G * G * G;
-    ta.jac = g.jac;
-    ta.QF = c->QF;
-    CKA(Launch<G>::trace(ta, g.nel, c->st));
-    CKA(cudaMemcpyAsync(A.b.qfr, c->QF, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-    CKA(Launch<G>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st));
-    A.launches += 2;
+    // forward prerequisites: raw traces (qfr), averaged traces (c->QF)
+    const double *qfr = qraw;
+    if (qraw) {
+      const unsigned nbm = (unsigned)(((long long)ml.n * G2 + 127) / 128);
+      k_face_avg<G><<<nbm, 128, 0, c->st>>>(ml.mc, ml.n, qraw, c->QF);
+      CKA(cudaGetLastError());
+      A.launches += 1;
+    } else {
+      TraceArgs ta{};
+      ta.JQ = Qs;
+      ta.sq = 5LL * G * G * G;
+      ta.jac = g.jac;
+      ta.QF = c->QF;
+      CKA(Launch<G>::trace(ta, g.nel, c->st));
+      CKA(cudaMemcpyAsync(A.b.qfr, c->QF, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+      CKA(Launch<G>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st));
+      A.launches += 2;
+      qfr = A.b.qfr;
+    }
     using C = VolAdjCfg<G>;
     static bool attr = false;
     if (!attr) {
@@ -119,7 +130,7 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
     CKA(cudaGetLastError());
     k_vol_adj<G><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
     CKA(cudaGetLastError());
-    k_face_inv_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.qfr, A.b.lff, A.b.lqf, A.b.lqr, ml.nh, ml.nrm,
+    k_face_inv_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, qfr, A.b.lff, A.b.lqf, A.b.lqr, ml.nh, ml.nrm,
                                              c->P.gamma);
     CKA(cudaGetLastError());
     k_trace_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq, A.b.lq, A.b.lg, ark);
@@ -132,10 +143,10 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
 }
 
 int stage_adjoint(Adj &A, const double *Qs, const double *JQe, double eps_w, bool direct_only, double cdt = 0.0,
-                  double ark = 1.0) {
+                  double ark = 1.0, const double *qraw = nullptr) {
   int r = DSEM_OK;
   cudaError_t e = with_G(A.g->G, [&](auto gc) -> cudaError_t {
-    r = stage_adjoint_G<decltype(gc)::value>(A, Qs, JQe, eps_w, direct_only, cdt, ark);
+    r = stage_adjoint_G<decltype(gc)::value>(A, Qs, JQe, eps_w, direct_only, cdt, ark, qraw);
     return cudaSuccess;
   });
   if (e != cudaSuccess) return dsem_int::fail(A.c, DSEM_ERR_UNSUPPORTED, "adjoint: element order not supported");
@@ -144,13 +155,14 @@ int stage_adjoint(Adj &A, const double *Qs, const double *JQe, double eps_w, boo
 
 unsigned ew_blocks(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16); }
 
-// Reverse of step n, its stage input states at st[0..kord) and its end state at qend.
-int reverse_step(Adj &A, int n, double *const *st, const double *qend) {
+// Reverse of step n, its stage input states at st[0..kord) and its end state at
+// qend; qf[0..kord): their raw face traces, or null.
+int reverse_step(Adj &A, int n, double *const *st, const double *qend, double *const *qf = nullptr) {
   dsem_ctx *c = A.c;
   const long long nq = (long long)c->nq;
   const bool win = A.in_window(n);
   if (win) {  // d eps_n / d JQ_n through the JQ values of the enstrophy sum
-    int r = stage_adjoint(A, st[c->kord - 1], qend, A.eps_w(), true);
+    int r = stage_adjoint(A, st[c->kord - 1], qend, A.eps_w(), true, 0.0, 1.0, qf ? qf[c->kord - 1] : nullptr);
     if (r) return r;
     k_rk_adj_post<<<ew_blocks(nq), 256, 0, c->st>>>(nq, A.b.lq, A.b.ldir, A.b.lg, 1.0);
     CKA(cudaGetLastError());
@@ -159,18 +171,21 @@ int reverse_step(Adj &A, int n, double *const *st, const double *qend) {
   for (int kk = c->kord; kk >= 1; --kk) {
     const bool eps_here = win && kk == c->kord;
     int r = stage_adjoint(A, st[kk - 1], qend, eps_here ? A.eps_w() : 0.0, false, c->crk[kk - 1] * A.dt,
-                          c->ark[kk - 1]);
+                          c->ark[kk - 1], qf ? qf[kk - 1] : nullptr);
     if (r) return r;
   }
   return DSEM_OK;
 }
 
-// One forward step from c->JQ; stage input states copied to st[0..kord) when st != nullptr.
-int forward_step(Adj &A, int n, double *const *st, std::vector<double> *s_win) {
+// One forward step from c->JQ; stage input states copied to st[0..kord) when st
+// != nullptr, their raw face traces (c->QF at the stage start) to qf[0..kord)
+// when qf != nullptr.
+int forward_step(Adj &A, int n, double *const *st, std::vector<double> *s_win, double *const *qf = nullptr) {
   dsem_ctx *c = A.c;
   const bool win = A.in_window(n);
   for (int kk = 1; kk <= c->kord; ++kk) {
     if (st) CKA(cudaMemcpyAsync(st[kk - 1], c->JQ, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    if (qf) CKA(cudaMemcpyAsync(qf[kk - 1], c->QF, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
     int r = dsem_int::stage(c, kk, win && kk == c->kord);
     if (r) return r;
     A.launches += 2 * (long long)c->groups.size() + 2 * (long long)c->mlists.size();
@@ -283,6 +298,10 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
     cudaGetLastError();
     return dsem_int::fail(c, DSEM_ERR_NOMEM, "adjoint: not enough device memory for the stage states (use snapshots > 0)");
   }
+  if (snapshots == 0 && cudaMalloc(&A.b.traces, nstage * bf) != cudaSuccess) {
+    cudaGetLastError();  // not enough memory: the reverse sweep recomputes the traces
+    A.b.traces = nullptr;
+  }
   for (int s = 0; s < snapshots; ++s) {
     double *p = nullptr;
     if (cudaMalloc(&p, bq) != cudaSuccess) {
@@ -303,10 +322,14 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   // ---- forward sweep
   std::vector<double> s_win;
   for (int n = 0; n < nsteps; ++n) {
-    std::vector<double *> st;
+    std::vector<double *> st, qf;
     if (snapshots == 0)
-      for (int k = 0; k < kord; ++k) st.push_back(A.b.stages + ((size_t)n * kord + k) * nq);
-    if ((r = forward_step(A, n, snapshots == 0 ? st.data() : nullptr, &s_win))) return r;
+      for (int k = 0; k < kord; ++k) {
+        st.push_back(A.b.stages + ((size_t)n * kord + k) * nq);
+        if (A.b.traces) qf.push_back(A.b.traces + ((size_t)n * kord + k) * nf);
+      }
+    if ((r = forward_step(A, n, snapshots == 0 ? st.data() : nullptr, &s_win, qf.empty() ? nullptr : qf.data())))
+      return r;
   }
   if ((r = dsem_int::check_flag(c))) return r;
   double Jv = 0.0, lr_explicit = 0.0;
@@ -330,18 +353,22 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
           if (x) cudaGraphExecDestroy(x);
       };
       for (int n = nsteps - 1; n >= 0; --n) {
-        std::vector<double *> st;
-        for (int k = 0; k < kord; ++k) st.push_back(A.b.stages + ((size_t)n * kord + k) * nq);
+        std::vector<double *> st, qf;
+        for (int k = 0; k < kord; ++k) {
+          st.push_back(A.b.stages + ((size_t)n * kord + k) * nq);
+          if (A.b.traces) qf.push_back(A.b.traces + ((size_t)n * kord + k) * nf);
+        }
+        double *const *qfp = qf.empty() ? nullptr : qf.data();
         const double *qend = n + 1 < nsteps ? A.b.stages + ((size_t)(n + 1) * kord) * nq : c->JQ;
         if (n == nsteps - 1) {
-          if ((r = reverse_step(A, n, st.data(), qend))) return drop(), r;
+          if ((r = reverse_step(A, n, st.data(), qend, qfp))) return drop(), r;
           continue;
         }
         const int kind = A.in_window(n) ? 1 : 0;
         cudaGraph_t graph = nullptr;
         cudaError_t ec = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
         if (ec != cudaSuccess) return drop(), dsem_int::fail(c, DSEM_ERR_CUDA, "adjoint: cudaStreamBeginCapture failed");
-        r = reverse_step(A, n, st.data(), qend);
+        r = reverse_step(A, n, st.data(), qend, qfp);
         ec = cudaStreamEndCapture(c->st, &graph);
         if (r) {
           if (graph) cudaGraphDestroy(graph);

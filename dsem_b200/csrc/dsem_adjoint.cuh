@@ -527,6 +527,27 @@ __global__ void __launch_bounds__(128) k_face_vis_adj(const MortarC *__restrict_
   }
 }
 
+// Averaged face states of k_face_inv from raw traces kept by the forward sweep
+// (the same expression; the Roe flux is not needed by the reverse sweep).
+template <int G>
+__global__ void __launch_bounds__(128) k_face_avg(const MortarC *__restrict__ mc, int nm, const double *__restrict__ QFR,
+                                                   double *__restrict__ QF) {
+  constexpr int G2 = G * G;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nm * G2) return;
+  const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
+  const MortarC M = mc[m];
+  int si, sj;
+  slave_index<G>(M.flags & 7, pt % G, pt / G, si, sj);
+  const int sp = si + G * sj;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double avg = (QFR[M.ms + v * G2 + pt] + QFR[M.ss + v * G2 + sp]) * 0.5;
+    QF[M.ms + v * G2 + pt] = avg;
+    QF[M.ss + v * G2 + sp] = avg;
+  }
+}
+
 // Roe flux and averaged state (k_face_inv), transposed: QFR = raw traces.
 template <int G>
 __global__ void __launch_bounds__(128) k_face_inv_adj(const MortarC *__restrict__ mc, int nm,
