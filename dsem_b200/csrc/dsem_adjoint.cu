@@ -200,6 +200,36 @@ int forward_step(Adj &A, int n, double *const *st, std::vector<double> *s_win, d
   return DSEM_OK;
 }
 
+// Captures the launches of f() on the context's stream and replays them through
+// *gx, which is instantiated on first use and updated in place afterwards (the
+// same launches with other pointers and scalars).
+template <class F> int replay(dsem_ctx *c, cudaGraphExec_t *gx, F &&f) {
+  cudaGraph_t graph = nullptr;
+  cudaError_t ec = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
+  if (ec != cudaSuccess) return dsem_int::fail(c, DSEM_ERR_CUDA, "adjoint: cudaStreamBeginCapture failed");
+  const int r = f();
+  ec = cudaStreamEndCapture(c->st, &graph);
+  if (r) {
+    if (graph) cudaGraphDestroy(graph);
+    return r;
+  }
+  if (ec != cudaSuccess) return dsem_int::fail(c, DSEM_ERR_CUDA, "adjoint: cudaStreamEndCapture failed");
+  if (*gx) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(*gx, graph, &info) != cudaSuccess) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(*gx);
+      *gx = nullptr;
+    }
+  }
+  if (!*gx) ec = cudaGraphInstantiate(gx, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ec != cudaSuccess) return dsem_int::fail(c, DSEM_ERR_CUDA, "adjoint: cudaGraphInstantiate failed");
+  ec = cudaGraphLaunch(*gx, c->st);
+  if (ec != cudaSuccess) return dsem_int::fail(c, DSEM_ERR_CUDA, "adjoint: cudaGraphLaunch failed");
+  return DSEM_OK;
+}
+
 int load_state(Adj &A, const double *src) {
   dsem_ctx *c = A.c;
   CKA(cudaMemcpyAsync(c->JQ, src, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
@@ -321,15 +351,39 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   if ((r = dsem_int::traces(c))) return r;
   // ---- forward sweep
   std::vector<double> s_win;
-  for (int n = 0; n < nsteps; ++n) {
-    std::vector<double *> st, qf;
-    if (snapshots == 0)
-      for (int k = 0; k < kord; ++k) {
-        st.push_back(A.b.stages + ((size_t)n * kord + k) * nq);
-        if (A.b.traces) qf.push_back(A.b.traces + ((size_t)n * kord + k) * nf);
+  {
+    // after the first (eager) step, steps are captured and replayed as CUDA
+    // graphs, one per kind of step (inside or outside the window); the window's
+    // enstrophy sums are read on the host after each replay
+    cudaGraphExec_t gx[2] = {nullptr, nullptr};
+    auto drop = [&]() {
+      for (auto &x : gx)
+        if (x) cudaGraphExecDestroy(x);
+    };
+    for (int n = 0; n < nsteps; ++n) {
+      std::vector<double *> st, qf;
+      if (snapshots == 0)
+        for (int k = 0; k < kord; ++k) {
+          st.push_back(A.b.stages + ((size_t)n * kord + k) * nq);
+          if (A.b.traces) qf.push_back(A.b.traces + ((size_t)n * kord + k) * nf);
+        }
+      double *const *stp = snapshots == 0 ? st.data() : nullptr;
+      double *const *qfp = qf.empty() ? nullptr : qf.data();
+      if (n == 0) {
+        if ((r = forward_step(A, n, stp, &s_win, qfp))) return drop(), r;
+        continue;
       }
-    if ((r = forward_step(A, n, snapshots == 0 ? st.data() : nullptr, &s_win, qf.empty() ? nullptr : qf.data())))
-      return r;
+      const bool win = A.in_window(n);
+      if ((r = replay(c, &gx[win ? 1 : 0], [&] { return forward_step(A, n, stp, nullptr, qfp); })))
+        return drop(), r;
+      if (win) {
+        double sv = 0.0, s2 = 0.0;
+        if ((r = dsem_int::eps_sums(c, &sv, &s2))) return drop(), r;
+        s_win.push_back(sv);
+        A.s2 = s2;
+      }
+    }
+    drop();
   }
   if ((r = dsem_int::check_flag(c))) return r;
   double Jv = 0.0, lr_explicit = 0.0;
@@ -364,30 +418,8 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
           if ((r = reverse_step(A, n, st.data(), qend, qfp))) return drop(), r;
           continue;
         }
-        const int kind = A.in_window(n) ? 1 : 0;
-        cudaGraph_t graph = nullptr;
-        cudaError_t ec = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
-        if (ec != cudaSuccess) return drop(), dsem_int::fail(c, DSEM_ERR_CUDA, "adjoint: cudaStreamBeginCapture failed");
-        r = reverse_step(A, n, st.data(), qend, qfp);
-        ec = cudaStreamEndCapture(c->st, &graph);
-        if (r) {
-          if (graph) cudaGraphDestroy(graph);
-          return drop(), r;
-        }
-        if (ec != cudaSuccess) return drop(), dsem_int::fail(c, DSEM_ERR_CUDA, "adjoint: cudaStreamEndCapture failed");
-        if (gx[kind]) {
-          cudaGraphExecUpdateResultInfo info;
-          if (cudaGraphExecUpdate(gx[kind], graph, &info) != cudaSuccess) {
-            cudaGetLastError();
-            cudaGraphExecDestroy(gx[kind]);
-            gx[kind] = nullptr;
-          }
-        }
-        if (!gx[kind]) ec = cudaGraphInstantiate(&gx[kind], graph, 0);
-        cudaGraphDestroy(graph);
-        if (ec != cudaSuccess) return drop(), dsem_int::fail(c, DSEM_ERR_CUDA, "adjoint: cudaGraphInstantiate failed");
-        ec = cudaGraphLaunch(gx[kind], c->st);
-        if (ec != cudaSuccess) return drop(), dsem_int::fail(c, DSEM_ERR_CUDA, "adjoint: cudaGraphLaunch failed");
+        r = replay(c, &gx[A.in_window(n) ? 1 : 0], [&] { return reverse_step(A, n, st.data(), qend, qfp); });
+        if (r) return drop(), r;
       }
       drop();
     } else {
