@@ -135,9 +135,7 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
     CKA(cudaGetLastError());
     k_trace_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq, A.b.lq, A.b.lg, ark);
     CKA(cudaGetLastError());
-    k_sum_into<<<1, 256, 0, c->st>>>(A.b.lrp, g.nel, A.b.lr);
-    CKA(cudaGetLastError());
-    A.launches += 6;
+    A.launches += 5;
     return DSEM_OK;
   }
 }
@@ -395,6 +393,7 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   CKA(cudaMemsetAsync(A.b.lq, 0, bq, c->st));
   CKA(cudaMemsetAsync(A.b.lg, 0, bq, c->st));
   CKA(cudaMemsetAsync(A.b.lr, 0, sizeof(double), c->st));
+  CKA(cudaMemsetAsync(A.b.lrp, 0, (size_t)A.g->nel * sizeof(double), c->st));  // per element, summed over stages
   if (window > 0) {
     if (snapshots == 0) {
       // Every reverse step launches the same kernels with other stage pointers:
@@ -427,6 +426,8 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
       if ((r = revolve(A, 0, nsteps, 0, 1))) return r;
     }
   }
+  k_sum_into<<<1, 256, 0, c->st>>>(A.b.lrp, A.g->nel, A.b.lr);  // dJ/d(1/Re) of the volume terms
+  CKA(cudaGetLastError());
   CKA(cudaEventRecord(e1, c->st));
   CKA(cudaEventSynchronize(e1));
   float t = 0.f;

@@ -416,6 +416,7 @@ __device__ __forceinline__ void vis_vjp(const double *Q, const double (&Gr)[3][N
   for (int i = 0; i < 3; ++i)  // Gv[i][j] = (Gr[j][1+i] - vel_i Gr[j][0]) / rho
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
+      if (!(i == D || j == D || i == j)) continue;  // lGv[i][j] is 0 there (the flux along D does not use it)
       const double l = lGv[i][j];
       lG[j][1 + i] += l * ri;
       lvel[i] += -Gr[j][0] * ri * l;
@@ -633,7 +634,7 @@ struct VolAdjArgs {
   const double *LVF;            // dJ/dVF before averaging
   double *LJQ;                  // out: dJ/dJQ (volume part)
   double *LQF;                  // out: dJ/dQF (averaged face state)
-  double *lr;                   // out: per element dJ/d(1/Re)
+  double *lr;                   // in/out: per element dJ/d(1/Re), accumulated over stages
   double eps_w;                 // weight of the enstrophy sum (0: none)
   const double *JQe;            // state whose JQ values the enstrophy sum uses (end of the step)
   int direct_only;              // 1: only dJ/dJQe of the enstrophy sum, into LJQ
@@ -1001,7 +1002,7 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
     __syncthreads();
     n = h;
   }
-  if (tid == 0) A.lr[k] = red[0];
+  if (tid == 0) A.lr[k] += red[0];
 }
 
 // RK bookkeeping of the reverse sweep
