@@ -117,6 +117,11 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
     va.JQe = JQe;
     va.direct_only = direct_only ? 1 : 0;
     va.P = c->P;
+    {  // one block per SM (shared memory): prefetch one wave ahead
+      int nsm = 0;
+      CKA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->dev));
+      va.pf = nsm;
+    }
     if (direct_only) {
       k_vol_adj<G><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
       CKA(cudaGetLastError());

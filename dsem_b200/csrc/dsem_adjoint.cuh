@@ -638,8 +638,20 @@ struct VolAdjArgs {
   double eps_w;                 // weight of the enstrophy sum (0: none)
   const double *JQe;            // state whose JQ values the enstrophy sum uses (end of the step)
   int direct_only;              // 1: only dJ/dJQe of the enstrophy sum, into LJQ
+  int pf;                       // L2 prefetch distance in elements (the blocks resident at once), 0: none
   Phys P;
 };
+
+// Issues L2 prefetches for the n doubles at p, one 128-byte line per thread.
+__device__ __forceinline__ void prefetch_l2(const double *p, int n, int tid, int nt) {
+  const char *b = reinterpret_cast<const char *>(p);
+  const long long lines = ((long long)n * 8 + 127) / 128;
+  for (long long i = tid; i < lines; i += nt) {
+    const char *a = b + i * 128;
+    if (a >= b + (long long)n * 8) a = b + (long long)n * 8 - 8;  // stay inside the range
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+  }
+}
 
 template <int G> struct VolAdjCfg {
   static constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
@@ -683,6 +695,17 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
 #ifdef DSEM_PHASE_TIMING
   t_ph_ = clock64();
 #endif
+  // the element that starts about one wave of blocks later: its inputs into L2
+  if (A.pf > 0 && !A.direct_only && k + A.pf < (int)gridDim.x) {
+    const long long n = k + A.pf;
+    prefetch_l2(A.JQ + n * 5 * NG, 5 * NG, tid, NT);
+    prefetch_l2(A.LQT + n * 5 * NG, 5 * NG, tid, NT);
+    prefetch_l2(A.jac + n * NG, NG, tid, NT);
+    prefetch_l2(A.gg + n * 3 * NG, 3 * NG, tid, NT);
+    prefetch_l2(A.QF + n * 30 * G2, 30 * G2, tid, NT);
+    prefetch_l2(A.gm + n * 3 * NL, 3 * NL, tid, NT);
+    prefetch_l2(A.LVF + n * 30 * G2, 30 * G2, tid, NT);
+  }
 
   {  // state, dJ/dQt, metrics and face states: all of a thread's loads in flight at once
     constexpr int NQ = (5 * NG + NT - 1) / NT, NM = (3 * NG + NT - 1) / NT, NF = (30 * G2 + NT - 1) / NT;
