@@ -74,6 +74,17 @@ __device__ __forceinline__ double ddiv(double a, double b, double rb) {
   return __fma_rn(r, rb, q0);
 }
 
+// Issues L2 prefetches for the n doubles at p, one 128-byte line per thread.
+__device__ __forceinline__ void prefetch_l2(const double *p, int n, int tid, int nt) {
+  const char *b = reinterpret_cast<const char *>(p);
+  const long long lines = ((long long)n * 8 + 127) / 128;
+  for (long long i = tid; i < lines; i += nt) {
+    const char *a = b + i * 128;
+    if (a >= b + (long long)n * 8) a = b + (long long)n * 8 - 8;  // stay inside the range
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+  }
+}
+
 // ------------------------------------------------------------ line helpers
 // Line (a,b) of direction d.  Gauss arrays: base/stride; grid-d arrays: base/stride.
 template <int G> __device__ __forceinline__ int gbase(int d, int a, int b) {
