@@ -291,6 +291,7 @@ def run_ensemble(args):
     ens = Ensemble(descs, [c[2] for c in cases])
     for k, q in enumerate(qs):
         ens.upload_case(k, q)
+    shapes, _ = ens.autotune(reps=3)  # launch shape of the volume kernel per order (untimed)
     ens.step_batch(dts, args.warmup)
     torch.cuda.synchronize()
     with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
@@ -302,6 +303,7 @@ def run_ensemble(args):
     for d, q, dt, c in zip(descs, qs, dts, cases):
         s = Solver(d, re=c[2])
         s.upload(q)
+        s.autotune(reps=3)
         s.step(dt, args.warmup)
         s.step(dt, args.steps)
         m, n = s.last_timing()
@@ -314,7 +316,8 @@ def run_ensemble(args):
            "dtype": "f64", "data": "synthetic (seeded Taylor-Green / isotropic initial conditions)",
            "config": {"workload": f"ensemble of {len(cases)} cases, seed {args.seed}: E in 4^3..12^3, p in 4/6/8, "
                                   "Re U[400,3200], Mach U[0.05,0.3]", "cases": len(cases),
-                      "unknowns": int(dof.sum()), "elements": int(sum(int(d["ngrid"]) for d in descs))},
+                      "unknowns": int(dof.sum()), "elements": int(sum(int(d["ngrid"]) for d in descs)),
+                      "volume_launch_shape_per_p": {str(k): v for k, v in shapes.items()}},
            "sequential": {"value": work / (ms_s * 1e-3), "ms_per_step": ms_s / args.steps,
                           "gpu_launches": launches_s},
            "speedup_vs_sequential": ms_s / ms_b, "gpu_launches": launches_b, "clocks": clk.summary()}
@@ -418,6 +421,7 @@ def main():
     dof = 5 * box.nel * G ** 3
     s = Solver(desc, re=RE)
     s.upload(q)
+    shapes, shape_ms = s.autotune(reps=3)  # launch shape of the volume kernel (untimed)
 
     def barrier():
         torch.cuda.synchronize()
@@ -484,7 +488,9 @@ def main():
                "config": {"workload": f"taylor-green {args.nex}^3 hex p={args.p}, Re=1600, Mach 0.1, 5-stage LSRK",
                           "unknowns_per_gpu": dof, "elements": box.nel, "parallelism": f"replicas x{world}",
                           "l2": "inputs larger than L2 (state 310 MB + face buffers 620 MB)",
-                          "stage_tflops_fp64": step_tf},
+                          "stage_tflops_fp64": step_tf,
+                          "volume_launch_shape": {"chosen": shapes[args.p],
+                                                  "ms_per_shape": [round(float(x), 4) for x in shape_ms[args.p - 1]]}},
                "e2e": {"value": e2e, "unit": "DOF-RK-stages/s", "h2d_bytes_per_step": nbytes,
                        "d2h_bytes_per_step": nbytes, "steps": k_e2e},
                "gpu_launches": launches, "clocks": clk.summary(), "roofline": roof}

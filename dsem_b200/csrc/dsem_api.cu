@@ -258,26 +258,34 @@ int enqueue_face_inv(dsem_ctx *c, long long *launches) {
   return DSEM_OK;
 }
 
+// volume kernel arguments of one order group
+VolArgs vol_args(const dsem_ctx *c, const Group &g) {
+  VolArgs a{};
+  a.JQ = c->JQ + g.q0;
+  a.sq = 5LL * g.G * g.G * g.G;
+  a.jac = g.jac;
+  a.gg = g.gg;
+  a.gm = g.gm;
+  a.muhg = g.muhg;
+  a.QF = c->QF + g.f0;
+  a.VF = c->VF + g.f0;
+  a.QTI = c->QTI + g.q0;
+  a.EVB = g.EVB;
+  a.P = c->P;
+  a.ecase = g.ecase;
+  a.rec = c->d_rec;
+  a.nuhg = c->les ? g.nuhg : nullptr;
+  return a;
+}
+
 int enqueue_vol(dsem_ctx *c, bool save, long long *launches) {
   const int mode = vol_mode(c, save);
   int r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
     auto &g = c->groups[j];
-    VolArgs a{};
-    a.JQ = c->JQ + g.q0;
-    a.sq = 5LL * g.G * g.G * g.G;
-    a.jac = g.jac;
-    a.gg = g.gg;
-    a.gm = g.gm;
-    a.muhg = g.muhg;
-    a.QF = c->QF + g.f0;
-    a.VF = c->VF + g.f0;
-    a.QTI = c->QTI + g.q0;
-    a.EVB = g.EVB;
-    a.P = c->P;
-    a.ecase = g.ecase;
-    a.rec = c->d_rec;
-    a.nuhg = c->les ? g.nuhg : nullptr;
-    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::vol(a, g.nel, g.diag, mode, st); }));
+    const VolArgs a = vol_args(c, g);
+    CK(with_G(g.G, [&](auto gg) {
+      return Launch<decltype(gg)::value>::vol(a, g.nel, g.diag, mode, st, c->vol_variant[g.G]);
+    }));
     return DSEM_OK;
   });
   if (r) return r;
@@ -1456,6 +1464,78 @@ int dsem_set_boundary(dsem_ctx *c, double twall, const double *Qext, const doubl
     }
   }
   if (Qext) c->bnd_ext_set = true;
+  return DSEM_OK;
+}
+
+// Chooses, per element order, the launch shape of the volume kernel (threads
+// per element and elements per SM) by timing the available shapes on the
+// context's own elements and state.  All shapes give identical results.
+int dsem_autotune(dsem_ctx *c, int reps, int *choice, double *ms) {
+  static_assert(DSEM_VOL_VARIANTS == dsem::VOL_VARIANTS, "variant count");
+  if (!c || reps < 1) return fail(c, DSEM_ERR_INVALID_ARG, "null context or reps < 1");
+  long long l = 0;
+  int r;
+  if (!c->traces_valid && (r = enqueue_traces(c, &l))) return r;
+  if (ms)
+    for (int i = 0; i < DSEM_MAX_ORDER * DSEM_VOL_VARIANTS; ++i) ms[i] = -1.0;
+  const int mode = vol_mode(c, false);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  for (auto &g : c->groups) {
+    const int slot = g.G - 2;  // order p = G - 1 at index p - 1
+    int nv = 1;
+    CK(with_G(g.G, [&](auto gg) {
+      nv = Launch<decltype(gg)::value>::vol_variants();
+      return cudaSuccess;
+    }));
+    if (!g.diag || mode == VOL_EV || mode == VOL_EV_SAVE) nv = 1;  // shapes exist for the plain diagonal kernel
+    const VolArgs a = vol_args(c, g);
+    int best = 0;
+    float tbest = 0.f;
+    for (int v = 0; v < nv; ++v) {
+      auto launch = [&]() {
+        return with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::vol(a, g.nel, true, mode, c->st, v); });
+      };
+      CK(launch());  // warm-up (and the kernel's one-time attributes)
+      CK(cudaEventRecord(e0, c->st));
+      for (int i = 0; i < reps; ++i) CK(launch());
+      CK(cudaEventRecord(e1, c->st));
+      CK(cudaEventSynchronize(e1));
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, e0, e1));
+      t /= (float)reps;
+      if (ms) ms[slot * DSEM_VOL_VARIANTS + v] = t;
+      if (v == 0 || t < tbest) {
+        tbest = t;
+        best = v;
+      }
+    }
+    c->vol_variant[g.G] = best;
+    if (choice) choice[slot] = best;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (c->gexec) {  // the captured step holds the old launch shapes
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  return DSEM_OK;
+}
+
+int dsem_set_vol_variant(dsem_ctx *c, int p, int variant) {
+  if (!c || p < 1 || p > DSEM_MAX_ORDER) return fail(c, DSEM_ERR_INVALID_ARG, "null context or order outside 1..8");
+  int nv = 1;
+  CK(with_G(p + 1, [&](auto gg) {
+    nv = Launch<decltype(gg)::value>::vol_variants();
+    return cudaSuccess;
+  }));
+  if (variant < 0 || variant >= nv) return fail(c, DSEM_ERR_INVALID_ARG, "no such launch shape for this order");
+  c->vol_variant[p + 1] = variant;
+  if (c->gexec) {
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
   return DSEM_OK;
 }
 

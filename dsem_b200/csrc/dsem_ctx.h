@@ -74,6 +74,7 @@ struct dsem_ctx {
   double ark[5] = {}, brk[5] = {}, crk[5] = {};
   std::vector<Group> groups;
   std::vector<MList> mlists;
+  int vol_variant[dsem::GMAX + 1] = {};  // launch shape of the volume kernel per order G (dsem_autotune)
   std::vector<BList> blists;  // boundary faces; their conditions need dsem_set_boundary first
   int nbnd = 0;
   bool bnd_need_twall = false, bnd_need_ext = false, bnd_twall_set = false, bnd_ext_set = false;

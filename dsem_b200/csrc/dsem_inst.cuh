@@ -26,9 +26,10 @@ template <int G, bool DIAG, bool EV, int SAVE> static cudaError_t vol_one(const 
 }
 
 // diagonal metrics: k_vol_diag (two elements per SM at p = 8)
-template <int G, bool EV, int SAVE> static cudaError_t vol_diag_one(const VolArgs &a, int nel, cudaStream_t s) {
-  using C = VolDiagCfg<G, EV, SAVE>;
-  auto kern = k_vol_diag<G, EV, SAVE>;
+template <int G, bool EV, int SAVE, int V = 0>
+static cudaError_t vol_diag_one(const VolArgs &a, int nel, cudaStream_t s) {
+  using C = VolDiagCfg<G, EV, SAVE, V>;
+  auto kern = k_vol_diag<G, EV, SAVE, V>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
@@ -53,7 +54,26 @@ template <int G> int Launch<G>::vol_threads(bool diag, int mode) {
   return diag ? VolDiagCfg<G, false, 0>::NT : VolCfg<G, false, false, 0>::NT;
 }
 
-template <int G> cudaError_t Launch<G>::vol(const VolArgs &a, int nel, bool diag, int mode, cudaStream_t s) {
+// launch-shape variants of k_vol_diag instantiated for this order (p = 4, 6, 8)
+template <int G> int Launch<G>::vol_variants() { return (G == 5 || G == 7 || G == 9) ? VOL_VARIANTS : 1; }
+
+template <int G> int Launch<G>::vol_variant_threads(int v) {
+  switch (v) {
+    case 1: return VolDiagShape<G, 1>::NT;
+    case 2: return VolDiagShape<G, 2>::NT;
+    default: return VolDiagShape<G, 0>::NT;
+  }
+}
+
+template <int G>
+cudaError_t Launch<G>::vol(const VolArgs &a, int nel, bool diag, int mode, cudaStream_t s, int variant) {
+  if constexpr (G == 5 || G == 7 || G == 9) {  // variants of the diagonal kernel without entropy viscosity
+    if (diag && (variant == 1 || variant == 2) && (mode == VOL_PLAIN || mode == VOL_SAVE)) {
+      if (mode == VOL_SAVE)
+        return variant == 1 ? vol_diag_one<G, false, 1, 1>(a, nel, s) : vol_diag_one<G, false, 1, 2>(a, nel, s);
+      return variant == 1 ? vol_diag_one<G, false, 0, 1>(a, nel, s) : vol_diag_one<G, false, 0, 2>(a, nel, s);
+    }
+  }
   switch (mode) {
     case VOL_SAVE: return diag ? vol_diag_one<G, false, 1>(a, nel, s) : vol_one<G, false, false, 1>(a, nel, s);
     case VOL_EV: return diag ? vol_diag_one<G, true, 0>(a, nel, s) : vol_one<G, false, true, 0>(a, nel, s);

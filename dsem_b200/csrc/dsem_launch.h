@@ -18,12 +18,16 @@ struct BndPhys;
 
 // volume kernel variants: metric layout x entropy viscosity x saved gradients
 enum VolMode { VOL_PLAIN = 0, VOL_SAVE = 1, VOL_EV = 2, VOL_EV_SAVE = 3 };
+// launch shapes of the diagonal volume kernel the autotuner chooses from
+constexpr int VOL_VARIANTS = 3;
 
 template <int G> struct Launch {
   static cudaError_t set_ops(const double *host_ops, int n);  // copies the operator table to constant memory
   static size_t vol_smem(bool diag, int mode);
   static int vol_threads(bool diag, int mode);
-  static cudaError_t vol(const VolArgs &a, int nel, bool diag, int mode, cudaStream_t s);
+  static cudaError_t vol(const VolArgs &a, int nel, bool diag, int mode, cudaStream_t s, int variant = 0);
+  static int vol_variants();                // launch shapes available for this order (1 or VOL_VARIANTS)
+  static int vol_variant_threads(int v);    // threads per element of shape v
   static cudaError_t update(const UpdArgs &a, int nel, cudaStream_t s);
   static cudaError_t trace(const TraceArgs &a, int nel, cudaStream_t s);
   static cudaError_t ev(const EvArgs &a, int nel, cudaStream_t s);

@@ -27,20 +27,33 @@
 
 namespace dsem {
 
-template <int G, bool EV, int SAVE> struct VolDiagCfg {
-  static constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
+// Launch shapes of k_vol_diag: threads per element (NT) and the elements an SM
+// must hold at once (MINB, which sets the register budget).  Variant 0 is the
+// default; the autotuner (dsem_autotune) times variants 1 and 2 against it for
+// p = 4, 6, 8.  Every variant evaluates each value with the same FMA chain, so
+// all give identical results.
 #ifndef DSEM_VOL_DIAG_NT8
 #define DSEM_VOL_DIAG_NT8 192  // 2 CTAs x 6 warps per SM leave 168 registers per thread: no spills at p = 8
 #endif
-  static constexpr int NT = G >= 8 ? DSEM_VOL_DIAG_NT8 : (G >= 6 ? 96 : (G >= 4 ? 64 : 32));
-  static constexpr int NPT = (NG + NT - 1) / NT;       // Gauss points per thread (divergence)
+template <int G, int V> struct VolDiagShape {
+  // p >= 7: 192 / 128 / 256 threads, two elements per SM (168 / 255 / 128 registers)
+  // p = 5, 6: 96 / 64 / 128 threads, four elements per SM (168 / 255 / 128 registers)
+  // p <= 4: 64 / 64 / 128 threads, eight / six / four elements per SM
+  static constexpr int NT = G >= 8 ? (V == 0 ? DSEM_VOL_DIAG_NT8 : (V == 1 ? 128 : 256))
+                                   : G >= 6 ? (V == 0 ? 96 : (V == 1 ? 64 : 128))
+                                            : G >= 4 ? (V == 2 ? 128 : 64) : 32;
 #ifdef DSEM_VOL_DIAG_MINB
-  static constexpr int MINB = DSEM_VOL_DIAG_MINB;
+  static constexpr int MINB = V == 0 ? DSEM_VOL_DIAG_MINB : (G >= 8 ? 2 : (G >= 6 ? 4 : (V == 1 ? 6 : 4)));
 #else
-  // elements per SM the registers must allow: 2 x 6 warps (168 registers) at p >= 7,
-  // 4 x 3 warps (168) at p = 5, 6, and 128 registers per thread below
-  static constexpr int MINB = G >= 8 ? 2 : (G >= 6 ? 4 : 512 / NT);
+  static constexpr int MINB = G >= 8 ? 2 : (G >= 6 ? 4 : (G >= 4 ? (V == 0 ? 8 : (V == 1 ? 6 : 4)) : 16));
 #endif
+};
+
+template <int G, bool EV, int SAVE, int V = 0> struct VolDiagCfg {
+  static constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
+  static constexpr int NT = VolDiagShape<G, V>::NT;
+  static constexpr int NPT = (NG + NT - 1) / NT;       // Gauss points per thread (divergence)
+  static constexpr int MINB = VolDiagShape<G, V>::MINB;
   static constexpr int NGR = 12;                        // Gauss gradients of fields 0..3
   static constexpr int NWORK = (6 * NL > 5 * NG) ? 6 * NL : 5 * NG;  // state (pass 1) / Lobatto arrays (pass 2)
   static constexpr size_t SMEM = sizeof(double) * (size_t)(NGR * NG + NWORK + 2 * G * L);
@@ -180,13 +193,13 @@ __device__ __forceinline__ void vol_diag_point(int qi, int s, int a, int b, cons
 
 // Pass 2 along direction D: Lobatto arrays of grid D, fluxes at its points,
 // interior divergence accumulated into acc (the thread's Gauss points).
-template <int G, bool EV, int SAVE, int D>
+template <int G, bool EV, int SAVE, int D, int V>
 __device__ __forceinline__ void vol_diag_dir(const VolArgs &A, const Phys &P, const double *JQ, const double *jac,
                                              const double *QF, const double *gg, const double *gm, const double *muhg,
                                              const double *nuhg,
                                              const double *GR, double *LB, double *T4, const double *Bm,
                                              const double *Dm, double *VF, double *QTI, int tid, long long &t_ph_) {
-  using C = VolDiagCfg<G, EV, SAVE>;
+  using C = VolDiagCfg<G, EV, SAVE, V>;
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G, NT = C::NT, NPT = C::NPT;
   const double gamma = P.gamma;
   const int xs = D == 0 ? 1 : (D == 1 ? G : G2);
@@ -314,10 +327,10 @@ __device__ __forceinline__ void vol_diag_dir(const VolArgs &A, const Phys &P, co
   PHASE_MARK(4 + 3 * (2 - D));
 }
 
-template <int G, bool EV, int SAVE>
-__global__ void __launch_bounds__(VolDiagCfg<G, EV, SAVE>::NT, VolDiagCfg<G, EV, SAVE>::MINB)
+template <int G, bool EV, int SAVE, int V = 0>
+__global__ void __launch_bounds__(VolDiagCfg<G, EV, SAVE, V>::NT, VolDiagCfg<G, EV, SAVE, V>::MINB)
     k_vol_diag(VolArgs A) {
-  using C = VolDiagCfg<G, EV, SAVE>;
+  using C = VolDiagCfg<G, EV, SAVE, V>;
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G, NT = C::NT, NPT = C::NPT;
   extern __shared__ double sm[];
   double *GR = sm;                  // [12][NG] Gauss gradients, field f*3 + direction
@@ -403,9 +416,9 @@ __global__ void __launch_bounds__(VolDiagCfg<G, EV, SAVE>::NT, VolDiagCfg<G, EV,
 
   // ---- pass 2: z, y, x
   double *QTI = A.QTI + (long long)k * 5 * NG;
-  vol_diag_dir<G, EV, SAVE, 2>(A, P, JQ, jac, QF, gg, gm, muhg, nuhg, GR, LB, T4, Bm, Dm, VF, QTI, tid, t_ph_);
-  vol_diag_dir<G, EV, SAVE, 1>(A, P, JQ, jac, QF, gg, gm, muhg, nuhg, GR, LB, T4, Bm, Dm, VF, QTI, tid, t_ph_);
-  vol_diag_dir<G, EV, SAVE, 0>(A, P, JQ, jac, QF, gg, gm, muhg, nuhg, GR, LB, T4, Bm, Dm, VF, QTI, tid, t_ph_);
+  vol_diag_dir<G, EV, SAVE, 2, V>(A, P, JQ, jac, QF, gg, gm, muhg, nuhg, GR, LB, T4, Bm, Dm, VF, QTI, tid, t_ph_);
+  vol_diag_dir<G, EV, SAVE, 1, V>(A, P, JQ, jac, QF, gg, gm, muhg, nuhg, GR, LB, T4, Bm, Dm, VF, QTI, tid, t_ph_);
+  vol_diag_dir<G, EV, SAVE, 0, V>(A, P, JQ, jac, QF, gg, gm, muhg, nuhg, GR, LB, T4, Bm, Dm, VF, QTI, tid, t_ph_);
   PHASE_MARK(20);
 }
 

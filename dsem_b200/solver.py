@@ -20,7 +20,7 @@ EXPORTS = ("dsem_create", "dsem_destroy", "dsem_last_error", "dsem_upload_q", "d
            "dsem_create_batch", "dsem_batch_size", "dsem_upload_q_case", "dsem_download_q_case", "dsem_step_batch",
            "dsem_diag_batch", "dsem_adjoint", "dsem_set_les", "dsem_get_nut", "dsem_state_size",
            "dsem_save_state", "dsem_load_state", "dsem_shard_info", "dsem_shard_stage", "dsem_diag_sums",
-           "dsem_set_boundary")
+           "dsem_set_boundary", "dsem_autotune", "dsem_set_vol_variant")
 
 
 class DsemError(RuntimeError):
@@ -76,6 +76,8 @@ def lib(path=None):
         L.dsem_diag_batch.argtypes = [vp, dp, C.c_int, dp, dp, dp]
         L.dsem_set_les.argtypes = [vp, C.c_double, C.c_double]
         L.dsem_set_boundary.argtypes = [vp, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]
+        L.dsem_autotune.argtypes = [vp, C.c_int, C.POINTER(C.c_int), dp]
+        L.dsem_set_vol_variant.argtypes = [vp, C.c_int, C.c_int]
         L.dsem_shard_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(dp), C.POINTER(dp)]
         L.dsem_shard_stage.argtypes = [vp, C.c_double, C.c_int, C.c_int]
         L.dsem_diag_sums.argtypes = [vp, dp]
@@ -203,6 +205,18 @@ class Solver:
                 raise ValueError("external states are [nmort][5][ldx][ldx]")
         self._check(lib().dsem_set_boundary(self.h, float(twall), None if keep[0] is None else _dptr(keep[0]),
                                             None if keep[1] is None else _dptr(keep[1]), int(ldx)))
+
+    def autotune(self, reps=5):
+        """Times the volume kernel's launch shapes per element order and keeps the
+        fastest: returns {p: chosen shape} and ms[p-1][shape] (-1: not timed)."""
+        choice = np.zeros(8, dtype=np.int32)
+        ms = np.zeros((8, 3))
+        self._check(lib().dsem_autotune(self.h, int(reps), choice.ctypes.data_as(C.POINTER(C.c_int)), _dptr(ms)))
+        orders = sorted({p for p in range(1, 9) if ms[p - 1, 0] >= 0})
+        return {p: int(choice[p - 1]) for p in orders}, ms
+
+    def set_vol_variant(self, p, variant):
+        self._check(lib().dsem_set_vol_variant(self.h, int(p), int(variant)))
 
     def set_les(self, cs, numax):
         """Static Smagorinsky model (cs = 0: off)."""

@@ -153,6 +153,21 @@ int dsem_state_size(const dsem_ctx *ctx, long long *nbytes);
 int dsem_save_state(dsem_ctx *ctx, void *buf, long long nbytes);
 int dsem_load_state(dsem_ctx *ctx, const void *buf, long long nbytes);
 
+/* ---- Autotuning of the volume kernel's launch shape ----
+ * No counterpart in DSEM (its element loops have no launch shape).  For each
+ * element order of the context, times the launch shapes of the volume kernel
+ * (threads per element, elements held per SM) on the context's own elements
+ * and current state, `reps` launches each, and keeps the fastest for the
+ * following steps.  Shapes exist for p = 4, 6 and 8 (other orders have one);
+ * all give identical results.  choice[p-1] receives the chosen shape of order p
+ * and ms[(p-1)*DSEM_VOL_VARIANTS + v] the mean time of shape v (-1: not timed);
+ * either may be NULL.  Call it after dsem_upload_q.  dsem_set_vol_variant
+ * sets a shape by hand. */
+#define DSEM_MAX_ORDER 8
+#define DSEM_VOL_VARIANTS 3
+int dsem_autotune(dsem_ctx *ctx, int reps, int *choice, double *ms);
+int dsem_set_vol_variant(dsem_ctx *ctx, int p, int variant);
+
 /* ---- Boundary faces (mortars with id(2) = 0) ----
  * Sets the wall temperature of isothermal walls (MODULE physics twall) and,
  * for inflow and outflow faces, the external state and viscous flux that DSEM
