@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--fd-check", action="store_true")
     ap.add_argument("--cases", type=int, default=64)
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--adj-steps", type=int, default=400, help="adjoint workload: steps of the run")
+    ap.add_argument("--adj-window", type=int, default=100, help="adjoint workload: steps in the objective")
     return ap.parse_args()
 
 
@@ -329,7 +331,7 @@ def run_adjoint(args):
     from dsem_b200 import mesh
     from dsem_b200.solver import Solver
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    nex, p, nsteps, window = 12, 6, 400, 100
+    nex, p, nsteps, window = 12, 6, args.adj_steps, min(args.adj_window, args.adj_steps)
     box = mesh.Box(nex, nex, nex, p)
     q = mesh.perturbed_taylor_green(box, seed=args.seed)
     dt = CFL * mesh.dtcalc(box, q)
@@ -340,7 +342,7 @@ def run_adjoint(args):
     s.step(dt, nsteps)
     fwd_ms, _ = s.last_timing()
     s.upload(q)
-    out = {"metric": "adjoint / forward time, 400 steps", "unit": "ratio", "n_gpus": 1, "higher_is_better": False,
+    out = {"metric": f"adjoint / forward time, {nsteps} steps", "unit": "ratio", "n_gpus": 1, "higher_is_better": False,
            "dtype": "f64", "data": "synthetic (Taylor-Green + seeded 5% isotropic perturbation)",
            "config": {"workload": f"perturbed taylor-green {nex}^3 hex p={p}, Re=1600, {nsteps} steps, J = sum eps dt "
                                   f"over the last {window}", "unknowns": 5 * box.nel * (p + 1) ** 3},
