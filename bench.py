@@ -206,7 +206,8 @@ def cpu_baseline(desc, q, dt, dof):
         c.stage(0.0, dt, kk, want_qt=False)
     t = time.perf_counter() - t0
     return {"value": dof * STAGES / t, "unit": "DOF-RK-stages/s", "cores": cores, "kind": "port",
-            "sample": "1 RK step (5 stages) of the same 22^3 p=8 case, C++ oracle with OpenMP over elements"}
+            "sample": f"1 RK step (5 stages) of the same case ({int(desc['ngrid'])} elements, "
+                      f"p={int(desc['ncg'][0]) - 1}), C++ oracle with OpenMP over elements"}
 
 
 def run_reference(args):
