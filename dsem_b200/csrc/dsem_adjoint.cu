@@ -79,12 +79,13 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
     constexpr int G2 = G * G;
     // forward prerequisites: raw traces (qfr), averaged traces (c->QF)
     const double *qfr = qraw;
-    if (qraw) {
+    const bool avg_in_vis = qraw && !direct_only;  // the viscous-face adjoint writes the averages
+    if (qraw && direct_only) {
       const unsigned nbm = (unsigned)(((long long)ml.n * G2 + 127) / 128);
       k_face_avg<G><<<nbm, 128, 0, c->st>>>(ml.mc, ml.n, qraw, c->QF);
       CKA(cudaGetLastError());
       A.launches += 1;
-    } else {
+    } else if (!qraw) {
       TraceArgs ta{};
       ta.JQ = Qs;
       ta.sq = 5LL * G * G * G;
@@ -131,7 +132,7 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
     const unsigned nb = (unsigned)(((long long)ml.n * G2 + 127) / 128);
     k_upd_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lg, A.b.lq, cdt, c->P.re, A.b.lff, A.b.lvf);
     CKA(cudaGetLastError());
-    k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lvf, ml.nrm);
+    k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lvf, ml.nrm, avg_in_vis ? qraw : nullptr, c->QF);
     CKA(cudaGetLastError());
     k_vol_adj<G><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
     CKA(cudaGetLastError());

@@ -505,8 +505,11 @@ __global__ void __launch_bounds__(256) k_upd_adj(double *__restrict__ LQT, const
 
 // BR1 average of the viscous normal flux (k_face_vis), transposed in place.
 template <int G>
+// With QFR non-null it also writes the averaged face states of k_face_inv into QF
+// (as k_face_avg), from raw traces kept by the forward sweep.
 __global__ void __launch_bounds__(128) k_face_vis_adj(const MortarC *__restrict__ mc, int nm, double *__restrict__ LVF,
-                                                       const double *__restrict__ nrm) {
+                                                       const double *__restrict__ nrm, const double *__restrict__ QFR,
+                                                       double *__restrict__ QF) {
   constexpr int G2 = G * G;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)nm * G2) return;
@@ -525,6 +528,14 @@ __global__ void __launch_bounds__(128) k_face_vis_adj(const MortarC *__restrict_
     const double lh = 0.5 * nm_m * lqb;
     LVF[M.ms + v * G2 + pt] = lh / nm_m;
     LVF[M.ss + v * G2 + sp] = (neg_n ? -lh : lh) / nm_s;
+  }
+  if (QFR) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const double avg = (QFR[M.ms + v * G2 + pt] + QFR[M.ss + v * G2 + sp]) * 0.5;
+      QF[M.ms + v * G2 + pt] = avg;
+      QF[M.ss + v * G2 + sp] = avg;
+    }
   }
 }
 
