@@ -98,11 +98,8 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
       qfr = A.b.qfr;
     }
     using C = VolAdjCfg<G>;
-    static bool attr = false;
-    if (!attr) {
-      CKA(cudaFuncSetAttribute(k_vol_adj<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
-      attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    CKA(set_smem_once(k_vol_adj<G>, C::SMEM, attr));
     VolAdjArgs va{};
     va.JQ = Qs;
     va.jac = g.jac;

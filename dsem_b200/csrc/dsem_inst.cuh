@@ -14,12 +14,9 @@ template <int G> cudaError_t Launch<G>::set_ops(const double *h, int n) {
 template <int G, bool DIAG, bool EV, int SAVE> static cudaError_t vol_one(const VolArgs &a, int nel, cudaStream_t s) {
   using C = VolCfg<G, DIAG, EV, SAVE>;
   auto kern = k_vol<G, DIAG, EV, SAVE>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  cudaError_t e = set_smem_once(kern, C::SMEM, attr);
+  if (e != cudaSuccess) return e;
   if (nel <= 0) return cudaSuccess;
   kern<<<nel, C::NT, C::SMEM, s>>>(a);
   return cudaGetLastError();
@@ -30,12 +27,9 @@ template <int G, bool EV, int SAVE, int V = 0>
 static cudaError_t vol_diag_one(const VolArgs &a, int nel, cudaStream_t s) {
   using C = VolDiagCfg<G, EV, SAVE, V>;
   auto kern = k_vol_diag<G, EV, SAVE, V>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  cudaError_t e = set_smem_once(kern, C::SMEM, attr);
+  if (e != cudaSuccess) return e;
   if (nel <= 0) return cudaSuccess;
   kern<<<nel, C::NT, C::SMEM, s>>>(a);
   return cudaGetLastError();

@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 namespace dsem {
 
 struct Phys;
@@ -15,6 +17,21 @@ struct MortarC;
 struct MortarCut;
 struct MortarB;
 struct BndPhys;
+
+// A kernel's dynamic shared-memory limit is a per-device setting: raises it to
+// smem on the current device the first time that device launches kern (mask:
+// the call site's record of the devices done, one bit per device id < 64).
+template <class K>
+cudaError_t set_smem_once(K kern, size_t smem, std::atomic<unsigned long long> &mask) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = (dev >= 0 && dev < 64) ? 1ULL << dev : 0ULL;
+  if (bit && (mask.load(std::memory_order_relaxed) & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess && bit) mask.fetch_or(bit, std::memory_order_relaxed);
+  return e;
+}
 
 // volume kernel variants: metric layout x entropy viscosity x saved gradients
 enum VolMode { VOL_PLAIN = 0, VOL_SAVE = 1, VOL_EV = 2, VOL_EV_SAVE = 3 };
