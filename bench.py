@@ -238,7 +238,7 @@ def run_reference(args):
     line = {"metric": "DOF-RK-stages/s FP64 at p=8", "value": v, "unit": "DOF-RK-stages/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"taylor-green {args.nex}^3 hex p={args.p}, Re=1600, Mach 0.1",
+            "config": {"workload": f"taylor-green {args.nex}^3 hex p={args.p}, Re=1600, Mach 0.1, 5-stage LSRK",
                        "unknowns": dof, "step": "one RK stage per sample"},
             "cpu_baseline": {"value": v, "unit": "DOF-RK-stages/s", "cores": cores, "kind": "port",
                              "sample": "one RK stage of the full case per step (C++ oracle, OpenMP)"},
