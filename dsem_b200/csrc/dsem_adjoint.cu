@@ -45,8 +45,12 @@ struct AdjBuf {
   std::vector<double *> slots;  // checkpoint slots (step states)
   double *stages = nullptr;     // stage states: all steps (snapshots == 0) or one step
   double *traces = nullptr;     // raw face traces of every stage state (snapshots == 0, when memory allows)
+  // entropy viscosity: dJ/dmu of the step being reversed, dJ/d(gradients saved by
+  // the previous step's last stage), and those gradients as they were on entry
+  double *lmuhg = nullptr, *levb = nullptr, *evb0 = nullptr;
   ~AdjBuf() {
-    for (double *p : {lq, lg, ljq, ldir, qfr, lff, lvf, lqf, lqr, lrp, lr, q0, stages, traces}) cudaFree(p);
+    for (double *p : {lq, lg, ljq, ldir, qfr, lff, lvf, lqf, lqr, lrp, lr, q0, stages, traces, lmuhg, levb, evb0})
+      cudaFree(p);
     for (double *p : slots) cudaFree(p);
   }
 };
@@ -59,6 +63,9 @@ struct Adj {
   double dt = 0.0, s2 = 0.0;
   int nsteps = 0, window = 0;
   long long launches = 0;
+  bool ev = false;            // entropy viscosity on
+  bool ev_valid0 = false;     // the gradients behind the first step's viscosity were valid on entry
+  bool levb_pending = false;  // b.levb holds the demand on the next-to-reverse step's saved gradients
   bool in_window(int n) const { return n >= nsteps - window; }  // step n (0-based) ends inside the window
   double eps_w() const { return dt * 100.0 * c->P.r_re / s2; }
 };
@@ -68,12 +75,13 @@ struct Adj {
 // qraw: the raw face traces of Qs kept by the forward sweep, or null to recompute them.
 template <int G>
 int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, bool direct_only, double cdt,
-                    double ark, const double *qraw) {
+                    double ark, const double *qraw, const double *levb) {
   dsem_ctx *c = A.c;
   const Group &g = *A.g;
   const MList &ml = *A.ml;
   if constexpr (G > 7) {
     (void)Qs; (void)JQe; (void)eps_w; (void)direct_only; (void)g; (void)ml; (void)cdt; (void)ark; (void)qraw;
+    (void)levb;
     return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
   } else {
     constexpr int G2 = G * G;
@@ -98,8 +106,9 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
       qfr = A.b.qfr;
     }
     using C = VolAdjCfg<G>;
-    static std::atomic<unsigned long long> attr{0};
-    CKA(set_smem_once(k_vol_adj<G>, C::SMEM, attr));
+    static std::atomic<unsigned long long> attr{0}, attr_ev{0};
+    CKA(set_smem_once(k_vol_adj<G, false>, C::SMEM, attr));
+    if (A.ev) CKA(set_smem_once(k_vol_adj<G, true>, C::SMEM, attr_ev));
     VolAdjArgs va{};
     va.JQ = Qs;
     va.jac = g.jac;
@@ -115,13 +124,18 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
     va.JQe = JQe;
     va.direct_only = direct_only ? 1 : 0;
     va.P = c->P;
+    if (A.ev && !direct_only) {
+      va.muhg = g.muhg;
+      va.lmuhg = A.b.lmuhg;
+      va.levb = levb;
+    }
     {  // one block per SM (shared memory): prefetch one wave ahead
       int nsm = 0;
       CKA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->dev));
       va.pf = nsm;
     }
     if (direct_only) {
-      k_vol_adj<G><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
+      k_vol_adj<G, false><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
       CKA(cudaGetLastError());
       ++A.launches;
       return DSEM_OK;
@@ -131,7 +145,10 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
     CKA(cudaGetLastError());
     k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lvf, ml.nrm, avg_in_vis ? qraw : nullptr, c->QF);
     CKA(cudaGetLastError());
-    k_vol_adj<G><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
+    if (A.ev)
+      k_vol_adj<G, true><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
+    else
+      k_vol_adj<G, false><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
     CKA(cudaGetLastError());
     k_face_inv_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, qfr, A.b.lff, A.b.lqf, A.b.lqr, ml.nh, ml.nrm,
                                              c->P.gamma);
@@ -144,24 +161,143 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
 }
 
 int stage_adjoint(Adj &A, const double *Qs, const double *JQe, double eps_w, bool direct_only, double cdt = 0.0,
-                  double ark = 1.0, const double *qraw = nullptr) {
+                  double ark = 1.0, const double *qraw = nullptr, const double *levb = nullptr) {
   int r = DSEM_OK;
   cudaError_t e = with_G(A.g->G, [&](auto gc) -> cudaError_t {
-    r = stage_adjoint_G<decltype(gc)::value>(A, Qs, JQe, eps_w, direct_only, cdt, ark, qraw);
+    r = stage_adjoint_G<decltype(gc)::value>(A, Qs, JQe, eps_w, direct_only, cdt, ark, qraw, levb);
     return cudaSuccess;
   });
   if (e != cudaSuccess) return dsem_int::fail(A.c, DSEM_ERR_UNSUPPORTED, "adjoint: element order not supported");
   return r;
 }
 
+// Entropy viscosity for the reverse sweep of a step whose start state is Qn:
+// first the gradients that fed it, saved by the previous step's last stage
+// (recomputed from that stage's stored input state Qprev and its raw face
+// traces, or kept from entry for the first step), then the viscosity itself
+// (k_ev, into the group's muhg).  *valid: whether those gradients existed.
+template <int G> int ev_forward_G(Adj &A, const double *Qn, const double *Qprev, const double *qraw_prev, bool *valid) {
+  dsem_ctx *c = A.c;
+  const Group &g = *A.g;
+  const MList &ml = *A.ml;
+  if constexpr (G > 7) {
+    (void)Qn; (void)Qprev; (void)qraw_prev; (void)valid; (void)g; (void)ml;
+    return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
+  } else {
+    constexpr int G2 = G * G, NG = G * G * G;
+    bool ok = true;
+    if (Qprev) {
+      if (qraw_prev) {
+        const unsigned nbm = (unsigned)(((long long)ml.n * G2 + 127) / 128);
+        k_face_avg<G><<<nbm, 128, 0, c->st>>>(ml.mc, ml.n, qraw_prev, c->QF);
+        CKA(cudaGetLastError());
+      } else {
+        TraceArgs ta{};
+        ta.JQ = Qprev;
+        ta.sq = 5LL * NG;
+        ta.jac = g.jac;
+        ta.QF = c->QF;
+        CKA(Launch<G>::trace(ta, g.nel, c->st));
+        CKA(Launch<G>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st));
+      }
+      VolArgs a{};  // the volume kernel with saved gradients: EVB (its fluxes are not used)
+      a.JQ = Qprev;
+      a.sq = 5LL * NG;
+      a.jac = g.jac;
+      a.gg = g.gg;
+      a.gm = g.gm;
+      a.muhg = g.muhg;
+      a.QF = c->QF;
+      a.VF = c->VF;
+      a.QTI = c->QTI;
+      a.EVB = g.EVB;
+      a.P = c->P;
+      a.ecase = g.ecase;
+      a.rec = c->d_rec;
+      CKA(Launch<G>::vol(a, g.nel, true, VOL_EV_SAVE, c->st));
+    } else if (A.ev_valid0) {
+      CKA(cudaMemcpyAsync(g.EVB, A.b.evb0, (size_t)g.nel * 15 * NG * sizeof(double), cudaMemcpyDeviceToDevice,
+                          c->st));
+    } else {
+      ok = false;
+    }
+    EvArgs e{};
+    e.JQ = Qn;
+    e.sq = 5LL * NG;
+    e.jac = g.jac;
+    e.hd = g.hd;
+    e.EVB = g.EVB;
+    e.muhg = g.muhg;
+    e.valid = ok ? 1 : 0;
+    e.P = c->P;
+    e.ecase = g.ecase;
+    e.rec = c->d_rec;
+    CKA(Launch<G>::ev(e, g.nel, c->st));
+    CKA(cudaMemsetAsync(A.b.lmuhg, 0, (size_t)g.nel * NG * sizeof(double), c->st));
+    A.launches += 3;
+    *valid = ok;
+    return DSEM_OK;
+  }
+}
+
+// dJ/dmu of the reversed step into dJ/dQn (b.lq) and the previous step's saved gradients (b.levb)
+template <int G> int ev_adjoint_G(Adj &A, const double *Qn) {
+  dsem_ctx *c = A.c;
+  const Group &g = *A.g;
+  if constexpr (G > 7) {
+    (void)Qn; (void)g;
+    return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
+  } else {
+    EvAdjArgs e{};
+    e.JQ = Qn;
+    e.jac = g.jac;
+    e.hd = g.hd;
+    e.EVB = g.EVB;
+    e.LMU = A.b.lmuhg;
+    e.LQ = A.b.lq;
+    e.LEVB = A.b.levb;
+    e.P = c->P;
+    k_ev_adj<G><<<g.nel, 128, 0, c->st>>>(e);
+    CKA(cudaGetLastError());
+    ++A.launches;
+    return DSEM_OK;
+  }
+}
+
+int ev_forward(Adj &A, const double *Qn, const double *Qprev, const double *qraw_prev, bool *valid) {
+  int r = DSEM_OK;
+  with_G(A.g->G, [&](auto gc) -> cudaError_t {
+    r = ev_forward_G<decltype(gc)::value>(A, Qn, Qprev, qraw_prev, valid);
+    return cudaSuccess;
+  });
+  return r;
+}
+
+int ev_adjoint(Adj &A, const double *Qn) {
+  int r = DSEM_OK;
+  with_G(A.g->G, [&](auto gc) -> cudaError_t {
+    r = ev_adjoint_G<decltype(gc)::value>(A, Qn);
+    return cudaSuccess;
+  });
+  return r;
+}
+
 unsigned ew_blocks(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16); }
 
 // Reverse of step n, its stage input states at st[0..kord) and its end state at
-// qend; qf[0..kord): their raw face traces, or null.
-int reverse_step(Adj &A, int n, double *const *st, const double *qend, double *const *qf = nullptr) {
+// qend; qf[0..kord): their raw face traces, or null.  With entropy viscosity,
+// qprev / qfprev: the previous step's last stage input state and its raw traces
+// (null for the first step).
+int reverse_step(Adj &A, int n, double *const *st, const double *qend, double *const *qf = nullptr,
+                 const double *qprev = nullptr, const double *qfprev = nullptr) {
   dsem_ctx *c = A.c;
   const long long nq = (long long)c->nq;
   const bool win = A.in_window(n);
+  bool ev_valid = false;
+  if (A.ev) {
+    const int r = ev_forward(A, st[0], qprev, qfprev, &ev_valid);
+    if (r) return r;
+  }
   if (win) {  // d eps_n / d JQ_n through the JQ values of the enstrophy sum
     int r = stage_adjoint(A, st[c->kord - 1], qend, A.eps_w(), true, 0.0, 1.0, qf ? qf[c->kord - 1] : nullptr);
     if (r) return r;
@@ -171,9 +307,17 @@ int reverse_step(Adj &A, int n, double *const *st, const double *qend, double *c
   }
   for (int kk = c->kord; kk >= 1; --kk) {
     const bool eps_here = win && kk == c->kord;
+    const double *levb = (A.ev && kk == c->kord && A.levb_pending) ? A.b.levb : nullptr;
     int r = stage_adjoint(A, st[kk - 1], qend, eps_here ? A.eps_w() : 0.0, false, c->crk[kk - 1] * A.dt,
-                          c->ark[kk - 1], qf ? qf[kk - 1] : nullptr);
+                          c->ark[kk - 1], qf ? qf[kk - 1] : nullptr, levb);
     if (r) return r;
+  }
+  if (A.ev) {  // the step's viscosity, from its start state and the previous step's gradients
+    if (ev_valid) {
+      const int r = ev_adjoint(A, st[0]);
+      if (r) return r;
+    }
+    A.levb_pending = ev_valid && qprev != nullptr;
   }
   return DSEM_OK;
 }
@@ -187,10 +331,15 @@ int forward_step(Adj &A, int n, double *const *st, std::vector<double> *s_win, d
   for (int kk = 1; kk <= c->kord; ++kk) {
     if (st) CKA(cudaMemcpyAsync(st[kk - 1], c->JQ, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
     if (qf) CKA(cudaMemcpyAsync(qf[kk - 1], c->QF, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-    int r = dsem_int::stage(c, kk, win && kk == c->kord);
+    if (A.ev && kk == 1) {  // the step's entropy viscosity (tstep.f90:36-38)
+      const int r = dsem_int::ev(c);
+      if (r) return r;
+    }
+    int r = dsem_int::stage(c, kk, (win || A.ev) && kk == c->kord);
     if (r) return r;
     A.launches += 2 * (long long)c->groups.size() + 2 * (long long)c->mlists.size();
   }
+  if (A.ev) c->ev_grad_valid = true;  // the last stage saved the gradients of the next viscosity
   if (win && s_win) {
     double s = 0.0, s2 = 0.0;
     int r = dsem_int::eps_sums(c, &s, &s2);
@@ -302,11 +451,14 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   if (!c) return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "null context");
   if (nsteps < 1 || window < 0 || window > nsteps || snapshots < 0 || !(dt > 0.0))
     return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "adjoint: need nsteps >= 1, 0 <= window <= nsteps, snapshots >= 0, dt > 0");
-  if (c->ncase != 1 || c->groups.size() != 1 || c->mlists.size() != 1 || c->nnc > 0 || !c->groups[0].diag || c->shock ||
-      c->les || c->ncut > 0 || c->nbnd > 0)
+  if (c->ncase != 1 || c->groups.size() != 1 || c->mlists.size() != 1 || c->nnc > 0 || !c->groups[0].diag ||
+      c->P.ducros || c->les || c->ncut > 0 || c->nbnd > 0)
     return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED,
                           "adjoint: one case, one element order, conforming periodic mortars, axis-aligned elements, no "
-                          "entropy viscosity, LES, boundary faces or sharding");
+                          "Ducros sensor, LES, boundary faces or sharding");
+  if (c->shock && snapshots > 0)
+    return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED,
+                          "adjoint: with entropy viscosity every stage state is kept (snapshots = 0)");
   if (c->groups[0].G > 7) return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
   if (dJdQ0 && ldx < c->groups[0].G) return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "ldx smaller than the number of Gauss points");
   int r = upload_ops_here(c);
@@ -323,6 +475,17 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   for (double **p : {&A.b.lq, &A.b.lg, &A.b.ljq, &A.b.ldir, &A.b.q0}) CKA(cudaMalloc(p, bq));
   for (double **p : {&A.b.qfr, &A.b.lff, &A.b.lvf, &A.b.lqf, &A.b.lqr}) CKA(cudaMalloc(p, bf));
   CKA(cudaMalloc(&A.b.lrp, (size_t)A.g->nel * sizeof(double)));
+  A.ev = c->shock != 0;
+  if (A.ev) {
+    const size_t ng = (size_t)A.g->nel * A.g->G * A.g->G * A.g->G;
+    CKA(cudaMalloc(&A.b.lmuhg, ng * sizeof(double)));
+    CKA(cudaMalloc(&A.b.levb, 15 * ng * sizeof(double)));
+    A.ev_valid0 = c->ev_grad_valid;
+    if (A.ev_valid0) {  // the gradients behind the first step's viscosity
+      CKA(cudaMalloc(&A.b.evb0, 15 * ng * sizeof(double)));
+      CKA(cudaMemcpyAsync(A.b.evb0, A.g->EVB, 15 * ng * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    }
+  }
   CKA(cudaMalloc(&A.b.lr, sizeof(double)));
   const size_t nstage = snapshots == 0 ? (size_t)nsteps * kord : (size_t)kord;
   if (cudaMalloc(&A.b.stages, nstage * bq) != cudaSuccess) {
@@ -416,11 +579,15 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
         }
         double *const *qfp = qf.empty() ? nullptr : qf.data();
         const double *qend = n + 1 < nsteps ? A.b.stages + ((size_t)(n + 1) * kord) * nq : c->JQ;
-        if (n == nsteps - 1) {
-          if ((r = reverse_step(A, n, st.data(), qend, qfp))) return drop(), r;
+        // the previous step's last stage (entropy viscosity)
+        const double *qprev = n > 0 ? A.b.stages + ((size_t)(n - 1) * kord + kord - 1) * nq : nullptr;
+        const double *qfprev = (n > 0 && A.b.traces) ? A.b.traces + ((size_t)(n - 1) * kord + kord - 1) * nf : nullptr;
+        if (n == nsteps - 1 || (A.ev && n == 0)) {  // launch sequences of their own: eager
+          if ((r = reverse_step(A, n, st.data(), qend, qfp, qprev, qfprev))) return drop(), r;
           continue;
         }
-        r = replay(c, &gx[A.in_window(n) ? 1 : 0], [&] { return reverse_step(A, n, st.data(), qend, qfp); });
+        r = replay(c, &gx[A.in_window(n) ? 1 : 0],
+                   [&] { return reverse_step(A, n, st.data(), qend, qfp, qprev, qfprev); });
         if (r) return drop(), r;
       }
       drop();

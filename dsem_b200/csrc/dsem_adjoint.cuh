@@ -350,10 +350,12 @@ template <int D> __device__ __forceinline__ void euler_vjp(const double *Q, doub
 }
 
 // Viscous flux along D (PhysLib.f90:419-583) with Gr[j][f] = d Q_f / d x_j:
-// fv = the flux, lQ += (dF/dQ)^T lf, lG += (dF/dGr)^T lf (amu held fixed).
+// fv = the flux, lQ += (dF/dQ)^T lf, lG += (dF/dGr)^T lf; with lamu non-null,
+// *lamu = (dF/d amu)^T lf (the entropy viscosity enters through amu = 1 + mu).
 template <int D>
 __device__ __forceinline__ void vis_vjp(const double *Q, const double (&Gr)[3][NV], double amu, const Phys &P,
-                                        const double *lf, double *fv, double *lQ, double (&lG)[3][NV]) {
+                                        const double *lf, double *fv, double *lQ, double (&lG)[3][NV],
+                                        double *lamu = nullptr) {
   const double g = P.gamma, rho = Q[0], ri = 1.0 / rho;
   const double vel[3] = {Q[1] * ri, Q[2] * ri, Q[3] * ri};
   const double S = vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2];
@@ -387,6 +389,13 @@ __device__ __forceinline__ void vis_vjp(const double *Q, const double (&Gr)[3][N
     ltau[i] = lf[1 + i] + vel[i] * l4;
   }
   const double ltD = kap * rden * l4;
+  if (lamu) {  // tau_i = amu T_i; kap = 1 + (amu - 1) 0.2 / (gamma - 1)
+    double la = l4 * 0.2 * P.r_gm1 * tD * rden;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      la += ltau[i] * (Gv[i][D] + Gv[D][i] - (i == D ? 2.0 / 3.0 * div : 0.0));
+    *lamu = la;
+  }
   double lGv[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
@@ -637,6 +646,117 @@ __global__ void __launch_bounds__(256) k_trace_adj(const double *__restrict__ LQ
   }
 }
 
+// Entropy viscosity at a step's start (k_ev: RHS_ent_trans and Entropy_Viscosity,
+// RHS.f90:207-278, EViscosity_GL.f90:19-101), transposed:
+// mu = min(max(cmu Re rho h^2 |D|, 0), mumax) with D the entropy residual of
+// ev_residual (without the Ducros sensor).  From dJ/dmu (LMU) it adds
+// dJ/dJQ of the step's start state into LQ and writes dJ/dEVB, the demand on
+// the gradients saved by the previous step's last stage, into LEVB.
+struct EvAdjArgs {
+  const double *JQ, *jac, *hd, *EVB, *LMU;
+  double *LQ, *LEVB;
+  Phys P;
+};
+
+template <int G> __global__ void __launch_bounds__(128) k_ev_adj(EvAdjArgs A) {
+  constexpr int NG = G * G * G;
+  const int k = blockIdx.x;
+  const double *JQ = A.JQ + (long long)k * 5 * NG;
+  const double *jac = A.jac + (long long)k * NG;
+  const double *hd = A.hd + (long long)k * NG;
+  const double *E = A.EVB + (long long)k * 15 * NG;
+  const Phys &P = A.P;
+  const double g = P.gamma, g1 = P.gamma - 1.0;
+  for (int p = threadIdx.x; p < NG; p += blockDim.x) {
+    double Q[NV], Gq[3][4], T1[3];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Q[v] = JQ[v * NG + p] * jac[p];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) Gq[d][v] = E[(v * 3 + d) * NG + p];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) T1[d] = E[(12 + d) * NG + p];
+    // forward (as ev_residual)
+    const double rho = Q[0], ri = 1.0 / rho;
+    const double vel[3] = {Q[1] * ri, Q[2] * ri, Q[3] * ri};
+    const double S = vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2];
+    const double pr = g1 * (Q[4] - 0.5 * rho * S);
+    const double Tt = pr * g * ri;
+    double Gv[3][3];  // d u_i / d x_j
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) Gv[i][j] = (Gq[j][1 + i] - vel[i] * Gq[j][0]) * ri;
+    const double div = Gv[0][0] + Gv[1][1] + Gv[2][2];
+    const double s01 = Gv[1][0] + Gv[0][1], s02 = Gv[0][2] + Gv[2][0], s12 = Gv[1][2] + Gv[2][1];
+    const double phi = 2.0 * (Gv[0][0] * Gv[0][0] + Gv[1][1] * Gv[1][1] + Gv[2][2] * Gv[2][2]) +
+                       (s01 * s01 + s02 * s02 + s12 * s12) - 2.0 * div * div / 3.0;
+    const double t2 = T1[0] * T1[0] + T1[1] * T1[1] + T1[2] * T1[2];
+    const double den = Tt * g1 * P.pr;
+    const double gam = t2 / den;
+    const double biS = ((phi + gam) / Tt) / P.re;
+    const double h2 = hd[p] * hd[p];
+    const double mur = P.cmu * P.re * rho * h2 * fabs(biS);
+    const bool active = isfinite(mur) && mur > 0.0 && mur < P.mumax;
+    double lQ[NV] = {0.0, 0.0, 0.0, 0.0, 0.0}, lGq[3][4] = {}, lT1[3] = {0.0, 0.0, 0.0};
+    if (active) {
+      const double lmur = A.LMU[(long long)k * NG + p];
+      double lrho = lmur * P.cmu * P.re * h2 * fabs(biS);
+      const double lbiS = lmur * P.cmu * P.re * rho * h2 * (biS < 0.0 ? -1.0 : 1.0);
+      const double lpg = lbiS / (Tt * P.re);  // d/d(phi + gam)
+      double lTt = -lbiS * (phi + gam) / (Tt * Tt * P.re);
+      // gam = t2 / (Tt (g - 1) Pr)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) lT1[d] = lpg * 2.0 * T1[d] / den;
+      lTt += -lpg * gam / Tt;
+      // phi
+      double lGv[3][3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) lGv[i][i] = lpg * (4.0 * Gv[i][i] - 4.0 * div / 3.0);
+      lGv[1][0] = lGv[0][1] = lpg * 2.0 * s01;
+      lGv[0][2] = lGv[2][0] = lpg * 2.0 * s02;
+      lGv[1][2] = lGv[2][1] = lpg * 2.0 * s12;
+      double lvel[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const double l = lGv[i][j];
+          lGq[j][1 + i] += l * ri;
+          lGq[j][0] += -vel[i] * ri * l;
+          lvel[i] += -Gq[j][0] * ri * l;
+          lrho += -Gv[i][j] * ri * l;
+        }
+      // Tt = p g / rho
+      const double lp = lTt * g * ri;
+      lrho += -lTt * Tt * ri;
+      // p = (g - 1)(rho E - rho S / 2)
+      lQ[4] += g1 * lp;
+      lrho += -g1 * 0.5 * S * lp;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) lvel[i] += -g1 * rho * vel[i] * lp;
+      // vel_i = m_i / rho
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        lQ[1 + i] += lvel[i] * ri;
+        lrho += -vel[i] * ri * lvel[i];
+      }
+      lQ[0] += lrho;
+    }
+    double *LQ = A.LQ + (long long)k * 5 * NG;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) LQ[v * NG + p] += jac[p] * lQ[v];
+    double *LE = A.LEVB + (long long)k * 15 * NG;
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) LE[(v * 3 + d) * NG + p] = lGq[d][v];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) LE[(12 + d) * NG + p] = lT1[d];
+  }
+}
+
 struct VolAdjArgs {
   const double *JQ;
   const double *jac, *gg, *gm;  // diagonal metric layout
@@ -650,6 +770,9 @@ struct VolAdjArgs {
   const double *JQe;            // state whose JQ values the enstrophy sum uses (end of the step)
   int direct_only;              // 1: only dJ/dJQe of the enstrophy sum, into LJQ
   int pf;                       // L2 prefetch distance in elements (the blocks resident at once), 0: none
+  const double *muhg;           // entropy viscosity at the Gauss points (null: none)
+  double *lmuhg;                // in/out with muhg: dJ/dmu at the Gauss points, accumulated over stages
+  const double *levb;           // dJ/d(gradients this stage saved for the next step's viscosity), or null
   Phys P;
 };
 
@@ -659,13 +782,14 @@ template <int G> struct VolAdjCfg {
   // one element per SM (shared memory); at least one thread per Lobatto point of a grid
   static constexpr int NT = NL <= 256 ? 256 : ((NL + 31) / 32) * 32;
   static constexpr size_t NDBL = 5 * NG + 15 * NG + 15 * NG + 5 * NL + 5 * NL + 11 * NL + 5 * NG + 5 * NG + 30 * G2 +
-                                 NT + 3 * NG + 30 * G2;
+                                 NT + 3 * NG + 30 * G2 + 2 * NG;
   static constexpr size_t SMEM = sizeof(double) * NDBL;
 };
 
 // Volume adjoint of one element (diagonal metrics): recomputes the Lobatto
 // arrays and Gauss gradients, then runs the volume operations in reverse.
-template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_adj(VolAdjArgs A) {
+// EVK: the entropy-viscosity variant (muhg, lmuhg and levb used; otherwise ignored)
+template <int G, bool EVK> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_adj(VolAdjArgs A) {
   using C = VolAdjCfg<G>;
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G, NT = C::NT;
   extern __shared__ double sm[];
@@ -681,6 +805,8 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
   double *red = LQFs + 30 * G2;  // [NT]
   double *gg = red + NT;         // [3][NG] metric diagonal at the Gauss points
   double *QF = gg + 3 * NG;      // [30][G2] averaged face states
+  double *MU = QF + 30 * G2;     // [NG] entropy viscosity (EV runs)
+  double *LMU = MU + NG;         // [NG] its adjoint
   const int k = blockIdx.x, tid = threadIdx.x;
   const double *JQ = A.JQ + (long long)k * 5 * NG;
   const double *jac = A.jac + (long long)k * NG;
@@ -743,7 +869,17 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
     for (int j = 0; j < NF; ++j)
       if (tid + j * NT < 30 * G2) QF[tid + j * NT] = fv[j];
   }
-  for (int i = tid; i < 15 * NG; i += NT) LGR[i] = 0.0;
+  // LGR starts from the next step's demand on the gradients this stage saves
+  // (fields 0..3: EVB has the same layout as GR); the energy gradients start at 0
+  if constexpr (EVK) {
+    for (int i = tid; i < 15 * NG; i += NT) LGR[i] = (A.levb && i < 12 * NG) ? A.levb[(long long)k * 15 * NG + i] : 0.0;
+    for (int i = tid; i < NG; i += NT) {
+      MU[i] = A.muhg[(long long)k * NG + i];
+      LMU[i] = 0.0;
+    }
+  } else {
+    for (int i = tid; i < 15 * NG; i += NT) LGR[i] = 0.0;
+  }
   for (int i = tid; i < 30 * G2; i += NT) LQFs[i] = 0.0;
   __syncthreads();
   PHASE_MARK(21);
@@ -895,6 +1031,17 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
         Gr[fi % 3][fi / 3] = LG[jf * NL + qs];
       }
       const double gd = gm[D * NL + qi];
+      // entropy viscosity at this Lobatto point (EV_Prolong, as k_vol_diag): amu = 1 + mu
+      constexpr bool ev = EVK;
+      double amu = 1.0, lam = 0.0;
+      if constexpr (ev) {
+        const int g0 = gbase<G>(D, a, b);
+        double acc = Op<G>::B(s, 0) * MU[g0];
+#pragma unroll
+        for (int kk = 1; kk < G; ++kk) acc = __fma_rn(Op<G>::B(s, kk), MU[g0 + kk * xs], acc);
+        amu = 1.0 + acc;
+      }
+      double *lamp = ev ? &lam : nullptr;
       if (s == 0 || s == L - 1) {  // face point: VF = gd * fv
         const int fc = s == 0 ? face_lo(D) : face_hi(D);
         double lvf[NV];
@@ -903,9 +1050,9 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
           lvf[v] = LVF[(fc - 1) * 5 * G2 + v * G2 + a + G * b];
           lfv[v] = gd * lvf[v];
         }
-        if (D == 0) vis_vjp<0>(Q, Gr, 1.0, P, lfv, fv, lQ, lG);
-        else if (D == 1) vis_vjp<1>(Q, Gr, 1.0, P, lfv, fv, lQ, lG);
-        else vis_vjp<2>(Q, Gr, 1.0, P, lfv, fv, lQ, lG);
+        if (D == 0) vis_vjp<0>(Q, Gr, amu, P, lfv, fv, lQ, lG, lamp);
+        else if (D == 1) vis_vjp<1>(Q, Gr, amu, P, lfv, fv, lQ, lG, lamp);
+        else vis_vjp<2>(Q, Gr, amu, P, lfv, fv, lQ, lG, lamp);
 #pragma unroll
         for (int v = 0; v < NV; ++v) lr += P.re * lvf[v] * (gd * fv[v]);
       } else {  // interior: F = gd fe - gd fv / Re, QTI += Dm F, Qt = -(QTI + ...)
@@ -919,13 +1066,13 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
 #pragma unroll
         for (int v = 0; v < NV; ++v) lfe[v] = gd * lF[v];
         if (D == 0) {
-          vis_vjp<0>(Q, Gr, 1.0, P, lfv, fv, lQ, lG);
+          vis_vjp<0>(Q, Gr, amu, P, lfv, fv, lQ, lG, lamp);
           euler_vjp<0>(Q, gamma, lfe, lQ);
         } else if (D == 1) {
-          vis_vjp<1>(Q, Gr, 1.0, P, lfv, fv, lQ, lG);
+          vis_vjp<1>(Q, Gr, amu, P, lfv, fv, lQ, lG, lamp);
           euler_vjp<1>(Q, gamma, lfe, lQ);
         } else {
-          vis_vjp<2>(Q, Gr, 1.0, P, lfv, fv, lQ, lG);
+          vis_vjp<2>(Q, Gr, amu, P, lfv, fv, lQ, lG, lamp);
           euler_vjp<2>(Q, gamma, lfe, lQ);
         }
 #pragma unroll
@@ -938,11 +1085,14 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
         const int fi = diag_field(D, jf);
         LG[jf * NL + qs] = lG[fi % 3][fi / 3];
       }
+      if constexpr (ev) LB[qs] = lam;  // dJ/d amu, in this point's (read) slot of field 0
     }
     __syncthreads();
     PHASE_MARK(27);
-    // transposed interpolations along the lines of D
-    for (int t = tid; t < 16 * G2; t += NT) {
+    // transposed interpolations along the lines of D (and, with EV, of dJ/d amu
+    // back to the Gauss-point viscosity)
+    constexpr int ntr = EVK ? 17 * G2 : 16 * G2;
+    for (int t = tid; t < ntr; t += NT) {
       const int j = t / G2, ln = t - j * G2, a = ln % G, b = ln / G;
       const int p0 = gbase<G>(D, a, b), l0 = lbase<G>(D, a, b);
       if (j < 11) {  // gradient field j of grid D -> its Gauss line
@@ -956,6 +1106,17 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
 #pragma unroll
           for (int s = 0; s < L; ++s) acc += Op<G>::B(s, kk) * y[s];
           LGR[fi * NG + p0 + kk * xs] += acc;
+        }
+      } else if (j == 16) {  // EV_Prolong transposed
+        double y[L];
+#pragma unroll
+        for (int s = 0; s < L; ++s) y[s] = LB[sw(l0 + s * xs)];
+#pragma unroll
+        for (int kk = 0; kk < G; ++kk) {
+          double acc = 0.0;
+#pragma unroll
+          for (int s = 0; s < L; ++s) acc += Op<G>::B(s, kk) * y[s];
+          LMU[p0 + kk * xs] += acc;
         }
       } else {  // state field v: interior Lobatto points -> q, end points -> QF
         const int v = j - 11;
@@ -1015,9 +1176,82 @@ template <int G> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1) k_vol_ad
   lob_dir(std::integral_constant<int, 2>{});
   PHASE_MARK(25);
 
+  // ---- reverse of the temperature gradients this stage saved for the next
+  // step's entropy viscosity (vol_diag_tgrad): T1_D = gmetg(D,D) D T(Lobatto
+  // line of the state along D), T = gamma p / rho (RHS.f90:66-83)
+  if (EVK && A.levb) {
+    const double *lt1 = A.levb + (long long)k * 15 * NG + 12 * NG;
+    auto tgrad_dir = [&](auto Dc) {
+      constexpr int D = decltype(Dc)::value;
+      constexpr int xs = D == 0 ? 1 : (D == 1 ? G : G2);
+      for (int ln = tid; ln < G2; ln += NT) {
+        const int a = ln % G, b = ln / G;
+        const int p0 = gbase<G>(D, a, b);
+        double y[NV][L];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          double x[G];
+#pragma unroll
+          for (int kk = 0; kk < G; ++kk) x[kk] = q[v * NG + p0 + kk * xs];
+          y[v][0] = QF[(face_lo(D) - 1) * 5 * G2 + v * G2 + ln];
+          y[v][L - 1] = QF[(face_hi(D) - 1) * 5 * G2 + v * G2 + ln];
+#pragma unroll
+          for (int s = 1; s < L - 1; ++s) {
+            double acc = Op<G>::B(s, 0) * x[0];
+#pragma unroll
+            for (int kk = 1; kk < G; ++kk) acc = __fma_rn(Op<G>::B(s, kk), x[kk], acc);
+            y[v][s] = acc;
+          }
+        }
+        double ltd[G];
+#pragma unroll
+        for (int kk = 0; kk < G; ++kk) ltd[kk] = gg[D * NG + p0 + kk * xs] * lt1[D * NG + p0 + kk * xs];
+        const double g = P.gamma, g1 = P.gamma - 1.0;
+        const int l0 = lbase<G>(D, a, b);
+#pragma unroll
+        for (int s = 0; s < L; ++s) {  // dJ/d(Lobatto state) of T at each point, into LB
+          double lT = 0.0;
+#pragma unroll
+          for (int kk = 0; kk < G; ++kk) lT += Op<G>::D(kk, s) * ltd[kk];
+          const double rho = y[0][s], ri = 1.0 / rho;
+          const double m2 = y[1][s] * y[1][s] + y[2][s] * y[2][s] + y[3][s] * y[3][s];
+          const double p = g1 * (y[4][s] - 0.5 * m2 * ri);
+          // T = g p / rho, p = (g - 1) (rho E - |m|^2 / (2 rho))
+          LB[0 * NL + l0 + s * xs] = (g * g1 * 0.5 * m2 * ri * ri * ri - g * p * ri * ri) * lT;
+#pragma unroll
+          for (int i = 1; i <= 3; ++i) LB[i * NL + l0 + s * xs] = -g * g1 * y[i][s] * ri * ri * lT;
+          LB[4 * NL + l0 + s * xs] = g * g1 * ri * lT;
+        }
+      }
+      __syncthreads();
+      for (int t = tid; t < 5 * G2; t += NT) {  // transposed interpolation: interior -> q, ends -> QF
+        const int v = t / G2, ln = t - v * G2, a = ln % G, b = ln / G;
+        const int p0 = gbase<G>(D, a, b), l0 = lbase<G>(D, a, b);
+        double y[L];
+#pragma unroll
+        for (int s = 0; s < L; ++s) y[s] = LB[v * NL + l0 + s * xs];
+#pragma unroll
+        for (int kk = 0; kk < G; ++kk) {
+          double acc = 0.0;
+#pragma unroll
+          for (int s = 1; s < L - 1; ++s) acc += Op<G>::B(s, kk) * y[s];
+          LQ[v * NG + p0 + kk * xs] += acc;
+        }
+        LQFs[(face_lo(D) - 1) * 5 * G2 + v * G2 + ln] += y[0];
+        LQFs[(face_hi(D) - 1) * 5 * G2 + v * G2 + ln] += y[L - 1];
+      }
+      __syncthreads();
+    };
+    tgrad_dir(std::integral_constant<int, 0>{});
+    tgrad_dir(std::integral_constant<int, 1>{});
+    tgrad_dir(std::integral_constant<int, 2>{});
+  }
+
   // ---- outputs
   for (int i = tid; i < 5 * NG; i += NT) LJQ[i] = jac[i % NG] * LQ[i];
   for (int i = tid; i < 30 * G2; i += NT) A.LQF[(long long)k * 30 * G2 + i] = LQFs[i];
+  if constexpr (EVK)
+    for (int i = tid; i < NG; i += NT) A.lmuhg[(long long)k * NG + i] += LMU[i];
   red[tid] = lr;
   __syncthreads();
   for (int n = NT; n > 1;) {  // pairwise halving, any NT

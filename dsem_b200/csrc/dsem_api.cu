@@ -1781,6 +1781,10 @@ int traces(dsem_ctx *c) {
   long long l = 0;
   return enqueue_traces(c, &l);
 }
+int ev(dsem_ctx *c) {
+  long long l = 0;
+  return enqueue_ev(c, &l);
+}
 int set_dt(dsem_ctx *c, const double *dt) { return ::set_dt(c, dt); }
 int unpack_state(dsem_ctx *c, const double *dev, double *host, int ldx) {
   return unpack_to_host(c, dev, host, ldx, 5, state_offs(c));

@@ -128,6 +128,7 @@ namespace dsem_int {
 int fail(dsem_ctx *c, int code, const std::string &msg);
 int stage(dsem_ctx *c, int kk, bool save);  // one RK stage on c->JQ (eager launches)
 int traces(dsem_ctx *c);                    // face traces of c->JQ
+int ev(dsem_ctx *c);                        // entropy viscosity of c->JQ (valid: c->ev_grad_valid)
 int set_dt(dsem_ctx *c, const double *dt);
 int unpack_state(dsem_ctx *c, const double *dev, double *host, int ldx);
 int check_flag(dsem_ctx *c);

@@ -120,3 +120,63 @@ def test_adjoint_rejects_unsupported_cases():
         s.adjoint(1e-3, 2, 1)
     assert e.value.code == -5
     s.close()
+
+
+EV = dict(cmu=4.0, mumax=2.0, shock=1)
+
+
+@pytest.mark.parametrize("n,p,nsteps,window,prestep", [(2, 3, 4, 2, 0), (2, 4, 3, 3, 2)])
+def test_adjoint_with_entropy_viscosity(oracle_mod, n, p, nsteps, window, prestep):
+    """Entropy viscosity (tstep.f90:36-38): each step's viscosity comes from its
+    start state and the gradients saved by the previous step's last stage; the
+    adjoint carries both dependencies.  With prestep > 0 the run starts after
+    some steps, so the first step's viscosity uses gradients from before the
+    run (held fixed, as the complex step holds them)."""
+    from dsem_b200.solver import Solver
+    re = 400.0
+    box, q, dt = _case(n, p, re, seed=11)
+    s = Solver(box.desc(), re=re, **EV)
+    s.upload(q)
+    c = oracle_mod.Case.from_desc(box.desc())
+    c.set_phys(re=re, **EV)
+    c.set_q(q)
+    if prestep:
+        s.step(dt, prestep)
+        c.step(0.0, dt, prestep)
+        assert np.array_equal(s.download(), c.get_q())
+    q0 = s.download()
+    J, g, lr, _ = s.adjoint(dt, nsteps, window, snapshots=0)
+    for d in _directions(q, p + 1, 4, seed=p + 20):
+        Jc, dJ = c.objective_cs(dt, nsteps, window, d, 1e-30)
+        assert abs(J - Jc) <= 1e-12 * abs(Jc)
+        ga = float(np.sum(g * d))
+        assert abs(ga - dJ) <= TOL * abs(dJ), (ga, dJ)
+    if not prestep:  # d/d(1/Re): central differences of the oracle's J
+        r = 1.0 / re
+        h = 1e-5 * r
+        vals = []
+        for rr in (r + h, r - h):
+            cc = oracle_mod.Case.from_desc(box.desc())
+            cc.set_phys(re=1.0 / rr, **EV)
+            cc.set_q(q0)
+            vals.append(cc.objective_cs(dt, nsteps, window, None, 0.0)[0])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(lr - fd) <= TOL * abs(fd), (lr, fd)
+    s.close()
+
+
+def test_entropy_viscosity_adjoint_limits():
+    from dsem_b200.solver import DsemError, Solver
+    box, q, dt = _case(2, 3, 400.0)
+    s = Solver(box.desc(), re=400.0, **EV)
+    s.upload(q)
+    with pytest.raises(DsemError) as e:  # binomial checkpointing keeps too little for the viscosity
+        s.adjoint(dt, 4, 2, snapshots=2)
+    assert e.value.code == -5
+    s.close()
+    s = Solver(box.desc(), re=400.0, cmu=0.5, mumax=2.0, shock=3)  # with the Ducros sensor
+    s.upload(q)
+    with pytest.raises(DsemError) as e:
+        s.adjoint(dt, 2, 1)
+    assert e.value.code == -5
+    s.close()
