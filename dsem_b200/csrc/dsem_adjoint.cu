@@ -73,15 +73,19 @@ struct Adj {
 // Adjoint of one stage.  Unless direct_only, the RK steps around it are fused in:
 // dJ/dQt += cdt dJ/dQ before, dJ/dQ += R'^T dJ/dQt and dJ/dQt *= ark after.
 // qraw: the raw face traces of Qs kept by the forward sweep, or null to recompute them.
+// The first part (dJ/dQt += cdt dJ/dQ and the face terms) runs here only when
+// upd; otherwise the previous stage of the reverse sweep ran it.  With next,
+// this stage's last kernel also runs that first part of the stage reversed
+// next, with its coefficient cdt_next.
 template <int G>
 int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, bool direct_only, double cdt,
-                    double ark, const double *qraw, const double *levb) {
+                    double ark, const double *qraw, const double *levb, bool upd, bool next, double cdt_next) {
   dsem_ctx *c = A.c;
   const Group &g = *A.g;
   const MList &ml = *A.ml;
   if constexpr (G > 7) {
     (void)Qs; (void)JQe; (void)eps_w; (void)direct_only; (void)g; (void)ml; (void)cdt; (void)ark; (void)qraw;
-    (void)levb;
+    (void)levb; (void)upd; (void)next; (void)cdt_next;
     return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
   } else {
     constexpr int G2 = G * G;
@@ -141,9 +145,13 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
       return DSEM_OK;
     }
     const unsigned nb = (unsigned)(((long long)ml.n * G2 + 127) / 128);
-    k_upd_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lg, A.b.lq, cdt, c->P.re, A.b.lff, A.b.lvf);
-    CKA(cudaGetLastError());
-    k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lvf, ml.nrm, avg_in_vis ? qraw : nullptr, c->QF);
+    if (upd) {
+      k_upd_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lg, A.b.lq, cdt, A.b.lff);
+      CKA(cudaGetLastError());
+      ++A.launches;
+    }
+    k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lff, c->P.re, A.b.lvf, ml.nrm,
+                                             avg_in_vis ? qraw : nullptr, c->QF);
     CKA(cudaGetLastError());
     if (A.ev)
       k_vol_adj<G, true><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
@@ -153,18 +161,23 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
     k_face_inv_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, qfr, A.b.lff, A.b.lqf, A.b.lqr, ml.nh, ml.nrm,
                                              c->P.gamma);
     CKA(cudaGetLastError());
-    k_trace_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq, A.b.lq, A.b.lg, ark);
+    if (next)
+      k_trace_adj<G, true><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq, A.b.lq, A.b.lg, ark, cdt_next, A.b.lff);
+    else
+      k_trace_adj<G, false><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq, A.b.lq, A.b.lg, ark, 0.0, nullptr);
     CKA(cudaGetLastError());
-    A.launches += 5;
+    A.launches += 4;
     return DSEM_OK;
   }
 }
 
 int stage_adjoint(Adj &A, const double *Qs, const double *JQe, double eps_w, bool direct_only, double cdt = 0.0,
-                  double ark = 1.0, const double *qraw = nullptr, const double *levb = nullptr) {
+                  double ark = 1.0, const double *qraw = nullptr, const double *levb = nullptr, bool upd = true,
+                  bool next = false, double cdt_next = 0.0) {
   int r = DSEM_OK;
   cudaError_t e = with_G(A.g->G, [&](auto gc) -> cudaError_t {
-    r = stage_adjoint_G<decltype(gc)::value>(A, Qs, JQe, eps_w, direct_only, cdt, ark, qraw, levb);
+    r = stage_adjoint_G<decltype(gc)::value>(A, Qs, JQe, eps_w, direct_only, cdt, ark, qraw, levb, upd, next,
+                                             cdt_next);
     return cudaSuccess;
   });
   if (e != cudaSuccess) return dsem_int::fail(A.c, DSEM_ERR_UNSUPPORTED, "adjoint: element order not supported");
@@ -309,7 +322,8 @@ int reverse_step(Adj &A, int n, double *const *st, const double *qend, double *c
     const bool eps_here = win && kk == c->kord;
     const double *levb = (A.ev && kk == c->kord && A.levb_pending) ? A.b.levb : nullptr;
     int r = stage_adjoint(A, st[kk - 1], qend, eps_here ? A.eps_w() : 0.0, false, c->crk[kk - 1] * A.dt,
-                          c->ark[kk - 1], qf ? qf[kk - 1] : nullptr, levb);
+                          c->ark[kk - 1], qf ? qf[kk - 1] : nullptr, levb, kk == c->kord, kk > 1,
+                          kk > 1 ? c->crk[kk - 2] * A.dt : 0.0);
     if (r) return r;
   }
   if (A.ev) {  // the step's viscosity, from its start state and the previous step's gradients

@@ -5,11 +5,12 @@
 //   -> volume: Lobatto arrays, Gauss gradients, fluxes, interior divergence QTI,
 //      viscous face flux VF -> BR1 average of VF -> Qt = -(QTI + face terms(FF - VF/Re)).
 // Reverse, given lambda = dJ/dQt (LQT):
-//   k_upd_adj       face terms           -> dJ/dFF (LFF), dJ/dVF after averaging (LVF)
-//   k_face_vis_adj  BR1 average          -> dJ/dVF before averaging (LVF, in place)
+//   k_upd_adj       face terms           -> dJ/dFF (LFF); dJ/dVF after averaging is -LFF/Re
+//   k_face_vis_adj  BR1 average          -> dJ/dVF before averaging (LVF)
 //   k_vol_adj       volume (recomputed)  -> dJ/dJQ (LJQ), dJ/dQF averaged (LQF), dJ/d(1/Re)
 //   k_face_inv_adj  Roe flux + average   -> dJ/dQFR (LQR)
 //   k_trace_adj     face traces          -> LJQ += jacob * trace^T LQR
+//                   (fused with the k_upd_adj of the stage reversed next)
 // The volume adjoint can also add the derivative of the enstrophy-dissipation
 // sum (energydissipation.f90:19-78) evaluated on the same gradients.
 // Derivatives are exact up to rounding; every pointwise function is
@@ -474,22 +475,11 @@ __device__ __forceinline__ void vort_vjp(const double *Qj, double jc, const doub
 
 // ---------------------------------------------------------------- kernels
 // Face terms of the divergence and the RK residual sign (k_update):
-// Qt = -(QTI + sum_faces D_edge FB), FB = FF - VF/Re.  First the RK step of
-// the reverse sweep for this element's entries: dJ/dQt += cdt dJ/dQ.
-template <int G>
-__global__ void __launch_bounds__(256) k_upd_adj(double *__restrict__ LQT, const double *__restrict__ LQ, double cdt,
-                                                  double re, double *__restrict__ LFF, double *__restrict__ LVF) {
+// Qt = -(QTI + sum_faces D_edge FB), FB = FF - VF/Re, transposed for one element
+// from its dJ/dQt (lam, shared) to dJ/dFF (LFF).  dJ/dVF is -LFF/Re, formed by
+// k_face_vis_adj.
+template <int G> __device__ __forceinline__ void face_terms_adj(const double *lam, int k, double *__restrict__ LFF) {
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G;
-  __shared__ double lam[5 * NG];  // this element's dJ/dQt after the RK step
-  const int k = blockIdx.x;
-  double *lamg = LQT + (long long)k * 5 * NG;
-  const double *lq = LQ + (long long)k * 5 * NG;
-  for (int i = threadIdx.x; i < 5 * NG; i += blockDim.x) {
-    const double x = lamg[i] + cdt * lq[i];
-    lamg[i] = x;
-    lam[i] = x;
-  }
-  __syncthreads();
   for (int t = threadIdx.x; t < 30 * G2; t += blockDim.x) {
     const int f = t / (5 * G2), r = t - f * 5 * G2, v = r / G2, ln = r - v * G2, i = ln % G, j = ln / G;
     const bool hi = (f == 1 || f == 3 || f == 4);
@@ -506,19 +496,37 @@ __global__ void __launch_bounds__(256) k_upd_adj(double *__restrict__ LQT, const
       const double dlo = Op<G>::D(n, 0), dhi = Op<G>::D(n, L - 1);
       acc += (hi ? dhi : dlo) * lam[v * NG + p];
     }
-    const double lfb = -acc;
-    LFF[(long long)k * 30 * G2 + t] = lfb;
-    LVF[(long long)k * 30 * G2 + t] = -lfb / re;
+    LFF[(long long)k * 30 * G2 + t] = -acc;
   }
 }
 
-// BR1 average of the viscous normal flux (k_face_vis), transposed in place.
+// The reverse sweep's first stage of a step: dJ/dQt += cdt dJ/dQ, then the face terms.
+template <int G>
+__global__ void __launch_bounds__(256) k_upd_adj(double *__restrict__ LQT, const double *__restrict__ LQ, double cdt,
+                                                  double *__restrict__ LFF) {
+  constexpr int NG = G * G * G;
+  __shared__ double lam[5 * NG];  // this element's dJ/dQt after the RK step
+  const int k = blockIdx.x;
+  double *lamg = LQT + (long long)k * 5 * NG;
+  const double *lq = LQ + (long long)k * 5 * NG;
+  for (int i = threadIdx.x; i < 5 * NG; i += blockDim.x) {
+    const double x = lamg[i] + cdt * lq[i];
+    lamg[i] = x;
+    lam[i] = x;
+  }
+  __syncthreads();
+  face_terms_adj<G>(lam, k, LFF);
+}
+
+// BR1 average of the viscous normal flux (k_face_vis), transposed: from dJ/dVF
+// after averaging (-LFF/Re) to dJ/dVF before it (LVF).
 template <int G>
 // With QFR non-null it also writes the averaged face states of k_face_inv into QF
 // (as k_face_avg), from raw traces kept by the forward sweep.
-__global__ void __launch_bounds__(128) k_face_vis_adj(const MortarC *__restrict__ mc, int nm, double *__restrict__ LVF,
-                                                       const double *__restrict__ nrm, const double *__restrict__ QFR,
-                                                       double *__restrict__ QF) {
+__global__ void __launch_bounds__(128) k_face_vis_adj(const MortarC *__restrict__ mc, int nm,
+                                                       const double *__restrict__ LFF, double re,
+                                                       double *__restrict__ LVF, const double *__restrict__ nrm,
+                                                       const double *__restrict__ QFR, double *__restrict__ QF) {
   constexpr int G2 = G * G;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)nm * G2) return;
@@ -532,7 +540,7 @@ __global__ void __launch_bounds__(128) k_face_vis_adj(const MortarC *__restrict_
   const bool neg_n = (M.flags >> 4) & 1, neg_s = (M.flags >> 3) & 1;
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
-    const double lm = LVF[M.ms + v * G2 + pt], ls = LVF[M.ss + v * G2 + sp];
+    const double lm = -LFF[M.ms + v * G2 + pt] / re, ls = -LFF[M.ss + v * G2 + sp] / re;
     const double lqb = lm + (neg_s ? -ls : ls);
     const double lh = 0.5 * nm_m * lqb;
     LVF[M.ms + v * G2 + pt] = lh / nm_m;
@@ -571,7 +579,7 @@ __global__ void __launch_bounds__(128) k_face_avg(const MortarC *__restrict__ mc
 
 // Roe flux and averaged state (k_face_inv), transposed: QFR = raw traces.
 template <int G>
-__global__ void __launch_bounds__(128) k_face_inv_adj(const MortarC *__restrict__ mc, int nm,
+__global__ void __launch_bounds__(128, 4) k_face_inv_adj(const MortarC *__restrict__ mc, int nm,
                                                        const double *__restrict__ QFR, const double *__restrict__ LFF,
                                                        const double *__restrict__ LQF, double *__restrict__ LQR,
                                                        const double *__restrict__ nh, const double *__restrict__ nrm,
@@ -616,13 +624,18 @@ __global__ void __launch_bounds__(128) k_face_inv_adj(const MortarC *__restrict_
 }
 
 // Face traces (write_traces), transposed: LJQ += jacob * trace^T LQR; then the
-// RK step of the reverse sweep: dJ/dQ += LJQ, dJ/dQt *= ark.
-template <int G>
+// RK step of the reverse sweep: dJ/dQ += LJQ, dJ/dQt *= ark.  With NEXT the
+// first part of the stage before it in the reverse sweep follows in the same
+// pass (k_upd_adj with cdt): dJ/dQt += cdt dJ/dQ and its face terms into LFF.
+// The operations and their order are those of the two kernels run apart.
+template <int G, bool NEXT>
 __global__ void __launch_bounds__(256) k_trace_adj(const double *__restrict__ LQR, const double *__restrict__ jac,
                                                     const double *__restrict__ LJQ, double *__restrict__ LQ,
-                                                    double *__restrict__ LQT, double ark) {
+                                                    double *__restrict__ LQT, double ark, double cdt,
+                                                    double *__restrict__ LFF) {
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G;
   __shared__ double F[30 * G2];  // this element's face adjoints
+  __shared__ double lam[NEXT ? 5 * NG : 1];  // its dJ/dQt after both RK steps
   __shared__ double b0[G], b1[G];  // end rows of the interpolation (thread-dependent index)
   const int k = blockIdx.x;
   for (int i = threadIdx.x; i < 30 * G2; i += blockDim.x) F[i] = LQR[(long long)k * 30 * G2 + i];
@@ -641,8 +654,20 @@ __global__ void __launch_bounds__(256) k_trace_adj(const double *__restrict__ LQ
     s += b0[l] * Fv[2 * 5 * G2 + n + G * m];          // face 3 (z = 0)
     s += b1[l] * Fv[4 * 5 * G2 + n + G * m];          // face 5
     const long long o = (long long)k * 5 * NG + i;
-    LQ[o] += LJQ[o] + jac[(long long)k * NG + p] * s;
-    LQT[o] *= ark;
+    const double lq = LQ[o] + (LJQ[o] + jac[(long long)k * NG + p] * s);
+    LQ[o] = lq;
+    const double lt = LQT[o] * ark;
+    if constexpr (NEXT) {
+      const double x = lt + cdt * lq;
+      LQT[o] = x;
+      lam[i] = x;
+    } else {
+      LQT[o] = lt;
+    }
+  }
+  if constexpr (NEXT) {
+    __syncthreads();
+    face_terms_adj<G>(lam, k, LFF);
   }
 }
 
