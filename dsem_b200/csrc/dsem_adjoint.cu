@@ -338,25 +338,40 @@ int reverse_step(Adj &A, int n, double *const *st, const double *qend, double *c
 
 // One forward step from c->JQ; stage input states copied to st[0..kord) when st
 // != nullptr, their raw face traces (c->QF at the stage start) to qf[0..kord)
-// when qf != nullptr.
-int forward_step(Adj &A, int n, double *const *st, std::vector<double> *s_win, double *const *qf = nullptr) {
+// when qf != nullptr.  With st, qf, jq_next and qf_next all given the step runs
+// out of place instead: st[0] and qf[0] already hold its start state and raw
+// traces, each stage writes the next stage's into st[kk] and qf[kk], and the
+// last stage writes the end state and its raw traces into jq_next and qf_next
+// (no copies; the same kernels and arithmetic).
+int forward_step(Adj &A, int n, double *const *st, std::vector<double> *s_win, double *const *qf = nullptr,
+                 double *jq_next = nullptr, double *qf_next = nullptr) {
   dsem_ctx *c = A.c;
   const bool win = A.in_window(n);
+  const bool oop = st && qf && jq_next && qf_next;
   for (int kk = 1; kk <= c->kord; ++kk) {
-    if (st) CKA(cudaMemcpyAsync(st[kk - 1], c->JQ, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-    if (qf) CKA(cudaMemcpyAsync(qf[kk - 1], c->QF, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    if (!oop && st) CKA(cudaMemcpyAsync(st[kk - 1], c->JQ, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    if (!oop && qf)
+      CKA(cudaMemcpyAsync(qf[kk - 1], c->QF, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
     if (A.ev && kk == 1) {  // the step's entropy viscosity (tstep.f90:36-38)
-      const int r = dsem_int::ev(c);
+      const int r = dsem_int::ev(c, oop ? st[0] : nullptr);
       if (r) return r;
     }
-    int r = dsem_int::stage(c, kk, (win || A.ev) && kk == c->kord);
+    const bool save = (win || A.ev) && kk == c->kord;
+    int r;
+    if (oop) {
+      const bool last = kk == c->kord;
+      const dsem_int::StageIO io{st[kk - 1], qf[kk - 1], last ? jq_next : st[kk], last ? qf_next : qf[kk]};
+      r = dsem_int::stage_io(c, kk, save, io);
+    } else {
+      r = dsem_int::stage(c, kk, save);
+    }
     if (r) return r;
     A.launches += 2 * (long long)c->groups.size() + 2 * (long long)c->mlists.size();
   }
   if (A.ev) c->ev_grad_valid = true;  // the last stage saved the gradients of the next viscosity
   if (win && s_win) {
     double s = 0.0, s2 = 0.0;
-    int r = dsem_int::eps_sums(c, &s, &s2);
+    int r = dsem_int::eps_sums(c, &s, &s2, oop ? jq_next : nullptr);
     if (r) return r;
     s_win->push_back(s);
     A.s2 = s2;
@@ -527,6 +542,13 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   CKA(cudaMemcpyAsync(A.b.q0, c->JQ, bq, cudaMemcpyDeviceToDevice, c->st));
   CKA(cudaMemsetAsync(c->flag, 0, sizeof(int), c->st));
   if ((r = dsem_int::traces(c))) return r;
+  // with every stage state and its raw traces kept, the sweep runs out of place
+  // through the stash: its first slot starts with the initial state and traces
+  const bool oop = snapshots == 0 && A.b.traces;
+  if (oop) {
+    CKA(cudaMemcpyAsync(A.b.stages, c->JQ, bq, cudaMemcpyDeviceToDevice, c->st));
+    CKA(cudaMemcpyAsync(A.b.traces, c->QF, bf, cudaMemcpyDeviceToDevice, c->st));
+  }
   // ---- forward sweep
   std::vector<double> s_win;
   {
@@ -547,16 +569,22 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
         }
       double *const *stp = snapshots == 0 ? st.data() : nullptr;
       double *const *qfp = qf.empty() ? nullptr : qf.data();
+      double *jq_next = nullptr, *qf_next = nullptr;  // out of place: where the step's end state goes
+      if (oop) {
+        const bool last = n + 1 == nsteps;
+        jq_next = last ? c->JQ : A.b.stages + (size_t)(n + 1) * kord * nq;
+        qf_next = last ? c->QF : A.b.traces + (size_t)(n + 1) * kord * nf;
+      }
       if (n == 0) {
-        if ((r = forward_step(A, n, stp, &s_win, qfp))) return drop(), r;
+        if ((r = forward_step(A, n, stp, &s_win, qfp, jq_next, qf_next))) return drop(), r;
         continue;
       }
       const bool win = A.in_window(n);
-      if ((r = replay(c, &gx[win ? 1 : 0], [&] { return forward_step(A, n, stp, nullptr, qfp); })))
+      if ((r = replay(c, &gx[win ? 1 : 0], [&] { return forward_step(A, n, stp, nullptr, qfp, jq_next, qf_next); })))
         return drop(), r;
       if (win) {
         double sv = 0.0, s2 = 0.0;
-        if ((r = dsem_int::eps_sums(c, &sv, &s2))) return drop(), r;
+        if ((r = dsem_int::eps_sums(c, &sv, &s2, jq_next))) return drop(), r;
         s_win.push_back(sv);
         A.s2 = s2;
       }

@@ -1272,20 +1272,36 @@ template <int G, bool EVK> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1
     tgrad_dir(std::integral_constant<int, 2>{});
   }
 
-  // ---- outputs
-  for (int i = tid; i < 5 * NG; i += NT) LJQ[i] = jac[i % NG] * LQ[i];
+  // ---- outputs (the Jacobian's loads all in flight at once)
+  {
+    constexpr int NQ = (5 * NG + NT - 1) / NT;
+    double jv[NQ];
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) {
+      const int i = tid + j * NT;
+      if (i < 5 * NG) jv[j] = jac[i % NG];
+    }
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) {
+      const int i = tid + j * NT;
+      if (i < 5 * NG) LJQ[i] = jv[j] * LQ[i];
+    }
+  }
   for (int i = tid; i < 30 * G2; i += NT) A.LQF[(long long)k * 30 * G2 + i] = LQFs[i];
   if constexpr (EVK)
     for (int i = tid; i < NG; i += NT) A.lmuhg[(long long)k * NG + i] += LMU[i];
-  red[tid] = lr;
+  // dJ/d(1/Re) of the element: warp sums, then the warps' sums in order
+  static_assert(NT % 32 == 0 && NT / 32 <= 32, "whole warps, at most 32");
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lr += __shfl_xor_sync(0xffffffffu, lr, o);
+  if ((tid & 31) == 0) red[tid >> 5] = lr;
   __syncthreads();
-  for (int n = NT; n > 1;) {  // pairwise halving, any NT
-    const int h = (n + 1) / 2;
-    if (tid < n - h) red[tid] += red[tid + h];
-    __syncthreads();
-    n = h;
+  if (tid == 0) {
+    double t = red[0];
+    for (int w = 1; w < NT / 32; ++w) t += red[w];
+    A.lr[k] += t;
   }
-  if (tid == 0) A.lr[k] += red[0];
+  PHASE_MARK(28);
 }
 
 // RK bookkeeping of the reverse sweep
@@ -1293,7 +1309,7 @@ __global__ void k_rk_adj_post(long long n, double *__restrict__ lq, const double
                               double *__restrict__ lg, double a) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     lq[i] += ljq[i];
-    lg[i] *= a;
+    if (a != 1.0) lg[i] *= a;
   }
 }
 // out[0] += sum of part[0..n) (one block, fixed order)

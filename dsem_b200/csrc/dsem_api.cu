@@ -321,29 +321,35 @@ int enqueue_face_vis(dsem_ctx *c, long long *launches) {
   return DSEM_OK;
 }
 
+// update kernel arguments of one order group for stage kk (0: Qt only)
+UpdArgs upd_args(const dsem_ctx *c, const Group &g, int kk, double *qt_out) {
+  UpdArgs u{};
+  u.JQ = c->JQ + g.q0;
+  u.gQ = c->gQ + g.q0;
+  u.sq = 5LL * g.G * g.G * g.G;
+  u.jac = g.jac;
+  u.QTI = c->QTI + g.q0;
+  u.FF = c->FF + g.f0;
+  u.VF = c->VF + g.f0;
+  u.QF = c->QF + g.f0;
+  u.Qt_out = qt_out ? qt_out + g.q0 : nullptr;
+  u.flag = c->flag;
+  u.re = c->P.re;
+  u.r_re = c->P.r_re;
+  u.update = kk > 0;
+  u.first = kk == 1;
+  u.ark = kk > 0 ? c->ark[kk - 1] : 0.0;
+  u.crk = kk > 0 ? c->crk[kk - 1] : 0.0;
+  u.ecase = g.ecase;
+  u.rec = c->d_rec;
+  u.dtc = c->d_dtc;
+  return u;
+}
+
 int enqueue_update(dsem_ctx *c, int kk, double *qt_out, long long *launches) {
   int r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
     auto &g = c->groups[j];
-    UpdArgs u{};
-    u.JQ = c->JQ + g.q0;
-    u.gQ = c->gQ + g.q0;
-    u.sq = 5LL * g.G * g.G * g.G;
-    u.jac = g.jac;
-    u.QTI = c->QTI + g.q0;
-    u.FF = c->FF + g.f0;
-    u.VF = c->VF + g.f0;
-    u.QF = c->QF + g.f0;
-    u.Qt_out = qt_out ? qt_out + g.q0 : nullptr;
-    u.flag = c->flag;
-    u.re = c->P.re;
-    u.r_re = c->P.r_re;
-    u.update = kk > 0;
-    u.first = kk == 1;
-    u.ark = kk > 0 ? c->ark[kk - 1] : 0.0;
-    u.crk = kk > 0 ? c->crk[kk - 1] : 0.0;
-    u.ecase = g.ecase;
-    u.rec = c->d_rec;
-    u.dtc = c->d_dtc;
+    const UpdArgs u = upd_args(c, g, kk, qt_out);
     CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::update(u, g.nel, st); }));
     return DSEM_OK;
   });
@@ -360,11 +366,12 @@ int enqueue_stage(dsem_ctx *c, int kk, bool save, double *qt_out, long long *lau
   return enqueue_update(c, kk, qt_out, launches);
 }
 
-int enqueue_ev(dsem_ctx *c, long long *launches) {
+int enqueue_ev(dsem_ctx *c, long long *launches, const double *jq = nullptr) {
+  if (!jq) jq = c->JQ;
   const int r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
     auto &g = c->groups[j];
     EvArgs a{};
-    a.JQ = c->JQ + g.q0;
+    a.JQ = jq + g.q0;
     a.sq = 5LL * g.G * g.G * g.G;
     a.jac = g.jac;
     a.hd = g.hd;
@@ -1781,9 +1788,35 @@ int traces(dsem_ctx *c) {
   long long l = 0;
   return enqueue_traces(c, &l);
 }
-int ev(dsem_ctx *c) {
+int ev(dsem_ctx *c, const double *jq) {
   long long l = 0;
-  return enqueue_ev(c, &l);
+  return enqueue_ev(c, &l, jq);
+}
+// One RK stage of a single-group context with periodic conforming mortars only,
+// out of place: state io.jq_in and its raw face traces io.qf_in (both left
+// unchanged) -> the updated state io.jq_out and its raw traces io.qf_out.  The
+// same kernels and arithmetic as stage(); c->QF receives the averaged traces.
+int stage_io(dsem_ctx *c, int kk, bool save, const StageIO &io) {
+  if (c->groups.size() != 1 || c->mlists.size() != 1 || c->nnc > 0 || c->ncut > 0 || !c->blists.empty() || kk < 1)
+    return fail(c, DSEM_ERR_UNSUPPORTED, "stage_io: one order group and periodic conforming mortars only");
+  const Group &g = c->groups[0];
+  const MList &ml = c->mlists[0];
+  VolArgs a = vol_args(c, g);
+  a.JQ = io.jq_in;
+  UpdArgs u = upd_args(c, g, kk, nullptr);
+  u.JQ = io.jq_in;
+  u.JQo = io.jq_out;
+  u.QF = io.qf_out;
+  const int mode = vol_mode(c, save);
+  CK(with_G(g.G, [&](auto gg) -> cudaError_t {
+    using Lg = Launch<decltype(gg)::value>;
+    cudaError_t e = Lg::face_inv_from(ml.mc, ml.n, io.qf_in, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st);
+    if (e == cudaSuccess) e = Lg::vol(a, g.nel, g.diag, mode, c->st, c->vol_variant[g.G]);
+    if (e == cudaSuccess) e = Lg::face_vis(ml.mc, ml.n, c->VF, ml.nrm, c->st);
+    if (e == cudaSuccess) e = Lg::update(u, g.nel, c->st);
+    return e;
+  }));
+  return DSEM_OK;
 }
 int set_dt(dsem_ctx *c, const double *dt) { return ::set_dt(c, dt); }
 int unpack_state(dsem_ctx *c, const double *dev, double *host, int ldx) {
@@ -1791,9 +1824,10 @@ int unpack_state(dsem_ctx *c, const double *dev, double *host, int ldx) {
 }
 int check_flag(dsem_ctx *c) { return ::check_flag(c); }
 // enstrophy sums of the last stage's gradients, in the caller's element order
-int eps_sums(dsem_ctx *c, double *s, double *s2) {
+int eps_sums(dsem_ctx *c, double *s, double *s2, const double *jq) {
+  if (!jq) jq = c->JQ;
   for (auto &g : c->groups) {
-    k_diag<<<g.nel, 128, sizeof(double) * 5 * g.G * g.G * g.G, c->st>>>(c->JQ + g.q0, g.jac, g.EVB, g.kew, g.G, g.nel, 1,
+    k_diag<<<g.nel, 128, sizeof(double) * 5 * g.G * g.G * g.G, c->st>>>(jq + g.q0, g.jac, g.EVB, g.kew, g.G, g.nel, 1,
                                                                          c->part + g.e0 * 5);
     CK(cudaGetLastError());
   }

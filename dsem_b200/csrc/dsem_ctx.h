@@ -128,9 +128,16 @@ namespace dsem_int {
 int fail(dsem_ctx *c, int code, const std::string &msg);
 int stage(dsem_ctx *c, int kk, bool save);  // one RK stage on c->JQ (eager launches)
 int traces(dsem_ctx *c);                    // face traces of c->JQ
-int ev(dsem_ctx *c);                        // entropy viscosity of c->JQ (valid: c->ev_grad_valid)
+int ev(dsem_ctx *c, const double *jq = nullptr);  // entropy viscosity of jq (null: c->JQ; valid: c->ev_grad_valid)
+struct StageIO {
+  double *jq_in;        // stage input state (read only)
+  const double *qf_in;  // its raw face traces (read only)
+  double *jq_out, *qf_out;  // updated state and its raw face traces
+};
+int stage_io(dsem_ctx *c, int kk, bool save, const StageIO &io);  // out-of-place stage (one group, periodic)
 int set_dt(dsem_ctx *c, const double *dt);
 int unpack_state(dsem_ctx *c, const double *dev, double *host, int ldx);
 int check_flag(dsem_ctx *c);
-int eps_sums(dsem_ctx *c, double *s, double *s2);  // enstrophy sums of the last saved gradients
+// enstrophy sums of the last saved gradients with the state jq (null: c->JQ)
+int eps_sums(dsem_ctx *c, double *s, double *s2, const double *jq = nullptr);
 }  // namespace dsem_int

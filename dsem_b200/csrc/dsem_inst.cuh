@@ -110,6 +110,15 @@ cudaError_t Launch<G>::face_inv(const MortarC *mc, int nm, double *QF, double *F
   return cudaGetLastError();
 }
 
+template <int G>
+cudaError_t Launch<G>::face_inv_from(const MortarC *mc, int nm, const double *QFR, double *QF, double *FF,
+                                     const double *nh, const double *nrm, double gamma, cudaStream_t s) {
+  if (nm <= 0) return cudaSuccess;
+  const long long n = (long long)nm * G * G;
+  k_face_inv_from<G><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(mc, nm, QFR, QF, FF, nh, nrm, gamma);
+  return cudaGetLastError();
+}
+
 template <int G> cudaError_t Launch<G>::face_vis(const MortarC *mc, int nm, double *VF, const double *nrm, cudaStream_t s) {
   if (nm <= 0) return cudaSuccess;
   const long long n = (long long)nm * G * G;

@@ -51,6 +51,9 @@ template <int G> struct Launch {
   static cudaError_t les(const LesArgs &a, int nel, cudaStream_t s);
   static cudaError_t face_inv(const MortarC *mc, int nm, double *QF, double *FF, const double *nh, const double *nrm,
                               double gamma, cudaStream_t s);
+  // the same from raw traces QFR kept elsewhere (left unchanged), averages into QF
+  static cudaError_t face_inv_from(const MortarC *mc, int nm, const double *QFR, double *QF, double *FF,
+                                   const double *nh, const double *nrm, double gamma, cudaStream_t s);
   static cudaError_t face_vis(const MortarC *mc, int nm, double *VF, const double *nrm, cudaStream_t s);
   static cudaError_t face_inv_cut(const MortarCut *mc, int nm, double *QF, double *FF, const double *ghost,
                                   const double *nh, const double *nrm, double gamma, cudaStream_t s);

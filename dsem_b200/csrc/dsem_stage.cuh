@@ -111,15 +111,14 @@ template <int G> __device__ __forceinline__ void slave_index(int orient, int i, 
   }
 }
 
+// Roe flux and averaged state at one mortar point, from the raw traces in QFin
+// to the averages in QF (QFin == QF: in place; each point is read and written by
+// its own thread only).
 template <int G>
-__global__ void __launch_bounds__(128) k_face_inv(const MortarC *__restrict__ mc, int nm, double *__restrict__ QF,
-                                                   double *__restrict__ FF, const double *__restrict__ nh,
-                                                   const double *__restrict__ nrm, double gamma) {
+__device__ __forceinline__ void face_inv_point(const MortarC &M, int pt, const double *QFin, double *QF,
+                                               double *__restrict__ FF, const double *__restrict__ nh,
+                                               const double *__restrict__ nrm, double gamma) {
   constexpr int G2 = G * G;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)nm * G2) return;
-  const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
-  const MortarC M = mc[m];
   const int i = pt % G, j = pt / G;
   int si, sj;
   slave_index<G>(M.flags & 7, i, j, si, sj);
@@ -127,8 +126,8 @@ __global__ void __launch_bounds__(128) k_face_inv(const MortarC *__restrict__ mc
   double Q1[NV], Q2[NV], f[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
-    Q1[v] = QF[M.ms + v * G2 + pt];
-    Q2[v] = QF[M.ss + v * G2 + sp];
+    Q1[v] = QFin[M.ms + v * G2 + pt];
+    Q2[v] = QFin[M.ss + v * G2 + sp];
   }
   const long long gp = (long long)M.geo * G2 + pt;
   const double n3[3] = {nh[gp * 3], nh[gp * 3 + 1], nh[gp * 3 + 2]};
@@ -143,6 +142,30 @@ __global__ void __launch_bounds__(128) k_face_inv(const MortarC *__restrict__ mc
     QF[M.ms + v * G2 + pt] = avg;
     QF[M.ss + v * G2 + sp] = avg;
   }
+}
+
+template <int G>
+__global__ void __launch_bounds__(128) k_face_inv(const MortarC *__restrict__ mc, int nm, double *QF,
+                                                   double *__restrict__ FF, const double *__restrict__ nh,
+                                                   const double *__restrict__ nrm, double gamma) {
+  constexpr int G2 = G * G;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nm * G2) return;
+  const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
+  face_inv_point<G>(mc[m], pt, QF, QF, FF, nh, nrm, gamma);
+}
+
+// The same with the raw traces kept elsewhere (QFR, left unchanged).
+template <int G>
+__global__ void __launch_bounds__(128) k_face_inv_from(const MortarC *__restrict__ mc, int nm,
+                                                        const double *__restrict__ QFR, double *__restrict__ QF,
+                                                        double *__restrict__ FF, const double *__restrict__ nh,
+                                                        const double *__restrict__ nrm, double gamma) {
+  constexpr int G2 = G * G;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nm * G2) return;
+  const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
+  face_inv_point<G>(mc[m], pt, QFR, QF, FF, nh, nrm, gamma);
 }
 
 template <int G>
@@ -1070,6 +1093,7 @@ struct UpdArgs {
   const double *jac;
   const double *QTI, *FF, *VF;
   double *QF;      // out: traces of the updated state
+  double *JQo;     // optional: the updated state goes here and JQ is left unchanged
   double *Qt_out;  // optional: [elem][5][G^3]
   int *flag;       // bit 0: non-finite Qt
   double ark, cdt, re, r_re;  // r_re = 1/re
@@ -1121,6 +1145,7 @@ template <int G> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
   }
   __syncthreads();
   double *JQ = A.JQ + (long long)k * A.sq;
+  double *JQw = A.JQo ? A.JQo + (long long)k * A.sq : JQ;  // where the updated state goes
   double *gQ = A.gQ + (long long)k * A.sq;
   const double *QTI = A.QTI + (long long)k * 5 * NG;
   const double *jac = A.jac + (long long)k * NG;
@@ -1161,7 +1186,7 @@ template <int G> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
       const double g = A.ark * g0 + Qt;
       q = q + cdt * g;
       gQ[i] = g;
-      JQ[i] = q;
+      JQw[i] = q;
     }
     QN[i] = q * jc[u];
     }
