@@ -38,7 +38,7 @@ int upload_ops_here(dsem_ctx *c) {  // this translation unit's copy of the opera
 }
 
 struct AdjBuf {
-  double *lq = nullptr, *lg = nullptr, *ljq = nullptr, *ldir = nullptr;
+  double *lq = nullptr, *lg = nullptr, *ljq = nullptr;
   double *qfr = nullptr, *lff = nullptr, *lvf = nullptr, *lqf = nullptr, *lqr = nullptr;
   double *lrp = nullptr, *lr = nullptr;
   double *q0 = nullptr;
@@ -48,8 +48,11 @@ struct AdjBuf {
   // entropy viscosity: dJ/dmu of the step being reversed, dJ/d(gradients saved by
   // the previous step's last stage), and those gradients as they were on entry
   double *lmuhg = nullptr, *levb = nullptr, *evb0 = nullptr;
+  double *eps_part = nullptr;  // [window][elements][5] enstrophy partials of the window's steps
+  double *evbw = nullptr;      // [window][elements][15][G^3] gradients saved by the window steps' last stages
   ~AdjBuf() {
-    for (double *p : {lq, lg, ljq, ldir, qfr, lff, lvf, lqf, lqr, lrp, lr, q0, stages, traces, lmuhg, levb, evb0})
+    for (double *p : {lq, lg, ljq, qfr, lff, lvf, lqf, lqr, lrp, lr, q0, stages, traces, lmuhg, levb, evb0,
+                      eps_part, evbw})
       cudaFree(p);
     for (double *p : slots) cudaFree(p);
   }
@@ -70,34 +73,29 @@ struct Adj {
   double eps_w() const { return dt * 100.0 * c->P.r_re / s2; }
 };
 
-// Adjoint of one stage.  Unless direct_only, the RK steps around it are fused in:
-// dJ/dQt += cdt dJ/dQ before, dJ/dQ += R'^T dJ/dQt and dJ/dQt *= ark after.
+// Adjoint of one stage, the RK steps around it fused in: dJ/dQt += cdt dJ/dQ
+// before, dJ/dQ += R'^T dJ/dQt and dJ/dQt *= ark after.  eps_w != 0: the stage
+// whose gradients enter the enstrophy sum (with the end state's JQ values JQe).
 // qraw: the raw face traces of Qs kept by the forward sweep, or null to recompute them.
 // The first part (dJ/dQt += cdt dJ/dQ and the face terms) runs here only when
 // upd; otherwise the previous stage of the reverse sweep ran it.  With next,
 // this stage's last kernel also runs that first part of the stage reversed
 // next, with its coefficient cdt_next.
 template <int G>
-int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, bool direct_only, double cdt,
-                    double ark, const double *qraw, const double *levb, bool upd, bool next, double cdt_next) {
+int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, double cdt, double ark,
+                    const double *qraw, const double *levb, bool upd, bool next, double cdt_next) {
   dsem_ctx *c = A.c;
   const Group &g = *A.g;
   const MList &ml = *A.ml;
   if constexpr (G > 7) {
-    (void)Qs; (void)JQe; (void)eps_w; (void)direct_only; (void)g; (void)ml; (void)cdt; (void)ark; (void)qraw;
+    (void)Qs; (void)JQe; (void)eps_w; (void)g; (void)ml; (void)cdt; (void)ark; (void)qraw;
     (void)levb; (void)upd; (void)next; (void)cdt_next;
     return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
   } else {
     constexpr int G2 = G * G;
     // forward prerequisites: raw traces (qfr), averaged traces (c->QF)
-    const double *qfr = qraw;
-    const bool avg_in_vis = qraw && !direct_only;  // the viscous-face adjoint writes the averages
-    if (qraw && direct_only) {
-      const unsigned nbm = (unsigned)(((long long)ml.n * G2 + 127) / 128);
-      k_face_avg<G><<<nbm, 128, 0, c->st>>>(ml.mc, ml.n, qraw, c->QF);
-      CKA(cudaGetLastError());
-      A.launches += 1;
-    } else if (!qraw) {
+    const double *qfr = qraw;  // given: the viscous-face adjoint writes the averages
+    if (!qraw) {
       TraceArgs ta{};
       ta.JQ = Qs;
       ta.sq = 5LL * G * G * G;
@@ -121,14 +119,13 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
     va.QF = c->QF;
     va.LQT = A.b.lg;
     va.LVF = A.b.lvf;
-    va.LJQ = direct_only ? A.b.ldir : A.b.ljq;
+    va.LJQ = A.b.ljq;
     va.LQF = A.b.lqf;
     va.lr = A.b.lrp;
     va.eps_w = eps_w;
     va.JQe = JQe;
-    va.direct_only = direct_only ? 1 : 0;
     va.P = c->P;
-    if (A.ev && !direct_only) {
+    if (A.ev) {
       va.muhg = g.muhg;
       va.lmuhg = A.b.lmuhg;
       va.levb = levb;
@@ -138,20 +135,13 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
       CKA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->dev));
       va.pf = nsm;
     }
-    if (direct_only) {
-      k_vol_adj<G, false><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
-      CKA(cudaGetLastError());
-      ++A.launches;
-      return DSEM_OK;
-    }
     const unsigned nb = (unsigned)(((long long)ml.n * G2 + 127) / 128);
     if (upd) {
       k_upd_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lg, A.b.lq, cdt, A.b.lff);
       CKA(cudaGetLastError());
       ++A.launches;
     }
-    k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lff, c->P.re, A.b.lvf, ml.nrm,
-                                             avg_in_vis ? qraw : nullptr, c->QF);
+    k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lff, c->P.re, A.b.lvf, ml.nrm, qraw, c->QF);
     CKA(cudaGetLastError());
     if (A.ev)
       k_vol_adj<G, true><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
@@ -171,16 +161,85 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, b
   }
 }
 
-int stage_adjoint(Adj &A, const double *Qs, const double *JQe, double eps_w, bool direct_only, double cdt = 0.0,
-                  double ark = 1.0, const double *qraw = nullptr, const double *levb = nullptr, bool upd = true,
-                  bool next = false, double cdt_next = 0.0) {
+int stage_adjoint(Adj &A, const double *Qs, const double *JQe, double eps_w, double cdt, double ark,
+                  const double *qraw, const double *levb, bool upd, bool next, double cdt_next) {
   int r = DSEM_OK;
   cudaError_t e = with_G(A.g->G, [&](auto gc) -> cudaError_t {
-    r = stage_adjoint_G<decltype(gc)::value>(A, Qs, JQe, eps_w, direct_only, cdt, ark, qraw, levb, upd, next,
-                                             cdt_next);
+    r = stage_adjoint_G<decltype(gc)::value>(A, Qs, JQe, eps_w, cdt, ark, qraw, levb, upd, next, cdt_next);
     return cudaSuccess;
   });
   if (e != cudaSuccess) return dsem_int::fail(A.c, DSEM_ERR_UNSUPPORTED, "adjoint: element order not supported");
+  return r;
+}
+
+// The gradients a forward step's last stage saves (into the group's EVB),
+// recomputed by the forward volume kernel itself (mode VOL_SAVE or VOL_EV_SAVE)
+// from that stage's input state Qs and its raw face traces qraw (null: recomputed).
+template <int G> int saved_grads_G(Adj &A, const double *Qs, const double *qraw, int mode) {
+  dsem_ctx *c = A.c;
+  const Group &g = *A.g;
+  const MList &ml = *A.ml;
+  constexpr int G2 = G * G, NG = G * G * G;
+  if (qraw) {
+    const unsigned nbm = (unsigned)(((long long)ml.n * G2 + 127) / 128);
+    k_face_avg<G><<<nbm, 128, 0, c->st>>>(ml.mc, ml.n, qraw, c->QF);
+    CKA(cudaGetLastError());
+  } else {
+    TraceArgs ta{};
+    ta.JQ = Qs;
+    ta.sq = 5LL * NG;
+    ta.jac = g.jac;
+    ta.QF = c->QF;
+    CKA(Launch<G>::trace(ta, g.nel, c->st));
+    CKA(Launch<G>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st));
+  }
+  VolArgs a{};  // the volume kernel with saved gradients: EVB (its fluxes are not used)
+  a.JQ = Qs;
+  a.sq = 5LL * NG;
+  a.jac = g.jac;
+  a.gg = g.gg;
+  a.gm = g.gm;
+  a.muhg = g.muhg;
+  a.QF = c->QF;
+  a.VF = c->VF;
+  a.QTI = c->QTI;
+  a.EVB = g.EVB;
+  a.P = c->P;
+  a.ecase = g.ecase;
+  a.rec = c->d_rec;
+  CKA(Launch<G>::vol(a, g.nel, true, mode, c->st));
+  A.launches += qraw ? 2 : 3;
+  return DSEM_OK;
+}
+
+// Direct part of a window step's enstrophy term into dJ/dQ of its end state
+// qend, from the gradients its last stage saved: evb, or (null) recomputed
+// from that stage's input state Qs and raw traces qraw into the group's EVB.
+template <int G> int eps_direct_G(Adj &A, const double *Qs, const double *qraw, const double *qend, const double *evb) {
+  dsem_ctx *c = A.c;
+  const Group &g = *A.g;
+  if constexpr (G > 7) {
+    (void)Qs; (void)qraw; (void)qend; (void)evb; (void)g;
+    return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
+  } else {
+    if (!evb) {
+      const int r = saved_grads_G<G>(A, Qs, qraw, VOL_SAVE);
+      if (r) return r;
+      evb = g.EVB;
+    }
+    k_eps_dir<G><<<g.nel, 128, 0, c->st>>>(qend, g.jac, evb, A.eps_w(), A.b.lq);
+    CKA(cudaGetLastError());
+    ++A.launches;
+    return DSEM_OK;
+  }
+}
+
+int eps_direct(Adj &A, const double *Qs, const double *qraw, const double *qend, const double *evb) {
+  int r = DSEM_OK;
+  with_G(A.g->G, [&](auto gc) -> cudaError_t {
+    r = eps_direct_G<decltype(gc)::value>(A, Qs, qraw, qend, evb);
+    return cudaSuccess;
+  });
   return r;
 }
 
@@ -197,37 +256,11 @@ template <int G> int ev_forward_G(Adj &A, const double *Qn, const double *Qprev,
     (void)Qn; (void)Qprev; (void)qraw_prev; (void)valid; (void)g; (void)ml;
     return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
   } else {
-    constexpr int G2 = G * G, NG = G * G * G;
+    constexpr int NG = G * G * G;
     bool ok = true;
     if (Qprev) {
-      if (qraw_prev) {
-        const unsigned nbm = (unsigned)(((long long)ml.n * G2 + 127) / 128);
-        k_face_avg<G><<<nbm, 128, 0, c->st>>>(ml.mc, ml.n, qraw_prev, c->QF);
-        CKA(cudaGetLastError());
-      } else {
-        TraceArgs ta{};
-        ta.JQ = Qprev;
-        ta.sq = 5LL * NG;
-        ta.jac = g.jac;
-        ta.QF = c->QF;
-        CKA(Launch<G>::trace(ta, g.nel, c->st));
-        CKA(Launch<G>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st));
-      }
-      VolArgs a{};  // the volume kernel with saved gradients: EVB (its fluxes are not used)
-      a.JQ = Qprev;
-      a.sq = 5LL * NG;
-      a.jac = g.jac;
-      a.gg = g.gg;
-      a.gm = g.gm;
-      a.muhg = g.muhg;
-      a.QF = c->QF;
-      a.VF = c->VF;
-      a.QTI = c->QTI;
-      a.EVB = g.EVB;
-      a.P = c->P;
-      a.ecase = g.ecase;
-      a.rec = c->d_rec;
-      CKA(Launch<G>::vol(a, g.nel, true, VOL_EV_SAVE, c->st));
+      const int r = saved_grads_G<G>(A, Qprev, qraw_prev, VOL_EV_SAVE);
+      if (r) return r;
     } else if (A.ev_valid0) {
       CKA(cudaMemcpyAsync(g.EVB, A.b.evb0, (size_t)g.nel * 15 * NG * sizeof(double), cudaMemcpyDeviceToDevice,
                           c->st));
@@ -247,7 +280,7 @@ template <int G> int ev_forward_G(Adj &A, const double *Qn, const double *Qprev,
     e.rec = c->d_rec;
     CKA(Launch<G>::ev(e, g.nel, c->st));
     CKA(cudaMemsetAsync(A.b.lmuhg, 0, (size_t)g.nel * NG * sizeof(double), c->st));
-    A.launches += 3;
+    ++A.launches;
     *valid = ok;
     return DSEM_OK;
   }
@@ -295,33 +328,28 @@ int ev_adjoint(Adj &A, const double *Qn) {
   return r;
 }
 
-unsigned ew_blocks(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16); }
-
 // Reverse of step n, its stage input states at st[0..kord) and its end state at
 // qend; qf[0..kord): their raw face traces, or null.  With entropy viscosity,
 // qprev / qfprev: the previous step's last stage input state and its raw traces
-// (null for the first step).
+// (null for the first step).  evb: the gradients step n's last stage saved, or
+// null to recompute them (used when step n is in the objective's window).
 int reverse_step(Adj &A, int n, double *const *st, const double *qend, double *const *qf = nullptr,
-                 const double *qprev = nullptr, const double *qfprev = nullptr) {
+                 const double *qprev = nullptr, const double *qfprev = nullptr, const double *evb = nullptr) {
   dsem_ctx *c = A.c;
-  const long long nq = (long long)c->nq;
   const bool win = A.in_window(n);
+  if (win) {  // d eps_n / d JQ_n through the JQ values of the enstrophy sum
+    int r = eps_direct(A, st[c->kord - 1], qf ? qf[c->kord - 1] : nullptr, qend, evb);
+    if (r) return r;
+  }
   bool ev_valid = false;
   if (A.ev) {
     const int r = ev_forward(A, st[0], qprev, qfprev, &ev_valid);
     if (r) return r;
   }
-  if (win) {  // d eps_n / d JQ_n through the JQ values of the enstrophy sum
-    int r = stage_adjoint(A, st[c->kord - 1], qend, A.eps_w(), true, 0.0, 1.0, qf ? qf[c->kord - 1] : nullptr);
-    if (r) return r;
-    k_rk_adj_post<<<ew_blocks(nq), 256, 0, c->st>>>(nq, A.b.lq, A.b.ldir, A.b.lg, 1.0);
-    CKA(cudaGetLastError());
-    ++A.launches;
-  }
   for (int kk = c->kord; kk >= 1; --kk) {
     const bool eps_here = win && kk == c->kord;
     const double *levb = (A.ev && kk == c->kord && A.levb_pending) ? A.b.levb : nullptr;
-    int r = stage_adjoint(A, st[kk - 1], qend, eps_here ? A.eps_w() : 0.0, false, c->crk[kk - 1] * A.dt,
+    int r = stage_adjoint(A, st[kk - 1], qend, eps_here ? A.eps_w() : 0.0, c->crk[kk - 1] * A.dt,
                           c->ark[kk - 1], qf ? qf[kk - 1] : nullptr, levb, kk == c->kord, kk > 1,
                           kk > 1 ? c->crk[kk - 2] * A.dt : 0.0);
     if (r) return r;
@@ -342,9 +370,10 @@ int reverse_step(Adj &A, int n, double *const *st, const double *qend, double *c
 // out of place instead: st[0] and qf[0] already hold its start state and raw
 // traces, each stage writes the next stage's into st[kk] and qf[kk], and the
 // last stage writes the end state and its raw traces into jq_next and qf_next
-// (no copies; the same kernels and arithmetic).
-int forward_step(Adj &A, int n, double *const *st, std::vector<double> *s_win, double *const *qf = nullptr,
-                 double *jq_next = nullptr, double *qf_next = nullptr) {
+// (no copies; the same kernels and arithmetic), and the gradients it saves into
+// evb_slot when given.
+int forward_step(Adj &A, int n, double *const *st, double *eps_part, double *const *qf = nullptr,
+                 double *jq_next = nullptr, double *qf_next = nullptr, double *evb_slot = nullptr) {
   dsem_ctx *c = A.c;
   const bool win = A.in_window(n);
   const bool oop = st && qf && jq_next && qf_next;
@@ -360,7 +389,8 @@ int forward_step(Adj &A, int n, double *const *st, std::vector<double> *s_win, d
     int r;
     if (oop) {
       const bool last = kk == c->kord;
-      const dsem_int::StageIO io{st[kk - 1], qf[kk - 1], last ? jq_next : st[kk], last ? qf_next : qf[kk]};
+      const dsem_int::StageIO io{st[kk - 1], qf[kk - 1], last ? jq_next : st[kk], last ? qf_next : qf[kk],
+                                 last ? evb_slot : nullptr};
       r = dsem_int::stage_io(c, kk, save, io);
     } else {
       r = dsem_int::stage(c, kk, save);
@@ -369,12 +399,10 @@ int forward_step(Adj &A, int n, double *const *st, std::vector<double> *s_win, d
     A.launches += 2 * (long long)c->groups.size() + 2 * (long long)c->mlists.size();
   }
   if (A.ev) c->ev_grad_valid = true;  // the last stage saved the gradients of the next viscosity
-  if (win && s_win) {
-    double s = 0.0, s2 = 0.0;
-    int r = dsem_int::eps_sums(c, &s, &s2, oop ? jq_next : nullptr);
+  if (win && eps_part) {  // the step's enstrophy partials, summed on the host after the sweep
+    int r = dsem_int::eps_enqueue(c, oop ? jq_next : nullptr, eps_part, oop ? evb_slot : nullptr);
     if (r) return r;
-    s_win->push_back(s);
-    A.s2 = s2;
+    ++A.launches;
   }
   return DSEM_OK;
 }
@@ -435,7 +463,7 @@ int revolve(Adj &A, int i, int j, int si, int sfree) {
     int r = load_state(A, A.b.slots[si]);
     if (r) return r;
     if ((r = forward_step(A, i, st.data(), nullptr))) return r;
-    return reverse_step(A, i, st.data(), c->JQ);
+    return reverse_step(A, i, st.data(), c->JQ, nullptr, nullptr, nullptr, A.g->EVB);
   }
   if (nfree == 0) {  // no free slot: re-advance from slot si for every step
     for (int m = j - 1; m >= i; --m) {
@@ -444,7 +472,7 @@ int revolve(Adj &A, int i, int j, int si, int sfree) {
       for (int n = i; n < m; ++n)
         if ((r = forward_step(A, n, nullptr, nullptr))) return r;
       if ((r = forward_step(A, m, st.data(), nullptr))) return r;
-      if ((r = reverse_step(A, m, st.data(), c->JQ))) return r;
+      if ((r = reverse_step(A, m, st.data(), c->JQ, nullptr, nullptr, nullptr, A.g->EVB))) return r;
     }
     return DSEM_OK;
   }
@@ -501,7 +529,7 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   A.window = window;
   const size_t nq = c->nq, nf = c->nface, bq = nq * sizeof(double), bf = nf * sizeof(double);
   const int kord = c->kord;
-  for (double **p : {&A.b.lq, &A.b.lg, &A.b.ljq, &A.b.ldir, &A.b.q0}) CKA(cudaMalloc(p, bq));
+  for (double **p : {&A.b.lq, &A.b.lg, &A.b.ljq, &A.b.q0}) CKA(cudaMalloc(p, bq));
   for (double **p : {&A.b.qfr, &A.b.lff, &A.b.lvf, &A.b.lqf, &A.b.lqr}) CKA(cudaMalloc(p, bf));
   CKA(cudaMalloc(&A.b.lrp, (size_t)A.g->nel * sizeof(double)));
   A.ev = c->shock != 0;
@@ -551,10 +579,20 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   }
   // ---- forward sweep
   std::vector<double> s_win;
+  const size_t npart = (size_t)c->ngrid * 5;
+  if (window > 0) CKA(cudaMalloc(&A.b.eps_part, (size_t)window * npart * sizeof(double)));
+  // the gradients saved by each window step's last stage, for the reverse
+  // sweep's direct enstrophy term (else recomputed there)
+  const size_t nevb = (size_t)A.g->nel * 15 * A.g->G * A.g->G * A.g->G;
+  if (oop && !A.ev && window > 0 && cudaMalloc(&A.b.evbw, (size_t)window * nevb * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    A.b.evbw = nullptr;
+  }
   {
     // after the first (eager) step, steps are captured and replayed as CUDA
     // graphs, one per kind of step (inside or outside the window); the window's
-    // enstrophy sums are read on the host after each replay
+    // enstrophy partials stay on the device until the sweep ends, so the host
+    // never waits for the GPU between steps
     cudaGraphExec_t gx[2] = {nullptr, nullptr};
     auto drop = [&]() {
       for (auto &x : gx)
@@ -575,21 +613,29 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
         jq_next = last ? c->JQ : A.b.stages + (size_t)(n + 1) * kord * nq;
         qf_next = last ? c->QF : A.b.traces + (size_t)(n + 1) * kord * nf;
       }
+      const bool win = A.in_window(n);
+      double *part = win ? A.b.eps_part + (size_t)(n - (nsteps - window)) * npart : nullptr;
+      double *evb = (win && A.b.evbw) ? A.b.evbw + (size_t)(n - (nsteps - window)) * nevb : nullptr;
       if (n == 0) {
-        if ((r = forward_step(A, n, stp, &s_win, qfp, jq_next, qf_next))) return drop(), r;
+        if ((r = forward_step(A, n, stp, part, qfp, jq_next, qf_next, evb))) return drop(), r;
         continue;
       }
-      const bool win = A.in_window(n);
-      if ((r = replay(c, &gx[win ? 1 : 0], [&] { return forward_step(A, n, stp, nullptr, qfp, jq_next, qf_next); })))
+      if ((r = replay(c, &gx[win ? 1 : 0],
+                      [&] { return forward_step(A, n, stp, part, qfp, jq_next, qf_next, evb); })))
         return drop(), r;
-      if (win) {
-        double sv = 0.0, s2 = 0.0;
-        if ((r = dsem_int::eps_sums(c, &sv, &s2, jq_next))) return drop(), r;
-        s_win.push_back(sv);
-        A.s2 = s2;
-      }
     }
     drop();
+  }
+  if (window > 0) {  // the window's enstrophy sums, step by step in the caller's element order
+    std::vector<double> hp((size_t)window * npart);
+    CKA(cudaMemcpyAsync(hp.data(), A.b.eps_part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CKA(cudaStreamSynchronize(c->st));
+    for (int w = 0; w < window; ++w) {
+      double sv = 0.0, s2 = 0.0;
+      dsem_int::eps_reduce(c, hp.data() + (size_t)w * npart, &sv, &s2);
+      s_win.push_back(sv);
+      A.s2 = s2;  // the normalisation: the window's last step
+    }
   }
   if ((r = dsem_int::check_flag(c))) return r;
   double Jv = 0.0, lr_explicit = 0.0;
@@ -624,12 +670,18 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
         // the previous step's last stage (entropy viscosity)
         const double *qprev = n > 0 ? A.b.stages + ((size_t)(n - 1) * kord + kord - 1) * nq : nullptr;
         const double *qfprev = (n > 0 && A.b.traces) ? A.b.traces + ((size_t)(n - 1) * kord + kord - 1) * nf : nullptr;
+        // the gradients step n's last stage saved: kept by the forward sweep, or with
+        // entropy viscosity the group's EVB (the forward sweep's last step, then
+        // each reverse step's recomputation for the step before it)
+        const double *evb = A.ev ? A.g->EVB
+                                 : ((A.in_window(n) && A.b.evbw) ? A.b.evbw + (size_t)(n - (nsteps - window)) * nevb
+                                                                 : nullptr);
         if (n == nsteps - 1 || (A.ev && n == 0)) {  // launch sequences of their own: eager
-          if ((r = reverse_step(A, n, st.data(), qend, qfp, qprev, qfprev))) return drop(), r;
+          if ((r = reverse_step(A, n, st.data(), qend, qfp, qprev, qfprev, evb))) return drop(), r;
           continue;
         }
         r = replay(c, &gx[A.in_window(n) ? 1 : 0],
-                   [&] { return reverse_step(A, n, st.data(), qend, qfp, qprev, qfprev); });
+                   [&] { return reverse_step(A, n, st.data(), qend, qfp, qprev, qfprev, evb); });
         if (r) return drop(), r;
       }
       drop();

@@ -793,7 +793,6 @@ struct VolAdjArgs {
   double *lr;                   // in/out: per element dJ/d(1/Re), accumulated over stages
   double eps_w;                 // weight of the enstrophy sum (0: none)
   const double *JQe;            // state whose JQ values the enstrophy sum uses (end of the step)
-  int direct_only;              // 1: only dJ/dJQe of the enstrophy sum, into LJQ
   int pf;                       // L2 prefetch distance in elements (the blocks resident at once), 0: none
   const double *muhg;           // entropy viscosity at the Gauss points (null: none)
   double *lmuhg;                // in/out with muhg: dJ/dmu at the Gauss points, accumulated over stages
@@ -844,11 +843,12 @@ template <int G, bool EVK> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1
   const double gamma = P.gamma;
   double lr = 0.0;
   long long t_ph_ = 0;
+  (void)t_ph_;
 #ifdef DSEM_PHASE_TIMING
   t_ph_ = clock64();
 #endif
   // the element that starts about one wave of blocks later: its inputs into L2
-  if (A.pf > 0 && !A.direct_only && k + A.pf < (int)gridDim.x) {
+  if (A.pf > 0 && k + A.pf < (int)gridDim.x) {
     const long long n = k + A.pf;
     prefetch_l2(A.JQ + n * 5 * NG, 5 * NG, tid, NT);
     prefetch_l2(A.LQT + n * 5 * NG, 5 * NG, tid, NT);
@@ -949,8 +949,7 @@ template <int G, bool EVK> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1
   PHASE_MARK(22);
 
   // ---- enstrophy term (energydissipation.f90:19-78) on these gradients and the
-  // JQ values of JQe: the gradient part goes to LGR; with direct_only the JQe
-  // part is the whole output
+  // JQ values of JQe: its gradient part, into LGR (the JQe part: k_eps_dir)
   if (A.eps_w != 0.0) {
     const double *JQe = A.JQe + (long long)k * 5 * NG;
     for (int p = tid; p < NG; p += NT) {
@@ -963,19 +962,12 @@ template <int G, bool EVK> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1
         lgr[f] = 0.0;
       }
       vort_vjp(Qj, jac[p], gr, A.eps_w, lq4, lgr);
-      if (A.direct_only) {
 #pragma unroll
-        for (int v = 0; v < 4; ++v) LJQ[v * NG + p] = lq4[v];
-        LJQ[4 * NG + p] = 0.0;
-      } else {
-#pragma unroll
-        for (int f = 0; f < 12; ++f) LGR[f * NG + p] += lgr[f];
-      }
+      for (int f = 0; f < 12; ++f) LGR[f * NG + p] += lgr[f];
     }
     __syncthreads();
   }
   PHASE_MARK(23);
-  if (A.direct_only) return;
 
   // ---- reverse of pass 2: fluxes and interior divergence, grid by grid
   auto flux_dir = [&](auto Dc) {
@@ -1304,14 +1296,35 @@ template <int G, bool EVK> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1
   PHASE_MARK(28);
 }
 
-// RK bookkeeping of the reverse sweep
-__global__ void k_rk_adj_post(long long n, double *__restrict__ lq, const double *__restrict__ ljq,
-                              double *__restrict__ lg, double a) {
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    lq[i] += ljq[i];
-    if (a != 1.0) lg[i] *= a;
+// Direct part of the enstrophy term of a window step (energydissipation.f90:19-78):
+// d eps / d JQe at fixed gradients, from the gradients the forward sweep saved
+// for the step's last stage (EVB, [elem][15][G^3], fields as GR), added into
+// dJ/dQ of the step's end state: LQ += w dvort/dJQe (the energy entry adds 0).
+template <int G>
+__global__ void __launch_bounds__(128) k_eps_dir(const double *__restrict__ JQe, const double *__restrict__ jac,
+                                                  const double *__restrict__ EVB, double w, double *__restrict__ LQ) {
+  constexpr int NG = G * G * G;
+  const int k = blockIdx.x;
+  const double *Jk = JQe + (long long)k * 5 * NG;
+  const double *E = EVB + (long long)k * 15 * NG;
+  const double *jk = jac + (long long)k * NG;
+  double *Lk = LQ + (long long)k * 5 * NG;
+  for (int p = threadIdx.x; p < NG; p += blockDim.x) {
+    double Qj[4], gr[12], lgr[12], lq4[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int v = 0; v < 4; ++v) Qj[v] = Jk[v * NG + p];
+#pragma unroll
+    for (int f = 0; f < 12; ++f) {
+      gr[f] = E[f * NG + p];
+      lgr[f] = 0.0;
+    }
+    vort_vjp(Qj, jk[p], gr, w, lq4, lgr);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) Lk[v * NG + p] += lq4[v];
+    Lk[4 * NG + p] += 0.0;
   }
 }
+
 // out[0] += sum of part[0..n) (one block, fixed order)
 __global__ void k_sum_into(const double *__restrict__ part, int n, double *__restrict__ out) {
   __shared__ double red[256];

@@ -1803,6 +1803,7 @@ int stage_io(dsem_ctx *c, int kk, bool save, const StageIO &io) {
   const MList &ml = c->mlists[0];
   VolArgs a = vol_args(c, g);
   a.JQ = io.jq_in;
+  if (io.evb) a.EVB = io.evb;
   UpdArgs u = upd_args(c, g, kk, nullptr);
   u.JQ = io.jq_in;
   u.JQo = io.jq_out;
@@ -1823,26 +1824,38 @@ int unpack_state(dsem_ctx *c, const double *dev, double *host, int ldx) {
   return unpack_to_host(c, dev, host, ldx, 5, state_offs(c));
 }
 int check_flag(dsem_ctx *c) { return ::check_flag(c); }
-// enstrophy sums of the last stage's gradients, in the caller's element order
-int eps_sums(dsem_ctx *c, double *s, double *s2, const double *jq) {
+// per-element enstrophy partials of the last stage's gradients with the state
+// jq (null: c->JQ) into part (device, [ngrid][5] in internal order); no sync
+int eps_enqueue(dsem_ctx *c, const double *jq, double *part, const double *evb) {
   if (!jq) jq = c->JQ;
+  if (evb && c->groups.size() != 1) return fail(c, DSEM_ERR_UNSUPPORTED, "eps_enqueue: one order group");
   for (auto &g : c->groups) {
-    k_diag<<<g.nel, 128, sizeof(double) * 5 * g.G * g.G * g.G, c->st>>>(jq + g.q0, g.jac, g.EVB, g.kew, g.G, g.nel, 1,
-                                                                         c->part + g.e0 * 5);
+    k_diag<<<g.nel, 128, sizeof(double) * 5 * g.G * g.G * g.G, c->st>>>(jq + g.q0, g.jac, evb ? evb : g.EVB, g.kew,
+                                                                         g.G, g.nel, 1, part + g.e0 * 5);
     CK(cudaGetLastError());
   }
-  c->host_part.resize((size_t)c->ngrid * 5);
-  CK(cudaMemcpyAsync(c->host_part.data(), c->part, c->host_part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
+  return DSEM_OK;
+}
+// the two enstrophy sums from host partials, in the caller's element order
+void eps_reduce(const dsem_ctx *c, const double *part, double *s, double *s2) {
   double a = 0.0, b = 0.0;
   for (int e = 0; e < c->ngrid; ++e) {
     const auto &g = c->groups[c->ext_group[e]];
-    const double *pp = &c->host_part[(size_t)(g.e0 + c->ext_k[e]) * 5];
+    const double *pp = &part[(size_t)(g.e0 + c->ext_k[e]) * 5];
     a += pp[3];
     b += pp[4];
   }
   *s = a;
   *s2 = b;
+}
+// enstrophy sums of the last stage's gradients, in the caller's element order
+int eps_sums(dsem_ctx *c, double *s, double *s2, const double *jq) {
+  int r = eps_enqueue(c, jq, c->part);
+  if (r) return r;
+  c->host_part.resize((size_t)c->ngrid * 5);
+  CK(cudaMemcpyAsync(c->host_part.data(), c->part, c->host_part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  eps_reduce(c, c->host_part.data(), s, s2);
   return DSEM_OK;
 }
 }  // namespace dsem_int

@@ -133,6 +133,7 @@ struct StageIO {
   double *jq_in;        // stage input state (read only)
   const double *qf_in;  // its raw face traces (read only)
   double *jq_out, *qf_out;  // updated state and its raw face traces
+  double *evb;              // where a saving stage puts its gradients (null: the group's EVB)
 };
 int stage_io(dsem_ctx *c, int kk, bool save, const StageIO &io);  // out-of-place stage (one group, periodic)
 int set_dt(dsem_ctx *c, const double *dt);
@@ -140,4 +141,9 @@ int unpack_state(dsem_ctx *c, const double *dev, double *host, int ldx);
 int check_flag(dsem_ctx *c);
 // enstrophy sums of the last saved gradients with the state jq (null: c->JQ)
 int eps_sums(dsem_ctx *c, double *s, double *s2, const double *jq = nullptr);
+// the same in two halves: per-element partials into device memory part
+// ([elements][5], no sync; gradients from evb, null: the group's EVB, one
+// group only when given), then the sums from a host copy of them
+int eps_enqueue(dsem_ctx *c, const double *jq, double *part, const double *evb = nullptr);
+void eps_reduce(const dsem_ctx *c, const double *part, double *s, double *s2);
 }  // namespace dsem_int
