@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cmath>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/dsem_gpu.h"
@@ -453,6 +454,31 @@ long long beta(int s, int t) {
   return (long long)(v + 0.5L);
 }
 
+// Binomial split of l steps with nfree free slots: the length of the left
+// segment, the left segment's beta(nfree, t - 1) for the smallest t with
+// beta(nfree, t) >= l.
+long long split_left(long long l, int nfree) {
+  int t = 1;
+  while (beta(nfree, t) < l) ++t;
+  return std::max<long long>(1, std::min<long long>(l - 1, beta(nfree, t - 1)));
+}
+
+// The snapshots revolve takes on its first descent, along the right edge of the
+// recursion from revolve(0, nsteps, 0, 1): (step index m, slot) pairs.  The
+// first forward sweep saves them as it passes, so the reverse sweep starts with
+// revolve_spine and skips re-advancing to them.
+std::vector<std::pair<int, int>> spine(int nsteps, int nslots) {
+  std::vector<std::pair<int, int>> v;
+  int i = 0, sfree = 1;
+  while (nsteps - i > 1 && nslots - sfree > 0) {
+    const int m = i + (int)split_left(nsteps - i, nslots - sfree);
+    v.emplace_back(m, sfree);
+    i = m;
+    ++sfree;
+  }
+  return v;
+}
+
 // Reverse steps [i, j) whose start state is in slot si; slots [sfree, end) are free.
 int revolve(Adj &A, int i, int j, int si, int sfree) {
   dsem_ctx *c = A.c;
@@ -476,17 +502,23 @@ int revolve(Adj &A, int i, int j, int si, int sfree) {
     }
     return DSEM_OK;
   }
-  const long long l = j - i;
-  int t = 1;
-  while (beta(nfree, t) < l) ++t;
-  const long long left = std::max<long long>(1, std::min<long long>(l - 1, beta(nfree, t - 1)));
-  const int m = i + (int)left;
+  const int m = i + (int)split_left(j - i, nfree);
   int r = load_state(A, A.b.slots[si]);
   if (r) return r;
   for (int n = i; n < m; ++n)
     if ((r = forward_step(A, n, nullptr, nullptr))) return r;
   CKA(cudaMemcpyAsync(A.b.slots[sfree], c->JQ, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
   if ((r = revolve(A, m, j, sfree, sfree + 1))) return r;
+  return revolve(A, i, m, si, sfree);
+}
+
+// revolve(i, j, si, sfree) with the snapshots of spine() already in their slots
+int revolve_spine(Adj &A, int i, int j, int si, int sfree) {
+  const int nfree = (int)A.b.slots.size() - sfree;
+  if (j - i == 1 || nfree == 0) return revolve(A, i, j, si, sfree);
+  const int m = i + (int)split_left(j - i, nfree);
+  const int r = revolve_spine(A, m, j, sfree, sfree + 1);  // slot sfree holds the state after m steps
+  if (r) return r;
   return revolve(A, i, m, si, sfree);
 }
 
@@ -598,7 +630,14 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
       for (auto &x : gx)
         if (x) cudaGraphExecDestroy(x);
     };
+    std::vector<std::pair<int, int>> sp;
+    if (snapshots > 0) sp = spine(nsteps, snapshots);
+    size_t ksp = 0;  // next snapshot of the spine
     for (int n = 0; n < nsteps; ++n) {
+      if (ksp < sp.size() && sp[ksp].first == n) {  // the state after n steps, for the reverse sweep
+        CKA(cudaMemcpyAsync(A.b.slots[sp[ksp].second], c->JQ, bq, cudaMemcpyDeviceToDevice, c->st));
+        ++ksp;
+      }
       std::vector<double *> st, qf;
       if (snapshots == 0)
         for (int k = 0; k < kord; ++k) {
@@ -687,7 +726,7 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
       drop();
     } else {
       CKA(cudaMemcpyAsync(A.b.slots[0], A.b.q0, bq, cudaMemcpyDeviceToDevice, c->st));
-      if ((r = revolve(A, 0, nsteps, 0, 1))) return r;
+      if ((r = revolve_spine(A, 0, nsteps, 0, 1))) return r;
     }
   }
   k_sum_into<<<1, 256, 0, c->st>>>(A.b.lrp, A.g->nel, A.b.lr);  // dJ/d(1/Re) of the volume terms
