@@ -483,13 +483,16 @@ std::vector<std::pair<int, int>> spine(int nsteps, int nslots) {
 int revolve(Adj &A, int i, int j, int si, int sfree) {
   dsem_ctx *c = A.c;
   const int nfree = (int)A.b.slots.size() - sfree;
-  std::vector<double *> st(c->kord);
+  std::vector<double *> st(c->kord), qf;
   for (int k = 0; k < c->kord; ++k) st[k] = A.b.stages + (size_t)k * c->nq;
+  if (A.b.traces)  // the raw face traces of the step about to be reversed
+    for (int k = 0; k < c->kord; ++k) qf.push_back(A.b.traces + (size_t)k * c->nface);
+  double *const *qfp = qf.empty() ? nullptr : qf.data();
   if (j - i == 1) {
     int r = load_state(A, A.b.slots[si]);
     if (r) return r;
-    if ((r = forward_step(A, i, st.data(), nullptr))) return r;
-    return reverse_step(A, i, st.data(), c->JQ, nullptr, nullptr, nullptr, A.g->EVB);
+    if ((r = forward_step(A, i, st.data(), nullptr, qfp))) return r;
+    return reverse_step(A, i, st.data(), c->JQ, qfp, nullptr, nullptr, A.g->EVB);
   }
   if (nfree == 0) {  // no free slot: re-advance from slot si for every step
     for (int m = j - 1; m >= i; --m) {
@@ -497,8 +500,8 @@ int revolve(Adj &A, int i, int j, int si, int sfree) {
       if (r) return r;
       for (int n = i; n < m; ++n)
         if ((r = forward_step(A, n, nullptr, nullptr))) return r;
-      if ((r = forward_step(A, m, st.data(), nullptr))) return r;
-      if ((r = reverse_step(A, m, st.data(), c->JQ, nullptr, nullptr, nullptr, A.g->EVB))) return r;
+      if ((r = forward_step(A, m, st.data(), nullptr, qfp))) return r;
+      if ((r = reverse_step(A, m, st.data(), c->JQ, qfp, nullptr, nullptr, A.g->EVB))) return r;
     }
     return DSEM_OK;
   }
@@ -581,7 +584,8 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
     cudaGetLastError();
     return dsem_int::fail(c, DSEM_ERR_NOMEM, "adjoint: not enough device memory for the stage states (use snapshots > 0)");
   }
-  if (snapshots == 0 && cudaMalloc(&A.b.traces, nstage * bf) != cudaSuccess) {
+  // raw face traces of every kept stage state (with snapshots: of the step being reversed)
+  if (cudaMalloc(&A.b.traces, nstage * bf) != cudaSuccess) {
     cudaGetLastError();  // not enough memory: the reverse sweep recomputes the traces
     A.b.traces = nullptr;
   }
