@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <string>
 #include <utility>
 #include <vector>
@@ -584,8 +585,12 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
     cudaGetLastError();
     return dsem_int::fail(c, DSEM_ERR_NOMEM, "adjoint: not enough device memory for the stage states (use snapshots > 0)");
   }
+  // DSEM_ADJOINT_LEAN=1 takes the paths used when device memory is short: no
+  // optional trace or gradient slots (the same results, bit for bit, more work)
+  const char *lean_env = std::getenv("DSEM_ADJOINT_LEAN");
+  const bool lean = lean_env && lean_env[0] == '1';
   // raw face traces of every kept stage state (with snapshots: of the step being reversed)
-  if (cudaMalloc(&A.b.traces, nstage * bf) != cudaSuccess) {
+  if (lean || cudaMalloc(&A.b.traces, nstage * bf) != cudaSuccess) {
     cudaGetLastError();  // not enough memory: the reverse sweep recomputes the traces
     A.b.traces = nullptr;
   }
@@ -620,7 +625,8 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   // the gradients saved by each window step's last stage, for the reverse
   // sweep's direct enstrophy term (else recomputed there)
   const size_t nevb = (size_t)A.g->nel * 15 * A.g->G * A.g->G * A.g->G;
-  if (oop && !A.ev && window > 0 && cudaMalloc(&A.b.evbw, (size_t)window * nevb * sizeof(double)) != cudaSuccess) {
+  if (oop && !A.ev && window > 0 && !lean &&
+      cudaMalloc(&A.b.evbw, (size_t)window * nevb * sizeof(double)) != cudaSuccess) {
     cudaGetLastError();
     A.b.evbw = nullptr;
   }

@@ -81,6 +81,24 @@ def test_adjoint_checkpointing_gives_the_same_gradient():
     s.close()
 
 
+@pytest.mark.parametrize("snaps", [0, 2])
+def test_adjoint_low_memory_paths_give_the_same_gradient(monkeypatch, snaps):
+    """Without the optional trace and saved-gradient slots (DSEM_ADJOINT_LEAN=1,
+    the paths taken when device memory is short) the reverse sweep recomputes
+    the face traces and the window's saved gradients: same gradient bit for bit."""
+    from dsem_b200.solver import Solver
+    box, q, dt = _case(2, 4, 800.0, seed=7)
+    s = Solver(box.desc(), re=800.0)
+    s.upload(q)
+    J0, g0, lr0, _ = s.adjoint(dt, 6, 3, snapshots=snaps)
+    monkeypatch.setenv("DSEM_ADJOINT_LEAN", "1")
+    J1, g1, lr1, _ = s.adjoint(dt, 6, 3, snapshots=snaps)
+    monkeypatch.delenv("DSEM_ADJOINT_LEAN")
+    assert J1 == J0 and lr1 == lr0
+    assert np.array_equal(g1, g0)
+    s.close()
+
+
 def test_adjoint_objective_is_the_diagnostic_sum():
     """J equals the sum of dt * eps reported by dsem_diag over the window, and
     the context's state is restored afterwards."""
