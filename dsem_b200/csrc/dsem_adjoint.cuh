@@ -11,12 +11,14 @@
 //   k_face_inv_adj  Roe flux + average   -> dJ/dQFR (LQR)
 //   k_trace_adj     face traces          -> LJQ += jacob * trace^T LQR
 //                   (fused with the k_upd_adj of the stage reversed next)
-// The volume adjoint can also add the derivative of the enstrophy-dissipation
-// sum (energydissipation.f90:19-78) evaluated on the same gradients.
+// The volume adjoint can also add the gradient part of the derivative of the
+// enstrophy-dissipation sum (energydissipation.f90:19-78) evaluated on the same
+// gradients; k_eps_dir adds its direct part.  Entropy viscosity (without the
+// Ducros sensor) enters through k_vol_adj<G, true> and k_ev_adj.
 // Derivatives are exact up to rounding; every pointwise function is
 // differentiated by hand-written reverse mode (riemann_dual / roe_vjp, the
-// forward-mode derivative of the Roe flux, is kept as its independent check).  Diagonal metrics, conforming mortars, no
-// entropy viscosity.
+// forward-mode derivative of the Roe flux, is kept as its independent check).
+// Diagonal metrics and conforming mortars only.
 #pragma once
 #include <type_traits>
 
