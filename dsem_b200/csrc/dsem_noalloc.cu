@@ -14,8 +14,10 @@
 // Contract (see include/dsem_gpu.h):
 //  - the first call on a device does the per-device set-up (symbol address of
 //    the scratch array, operator tables in constant memory, kernel
-//    attributes), with that device current; make that first call before any
-//    stream capture;
+//    attributes), with that device current;
+//  - no call may be made while its stream is being captured: every call
+//    clears the scratch, reads its flag back and waits for the stream, so it
+//    returns DSEM_ERR_INVALID_ARG on a capturing stream;
 //  - every call shares the one scratch array and leaves its contents behind;
 //    calls whose work overlaps on the GPU (two streams, two host threads)
 //    race on it and must be serialised by the caller;
@@ -95,14 +97,24 @@ int setup_device(int dev, double **out) {
 
 // Mortar kernels reading the caller's DSEM_MORTAR_INTS rows directly
 // (1-based element ids; elements of one order, slots [elem][face][var][G^2]).
-// The rows live in device memory, so they are range-checked here: a row with
-// an element outside 1..nel, a face outside 1..6 or an orientation outside
-// 0..7 is skipped and sets bit 2 of the flag.
-__device__ __forceinline__ bool row_ok(const int *r, int nel, int *flag, int pt) {
+// The rows live in device memory, so they are checked here:
+//  - a row with an element outside 1..nel, a face outside 1..6 or an
+//    orientation outside 0..7 is skipped and sets bit 2 of the flag;
+//  - a row that is not a conforming mortar of this order (len(1..2,1..2) or
+//    lenmortar(1..2) other than G, or any conforming(i,j) == 0: a
+//    p-nonconforming mortar, which dsem_rhs sends through the L2 projections)
+//    is skipped and sets bit 3 of the flag.
+__device__ __forceinline__ bool row_ok(const int *r, int nel, int G, int *flag, int pt) {
   const bool ok = r[0] >= 1 && r[0] <= nel && r[1] >= 1 && r[1] <= nel && r[2] >= 1 && r[2] <= 6 && r[3] >= 1 &&
                   r[3] <= 6 && r[10] >= 0 && r[10] <= 7;
-  if (!ok && pt == 0) atomicOr(flag, 4);
-  return ok;
+  if (!ok) {
+    if (pt == 0) atomicOr(flag, 4);
+    return false;
+  }
+  const bool conf = r[4] == G && r[5] == G && r[6] == G && r[7] == G && r[8] == G && r[9] == G && r[13] != 0 &&
+                    r[14] != 0 && r[15] != 0 && r[16] != 0;
+  if (!conf && pt == 0) atomicOr(flag, 8);
+  return conf;
 }
 
 template <int G>
@@ -115,7 +127,7 @@ __global__ void __launch_bounds__(128) k_face_inv_rows(const int *__restrict__ r
   if (t >= (long long)nm * G2) return;
   const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
   const int *r = rows + (long long)DSEM_MORTAR_INTS * m;
-  if (!row_ok(r, nel, flag, pt)) return;
+  if (!row_ok(r, nel, G, flag, pt)) return;
   const long long ms = (long long)(r[0] - 1) * 30 * G2 + (long long)(r[2] - 1) * 5 * G2;
   const long long ss = (long long)(r[1] - 1) * 30 * G2 + (long long)(r[3] - 1) * 5 * G2;
   int si, sj;
@@ -148,7 +160,7 @@ __global__ void __launch_bounds__(128) k_face_vis_rows(const int *__restrict__ r
   if (t >= (long long)nm * G2) return;
   const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
   const int *r = rows + (long long)DSEM_MORTAR_INTS * m;
-  if (!row_ok(r, nel, flag, pt)) return;
+  if (!row_ok(r, nel, G, flag, pt)) return;
   const long long ms = (long long)(r[0] - 1) * 30 * G2 + (long long)(r[2] - 1) * 5 * G2;
   const long long ss = (long long)(r[1] - 1) * 30 * G2 + (long long)(r[3] - 1) * 5 * G2;
   int si, sj;
@@ -228,6 +240,9 @@ int run(double *scratch, int nel, int nmort, const int *rows, const double *nh, 
   NK(cudaStreamSynchronize(st));
 #undef NK
   if (h & 4) return nfail(DSEM_ERR_INVALID_ARG, "dsem_rhs_noalloc: mortar row with an element, face or orientation out of range");
+  if (h & 8)
+    return nfail(DSEM_ERR_UNSUPPORTED,
+                 "dsem_rhs_noalloc: mortar row is not a conforming mortar of order p (lengths or conforming flags)");
   if (h & 1) return nfail(DSEM_ERR_NONFINITE, "NaN or Inf in the right-hand side");
   return DSEM_OK;
 }
@@ -257,6 +272,13 @@ int dsem_rhs_noalloc(int nel, int p, int nmort, const int *mortar, const double 
   int r = setup_device(dev, &scratch);
   if (r) return r;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // every call memsets, reads the flag back and waits for the stream: none of
+  // that may be recorded into a caller's graph
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(st, &cap);
+  if (e != cudaSuccess) return nfail(DSEM_ERR_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
+  if (cap != cudaStreamCaptureStatusNone)
+    return nfail(DSEM_ERR_INVALID_ARG, "dsem_rhs_noalloc: the stream is being captured; call it outside any capture");
   e = with_G(G, [&](auto g) {
     r = run<decltype(g)::value>(scratch, nel, nmort, mortar, n_hat, norm, JQ, jac, gmetg_diag, gmet_diag, gamma, re,
                                 pr, mach, Qt, st);

@@ -273,7 +273,13 @@ int dsem_adjoint(dsem_ctx *ctx, double dt, int nsteps, int window, int snapshots
  *     gmetg_diag  [nel][3][G^3]   gmetg(d,d) at the Gauss points
  *     gmet_diag   [nel][3][L*G^2] gmet(d,d) on staggered grid d
  *   The first call on a device does a one-time set-up with that device current
- *   (scratch address, operator tables); make it before any stream capture.
+ *   (scratch address, operator tables).  No call may be made while `stream` is
+ *   being captured into a CUDA graph: each call clears the scratch, reads an
+ *   error flag back and waits for the stream, and returns DSEM_ERR_INVALID_ARG
+ *   on a capturing stream.  Mortar rows that are not conforming mortars of
+ *   order p (len/lenmortar != p+1 or a conforming flag of 0) are refused with
+ *   DSEM_ERR_UNSUPPORTED; rows with ids, faces or orientations out of range
+ *   with DSEM_ERR_INVALID_ARG.
  *   Every call shares the scratch array and leaves its contents behind: calls
  *   whose work overlaps on the GPU race on it.  The call runs on `stream`
  *   (cudaStream_t, NULL = default stream) and waits for it before returning. */

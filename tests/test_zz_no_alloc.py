@@ -78,12 +78,17 @@ def test_noalloc_matches_rhs_twice(lib, n, p):
 
 
 def test_noalloc_rejects_oversized_mesh(lib):
-    """Sizes beyond the static scratch are refused with a clear message, before any device work."""
+    """Sizes beyond the static scratch are refused with a clear message, before any device work.
+    The buffers are real (one double each), so even a call that went past the size check could
+    only fail, never touch an invalid address."""
+    import torch
     p = 8
     nel = 96  # 96 * (90*81 + 5*729) + 1 > 2^20
-    rc = lib.dsem_rhs_noalloc(nel, p, 0, None, None, None, C.c_void_p(1), C.c_void_p(1), C.c_void_p(1),
-                              C.c_void_p(1), C.c_double(1.4), C.c_double(1600.0), C.c_double(0.72), C.c_double(1.0),
-                              C.c_void_p(1), None)
+    bufs = [torch.zeros(1, dtype=torch.float64, device="cuda") for _ in range(5)]
+    dp = lambda t: C.c_void_p(t.data_ptr())
+    rc = lib.dsem_rhs_noalloc(nel, p, 0, None, None, None, dp(bufs[0]), dp(bufs[1]), dp(bufs[2]), dp(bufs[3]),
+                              C.c_double(1.4), C.c_double(1600.0), C.c_double(0.72), C.c_double(1.0), dp(bufs[4]),
+                              None)
     assert rc == -1
     assert b"too large" in lib.dsem_last_error(None)
 
@@ -101,5 +106,23 @@ def test_noalloc_rejects_out_of_range_mortar_rows(lib, field, value):
     rc, _ = call_noalloc(lib, box, arrs, torch, 3)
     assert rc == -1
     assert b"out of range" in lib.dsem_last_error(None)
+    rc, _ = call_noalloc(lib, box, internal_arrays(box, mesh.taylor_green(box)), torch, 3)
+    assert rc == 0
+
+
+@pytest.mark.parametrize("field,value", [(13, 0), (16, 0), (4, 3), (8, 5)])
+def test_noalloc_rejects_nonconforming_rows(lib, field, value):
+    """A row that dsem_rhs would send through the p-nonconforming projections (a conforming
+    flag of 0) or whose lengths do not match the order is refused, not evaluated as a
+    conforming mortar; the next call with valid rows succeeds."""
+    import torch
+    box = mesh.Box(2, 2, 2, 3)
+    arrs = internal_arrays(box, mesh.taylor_green(box))
+    rows = arrs["mortar"].reshape(box.nmort, -1).copy()
+    rows[2, field] = value
+    arrs["mortar"] = rows
+    rc, _ = call_noalloc(lib, box, arrs, torch, 3)
+    assert rc == -5
+    assert b"conforming" in lib.dsem_last_error(None)
     rc, _ = call_noalloc(lib, box, internal_arrays(box, mesh.taylor_green(box)), torch, 3)
     assert rc == 0
