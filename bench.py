@@ -13,8 +13,15 @@ the whole mesh.  Metric: DOF-RK-stages/s = unknowns x 5 x steps / seconds.
 
 value : device-resident throughput, CUDA events on the library's stream
         around exactly K steps (CUDA graph per step), max over ranks.
-e2e   : the same metric through the C-ABI with host buffers: each step uploads
-        the state from pinned host memory, advances one step and downloads it.
+e2e   : the same metric through the C-ABI with host buffers, one context:
+        each step uploads the state from pinned host memory, advances one step
+        and downloads it.  e2e_concurrent: three contexts (three copies of the
+        case) on three host threads, whose copies overlap each other's steps.
+At N = 1 the line also carries the other two parts of the metric: "ensemble"
+(the cfg-4 64-case ensemble against the same cases one by one) and "adjoint"
+(the cfg-5 adjoint/forward time ratio at 20 snapshots, the store-all variant
+beside it, and GPU central differences along 8 seeded directions), each with
+its own clock record.  --no-extras leaves them out.
 Multi-GPU (torchrun): replicas only -- every rank advances its own copy of the
 case, no data-path collective; value sums the ranks' unknowns.
 
@@ -61,6 +68,9 @@ def parse():
     ap.add_argument("--p", type=int, default=P)
     ap.add_argument("--workload", default="tgv", choices=["tgv", "ensemble", "adjoint"])
     ap.add_argument("--fd-check", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default workload: leave out the ensemble and adjoint objects of the line")
+    ap.add_argument("--ens-steps", type=int, default=10, help="ensemble object: timed steps")
     ap.add_argument("--cases", type=int, default=64)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--adj-steps", type=int, default=400, help="adjoint workload: steps of the run")
@@ -282,56 +292,69 @@ def ensemble_inputs(cases, seed):
     return descs, qs, np.array(dts)
 
 
-def run_ensemble(args):
+def measure_ensemble(args, steps, warmup):
+    """cfg 4: the 64-case ensemble in one context against the same cases run one by one.
+    Returns the ensemble object of the bench line."""
     import torch
     from dsem_b200.solver import Ensemble, Solver
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     cases = ensemble_cases(args.cases, args.seed)
     descs, qs, dts = ensemble_inputs(cases, args.seed)
     dof = np.array([5 * int(d["ngrid"]) * (c[1] + 1) ** 3 for d, c in zip(descs, cases)])
-    work = float(dof.sum()) * STAGES * args.steps
+    work = float(dof.sum()) * STAGES * steps
     # one ensemble context
     ens = Ensemble(descs, [c[2] for c in cases])
     for k, q in enumerate(qs):
         ens.upload_case(k, q)
     shapes, _ = ens.autotune(reps=3)  # launch shape of the volume kernel per order (untimed)
-    ens.step_batch(dts, args.warmup)
+    ens.step_batch(dts, warmup)
     torch.cuda.synchronize()
     with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
-        ens.step_batch(dts, args.steps)
+        ens.step_batch(dts, steps)
     ms_b, launches_b = ens.last_timing()
     ens.close()
-    # the same cases one after another
+    # the same cases one after another, each with the launch shape the ensemble's tuner chose for its order
     ms_s, launches_s = 0.0, 0
     for d, q, dt, c in zip(descs, qs, dts, cases):
         s = Solver(d, re=c[2])
         s.upload(q)
-        s.autotune(reps=3)
-        s.step(dt, args.warmup)
-        s.step(dt, args.steps)
+        s.set_vol_variant(c[1], shapes[c[1]])
+        s.step(dt, warmup)
+        s.step(dt, steps)
         m, n = s.last_timing()
         ms_s += m
         launches_s += n
         s.close()
-    out = {"metric": "DOF-RK-stages/s FP64, 64-case ensemble", "value": work / (ms_b * 1e-3),
-           "unit": "DOF-RK-stages/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": ms_b / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f64", "data": "synthetic (seeded Taylor-Green / isotropic initial conditions)",
-           "config": {"workload": f"ensemble of {len(cases)} cases, seed {args.seed}: E in 4^3..12^3, p in 4/6/8, "
-                                  "Re U[400,3200], Mach U[0.05,0.3]", "cases": len(cases),
-                      "unknowns": int(dof.sum()), "elements": int(sum(int(d["ngrid"]) for d in descs)),
-                      "volume_launch_shape_per_p": {str(k): v for k, v in shapes.items()}},
-           "sequential": {"value": work / (ms_s * 1e-3), "ms_per_step": ms_s / args.steps,
-                          "gpu_launches": launches_s},
-           "speedup_vs_sequential": ms_s / ms_b, "gpu_launches": launches_b, "clocks": clk.summary()}
+    return {"metric": "DOF-RK-stages/s FP64, 64-case ensemble", "value": work / (ms_b * 1e-3),
+            "unit": "DOF-RK-stages/s", "steps": steps, "warmup": warmup, "ms_per_step": ms_b / steps,
+            "workload": f"ensemble of {len(cases)} cases, seed {args.seed}: E in 4^3..12^3, p in 4/6/8, "
+                        "Re U[400,3200], Mach U[0.05,0.3]", "cases": len(cases),
+            "unknowns": int(dof.sum()), "elements": int(sum(int(d["ngrid"]) for d in descs)),
+            "volume_launch_shape_per_p": {str(k): v for k, v in shapes.items()},
+            "sequential": {"value": work / (ms_s * 1e-3), "ms_per_step": ms_s / steps, "gpu_launches": launches_s},
+            "speedup_vs_sequential": ms_s / ms_b, "gpu_launches": launches_b, "clocks": clk.summary()}
+
+
+def run_ensemble(args):
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    e = measure_ensemble(args, args.steps, args.warmup)
+    out = {"metric": e["metric"], "value": e["value"], "unit": e["unit"], "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": e["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Taylor-Green / isotropic initial conditions)",
+           "config": {"workload": e["workload"], "cases": e["cases"], "unknowns": e["unknowns"],
+                      "elements": e["elements"], "volume_launch_shape_per_p": e["volume_launch_shape_per_p"]},
+           "sequential": e["sequential"], "speedup_vs_sequential": e["speedup_vs_sequential"],
+           "gpu_launches": e["gpu_launches"], "clocks": e["clocks"]}
     print(json.dumps(out), flush=True)
 
 
-def run_adjoint(args):
-    import torch
+def measure_adjoint(args, fd_check):
+    """cfg 5: adjoint / forward time ratio at 20 binomial snapshots (the stated
+    configuration) and with every stage state kept; optional GPU central
+    differences along 8 seeded directions and in 1/Re.  Returns the adjoint
+    object of the bench line."""
     from dsem_b200 import mesh
     from dsem_b200.solver import Solver
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     nex, p, nsteps, window = 12, 6, args.adj_steps, min(args.adj_window, args.adj_steps)
     box = mesh.Box(nex, nex, nex, p)
     q = mesh.perturbed_taylor_green(box, seed=args.seed)
@@ -340,26 +363,32 @@ def run_adjoint(args):
     s.upload(q)
     s.step(dt, 3)  # warm-up (graph capture), then back to the initial state
     s.upload(q)
-    s.step(dt, nsteps)
-    fwd_ms, _ = s.last_timing()
-    s.upload(q)
-    out = {"metric": f"adjoint / forward time, {nsteps} steps", "unit": "ratio", "n_gpus": 1, "higher_is_better": False,
-           "dtype": "f64", "data": "synthetic (Taylor-Green + seeded 5% isotropic perturbation)",
-           "config": {"workload": f"perturbed taylor-green {nex}^3 hex p={p}, Re=1600, {nsteps} steps, J = sum eps dt "
-                                  f"over the last {window}", "unknowns": 5 * box.nel * (p + 1) ** 3},
-           "forward_ms": fwd_ms}
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    out = {"metric": f"adjoint / forward time, {nsteps} steps, 20 snapshots", "unit": "ratio",
+           "higher_is_better": False,
+           "workload": f"perturbed taylor-green {nex}^3 hex p={p}, Re=1600, {nsteps} steps, J = sum eps dt "
+                       f"over the last {window}, revolve checkpointing at 20 stored states",
+           "unknowns": 5 * box.nel * (p + 1) ** 3}
     res = {}
-    for snaps in (0, 20):
-        J, g, lr, ms = s.adjoint(dt, nsteps, window, snapshots=snaps)
-        res[snaps] = (J, g, lr, ms)
-        out[f"adjoint_ms_snapshots_{snaps}"] = ms
-        out[f"ratio_snapshots_{snaps}"] = ms / fwd_ms
-    out["value"] = out["ratio_snapshots_0"]
-    J, g, lr, _ = res[0]
+    with Clocks(dev) as clk:
+        s.step(dt, nsteps)
+        fwd_ms, _ = s.last_timing()
+        out["forward_ms"] = fwd_ms
+        for snaps in (20, 0):
+            s.upload(q)
+            J, g, lr, ms = s.adjoint(dt, nsteps, window, snapshots=snaps)
+            res[snaps] = (J, g, lr, ms)
+            out[f"adjoint_ms_snapshots_{snaps}"] = ms
+            out[f"ratio_snapshots_{snaps}"] = ms / fwd_ms
+    out["clocks"] = clk.summary()
+    out["value"] = out["ratio_snapshots_20"]
+    out["store_all_variant"] = {"value": out["ratio_snapshots_0"],
+                                "note": "every stage state and its face traces kept in HBM (snapshots = 0)"}
+    J, g, lr, _ = res[20]
     out["J"] = J
     out["dJ_dinvRe"] = lr
     out["gradients_identical_across_checkpointing"] = bool(np.array_equal(res[0][1], res[20][1]))
-    if args.fd_check:  # central differences on the GPU along 8 seeded directions
+    if fd_check:  # central differences on the GPU along 8 seeded directions
         rng = np.random.default_rng(2024)
         G = p + 1
         rel = []
@@ -384,8 +413,21 @@ def run_adjoint(args):
             Jr.append(sr.adjoint(dt, nsteps, window, want_grad=False)[0])
             sr.close()
         fdr = (Jr[0] - Jr[1]) / (2 * hr)
-        out["fd_check"] = {"directions": 8, "max_rel_err_q0": max(rel), "rel_err_inv_re": abs(lr - fdr) / abs(fdr)}
+        out["fd_check"] = {"directions": 8, "step": h, "max_rel_err_q0": max(rel),
+                           "rel_err_inv_re": abs(lr - fdr) / abs(fdr)}
     s.close()
+    return out
+
+
+def run_adjoint(args):
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    a = measure_adjoint(args, args.fd_check)
+    out = {"metric": a["metric"], "value": a["value"], "unit": "ratio", "n_gpus": 1, "higher_is_better": False,
+           "dtype": "f64", "data": "synthetic (Taylor-Green + seeded 5% isotropic perturbation)",
+           "config": {"workload": a["workload"], "unknowns": a["unknowns"]}}
+    out.update({k: v for k, v in a.items() if k not in ("metric", "value", "unit", "higher_is_better", "workload",
+                                                        "unknowns")})
     print(json.dumps(out), flush=True)
 
 
@@ -444,24 +486,15 @@ def main():
     ms_max = float(t.item())
     value = world * dof * STAGES * args.steps / (ms_max * 1e-3)
 
-    # ---- end to end through the C-ABI with host buffers (pinned), ldx = nx = p+2.  NCTX
-    # contexts, each driven by its own host thread (one context per thread is the C-ABI's
-    # threading model); every step of each: its state from pinned host memory to the device,
-    # one RK step, the state back to pinned host memory.  The contexts' copies overlap the
-    # others' compute (a step moves ~0.85 GB over the host link and computes for ~13 ms).
+    # ---- end to end through the C-ABI with host buffers (pinned), ldx = nx = p+2: every step,
+    # the state from pinned host memory to the device, one RK step, the state back to pinned
+    # host memory.  Headline (e2e): one context, the drop-in's model (one context per rank),
+    # where each step's copies and compute run one after another.  Beside it (e2e_concurrent):
+    # NCTX contexts on NCTX host threads (the C-ABI's threading model), each its own copy of
+    # the case, so that one context's copies overlap the others' compute.
     import threading
     NCTX = 3
     ldx = G + 1
-    ctxs = [s]
-    for _ in range(NCTX - 1):
-        sx = Solver(desc, re=RE)
-        sx.upload(q)
-        sx.set_vol_variant(args.p, shapes[args.p])
-        ctxs.append(sx)
-    hqs = [torch.empty((box.nel, 5, ldx, ldx, ldx), dtype=torch.float64, pin_memory=True) for _ in range(NCTX)]
-    hq_nps = [h.numpy() for h in hqs]
-    for sv, h in zip(ctxs, hq_nps):
-        sv.download(out=h)
     k_e2e = max(1, min(args.steps, 10))
 
     def serve(solver, hq_np, n):
@@ -470,20 +503,35 @@ def main():
             solver.step(dt, 1)
             solver.download(out=hq_np)
 
+    def timed_e2e(ctxs, hq_nps):
+        barrier()
+        t0 = time.perf_counter()
+        workers = [threading.Thread(target=serve, args=(sv, h, k_e2e)) for sv, h in zip(ctxs, hq_nps)]
+        for w in workers:
+            w.start()
+        for w in workers:
+            w.join()
+        barrier()
+        te = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        return world * dof * STAGES * len(ctxs) * k_e2e / float(te.item())
+
+    hqs = [torch.empty((box.nel, 5, ldx, ldx, ldx), dtype=torch.float64, pin_memory=True) for _ in range(NCTX)]
+    hq_nps = [h.numpy() for h in hqs]
+    s.download(out=hq_nps[0])
+    serve(s, hq_nps[0], 1)  # warm-up of the host path
+    e2e_single = timed_e2e([s], hq_nps[:1])
+    ctxs = [s]
+    for _ in range(NCTX - 1):
+        sx = Solver(desc, re=RE)
+        sx.upload(q)
+        sx.set_vol_variant(args.p, shapes[args.p])
+        ctxs.append(sx)
     for sv, h in zip(ctxs[1:], hq_nps[1:]):
+        sv.download(out=h)
         serve(sv, h, 1)  # warm-up of the other contexts (graph capture)
-    barrier()
-    t0 = time.perf_counter()
-    workers = [threading.Thread(target=serve, args=(sv, h, k_e2e)) for sv, h in zip(ctxs, hq_nps)]
-    for w in workers:
-        w.start()
-    for w in workers:
-        w.join()
-    barrier()
-    te = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e = world * dof * STAGES * NCTX * k_e2e / float(te.item())
+    e2e_conc = timed_e2e(ctxs, hq_nps)
     nbytes = hq_nps[0].nbytes
     for sv in ctxs[1:]:
         sv.close()
@@ -498,7 +546,7 @@ def main():
         achieved = vol_flops(G) * box.nel / t_vol / 1e12
         hbm_ach = vol_bytes(G) * box.nel / t_vol / 1e9
         tr = profiled_traffic()
-        roof = {"bound": "tensor", "pipe": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+        roof = {"bound": "fp64", "pipe": "fp64 (DFMA, SIMT)", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp64_peak, "kernel": "k_vol_diag (volume kernel, diagonal metrics)",
                 "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                 "traffic": (tr["bytes_per_launch"] if tr else None),
@@ -519,14 +567,24 @@ def main():
                           "stage_tflops_fp64": step_tf,
                           "volume_launch_shape": {"chosen": shapes[args.p],
                                                   "ms_per_shape": [round(float(x), 4) for x in shape_ms[args.p - 1]]}},
-               "e2e": {"value": e2e, "unit": "DOF-RK-stages/s", "h2d_bytes_per_step": nbytes,
-                       "d2h_bytes_per_step": nbytes, "steps": NCTX * k_e2e,
-                       "driver": f"{NCTX} contexts on {NCTX} host threads, upload + step + download per step"},
+               "e2e": {"value": e2e_single, "unit": "DOF-RK-stages/s", "h2d_bytes_per_step": nbytes,
+                       "d2h_bytes_per_step": nbytes, "steps": k_e2e,
+                       "driver": "one context: upload + step + download per step, one after another"},
+               "e2e_concurrent": {"value": e2e_conc, "unit": "DOF-RK-stages/s", "h2d_bytes_per_step": nbytes,
+                                  "d2h_bytes_per_step": nbytes, "steps": NCTX * k_e2e,
+                                  "driver": f"{NCTX} contexts (three copies of the case) on {NCTX} host threads, "
+                                            "upload + step + download per step; copies overlap other contexts' steps"},
                "gpu_launches": launches, "clocks": clk.summary(), "roofline": roof}
         if world == 1:
             out["cpu_baseline"] = cpu_baseline(desc, q, dt, dof)
-        print(json.dumps(out), flush=True)
     s.close()
+    if rank == 0 and world == 1 and not args.no_extras:
+        # the other two parts of the metric: batched-ensemble speed-up (cfg 4) and the
+        # adjoint/forward time ratio at 20 snapshots (cfg 5), each with its own clock record
+        out["ensemble"] = measure_ensemble(args, args.ens_steps, args.warmup)
+        out["adjoint"] = measure_adjoint(args, fd_check=True)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -15,6 +15,7 @@
 
 #include "../../include/dsem_gpu.h"
 #include "dsem_ctx.h"
+#include "dsem_lobatto.cuh"
 #include "dsem_host_math.h"
 #include "dsem_launch.h"
 #include "dsem_stage.cuh"
@@ -358,9 +359,29 @@ int enqueue_update(dsem_ctx *c, int kk, double *qt_out, long long *launches) {
   return DSEM_OK;
 }
 
+// the Lobatto arrays of the stage about to run (its state and averaged face
+// traces) into c->QLB (d%Qlgg/Qglg/Qggl of the last stage, for the restart file)
+int enqueue_lob_keep(dsem_ctx *c, long long *launches) {
+  const int r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
+    auto &g = c->groups[j];
+    LobArgs a{};
+    a.JQ = c->JQ + g.q0;
+    a.sq = 5LL * g.G * g.G * g.G;
+    a.jac = g.jac;
+    a.QF = c->QF + g.f0;
+    a.QLB = c->QLB + g.l0;
+    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::lob_keep(a, g.nel, st); }));
+    return DSEM_OK;
+  });
+  if (r) return r;
+  *launches += (long long)c->groups.size();
+  return DSEM_OK;
+}
+
 int enqueue_stage(dsem_ctx *c, int kk, bool save, double *qt_out, long long *launches) {
   int r;
   if ((r = enqueue_face_inv(c, launches))) return r;
+  if (kk == c->kord && c->keep_lob && (r = enqueue_lob_keep(c, launches))) return r;
   if ((r = enqueue_vol(c, save, launches))) return r;
   if ((r = enqueue_face_vis(c, launches))) return r;
   return enqueue_update(c, kk, qt_out, launches);
@@ -1070,6 +1091,7 @@ void dsem_destroy(dsem_ctx *c) {
     cudaFree(bl.qext);
     cudaFree(bl.fvext);
   }
+  cudaFree(c->QLB);
   cudaFree(c->JQ);
   cudaFree(c->gQ);
   cudaFree(c->QTI);
@@ -1146,6 +1168,7 @@ int set_dt(dsem_ctx *c, const double *dt) {
 }
 
 int step_impl(dsem_ctx *c, int nsteps) {
+  const int nsteps0 = nsteps;
   long long l = 0;
   int r;
   if (!c->traces_valid && (r = enqueue_traces(c, &l))) return r;
@@ -1162,7 +1185,8 @@ int step_impl(dsem_ctx *c, int nsteps) {
   }
   long long launches = per_step;
   if (nsteps > 0) {
-    const int key = (save ? 1 : 0) | (c->ev_grad_valid ? 2 : 0) | (c->grad_valid ? 4 : 0) | (c->les ? 8 : 0);
+    const int key = (save ? 1 : 0) | (c->ev_grad_valid ? 2 : 0) | (c->grad_valid ? 4 : 0) | (c->les ? 8 : 0) |
+                    (c->keep_lob ? 16 : 0);
     if (!c->gexec || c->graph_key != key) {
       if (c->gexec) cudaGraphExecDestroy(c->gexec);
       c->gexec = nullptr;
@@ -1191,6 +1215,7 @@ int step_impl(dsem_ctx *c, int nsteps) {
   c->last_ms = ms;
   c->last_launches = launches;
   if (save) c->grad_valid = true;
+  if (c->keep_lob && nsteps0 > 0) c->lob_valid = true;
   return check_flag(c);
 }
 
@@ -1267,8 +1292,25 @@ int dsem_stage(dsem_ctx *c, double time, double dt, int kk, double *Qt, int ldx)
   if (r) return r;
   c->grad_valid = true;
   c->ev_grad_valid = c->shock != 0;
+  if (kk == c->kord && c->keep_lob) c->lob_valid = true;
   if (Qt && (r = unpack_to_host(c, c->Qt, Qt, ldx, 5, state_offs(c)))) return r;
   return check_flag(c);
+}
+
+int dsem_keep_lobatto(dsem_ctx *c, int on) {
+  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (c->ncut) return fail(c, DSEM_ERR_UNSUPPORTED, "sharded contexts do not keep Lobatto arrays");
+  if (on && !c->QLB) {
+    long long n = 0;
+    for (auto &g : c->groups) {
+      g.l0 = n;
+      n += (long long)g.nel * 15 * (g.G + 1) * g.G * g.G;
+    }
+    CK(cudaMalloc(&c->QLB, (size_t)std::max(n, 1LL) * sizeof(double)));
+  }
+  c->keep_lob = on != 0;
+  c->lob_valid = false;
+  return DSEM_OK;
 }
 
 int dsem_step(dsem_ctx *c, double time, double dt, int nsteps) {
@@ -1375,7 +1417,9 @@ int dsem_shard_info(const dsem_ctx *c, int *nghost, int *doubles_per_face, doubl
   return DSEM_OK;
 }
 
-int dsem_shard_stage(dsem_ctx *c, double dt, int kk, int phase) {
+namespace {
+// Enqueues one phase of a sharded stage on the context's stream (no wait).
+int shard_enqueue(dsem_ctx *c, double dt, int kk, int phase) {
   if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
   if (kk < 1 || kk > c->kord || phase < 0 || phase > 2)
     return fail(c, DSEM_ERR_INVALID_ARG, "stage index outside 1..kord or phase outside 0..2");
@@ -1408,11 +1452,30 @@ int dsem_shard_stage(dsem_ctx *c, double dt, int kk, int phase) {
       const bool save = c->shock || c->keep_grad || c->les;
       c->grad_valid = c->grad_valid || save;
       c->ev_grad_valid = c->ev_grad_valid || c->shock;
-      CK(cudaStreamSynchronize(c->st));
-      return check_flag(c);
     }
   }
+  return DSEM_OK;
+}
+}  // namespace
+
+int dsem_shard_stage(dsem_ctx *c, double dt, int kk, int phase) {
+  int r = shard_enqueue(c, dt, kk, phase);
+  if (r) return r;
+  if (phase == 2 && kk == c->kord) return check_flag(c);
   CK(cudaStreamSynchronize(c->st));
+  return DSEM_OK;
+}
+
+int dsem_shard_enqueue(dsem_ctx *c, double dt, int kk, int phase) { return shard_enqueue(c, dt, kk, phase); }
+
+int dsem_shard_finish(dsem_ctx *c) {
+  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  return check_flag(c);
+}
+
+int dsem_get_stream(const dsem_ctx *c, void **stream) {
+  if (!c || !stream) return DSEM_ERR_INVALID_ARG;
+  *stream = static_cast<void *>(c->st);
   return DSEM_OK;
 }
 
@@ -1820,6 +1883,63 @@ int stage_io(dsem_ctx *c, int kk, bool save, const StageIO &io) {
   return DSEM_OK;
 }
 int set_dt(dsem_ctx *c, const double *dt) { return ::set_dt(c, dt); }
+// kept Lobatto arrays of caller element e: [3][5][L*G^2] at host + 15*L*G^2*e' (e' = running
+// offset over the caller's elements, returned by lob_offsets)
+std::vector<long long> lob_offsets(const dsem_ctx *c) {
+  std::vector<long long> off(c->ngrid + 1, 0);
+  for (int e = 0; e < c->ngrid; ++e) {
+    const int G = c->groups[c->ext_group[e]].G;
+    off[e + 1] = off[e] + 15LL * (G + 1) * G * G;
+  }
+  return off;
+}
+int lob_download(dsem_ctx *c, double *host) {
+  if (!c->QLB || !c->lob_valid) return fail(c, DSEM_ERR_INVALID_ARG, "no kept Lobatto arrays (dsem_keep_lobatto, then step)");
+  const auto off = lob_offsets(c);
+  for (int e = 0; e < c->ngrid; ++e) {
+    const Group &g = c->groups[c->ext_group[e]];
+    const long long n = 15LL * (g.G + 1) * g.G * g.G;
+    CK(cudaMemcpyAsync(host + off[e], c->QLB + g.l0 + (long long)c->ext_k[e] * n, n * sizeof(double),
+                       cudaMemcpyDeviceToHost, c->st));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return DSEM_OK;
+}
+// Lobatto arrays of every caller element (lob_offsets layout) to the device, and the saved
+// gradients rebuilt from them: the next step's entropy viscosity / Smagorinsky model use them
+int lob_upload_grad(dsem_ctx *c, const double *host) {
+  if (!c->QLB) {
+    int r = dsem_keep_lobatto(c, 1);
+    if (r) return r;
+    c->keep_lob = false;
+  }
+  const auto off = lob_offsets(c);
+  for (int e = 0; e < c->ngrid; ++e) {
+    const Group &g = c->groups[c->ext_group[e]];
+    const long long n = 15LL * (g.G + 1) * g.G * g.G;
+    CK(cudaMemcpyAsync(c->QLB + g.l0 + (long long)c->ext_k[e] * n, host + off[e], n * sizeof(double),
+                       cudaMemcpyHostToDevice, c->st));
+  }
+  for (auto &g : c->groups) {
+    LobArgs a{};
+    a.gg = g.gg;
+    a.QLB = c->QLB + g.l0;
+    a.EVB = g.EVB;
+    a.gamma = c->P.gamma;
+    CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::lob_grad(a, g.nel, g.diag, c->st); }));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  c->grad_valid = true;
+  c->ev_grad_valid = true;
+  c->lob_valid = true;
+  return DSEM_OK;
+}
+// the saved gradients are not valid (a restart file whose Lobatto arrays were never computed)
+void grad_invalidate(dsem_ctx *c) {
+  c->grad_valid = false;
+  c->ev_grad_valid = false;
+  c->lob_valid = false;
+}
 int unpack_state(dsem_ctx *c, const double *dev, double *host, int ldx) {
   return unpack_to_host(c, dev, host, ldx, 5, state_offs(c));
 }

@@ -35,6 +35,7 @@ struct Group {
   double *jac = nullptr, *gg = nullptr, *gm = nullptr, *hd = nullptr;
   double *muhg = nullptr, *EVB = nullptr, *kew = nullptr;
   double *nuhg = nullptr;  // Smagorinsky viscosity at Gauss points (LES on)
+  long long l0 = 0;        // offset of the group's kept Lobatto arrays in dsem_ctx::QLB (doubles)
   int *int2ext = nullptr;  // device: caller element id of each group element
   int *ecase = nullptr;    // device: case of each group element
   std::vector<int> case_lo, case_hi;  // group elements [lo, hi) of each case
@@ -92,6 +93,10 @@ struct dsem_ctx {
   bool grad_valid = false;     // EVB holds the Q gradients of the last Fluxes call
   bool ev_grad_valid = false;  // ... and the temperature gradients (EV)
   int keep_grad = 0;
+  // Lobatto arrays of the last stage (DSEM's d%Qlgg/Qglg/Qggl) kept for the restart file
+  double *QLB = nullptr;  // [elem][3][5][L*G^2] per group at Group::l0
+  bool keep_lob = false;  // the last stage of every step stores them (dsem_keep_lobatto)
+  bool lob_valid = false; // QLB holds the arrays of the last stage run
   cudaGraphExec_t gexec = nullptr;
   int graph_key = -1;
   long long graph_launches = 0;
@@ -139,6 +144,11 @@ int stage_io(dsem_ctx *c, int kk, bool save, const StageIO &io);  // out-of-plac
 int set_dt(dsem_ctx *c, const double *dt);
 int unpack_state(dsem_ctx *c, const double *dev, double *host, int ldx);
 int check_flag(dsem_ctx *c);
+// kept Lobatto arrays (dsem_keep_lobatto): per caller element [3][5][L*G^2] at lob_offsets()[e]
+std::vector<long long> lob_offsets(const dsem_ctx *c);
+int lob_download(dsem_ctx *c, double *host);
+int lob_upload_grad(dsem_ctx *c, const double *host);
+void grad_invalidate(dsem_ctx *c);
 // enstrophy sums of the last saved gradients with the state jq (null: c->JQ)
 int eps_sums(dsem_ctx *c, double *s, double *s2, const double *jq = nullptr);
 // the same in two halves: per-element partials into device memory part

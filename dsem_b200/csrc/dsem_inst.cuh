@@ -3,6 +3,7 @@
 #include "dsem_launch.h"
 #include "dsem_stage.cuh"
 #include "dsem_vol_diag.cuh"
+#include "dsem_lobatto.cuh"
 
 namespace dsem {
 
@@ -86,6 +87,21 @@ template <int G> cudaError_t Launch<G>::update(const UpdArgs &a, int nel, cudaSt
 template <int G> cudaError_t Launch<G>::trace(const TraceArgs &a, int nel, cudaStream_t s) {
   if (nel <= 0) return cudaSuccess;
   k_trace<G><<<nel, 256, sizeof(double) * 5 * G * G * G, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int G> cudaError_t Launch<G>::lob_keep(const LobArgs &a, int nel, cudaStream_t s) {
+  if (nel <= 0) return cudaSuccess;
+  k_lob_keep<G><<<nel, 256, sizeof(double) * 5 * G * G * G, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int G> cudaError_t Launch<G>::lob_grad(const LobArgs &a, int nel, bool diag, cudaStream_t s) {
+  if (nel <= 0) return cudaSuccess;
+  if (diag)
+    k_lob_grad<G, true><<<nel, 256, 0, s>>>(a);
+  else
+    k_lob_grad<G, false><<<nel, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

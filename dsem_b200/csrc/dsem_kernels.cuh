@@ -85,6 +85,17 @@ __device__ __forceinline__ void prefetch_l2(const double *p, int n, int tid, int
   }
 }
 
+// One bulk L2 prefetch (cp.async.bulk.prefetch, a single instruction) of the
+// n doubles at p.  The range is shrunk to whole 16-byte chunks inside
+// [p, p + n): the start is rounded up and the end down, so nothing outside the
+// array is touched; at most 8 bytes at either end are not prefetched.
+__device__ __forceinline__ void prefetch_l2_bulk(const double *p, int n) {
+  const unsigned long long a = reinterpret_cast<unsigned long long>(p);
+  const unsigned long long lo = (a + 15ULL) & ~15ULL, hi = (a + 8ULL * (unsigned long long)n) & ~15ULL;
+  if (hi > lo)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((unsigned)(hi - lo)) : "memory");
+}
+
 // ------------------------------------------------------------ line helpers
 // Line (a,b) of direction d.  Gauss arrays: base/stride; grid-d arrays: base/stride.
 template <int G> __device__ __forceinline__ int gbase(int d, int a, int b) {

@@ -17,6 +17,7 @@ struct MortarC;
 struct MortarCut;
 struct MortarB;
 struct BndPhys;
+struct LobArgs;
 
 // A kernel's dynamic shared-memory limit is a per-device setting: raises it to
 // smem on the current device the first time that device launches kern (mask:
@@ -47,6 +48,9 @@ template <int G> struct Launch {
   static int vol_variant_threads(int v);    // threads per element of shape v
   static cudaError_t update(const UpdArgs &a, int nel, cudaStream_t s);
   static cudaError_t trace(const TraceArgs &a, int nel, cudaStream_t s);
+  // Lobatto arrays of the stage kept in a.QLB; gradients rebuilt from them into a.EVB
+  static cudaError_t lob_keep(const LobArgs &a, int nel, cudaStream_t s);
+  static cudaError_t lob_grad(const LobArgs &a, int nel, bool diag, cudaStream_t s);
   static cudaError_t ev(const EvArgs &a, int nel, cudaStream_t s);
   static cudaError_t les(const LesArgs &a, int nel, cudaStream_t s);
   static cudaError_t face_inv(const MortarC *mc, int nm, double *QF, double *FF, const double *nh, const double *nrm,

@@ -15,8 +15,10 @@ Drivers
   ShardedRun   all shards in one process on one GPU, the exchange a device
                copy (used by the tests: the sharded run must reproduce the
                single-context run bit for bit);
-  run_rank     one shard per process and GPU under torch.distributed, the
-               exchange NCCL send/recv of the blocks over NVLink.
+  run_rank     one shard per process under torch.distributed: with NCCL
+               (one GPU per rank) the blocks move by send/recv ordered on the
+               library's stream, with gloo they are staged through host
+               memory (the form the tests run, two ranks on one GPU).
 """
 import numpy as np
 
@@ -207,32 +209,80 @@ class ShardedRun:
         return tot
 
 
-def run_rank(desc, part, rank, JQ, dt, nsteps, **phys):
-    """This process's shard under torch.distributed (one GPU per rank, NCCL):
-    advances nsteps and returns the shard's final state and element ids."""
+def _diag_sums(solver):
+    import ctypes as C
+    v = (C.c_double * 7)()
+    _check(solver, lib().dsem_diag_sums(solver.h, v))
+    return np.array(v[:])
+
+
+def run_rank(desc, part, rank, JQ, dt, nsteps, diag=False, **phys):
+    """This process's shard under torch.distributed (initialised by the caller):
+    advances nsteps and returns (the shard's final state, its global element ids,
+    the all-reduced diagnostic sums or None).
+
+    The exchange after phases 0 and 1 of every stage (send_q_to_mortars_mpi,
+    send_flux_to_mortars_mpi: send_q.f90:771-895, send_flux.f90:464-692):
+      nccl  one send/recv per neighbour block, issued on the library's own CUDA
+            stream (dsem_get_stream, a torch external stream) between the
+            enqueued phases (dsem_shard_enqueue): no host wait inside a step; the
+            step ends with one dsem_shard_finish (its non-finite check);
+      gloo  (a CPU transport, e.g. ranks that share one GPU) the blocks are
+            staged through host memory; copies run on the library's stream.
+    diag: the shard keeps the last stage's gradients; after the last step its
+    seven diagnostic sums are added over the ranks (all-reduce), element-1
+    jacobian and validity taken from rank 0, as dsem_diag_sums documents."""
+    import ctypes as C
+
     import torch
     import torch.distributed as dist
     p = partition(desc, part)[rank]
     s = Solver(p["desc"], **phys)
     s.upload(JQ[p["elements"]])
+    if diag:
+        _diag_sums(s)  # asks the shard to keep the last stage's gradients
     send, ghost, per = _buffers(s)
     L = lib()
+    nccl = dist.get_backend() == "nccl"
+    sp = C.c_void_p()
+    _check(s, L.dsem_get_stream(s.h, C.byref(sp)))
+    stream = torch.cuda.ExternalStream(sp.value)
 
     def exchange():
-        torch.cuda.synchronize()
-        ops = []
-        for nb, g0, n in p["plan"]:
-            ops.append(dist.P2POp(dist.isend, send[g0 * per:(g0 + n) * per].contiguous(), nb))
-            ops.append(dist.P2POp(dist.irecv, ghost[g0 * per:(g0 + n) * per], nb))
-        if ops:
-            for w in dist.batch_isend_irecv(ops):
-                w.wait()
-        torch.cuda.synchronize()
+        if not p["plan"]:
+            return
+        with torch.cuda.stream(stream):
+            if nccl:
+                ops = []
+                for nb, g0, n in p["plan"]:
+                    ops.append(dist.P2POp(dist.isend, send[g0 * per:(g0 + n) * per], nb))
+                    ops.append(dist.P2POp(dist.irecv, ghost[g0 * per:(g0 + n) * per], nb))
+                for w in dist.batch_isend_irecv(ops):
+                    w.wait()  # orders the library stream after the transfer; no host wait
+            else:
+                hs = send.cpu()  # waits for the stream (the packed blocks)
+                hg = torch.empty_like(hs)
+                reqs = []
+                for nb, g0, n in p["plan"]:
+                    reqs.append(dist.isend(hs[g0 * per:(g0 + n) * per], nb))
+                    reqs.append(dist.irecv(hg[g0 * per:(g0 + n) * per], nb))
+                for w in reqs:
+                    w.wait()
+                ghost.copy_(hg)
 
     for _ in range(nsteps):
         for kk in range(1, s.kord + 1):
             for phase in range(3):
-                _check(s, L.dsem_shard_stage(s.h, float(dt), kk, phase))
+                _check(s, L.dsem_shard_enqueue(s.h, float(dt), kk, phase))
                 if phase < 2:
                     exchange()
-    return s.download(), p["elements"]
+        _check(s, L.dsem_shard_finish(s.h))
+    sums = None
+    if diag:
+        a = _diag_sums(s)
+        t = torch.tensor(a[:5], dtype=torch.float64, device="cuda" if nccl else "cpu")
+        dist.all_reduce(t)
+        head = torch.tensor(a[5:], dtype=torch.float64, device=t.device)
+        dist.broadcast(head, 0)
+        sums = np.concatenate([t.cpu().numpy(), head.cpu().numpy()])
+    return s.download(), p["elements"], sums

@@ -20,7 +20,8 @@ EXPORTS = ("dsem_create", "dsem_destroy", "dsem_last_error", "dsem_upload_q", "d
            "dsem_create_batch", "dsem_batch_size", "dsem_upload_q_case", "dsem_download_q_case", "dsem_step_batch",
            "dsem_diag_batch", "dsem_adjoint", "dsem_set_les", "dsem_get_nut", "dsem_state_size",
            "dsem_save_state", "dsem_load_state", "dsem_shard_info", "dsem_shard_stage", "dsem_diag_sums",
-           "dsem_set_boundary", "dsem_autotune", "dsem_set_vol_variant")
+           "dsem_set_boundary", "dsem_autotune", "dsem_set_vol_variant", "dsem_shard_enqueue", "dsem_shard_finish",
+           "dsem_get_stream", "dsem_keep_lobatto", "dsem_write_restart", "dsem_read_restart")
 
 
 class DsemError(RuntimeError):
@@ -80,6 +81,12 @@ def lib(path=None):
         L.dsem_set_vol_variant.argtypes = [vp, C.c_int, C.c_int]
         L.dsem_shard_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(dp), C.POINTER(dp)]
         L.dsem_shard_stage.argtypes = [vp, C.c_double, C.c_int, C.c_int]
+        L.dsem_shard_enqueue.argtypes = [vp, C.c_double, C.c_int, C.c_int]
+        L.dsem_shard_finish.argtypes = [vp]
+        L.dsem_get_stream.argtypes = [vp, C.POINTER(vp)]
+        L.dsem_keep_lobatto.argtypes = [vp, C.c_int]
+        L.dsem_write_restart.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int, C.c_double]
+        L.dsem_read_restart.argtypes = [vp, C.c_char_p, C.c_int, C.POINTER(C.c_double)]
         L.dsem_diag_sums.argtypes = [vp, dp]
         L.dsem_state_size.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.dsem_save_state.argtypes = [vp, C.c_void_p, C.c_longlong]
@@ -182,6 +189,23 @@ class Solver:
         ms = np.zeros(4)
         self._check(lib().dsem_profile_rhs(self.h, int(reps), _dptr(ms)))
         return ms
+
+    def keep_lobatto(self, on=True):
+        """The last stage of every step keeps its Lobatto arrays (d%Qlgg/Qglg/Qggl) for restart files."""
+        self._check(lib().dsem_keep_lobatto(self.h, int(bool(on))))
+
+    def write_restart(self, template, out, time=0.0, max_materials=1):
+        """DSEM restart file `out`: `template` (a DSEM restart file of the same mesh) with this
+        context's state (dsem_write_restart)."""
+        self._check(lib().dsem_write_restart(self.h, str(template).encode(), str(out).encode(), int(max_materials),
+                                             float(time)))
+
+    def read_restart(self, path, max_materials=1):
+        """State (and, when present, the Lobatto arrays the next step's viscosity models read)
+        from a DSEM restart file; returns its time (dsem_read_restart)."""
+        t = C.c_double()
+        self._check(lib().dsem_read_restart(self.h, str(path).encode(), int(max_materials), C.byref(t)))
+        return t.value
 
     def save_state(self):
         """Snapshot of the device state (bytes) for dsem_load_state."""

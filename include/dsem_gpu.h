@@ -206,6 +206,44 @@ int dsem_set_boundary(dsem_ctx *ctx, double twall, const double *Qext, const dou
 int dsem_shard_info(const dsem_ctx *ctx, int *nghost, int *doubles_per_face, double **send, double **ghost);
 int dsem_shard_stage(dsem_ctx *ctx, double dt, int kk, int phase);
 int dsem_diag_sums(dsem_ctx *ctx, double *sums);
+/* Stream-ordered form of the same phases, for a caller that orders its
+ * exchange on the context's stream (an NCCL send/recv issued on that stream
+ * after phase 0 or 1 and before the next phase): dsem_shard_enqueue enqueues a
+ * phase and returns without waiting; dsem_shard_finish waits for the stream
+ * and reports a non-finite stage (DSEM_ERR_NONFINITE), once per step or
+ * before the state is read; dsem_get_stream returns the context's CUDA stream
+ * (a cudaStream_t).  No host round trip is needed between phases. */
+int dsem_shard_enqueue(dsem_ctx *ctx, double dt, int kk, int phase);
+int dsem_shard_finish(dsem_ctx *ctx);
+int dsem_get_stream(const dsem_ctx *ctx, void **stream);
+
+/* ---- DSEM restart files (write_restart / read_restart) ----
+ * Replace write_restart / read_restart (src/Parabolic3D/stac3m/restart.f90:
+ * 19-312, 319-929; called at 3DDriver_parfmdf.f90:516,622) for a context's
+ * state: the file is DSEM's own Fortran unformatted sequential layout (one
+ * record per WRITE, 4-byte lengths around each), so DSEM can restart from a
+ * file the library wrote and the library from a file DSEM wrote.
+ * dsem_keep_lobatto(ctx, 1): the last stage of every step also stores its
+ *   three Lobatto arrays (d%Qlgg, d%Qglg, d%Qggl), which the file carries for
+ *   the entropy viscosity of the next step (off by default; costs one extra
+ *   kernel per step and [elements][3][5][(p+2)(p+1)^2] doubles of memory).
+ * dsem_write_restart(ctx, template, out, max_materials, time): copies
+ *   `template` -- a restart file DSEM wrote for the same mesh, e.g. by the
+ *   serial zero-step run of its restart workflow -- record by record into
+ *   `out`, with each element's Q and g_Q, and its Lobatto arrays when kept,
+ *   taken from the device, and the time in the case record; every other
+ *   record passes through.  max_materials is size.f90's (1 in DSEM's cases).
+ * dsem_read_restart(ctx, path, max_materials, &time): uploads Q from the file;
+ *   when its Lobatto arrays were computed (a file written after a step), the
+ *   gradients the next step's entropy viscosity and Smagorinsky model read
+ *   are rebuilt from them, so the run continues as if it had not stopped;
+ *   zeroed arrays (DSEM's zero-step file) give a fresh start (mu_EV = 0 on
+ *   the first step).  One-case, unsharded contexts; the padding nx of the
+ *   file's (nx,nx,nx,5) arrays is read from the records. */
+int dsem_keep_lobatto(dsem_ctx *ctx, int on);
+int dsem_write_restart(dsem_ctx *ctx, const char *template_path, const char *out_path, int max_materials,
+                       double time);
+int dsem_read_restart(dsem_ctx *ctx, const char *path, int max_materials, double *time);
 
 /* ---- Ensembles: ncase independent runs in one context ----
  * No DSEM counterpart (DSEM runs one case per job; each would call tstep,

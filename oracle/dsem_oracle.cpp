@@ -2107,6 +2107,31 @@ void orc_get_q(const orc_case *h, double *JQ, int ldx) {
             JQ[e * NV * L3 + n + (size_t)ldx * (m + (size_t)ldx * (l + (size_t)ldx * v))] = E.Q[v * ng + gidx(G, n, m, l)];
   }
 }
+// Lobatto arrays of the last Fluxes call (d%Qlgg, d%Qglg, d%Qggl, the arrays
+// write_restart stores: Parabolic3D/stac3m/restart.f90:116-118), in DSEM's
+// DIMENSION(nx,ny,nz,neq) layout with nx = ny = nz = ldx: out[e][grid d][v][ldx^3],
+// grid d having L = G+1 points along d; padding left zero.  Returns 0 when the
+// arrays were never computed (DSEM's zeroed arrays).
+int orc_get_lobatto(const orc_case *h, double *out, int ldx) {
+  const size_t L3 = (size_t)ldx * ldx * ldx;
+  std::fill(out, out + h->c->el.size() * 3 * NV * L3, 0.0);
+  if (!h->c->ql_valid) return 0;
+  for (size_t e = 0; e < h->c->el.size(); ++e) {
+    const auto &E = h->c->el[e];
+    const int G = E.G, L = E.L;
+    const size_t nl = E.nl();
+    for (int d = 0; d < 3; ++d) {
+      const int ex = d == 0 ? L : G, ey = d == 1 ? L : G, ez = d == 2 ? L : G;
+      for (int v = 0; v < NV; ++v)
+        for (int z = 0; z < ez; ++z)
+          for (int y = 0; y < ey; ++y)
+            for (int x = 0; x < ex; ++x)
+              out[((e * 3 + d) * NV + v) * L3 + x + (size_t)ldx * (y + (size_t)ldx * z)] =
+                  re_(E.QL[d][v * nl + x + (size_t)ex * (y + (size_t)ey * z)]);
+    }
+  }
+  return 1;
+}
 double orc_dtcalc(const orc_case *h) { return dtcalc(*h->c); }
 void orc_rhs(orc_case *h, double tk, double *Qt, int ldx) {
   (void)tk;

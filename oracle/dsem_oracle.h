@@ -62,6 +62,7 @@ void orc_ke_weights(int G, double *w);
 void orc_init_tgv(orc_case *c, double twall, double v0);
 void orc_set_q(orc_case *c, const double *JQ, int ldx);
 void orc_get_q(const orc_case *c, double *JQ, int ldx);
+int orc_get_lobatto(const orc_case *c, double *out, int ldx);
 /* Inviscid time step (dtcalc), minimum over elements, before the CFL factor. */
 double orc_dtcalc(const orc_case *c);
 

@@ -47,6 +47,8 @@ def lib():
         L.orc_init_tgv.argtypes = [vp, C.c_double, C.c_double]
         L.orc_set_q.argtypes = [vp, _dp, C.c_int]
         L.orc_get_q.argtypes = [vp, _dp, C.c_int]
+        L.orc_get_lobatto.argtypes = [vp, _dp, C.c_int]
+        L.orc_get_lobatto.restype = C.c_int
         L.orc_dtcalc.argtypes = [vp]
         L.orc_dtcalc.restype = C.c_double
         L.orc_rhs.argtypes = [vp, C.c_double, _dp, C.c_int]
@@ -196,6 +198,14 @@ class Case:
         q = np.zeros(self.qshape())
         lib().orc_get_q(self.h, q.ravel(), self.ldx)
         return q
+
+    def lobatto(self):
+        """Lobatto arrays of the last Fluxes call (d%Qlgg, d%Qglg, d%Qggl) as
+        [nel][grid d][5][ldx][ldx][ldx] (x fastest, DSEM's padded layout), and
+        whether they were ever computed."""
+        out = np.zeros((self.nel, 3, 5, self.ldx, self.ldx, self.ldx))
+        ok = lib().orc_get_lobatto(self.h, out.ravel(), self.ldx)
+        return out, bool(ok)
 
     def dtcalc(self):
         return lib().orc_dtcalc(self.h)

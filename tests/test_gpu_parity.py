@@ -216,3 +216,58 @@ def test_rhs_degenerate_and_anisotropic_boxes(oracle_mod, dims, p):
     s.step(dt, 1)
     c.step(0.0, dt, 1)
     assert np.array_equal(s.download(), c.get_q())
+
+
+def _history(s, c, dt, nsteps):
+    """KE, -dKE/dt and the enstrophy dissipation after every step, GPU and oracle."""
+    hg, ho = [], []
+    for k in range(nsteps):
+        s.step(dt, 1)
+        c.step(0.0, dt, 1)
+        hg.append(s.diag(dt, first=(k == 0)))
+        ho.append(c.diag(dt, k == 0))
+    return np.array(hg), np.array(ho)
+
+
+def _assert_history(hg, ho):
+    # column 1 (-dKE/dt) is undefined on the first call (prestep = 0)
+    assert relmax(hg[:, 0], ho[:, 0]) <= HIST_TOL
+    assert relmax(hg[1:, 1], ho[1:, 1]) <= HIST_TOL
+    assert relmax(hg[:, 2], ho[:, 2]) <= HIST_TOL
+
+
+def test_cfg3_full_size_100_steps(oracle_mod):
+    """Config 3 at its stated size: 16^3 periodic elements at p = 6 with the middle third
+    in x at p = 8 (p-nonconforming band, 1,536 + 2,560 elements), a seeded divergence-free
+    isotropic field with E(k) ~ k^4 exp(-2 (k/4)^2) at turbulent Mach 0.3, Re = 115
+    (Re_lambda ~ 100: lambda = 2/k0, u' = 1.73), entropy viscosity on (Cmu = 1,
+    mumax = 0.5), 100 steps.  KE / dissipation histories to 1e-9, state and entropy
+    viscosity at the end to 1e-12 (tstep.f90:36-116, EV_routines/Main/Driver.f90:21-60)."""
+    n = 16
+    box = mesh.Box(n, n, n, _band(n, 6, 8))
+    assert box.nel == 4096 and (~box.mortar[:, 13:17].all(axis=1)).sum() == 2 * n * n
+    q = mesh.random_isotropic(box, seed=2024, k0=4.0, mach_t=0.3)
+    phys = dict(re=115.0, cmu=1.0, mumax=0.5, shock=1)
+    s, c = _pair(oracle_mod, box, q, **phys)
+    dt = 0.3 * c.dtcalc()
+    hg, ho = _history(s, c, dt, 100)
+    _assert_history(hg, ho)
+    assert relmax(s.download(), c.get_q()) <= RHS_TOL
+    mo = c.muhg()
+    assert np.abs(mo).max() > 0
+    assert np.abs(s.muhg() - mo).max() <= RHS_TOL * np.abs(mo).max()
+
+
+def test_cfg2_full_size_history(oracle_mod):
+    """Config 2 at its stated size (22^3 elements, p = 8, Taylor-Green, Re = 1600, CFL 0.5):
+    KE / dissipation after each of 20 steps to 1e-9 and the state after them to 1e-12.
+    DSEM_CFG2_STEPS raises the count (200 is the configuration's run length)."""
+    import os
+    nsteps = int(os.environ.get("DSEM_CFG2_STEPS", "20"))
+    box = mesh.Box(22, 22, 22, 8)
+    q = mesh.taylor_green(box)
+    s, c = _pair(oracle_mod, box, q, re=1600.0)
+    dt = 0.5 * c.dtcalc()
+    hg, ho = _history(s, c, dt, nsteps)
+    _assert_history(hg, ho)
+    assert relmax(s.download(), c.get_q()) <= RHS_TOL

@@ -1,5 +1,5 @@
 """One case sharded over several contexts (dsem_shard_stage): the sharded run
-reproduces the single-context run bit for bit.  All shards run in this
+reproduces the single-context run bit for bit, and the CPU oracle's run.  All shards run in this
 process on one GPU and exchange their cut-mortar blocks by device copies,
 the same blocks NCCL moves between GPUs in a multi-GPU run."""
 import numpy as np
@@ -21,7 +21,7 @@ def _single(box, q, dt, nsteps, diag=False, **phys):
 
 
 @pytest.mark.parametrize("parts,kind", [(2, "slab"), (3, "slab"), (3, "random"), (4, "random")])
-def test_sharded_steps_match_single_context(parts, kind):
+def test_sharded_steps_match_single_context(oracle_mod, parts, kind):
     from dsem_b200.shard import ShardedRun, slab_partition
     box = mesh.Box(4, 4, 4, 3)
     q = mesh.random_isotropic(box, seed=11, k0=2.0, mach_t=0.2)
@@ -32,7 +32,14 @@ def test_sharded_steps_match_single_context(parts, kind):
     run.diag_sums()  # asks every shard for the last stage's gradients
     run.step(dt, 3)
     ref = _single(box, q, dt, 3, diag=True, re=1200.0)
-    assert np.array_equal(run.download(), ref.download())
+    got = run.download()
+    assert np.array_equal(got, ref.download())
+    # and the CPU oracle's single-case run
+    c = oracle_mod.Case.from_desc(box.desc())
+    c.set_phys(re=1200.0)
+    c.set_q(q)
+    c.step(0.0, dt, 3)
+    assert np.array_equal(got, c.get_q())
     # diagnostics: shard sums add up to the single context's
     sums = run.diag_sums()
     assert sums[6] == 1.0
@@ -44,7 +51,7 @@ def test_sharded_steps_match_single_context(parts, kind):
     assert abs(eps_s - eps) <= 1e-13 * abs(eps)
 
 
-def test_sharded_rotated_elements_and_ev():
+def test_sharded_rotated_elements_and_ev(oracle_mod):
     """Cut mortars through rotated elements (all orientation codes) with entropy viscosity."""
     from dsem_b200.shard import ShardedRun
     rot = [0] * 27
@@ -58,7 +65,13 @@ def test_sharded_rotated_elements_and_ev():
     run.upload(q)
     run.step(dt, 2)
     ref = _single(box, q, dt, 2, **phys)
-    assert np.array_equal(run.download(), ref.download())
+    got = run.download()
+    assert np.array_equal(got, ref.download())
+    c = oracle_mod.Case.from_desc(box.desc())
+    c.set_phys(**phys)
+    c.set_q(q)
+    c.step(0.0, dt, 2)
+    assert np.abs(got - c.get_q()).max() <= 1e-12 * np.abs(c.get_q()).max()
 
 
 def test_sharded_les_matches_single_context():
