@@ -398,6 +398,7 @@ int enqueue_ev(dsem_ctx *c, long long *launches, const double *jq = nullptr) {
     a.hd = g.hd;
     a.EVB = g.EVB;
     a.muhg = g.muhg;
+    a.sens = c->les_sensors ? g.sens : nullptr;
     a.valid = c->ev_grad_valid ? 1 : 0;
     a.P = c->P;
     a.ecase = g.ecase;
@@ -421,6 +422,8 @@ int enqueue_les(dsem_ctx *c, long long *launches) {
     a.hd = g.hd;
     a.EVB = g.EVB;
     a.nuhg = g.nuhg;
+    a.sens = g.sens;
+    a.sensors = c->les_sensors;
     a.valid = c->grad_valid ? 1 : 0;
     a.re = c->P.re;
     a.cs = c->les_cs;
@@ -1063,6 +1066,7 @@ void dsem_destroy(dsem_ctx *c) {
     cudaFree(g.int2ext);
     cudaFree(g.ecase);
     cudaFree(g.nuhg);
+    cudaFree(g.sens);
   }
   cudaFree(c->d_rec);
   cudaFree(c->d_dtc);
@@ -1633,6 +1637,26 @@ int dsem_set_les(dsem_ctx *c, double cs, double numax) {
   return DSEM_OK;
 }
 
+int dsem_set_les_sensors(dsem_ctx *c, int shock_sensor, int rho_sensor) {
+  if (!c) return fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  const int f = (shock_sensor ? 1 : 0) | (rho_sensor ? 2 : 0);
+  if (f) {
+    for (auto &g : c->groups) {
+      if (!g.sens) {
+        const size_t n = (size_t)g.nel * 2 * g.G * g.G * g.G;
+        CK(cudaMalloc(&g.sens, n * sizeof(double)));
+        CK(cudaMemset(g.sens, 0, n * sizeof(double)));
+      }
+    }
+  }
+  c->les_sensors = f;
+  if (c->gexec) {  // the captured step changes
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  return DSEM_OK;
+}
+
 int dsem_get_nut(dsem_ctx *c, double *nu, int ldx) {
   if (!c || !nu) return fail(c, DSEM_ERR_INVALID_ARG, "null argument");
   if (!c->les) return fail(c, DSEM_ERR_INVALID_ARG, "LES is off (dsem_set_les)");
@@ -1792,7 +1816,9 @@ int dsem_profile_rhs(dsem_ctx *c, int reps, double *ms) {
       a.QTI = c->QTI + g.q0;
       a.EVB = g.EVB;
       a.P = c->P;
-      CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::vol(a, g.nel, g.diag, mode, c->st); }));
+      CK(with_G(g.G, [&](auto gg) {
+        return Launch<decltype(gg)::value>::vol(a, g.nel, g.diag, mode, c->st, c->vol_variant[g.G]);
+      }));
     }
     CK(cudaEventRecord(ev[2], c->st));
     for (auto &ml : c->mlists)

@@ -36,6 +36,7 @@ struct Group {
   double *muhg = nullptr, *EVB = nullptr, *kew = nullptr;
   double *nuhg = nullptr;  // Smagorinsky viscosity at Gauss points (LES on)
   long long l0 = 0;        // offset of the group's kept Lobatto arrays in dsem_ctx::QLB (doubles)
+  double *sens = nullptr;  // [elem][2][G^3] Ducros and density sensors (Smagorinsky sensors on)
   int *int2ext = nullptr;  // device: caller element id of each group element
   int *ecase = nullptr;    // device: case of each group element
   std::vector<int> case_lo, case_hi;  // group elements [lo, hi) of each case
@@ -72,6 +73,7 @@ struct dsem_ctx {
   int shock = 0, iord = 4, kord = 5;
   int les = 0;                     // static Smagorinsky model (dsem_set_les)
   double les_cs = 0.0, les_numax = 0.0;
+  int les_sensors = 0;             // bit 0: shockSensor, bit 1: rhoSensor (dsem_set_les_sensors)
   double ark[5] = {}, brk[5] = {}, crk[5] = {};
   std::vector<Group> groups;
   std::vector<MList> mlists;

@@ -327,6 +327,15 @@ __device__ __forceinline__ double ev_residual(const Phys &P, const double *Q, co
   return (((phi + gam) / Tt) / P.re);
 }
 
+// Density-based sensor of calculate_terms (RHS.f90:264-275) from the density gradient
+__device__ __forceinline__ double rho_sensor(double rx, double ry, double rz) {
+  const double eps = 1.0e-9;
+  const double rhoX2 = rx * rx, rhoY2 = ry * ry, rhoZ2 = rz * rz;
+  return sqrt((1.0 / ((1.0 / (rhoX2 + eps)) + (1.0 / (rhoY2 + eps)) + 1.0)) +
+              (1.0 / ((1.0 / (rhoX2 + eps)) + (1.0 / (rhoZ2 + eps)) + 1.0)) +
+              (1.0 / ((1.0 / (rhoY2 + eps)) + (1.0 / (rhoZ2 + eps)) + 1.0)));
+}
+
 // gradient fields interpolated to grid d for the directional viscous flux
 // (field id = var*3 + derivative direction)
 __device__ __forceinline__ int diag_field(int d, int j) {

@@ -1202,6 +1202,7 @@ struct EvArgs {
   long long sq;
   const double *jac, *hd, *EVB;
   double *muhg;
+  double *sens;  // optional: [elem][2][G^3] Ducros and density sensors for the Smagorinsky model
   int valid;
   Phys P;
   const int *ecase;   // optional: case of each element (ensembles)
@@ -1241,6 +1242,10 @@ template <int G> __global__ void __launch_bounds__(256) k_ev(EvArgs A) {
       T1[2] = EVB[14 * NG + p];
       double duc;
       const double biS = ev_residual(P, Q, Qx, Qy, Qz, T1, duc);
+      if (A.sens) {  // d%ducros, d%rhoSensor (RHS.f90:180-181)
+        A.sens[(long long)k * 2 * NG + p] = duc;
+        A.sens[(long long)k * 2 * NG + NG + p] = rho_sensor(Qx[0], Qy[0], Qz[0]);
+      }
       const double rho = JQ[p] * jac[p];
       const double h = hd[p];
       double mur = P.cmu * P.re * rho * (h * h) * fabs(biS);
@@ -1260,6 +1265,8 @@ struct LesArgs {
   long long sq;
   const double *jac, *hd, *EVB;
   double *nuhg;
+  const double *sens;  // [elem][2][G^3] Ducros and density sensors (k_ev; zero without entropy viscosity)
+  int sensors;         // bit 0: shockSensor, bit 1: rhoSensor (staticSmag.f90:68-69)
   int valid;  // EVB holds the gradients of the last Fluxes call
   double re, cs, numax;
   const int *ecase;   // optional: case of each element (ensembles)
@@ -1268,7 +1275,9 @@ struct LesArgs {
 
 // Static Smagorinsky viscosity at Gauss points (simpleSmag and filteredStrain,
 // turbulence/staticSmago/staticSmag.f90:32-183): DSEM's rho = Q jacob(1,1,1)
-// and velocities Q(2..4)/rho are kept as written.
+// and velocities Q(2..4)/rho are kept as written; the optional shock and
+// density sensors scale it (:68-69) with the values the step's entropy
+// viscosity left (zero when it is off, as DSEM's zeroed arrays).
 template <int G> __global__ void __launch_bounds__(128) k_les(LesArgs A) {
   constexpr int NG = G * G * G;
   const int k = blockIdx.x;
@@ -1301,7 +1310,9 @@ template <int G> __global__ void __launch_bounds__(128) k_les(LesArgs A) {
     const double S = sqrt(2.0 * S11 * S11 + 2.0 * S12 * S12 + 2.0 * S13 * S13 + 2.0 * S21 * S21 + 2.0 * S22 * S22 +
                           2.0 * S23 * S23 + 2.0 * S31 * S31 + 2.0 * S32 * S32 + 2.0 * S33 * S33);
     const double dg = hd[p];
-    const double nu = re * (A.cs * dg) * (A.cs * dg) * S;
+    double nu = re * (A.cs * dg) * (A.cs * dg) * S;
+    if (A.sensors & 1) nu = nu * (1.0 - A.sens[(long long)k * 2 * NG + p]);
+    if (A.sensors & 2) nu = nu * A.sens[(long long)k * 2 * NG + NG + p];
     const double mx = nu >= 0.0 ? nu : 0.0;
     A.nuhg[(long long)k * NG + p] = mx <= A.numax ? mx : A.numax;
   }

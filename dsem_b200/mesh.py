@@ -1,4 +1,5 @@
-"""Mesh descriptors for standalone runs: periodic boxes of straight hex8 elements.
+"""Mesh descriptors for standalone runs: periodic boxes of hex8 elements, straight or
+curved by a smooth periodic deformation (Box(warp=...)).
 
 DSEM's Fortran driver computes the geometry itself and packs it into the
 descriptor of include/dsem_gpu.h.  For runs without it this module builds the
@@ -126,9 +127,10 @@ class Box:
     to the conditions of its low and high faces, e.g. {"y": ("walladiab",
     "wallisoth")}; those faces become boundary mortars (id(2) = 0)."""
 
-    def __init__(self, nex, ney, nez, orders, length=2 * np.pi, rot=None, ldx=None, bc=None):
+    def __init__(self, nex, ney, nez, orders, length=2 * np.pi, rot=None, ldx=None, bc=None, warp=0.0):
         self.nex, self.ney, self.nez = nex, ney, nez
         self.length = float(length)
+        self.warp = float(warp)
         self.bc = {}
         for ax, pair in (bc or {}).items():
             codes = tuple(BC_CODES.get(x, -1) if isinstance(x, str) else int(x) for x in pair)
@@ -247,6 +249,27 @@ class Box:
             self.bcond[m[0], m[2] - 1] = code
 
     # ------------------------------------------------------------ geometry
+    def _map(self, c, X, Y, Z):
+        """Physical points and d(x)/d(X) of the element map at computational points: the
+        hex8 map (hex8, grad_hex8) followed, when warp != 0, by the smooth periodic
+        deformation x_i -> x_i + warp * length * sin(k x_j) sin(k x_l) (k = 2 pi / length,
+        (i, j, l) cyclic), which curves every element and keeps the box periodic."""
+        x = hex8(c, X, Y, Z)
+        g = grad_hex8(c, X, Y, Z)
+        if self.warp == 0.0:
+            return x, g
+        a, k = self.warp * self.length, 2.0 * np.pi / self.length
+        s_, c_ = np.sin(k * x), np.cos(k * x)
+        W = np.zeros(x.shape + (3,))
+        xw = x.copy()
+        for i in range(3):
+            j, l = (i + 1) % 3, (i + 2) % 3
+            xw[..., i] += a * s_[..., j] * s_[..., l]
+            W[..., i, i] = 1.0
+            W[..., i, j] = a * k * c_[..., j] * s_[..., l]
+            W[..., i, l] = a * k * s_[..., j] * c_[..., l]
+        return xw, np.einsum("...ij,...jk->...ik", W, g)
+
     def _geometry(self):
         ne, ldx = self.nel, self.ldx
         L3 = ldx ** 3
@@ -264,9 +287,8 @@ class Box:
             X = cxg[None, None, :]
             Y = cxg[None, :, None]
             Z = cxg[:, None, None]
-            gx = grad_hex8(c, X, Y, Z)
+            xg, gx = self._map(c, X, Y, Z)
             gc, J = invert_metric(gx)
-            xg = hex8(c, X, Y, Z)
             q = (np.arange(G)[None, None, :] + ldx * (np.arange(G)[None, :, None] + ldx * np.arange(G)[:, None, None]))
             q = np.broadcast_to(q, (G, G, G)).ravel()
             self.jacob[np.ix_(ids, q)] = (1.0 / J).reshape(len(ids), -1)
@@ -281,7 +303,7 @@ class Box:
                 X = pts[0][None, None, :]
                 Y = pts[1][None, :, None]
                 Z = pts[2][:, None, None]
-                gx = grad_hex8(c, X, Y, Z)
+                gx = self._map(c, X, Y, Z)[1]
                 gc, J = invert_metric(gx)
                 row = J[..., None] * gc[..., d, :]  # [ids, l, m, n, 3]
                 nn = np.arange(ext[0])[None, None, :]
@@ -322,7 +344,7 @@ class Box:
         cxg = gauss_points(G)
         pt = [cxg[0], cxg[0], cxg[0]]
         pt[d] = cx[-1] if face in (2, 4, 5) else cx[0]
-        gx = grad_hex8(self.corner[e], np.float64(pt[0]), np.float64(pt[1]), np.float64(pt[2]))
+        gx = self._map(self.corner[e], np.float64(pt[0]), np.float64(pt[1]), np.float64(pt[2]))[1]
         gc, J = invert_metric(gx)
         g = J * gc[d, :]
         return g / math.sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2])
@@ -339,7 +361,7 @@ class Box:
             X, Y, Z = A, B, np.full_like(A * B, end)
         else:
             X, Y, Z = np.full_like(A * B, end), A, B
-        gx = grad_hex8(self.corner[e], X + 0 * B, Y + 0 * A, Z + 0 * A)
+        gx = self._map(self.corner[e], X + 0 * B, Y + 0 * A, Z + 0 * A)[1]
         gc, J = invert_metric(gx)
         r = gc[..., d, :]
         sqr = np.sqrt(r[..., 0] * r[..., 0] + r[..., 1] * r[..., 1] + r[..., 2] * r[..., 2])
@@ -373,7 +395,7 @@ class Box:
             A, B = c1[None, :], c1[:, None]
             end = np.full_like(A * B, END_VALS[face - 1])
             X, Y, Z = {1: (A + 0 * B, end, B + 0 * A), 2: (A + 0 * B, B + 0 * A, end), 0: (end, A + 0 * B, B + 0 * A)}[d]
-            out[j, :G, :G] = hex8(self.corner[e], X, Y, Z)
+            out[j, :G, :G] = self._map(self.corner[e], X, Y, Z)[0]
         return out
 
     def gauss_xyz(self):

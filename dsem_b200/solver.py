@@ -21,7 +21,8 @@ EXPORTS = ("dsem_create", "dsem_destroy", "dsem_last_error", "dsem_upload_q", "d
            "dsem_diag_batch", "dsem_adjoint", "dsem_set_les", "dsem_get_nut", "dsem_state_size",
            "dsem_save_state", "dsem_load_state", "dsem_shard_info", "dsem_shard_stage", "dsem_diag_sums",
            "dsem_set_boundary", "dsem_autotune", "dsem_set_vol_variant", "dsem_shard_enqueue", "dsem_shard_finish",
-           "dsem_get_stream", "dsem_keep_lobatto", "dsem_write_restart", "dsem_read_restart")
+           "dsem_get_stream", "dsem_keep_lobatto", "dsem_write_restart", "dsem_read_restart",
+           "dsem_set_les_sensors")
 
 
 class DsemError(RuntimeError):
@@ -76,6 +77,7 @@ def lib(path=None):
         L.dsem_step_batch.argtypes = [vp, dp, C.c_int]
         L.dsem_diag_batch.argtypes = [vp, dp, C.c_int, dp, dp, dp]
         L.dsem_set_les.argtypes = [vp, C.c_double, C.c_double]
+        L.dsem_set_les_sensors.argtypes = [vp, C.c_int, C.c_int]
         L.dsem_set_boundary.argtypes = [vp, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]
         L.dsem_autotune.argtypes = [vp, C.c_int, C.POINTER(C.c_int), dp]
         L.dsem_set_vol_variant.argtypes = [vp, C.c_int, C.c_int]
@@ -245,6 +247,10 @@ class Solver:
     def set_les(self, cs, numax):
         """Static Smagorinsky model (cs = 0: off)."""
         self._check(lib().dsem_set_les(self.h, float(cs), float(numax)))
+
+    def set_les_sensors(self, shock_sensor=False, rho_sensor=False):
+        """DSEM's shockSensor / rhoSensor scaling of the Smagorinsky viscosity."""
+        self._check(lib().dsem_set_les_sensors(self.h, int(bool(shock_sensor)), int(bool(rho_sensor))))
 
     def nut(self):
         m = np.zeros((self.ngrid, self.ldx, self.ldx, self.ldx))

@@ -139,6 +139,13 @@ int dsem_profile_rhs(dsem_ctx *ctx, int reps, double *ms);
  * `smagorinsky`, C_s, numax; its shock and density sensors are not supported.
  * Axis-aligned elements only (DSEM_ERR_UNSUPPORTED otherwise). */
 int dsem_set_les(dsem_ctx *ctx, double cs, double numax);
+/* The Smagorinsky model's shock and density sensors (DSEM's shockSensor and
+ * rhoSensor inputs, input_lib.f90:163-164): nu_t is scaled by (1 - Ducros
+ * sensor) and by the density-based sensor that the step's entropy viscosity
+ * evaluates (staticSmag.f90:68-69, RHS.f90:264-275).  Without entropy
+ * viscosity both sensors stay 0, as DSEM's zeroed arrays: the shock sensor
+ * then leaves nu_t unchanged and the density sensor zeroes it. */
+int dsem_set_les_sensors(dsem_ctx *ctx, int shock_sensor, int rho_sensor);
 /* nu_t at Gauss points after the last evaluation (ldx layout, one field). */
 int dsem_get_nut(dsem_ctx *ctx, double *nu, int ldx);
 

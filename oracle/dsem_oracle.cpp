@@ -281,6 +281,7 @@ template <class T> struct Elem {
   int bcond[6] = {};  // d%bcond as BC_* codes (faces without a neighbour)
   std::vector<double> jacob, gmetg, gmet[3], xg, hdelta;
   std::vector<T> Q, gQ, QL[3], F[3], R[3], muhg, muh[3], nutg, nut[3];
+  std::vector<T> ducros, rhos;  // d%ducros, d%rhoSensor at the Gauss points (RHS.f90:180-181; zero_domain: 0)
   size_t ng() const { return (size_t)G * G * G; }
   size_t nl() const { return (size_t)L * G * G; }
 };
@@ -308,6 +309,7 @@ template <class T> struct Case {
   double gamma = 1.4, re = 1600.0, pr = 0.72, mach = 1.0, cmu = 0.0, mumax = 0.0;
   bool shock = false, ducros = false;
   bool les = false;               // static Smagorinsky (staticSmag.f90)
+  bool shock_sensor = false, rho_sensor = false;  // shockSensor, rhoSensor (input_lib.f90:163-164)
   double cs = 0.0, numax = 0.0;  // C_s, numax
   int iord = 4, kord = 5;
   double ark[5] = {}, brk[5] = {}, crk[5] = {};
@@ -1095,6 +1097,15 @@ T ev_residual(const Case<T> &c, const T *Q, const T *Qx, const T *Qy, const T *Q
   return (((phi + gam) / Tt) / c.re);
 }
 
+// Density-based sensor of calculate_terms (RHS.f90:264-275) from the density gradient.
+template <class T> T rho_sensor(const T &rx, const T &ry, const T &rz) {
+  const double eps = 1.0e-9;
+  T rhoX2 = rx * rx, rhoY2 = ry * ry, rhoZ2 = rz * rz;
+  return std::sqrt((1.0 / ((1.0 / (rhoX2 + eps)) + (1.0 / (rhoY2 + eps)) + 1.0)) +
+                   (1.0 / ((1.0 / (rhoX2 + eps)) + (1.0 / (rhoZ2 + eps)) + 1.0)) +
+                   (1.0 / ((1.0 / (rhoY2 + eps)) + (1.0 / (rhoZ2 + eps)) + 1.0)));
+}
+
 // Entropy (EV_routines/Main/Driver.f90:21-60): RHS_ent_trans (RHS.f90:21-190),
 // Entropy_Viscosity (EViscosity_GL.f90:19-101), EV_Prolong (Prolong_gtol.f90:7-51).
 // Uses the Lobatto arrays left by the previous Fluxes call; before any Fluxes
@@ -1136,6 +1147,8 @@ template <class T> void entropy(Case<T> &c) {
         for (int k = 0; k < 3; ++k) T1[k] = gt[k * ng + p];
         T duc;
         T biS = ev_residual(c, Q, Qx, Qy, Qz, T1, duc);
+        E.ducros[p] = duc;  // the sensors the Smagorinsky model reads (RHS.f90:180-181)
+        E.rhos[p] = rho_sensor(Qx[0], Qy[0], Qz[0]);
         T rho = E.Q[p] * E.jacob[p];
         double h = E.hdelta[p];
         T mur = c.cmu * c.re * rho * (h * h) * rabs(biS);
@@ -1190,6 +1203,8 @@ template <class T> void smagorinsky(Case<T> &c) {
                       2.0 * S23 * S23 + 2.0 * S31 * S31 + 2.0 * S32 * S32 + 2.0 * S33 * S33);
       const double dg = E.hdelta[p];
       T nu = c.re * (c.cs * dg) * (c.cs * dg) * S;
+      if (c.shock_sensor) nu = nu * (1.0 - E.ducros[p]);  // staticSmag.f90:68-69
+      if (c.rho_sensor) nu = nu * E.rhos[p];
       E.nutg[p] = rmin(rmax(nu, T(0.0)), T(c.numax));
     }
     const int eg[3] = {G, G, G};
@@ -1477,6 +1492,8 @@ template <class T> Case<T> *build_box(int nex, int ney, int nez, double lx, doub
         const size_t ng = E.ng();
         E.Q.assign(NV * ng, T(0.0));
         E.gQ.assign(NV * ng, T(0.0));
+    E.ducros.assign(ng, T(0.0));
+    E.rhos.assign(ng, T(0.0));
       }
   // generate_mortars (set_mortars.f90:20-224): first element to present a face is the master
   std::map<std::array<int, 4>, int> faces;
@@ -1687,6 +1704,8 @@ template <class T> Case<T> *from_desc(int ngrid, int nmort, int ldx, const int *
       E.hdelta[p] = std::pow(std::fabs(1.0 / E.jacob[p]), 1.0 / 3.0) / std::pow((double)(G * G * G), 1.0 / 3.0);
     E.Q.assign(NV * ng, T(0.0));
     E.gQ.assign(NV * ng, T(0.0));
+    E.ducros.assign(ng, T(0.0));
+    E.rhos.assign(ng, T(0.0));
   }
   c->mo.resize(nmort);
   for (int j = 0; j < nmort; ++j) {
@@ -1934,6 +1953,8 @@ template <class T> Case<T> *convert_case(const Case<double> &c) {
     }
     B.muhg = cv(A.muhg);
     B.nutg = cv(A.nutg);
+    B.ducros = cv(A.ducros);
+    B.rhos = cv(A.rhos);
   }
   o->mo.resize(c.mo.size());
   for (size_t j = 0; j < c.mo.size(); ++j) {
@@ -1969,6 +1990,8 @@ template <class T> Case<T> *convert_case(const Case<double> &c) {
   o->shock = c.shock;
   o->ducros = c.ducros;
   o->les = c.les;
+  o->shock_sensor = c.shock_sensor;
+  o->rho_sensor = c.rho_sensor;
   o->cs = c.cs;
   o->numax = c.numax;
   o->iord = c.iord;
@@ -2224,6 +2247,10 @@ void orc_set_les(orc_case *h, double cs, double numax) {
     E.nutg.assign(E.ng(), 0.0);
     for (int d = 0; d < 3; ++d) E.nut[d].assign(E.nl(), 0.0);
   }
+}
+void orc_set_les_sensors(orc_case *h, int shock_sensor, int rho_sensor) {
+  h->c->shock_sensor = shock_sensor != 0;
+  h->c->rho_sensor = rho_sensor != 0;
 }
 void orc_get_nut(const orc_case *h, double *nu, int ldx) {
   for (size_t e = 0; e < h->c->el.size(); ++e) {

@@ -91,6 +91,7 @@ void orc_rk(const orc_case *c, double *ark, double *brk, double *crk);
  * clip numax; evaluated at the start of each step like the entropy viscosity.
  * orc_get_nut: its Gauss-point viscosity after the last evaluation. */
 void orc_set_les(orc_case *c, double cs, double numax);
+void orc_set_les_sensors(orc_case *c, int shock_sensor, int rho_sensor);
 /* boundary faces: d%bcond per element face ([ngrid][6]: 1 walladiab, 2 wallisoth,
  * 3 inflow, 4 outflow), then twall and the external mortar states
  * ([nmort][5][ldx][ldx], i fastest; null without inflow/outflow faces) */

@@ -62,6 +62,7 @@ def lib():
         L.orc_set_threads.restype = C.c_int
         L.orc_rk.argtypes = [vp, _dp, _dp, _dp]
         L.orc_set_les.argtypes = [vp, C.c_double, C.c_double]
+        L.orc_set_les_sensors.argtypes = [vp, C.c_int, C.c_int]
         L.orc_set_bcond.argtypes = [vp, _ip]
         L.orc_set_bcond.restype = C.c_int
         L.orc_set_boundary.argtypes = [vp, C.c_double, vp, vp, C.c_int]
@@ -238,6 +239,9 @@ class Case:
 
     def set_les(self, cs, numax):
         lib().orc_set_les(self.h, float(cs), float(numax))
+
+    def set_les_sensors(self, shock_sensor, rho_sensor):
+        lib().orc_set_les_sensors(self.h, int(bool(shock_sensor)), int(bool(rho_sensor)))
 
     def nut(self):
         m = np.zeros((self.nel, self.ldx, self.ldx, self.ldx))

@@ -76,3 +76,32 @@ def test_les_off_changes_nothing(oracle_mod):
     with pytest.raises(DsemError) as e:
         r.set_les(0.1, 1e3)
     assert e.value.code == -5
+
+
+@pytest.mark.parametrize("shock_sensor,rho_sensor,ev", [(True, False, True), (False, True, True), (True, True, True),
+                                                         (True, True, False)])
+def test_les_sensors_match_oracle(oracle_mod, shock_sensor, rho_sensor, ev):
+    """DSEM's shockSensor / rhoSensor (staticSmag.f90:68-69): nu_t scaled by (1 - Ducros sensor) and by
+    the density-based sensor that the step's entropy viscosity evaluates (RHS.f90:264-275).  Without
+    entropy viscosity both stay zero, as DSEM's zeroed arrays (the density sensor then zeroes nu_t)."""
+    box = mesh.Box(3, 3, 3, 4)
+    q = mesh.random_isotropic(box, seed=33, k0=1.5, mach_t=0.3)
+    phys = dict(re=1600.0, cmu=1.0, mumax=0.5, shock=1) if ev else dict(re=1600.0)
+    dt = 0.05 * mesh.dtcalc(box, q)
+    s, c = _pair(oracle_mod, box, q, 0.12, 1e3, **phys)
+    s.set_les_sensors(shock_sensor, rho_sensor)
+    c.set_les_sensors(shock_sensor, rho_sensor)
+    plain = _pair(oracle_mod, box, q, 0.12, 1e3, **phys)[1]
+    for _ in range(3):
+        s.step(dt, 1)
+        c.step(0.0, dt, 1)
+        plain.step(0.0, dt, 1)
+    qo = c.get_q()
+    assert np.abs(s.download() - qo).max() <= 1e-12 * np.abs(qo).max()
+    nu, nuo, nup = s.nut(), c.nut(), plain.nut()
+    assert np.abs(nu - nuo).max() <= 1e-12 * max(np.abs(nuo).max(), 1e-300)
+    if rho_sensor and not ev:
+        assert not nuo.any()
+    else:
+        assert nuo.max() > 0.0
+        assert not np.array_equal(nuo, nup)  # the sensors change the viscosity
