@@ -4,7 +4,9 @@
 //
 // Forward sweep: the steps as dsem_step runs them; stage states are kept in
 // HBM (every stage of every step when snapshots == 0, else binomial
-// checkpoints of step states with the steps recomputed in the reverse sweep).
+// checkpoints of step states with the steps recomputed in the reverse sweep;
+// with entropy viscosity a checkpoint also keeps the gradients its step's
+// viscosity reads).
 // Reverse sweep, step n = N..1, stage k = kord..1 (2N-storage RK,
 // tstep.f90:66-114):  lg += crk_k dt lQ;  lQ += R'(Q_{k-1})^T lg;  lg *= ark_k,
 // with the enstrophy terms of eps_n added at stage kord of each window step.
@@ -52,11 +54,18 @@ struct AdjBuf {
   double *lmuhg = nullptr, *levb = nullptr, *evb0 = nullptr;
   double *eps_part = nullptr;  // [window][elements][5] enstrophy partials of the window's steps
   double *evbw = nullptr;      // [window][elements][15][G^3] gradients saved by the window steps' last stages
+  // entropy viscosity with checkpoints: each slot also keeps the gradients its step's
+  // viscosity reads (saved by the step before it) and whether they existed; evb_prev
+  // holds those of the step being reversed
+  std::vector<double *> slot_evb;
+  std::vector<char> slot_valid;
+  double *evb_prev = nullptr;
   ~AdjBuf() {
     for (double *p : {lq, lg, ljq, qfr, lff, lvf, lqf, lqr, lrp, lr, q0, stages, traces, lmuhg, levb, evb0,
-                      eps_part, evbw})
+                      eps_part, evbw, evb_prev})
       cudaFree(p);
     for (double *p : slots) cudaFree(p);
+    for (double *p : slot_evb) cudaFree(p);
   }
 };
 
@@ -71,6 +80,8 @@ struct Adj {
   bool ev = false;            // entropy viscosity on
   bool ev_valid0 = false;     // the gradients behind the first step's viscosity were valid on entry
   bool levb_pending = false;  // b.levb holds the demand on the next-to-reverse step's saved gradients
+  bool ckpt = false;          // binomial checkpoints (snapshots > 0)
+  bool prev_valid = false;    // checkpoints: b.evb_prev holds valid gradients
   bool in_window(int n) const { return n >= nsteps - window; }  // step n (0-based) ends inside the window
   double eps_w() const { return dt * 100.0 * c->P.r_re / s2; }
 };
@@ -247,9 +258,11 @@ int eps_direct(Adj &A, const double *Qs, const double *qraw, const double *qend,
 
 // Entropy viscosity for the reverse sweep of a step whose start state is Qn:
 // first the gradients that fed it, saved by the previous step's last stage
-// (recomputed from that stage's stored input state Qprev and its raw face
-// traces, or kept from entry for the first step), then the viscosity itself
-// (k_ev, into the group's muhg).  *valid: whether those gradients existed.
+// (with every stage kept: recomputed from that stage's stored input state Qprev
+// and its raw face traces, or kept from entry for the first step; with
+// checkpoints: copied aside before the step's recomputation, keep_prev), then
+// the viscosity itself (k_ev, into the group's muhg).  *valid: whether those
+// gradients existed.
 template <int G> int ev_forward_G(Adj &A, const double *Qn, const double *Qprev, const double *qraw_prev, bool *valid) {
   dsem_ctx *c = A.c;
   const Group &g = *A.g;
@@ -260,7 +273,12 @@ template <int G> int ev_forward_G(Adj &A, const double *Qn, const double *Qprev,
   } else {
     constexpr int NG = G * G * G;
     bool ok = true;
-    if (Qprev) {
+    if (A.ckpt) {  // kept before the step's recomputation overwrote them
+      ok = A.prev_valid;
+      if (ok)
+        CKA(cudaMemcpyAsync(g.EVB, A.b.evb_prev, (size_t)g.nel * 15 * NG * sizeof(double), cudaMemcpyDeviceToDevice,
+                            c->st));
+    } else if (Qprev) {
       const int r = saved_grads_G<G>(A, Qprev, qraw_prev, VOL_EV_SAVE);
       if (r) return r;
     } else if (A.ev_valid0) {
@@ -361,7 +379,7 @@ int reverse_step(Adj &A, int n, double *const *st, const double *qend, double *c
       const int r = ev_adjoint(A, st[0]);
       if (r) return r;
     }
-    A.levb_pending = ev_valid && qprev != nullptr;
+    A.levb_pending = ev_valid && n > 0;  // gradients saved inside the run (not held fixed from before it)
   }
   return DSEM_OK;
 }
@@ -439,10 +457,43 @@ template <class F> int replay(dsem_ctx *c, cudaGraphExec_t *gx, F &&f) {
   return DSEM_OK;
 }
 
-int load_state(Adj &A, const double *src) {
+size_t evb_bytes(const Adj &A) {
+  const Group &g = *A.g;
+  return (size_t)g.nel * 15 * g.G * g.G * g.G * sizeof(double);
+}
+
+// The state of slot si into the context; with entropy viscosity also the
+// gradients behind the viscosity of the slot's step and their validity.
+int load_slot(Adj &A, int si) {
   dsem_ctx *c = A.c;
-  CKA(cudaMemcpyAsync(c->JQ, src, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  CKA(cudaMemcpyAsync(c->JQ, A.b.slots[si], c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  if (A.ev) {
+    CKA(cudaMemcpyAsync(A.g->EVB, A.b.slot_evb[si], evb_bytes(A), cudaMemcpyDeviceToDevice, c->st));
+    c->ev_grad_valid = A.b.slot_valid[si] != 0;
+  }
   return dsem_int::traces(c);
+}
+
+// The context's state into slot si (and, with entropy viscosity, the gradients the
+// next step's viscosity reads).
+int save_slot(Adj &A, int si) {
+  dsem_ctx *c = A.c;
+  CKA(cudaMemcpyAsync(A.b.slots[si], c->JQ, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  if (A.ev) {
+    CKA(cudaMemcpyAsync(A.b.slot_evb[si], A.g->EVB, evb_bytes(A), cudaMemcpyDeviceToDevice, c->st));
+    A.b.slot_valid[si] = c->ev_grad_valid ? 1 : 0;
+  }
+  return DSEM_OK;
+}
+
+// Before the recomputation of a step about to be reversed: the gradients its
+// viscosity reads, which that step's last stage overwrites.
+int keep_prev(Adj &A) {
+  if (!A.ev) return DSEM_OK;
+  dsem_ctx *c = A.c;
+  CKA(cudaMemcpyAsync(A.b.evb_prev, A.g->EVB, evb_bytes(A), cudaMemcpyDeviceToDevice, c->st));
+  A.prev_valid = c->ev_grad_valid;
+  return DSEM_OK;
 }
 
 // binomial checkpoint count beta(s, t) = C(s + t, s), saturated
@@ -490,28 +541,28 @@ int revolve(Adj &A, int i, int j, int si, int sfree) {
     for (int k = 0; k < c->kord; ++k) qf.push_back(A.b.traces + (size_t)k * c->nface);
   double *const *qfp = qf.empty() ? nullptr : qf.data();
   if (j - i == 1) {
-    int r = load_state(A, A.b.slots[si]);
+    int r = load_slot(A, si);
     if (r) return r;
-    if ((r = forward_step(A, i, st.data(), nullptr, qfp))) return r;
+    if ((r = keep_prev(A)) || (r = forward_step(A, i, st.data(), nullptr, qfp))) return r;
     return reverse_step(A, i, st.data(), c->JQ, qfp, nullptr, nullptr, A.g->EVB);
   }
   if (nfree == 0) {  // no free slot: re-advance from slot si for every step
     for (int m = j - 1; m >= i; --m) {
-      int r = load_state(A, A.b.slots[si]);
+      int r = load_slot(A, si);
       if (r) return r;
       for (int n = i; n < m; ++n)
         if ((r = forward_step(A, n, nullptr, nullptr))) return r;
-      if ((r = forward_step(A, m, st.data(), nullptr, qfp))) return r;
+      if ((r = keep_prev(A)) || (r = forward_step(A, m, st.data(), nullptr, qfp))) return r;
       if ((r = reverse_step(A, m, st.data(), c->JQ, qfp, nullptr, nullptr, A.g->EVB))) return r;
     }
     return DSEM_OK;
   }
   const int m = i + (int)split_left(j - i, nfree);
-  int r = load_state(A, A.b.slots[si]);
+  int r = load_slot(A, si);
   if (r) return r;
   for (int n = i; n < m; ++n)
     if ((r = forward_step(A, n, nullptr, nullptr))) return r;
-  CKA(cudaMemcpyAsync(A.b.slots[sfree], c->JQ, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  if ((r = save_slot(A, sfree))) return r;
   if ((r = revolve(A, m, j, sfree, sfree + 1))) return r;
   return revolve(A, i, m, si, sfree);
 }
@@ -549,9 +600,6 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
     return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED,
                           "adjoint: one case, one element order, conforming periodic mortars, axis-aligned elements, no "
                           "Ducros sensor, LES, boundary faces or sharding");
-  if (c->shock && snapshots > 0)
-    return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED,
-                          "adjoint: with entropy viscosity every stage state is kept (snapshots = 0)");
   if (c->groups[0].G > 7) return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
   if (dJdQ0 && ldx < c->groups[0].G) return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "ldx smaller than the number of Gauss points");
   int r = upload_ops_here(c);
@@ -594,14 +642,21 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
     cudaGetLastError();  // not enough memory: the reverse sweep recomputes the traces
     A.b.traces = nullptr;
   }
+  A.ckpt = snapshots > 0;
   for (int s = 0; s < snapshots; ++s) {
-    double *p = nullptr;
-    if (cudaMalloc(&p, bq) != cudaSuccess) {
+    double *p = nullptr, *pe = nullptr;
+    if (cudaMalloc(&p, bq) != cudaSuccess || (A.ev && cudaMalloc(&pe, evb_bytes(A)) != cudaSuccess)) {
       cudaGetLastError();
+      cudaFree(p);
       return dsem_int::fail(c, DSEM_ERR_NOMEM, "adjoint: not enough device memory for the snapshots");
     }
     A.b.slots.push_back(p);
+    if (A.ev) {
+      A.b.slot_evb.push_back(pe);
+      A.b.slot_valid.push_back(0);
+    }
   }
+  if (A.ev && A.ckpt) CKA(cudaMalloc(&A.b.evb_prev, evb_bytes(A)));
   std::vector<double> tmp(1, dt);
   if ((r = dsem_int::set_dt(c, tmp.data()))) return r;
   cudaEvent_t e0, e1;
@@ -645,7 +700,7 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
     size_t ksp = 0;  // next snapshot of the spine
     for (int n = 0; n < nsteps; ++n) {
       if (ksp < sp.size() && sp[ksp].first == n) {  // the state after n steps, for the reverse sweep
-        CKA(cudaMemcpyAsync(A.b.slots[sp[ksp].second], c->JQ, bq, cudaMemcpyDeviceToDevice, c->st));
+        if ((r = save_slot(A, sp[ksp].second))) return drop(), r;
         ++ksp;
       }
       std::vector<double *> st, qf;
@@ -736,6 +791,10 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
       drop();
     } else {
       CKA(cudaMemcpyAsync(A.b.slots[0], A.b.q0, bq, cudaMemcpyDeviceToDevice, c->st));
+      if (A.ev) {  // the first step's viscosity reads the gradients from before the run
+        if (A.ev_valid0) CKA(cudaMemcpyAsync(A.b.slot_evb[0], A.b.evb0, evb_bytes(A), cudaMemcpyDeviceToDevice, c->st));
+        A.b.slot_valid[0] = A.ev_valid0 ? 1 : 0;
+      }
       if ((r = revolve_spine(A, 0, nsteps, 0, 1))) return r;
     }
   }

@@ -289,8 +289,10 @@ int dsem_diag_batch(dsem_ctx *ctx, const double *dt, int first, double *ke, doub
  * may be NULL): J; dJ/d(JQ at the start) in the ldx layout of dsem_upload_q;
  * dJ/d(1/Re); the device milliseconds of the whole call.  The state is
  * restored on return.  Supported: one case, one element order with p <= 6,
- * axis-aligned elements, conforming mortars, shock = 0
- * (DSEM_ERR_UNSUPPORTED otherwise). */
+ * axis-aligned elements, conforming periodic mortars, shock = 0 or 1 (entropy
+ * viscosity without the Ducros sensor; with snapshots > 0 each snapshot also
+ * keeps the gradients its step's viscosity reads), no LES, boundary faces or
+ * sharding (DSEM_ERR_UNSUPPORTED otherwise). */
 int dsem_adjoint(dsem_ctx *ctx, double dt, int nsteps, int window, int snapshots, double *J, double *dJdQ0,
                  int ldx, double *dJdinvRe, double *ms);
 
