@@ -292,10 +292,10 @@ __device__ __forceinline__ void vol_diag_dir(const VolArgs &A, const Phys &P, co
     vol_diag_point<G, D>(l0 + s0 * ls, s0, a, b, c0, les, nu0, EV, mu0, P, gm, LB, VF);
     if (two) vol_diag_point<G, D>(l0 + s1 * ls, s1, a, b, c1, les, nu1, EV, mu1, P, gm, LB, VF);
   }
-  __syncthreads();
-  PHASE_MARK(3 + 3 * (2 - D));
   // (c) interior divergence along D at this thread's Gauss points (updatea.f90:100-113),
-  // summed over the directions in z, y, x order through the element's QTI slot
+  // summed over the directions in z, y, x order through the element's QTI slot; the
+  // thread's own partial sums of the earlier directions (its own writes of the previous
+  // phase (c)) are loaded before the barrier, so that their latency overlaps the wait
   double prev[NPT][NV];
   if (D != 2) {
 #pragma unroll
@@ -305,6 +305,8 @@ __device__ __forceinline__ void vol_diag_dir(const VolArgs &A, const Phys &P, co
       for (int v = 0; v < NV; ++v) prev[j][v] = p < NG ? QTI[v * NG + p] : 0.0;
     }
   }
+  __syncthreads();
+  PHASE_MARK(3 + 3 * (2 - D));
 #pragma unroll
   for (int j = 0; j < NPT; ++j) {
     const int p = tid + j * NT;
@@ -361,6 +363,15 @@ __global__ void __launch_bounds__(VolDiagCfg<G, EV, SAVE, V>::NT, VolDiagCfg<G, 
   t_ph_ = clock64();
 #endif
 
+  // the element's metrics, face states and viscosities, read from the phases below,
+  // are requested into L2 now (one bulk prefetch per array)
+  if (tid == 0) {
+    prefetch_l2_bulk(gg, 3 * NG);
+    prefetch_l2_bulk(gm, 3 * NL);
+    prefetch_l2_bulk(QF, 30 * G2);
+    if (EV) prefetch_l2_bulk(muhg, NG);
+    if (nuhg) prefetch_l2_bulk(nuhg, NG);
+  }
   // operators to shared memory (rows are read at per-thread indices)
   for (int i = tid; i < L * G; i += NT) {
     Bm[i] = Op<G>::B(i / G, i % G);
