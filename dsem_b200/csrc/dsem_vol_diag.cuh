@@ -204,9 +204,11 @@ __device__ __forceinline__ void vol_diag_dir(const VolArgs &A, const Phys &P, co
   const double gamma = P.gamma;
   const int xs = D == 0 ? 1 : (D == 1 ? G : G2);
   const int ls = xs;  // Lobatto-grid stride along D (lstride)
-  // (a) Lobatto arrays of grid D; the energy gradient along D on grid D
-  for (int t = tid; t < 5 * G2; t += NT) {
-    const int v = 4 - t / G2, ln = t % G2, a = ln % G, b = ln / G;  // field 4 (the longest task) first
+  // (a) Lobatto arrays of grid D; the energy gradient along D on grid D (round robin, the
+  // field-4 tasks -- line build, derivative and interpolation of the energy gradient, the
+  // longest -- first)
+  auto a_task = [&](int v, int ln) {
+    const int a = ln % G, b = ln / G;
     const int p0 = gbase<G>(D, a, b), l0 = lbase<G>(D, a, b);
     double x[G], y[L];
 #pragma unroll
@@ -238,13 +240,19 @@ __device__ __forceinline__ void vol_diag_dir(const VolArgs &A, const Phys &P, co
 #pragma unroll
       for (int s = 0; s < L; ++s) T4[l0 + s * ls] = t4[s];
     }
-  }
+  };
+  for (int t = tid; t < 5 * G2; t += NT) a_task(4 - t / G2, t % G2);
   __syncthreads();
   PHASE_MARK(2 + 3 * (2 - D));
   // (b) fluxes at the Lobatto points of grid D (Vis_Fluxes_new.f90:115-228, fluxesH_newa.f90:276-352),
-  // two points (s, s + NH) of one line per task so that both share the gradient loads
+  // two points (s, s + NH) of one line per task so that both share the gradient loads.
+  // Whole rounds of tasks first; the tasks of a last, partial round are split into
+  // single points over twice as many threads, so that no thread computes two points
+  // more than another.
   constexpr int NH = (L + 1) / 2;
-  for (int t = tid; t < NH * G2; t += NT) {
+  constexpr int NTB = NH * G2, RB = NTB / NT, LEFTB = NTB - RB * NT;
+  constexpr bool SPLITB = LEFTB > 0 && 2 * LEFTB <= NT;
+  auto b_task = [&](int t) {
     const int h = t / G2, ln = t - h * G2, a = ln % G, b = ln / G;
     const int g0 = gbase<G>(D, a, b), l0 = lbase<G>(D, a, b);
     const int s0 = h, s1 = h + NH;
@@ -291,6 +299,33 @@ __device__ __forceinline__ void vol_diag_dir(const VolArgs &A, const Phys &P, co
     }
     vol_diag_point<G, D>(l0 + s0 * ls, s0, a, b, c0, les, nu0, EV, mu0, P, gm, LB, VF);
     if (two) vol_diag_point<G, D>(l0 + s1 * ls, s1, a, b, c1, les, nu1, EV, mu1, P, gm, LB, VF);
+  };
+  // one point of task t: s = h (which == 0) or h + NH, the same chains as b_task
+  auto b_point = [&](int t, int which) {
+    const int h = t / G2, ln = t - h * G2, a = ln % G, b = ln / G;
+    const int s0 = which ? h + NH : h;
+    if (s0 >= L) return;
+    const int g0 = gbase<G>(D, a, b), l0 = lbase<G>(D, a, b);
+    double br0[G];
+#pragma unroll
+    for (int kk = 0; kk < G; ++kk) br0[kk] = Bm[s0 * G + kk];
+    double c0[11];
+#pragma unroll
+    for (int jf = 0; jf < 11; ++jf) c0[jf] = jf == 4 ? T4[l0 + s0 * ls] : chain<G>(br0, GR + diag_field(D, jf) * NG + g0, xs);
+    double mu0 = 0.0, nu0 = 0.0;
+    if (EV) mu0 = chain<G>(br0, muhg + g0, xs);
+    const bool les = nuhg != nullptr;
+    if (les) {
+      nu0 = chain<G>(br0, nuhg + g0, xs);
+      if (nu0 < 0.0) nu0 = 0.0;
+    }
+    vol_diag_point<G, D>(l0 + s0 * ls, s0, a, b, c0, les, nu0, EV, mu0, P, gm, LB, VF);
+  };
+  if constexpr (SPLITB) {
+    for (int t = tid; t < RB * NT; t += NT) b_task(t);
+    if (tid < 2 * LEFTB) b_point(RB * NT + (tid >> 1), tid & 1);
+  } else {
+    for (int t = tid; t < NTB; t += NT) b_task(t);
   }
   // (c) interior divergence along D at this thread's Gauss points (updatea.f90:100-113),
   // summed over the directions in z, y, x order through the element's QTI slot; the
