@@ -80,7 +80,8 @@ struct Adj {
   bool ev = false;            // entropy viscosity on
   bool ev_valid0 = false;     // the gradients behind the first step's viscosity were valid on entry
   bool levb_pending = false;  // b.levb holds the demand on the next-to-reverse step's saved gradients
-  bool ckpt = false;          // binomial checkpoints (snapshots > 0)
+  bool ckpt = false;          // checkpoints (snapshots > 0): revolve or segments
+  int seg_k = 0;              // segments: steps per segment (0: revolve or store-all)
   bool prev_valid = false;    // checkpoints: b.evb_prev holds valid gradients
   bool in_window(int n) const { return n >= nsteps - window; }  // step n (0-based) ends inside the window
   double eps_w() const { return dt * 100.0 * c->P.r_re / s2; }
@@ -258,9 +259,9 @@ int eps_direct(Adj &A, const double *Qs, const double *qraw, const double *qend,
 
 // Entropy viscosity for the reverse sweep of a step whose start state is Qn:
 // first the gradients that fed it, saved by the previous step's last stage
-// (with every stage kept: recomputed from that stage's stored input state Qprev
-// and its raw face traces, or kept from entry for the first step; with
-// checkpoints: copied aside before the step's recomputation, keep_prev), then
+// (when that stage's input state Qprev is kept: recomputed from it and its raw
+// face traces; else with checkpoints: copied aside before the step's
+// recomputation, keep_prev; else kept from entry for the first step), then
 // the viscosity itself (k_ev, into the group's muhg).  *valid: whether those
 // gradients existed.
 template <int G> int ev_forward_G(Adj &A, const double *Qn, const double *Qprev, const double *qraw_prev, bool *valid) {
@@ -273,14 +274,14 @@ template <int G> int ev_forward_G(Adj &A, const double *Qn, const double *Qprev,
   } else {
     constexpr int NG = G * G * G;
     bool ok = true;
-    if (A.ckpt) {  // kept before the step's recomputation overwrote them
+    if (Qprev) {
+      const int r = saved_grads_G<G>(A, Qprev, qraw_prev, VOL_EV_SAVE);
+      if (r) return r;
+    } else if (A.ckpt) {  // kept before the step's recomputation overwrote them
       ok = A.prev_valid;
       if (ok)
         CKA(cudaMemcpyAsync(g.EVB, A.b.evb_prev, (size_t)g.nel * 15 * NG * sizeof(double), cudaMemcpyDeviceToDevice,
                             c->st));
-    } else if (Qprev) {
-      const int r = saved_grads_G<G>(A, Qprev, qraw_prev, VOL_EV_SAVE);
-      if (r) return r;
     } else if (A.ev_valid0) {
       CKA(cudaMemcpyAsync(g.EVB, A.b.evb0, (size_t)g.nel * 15 * NG * sizeof(double), cudaMemcpyDeviceToDevice,
                           c->st));
@@ -577,7 +578,76 @@ int revolve_spine(Adj &A, int i, int j, int si, int sfree) {
   return revolve(A, i, m, si, sfree);
 }
 
+// ---- two-level scheme (DSEM_ADJ_SEGMENTS): b.stages / b.traces hold the stage
+// states and raw face traces of one segment, its step i at [i * kord, (i + 1) * kord).
+
+// Steps [b, e) out of place through the segment stash, starting from c->JQ and
+// c->QF (copied into the stash's first slot); the segment's end state and its
+// raw traces go to c->JQ and c->QF.  eps_part: the window's enstrophy partials
+// (the first sweep), or null (a recomputation).  With b.evbw the gradients that
+// each window step's last stage saves go to its slot [step in segment].
+int seg_forward(Adj &A, int b, int e, double *eps_part, cudaGraphExec_t *gx) {
+  dsem_ctx *c = A.c;
+  const int kord = c->kord;
+  const size_t nq = c->nq, nf = c->nface, npart = (size_t)c->ngrid * 5;
+  const size_t nevb = (size_t)A.g->nel * 15 * A.g->G * A.g->G * A.g->G;
+  CKA(cudaMemcpyAsync(A.b.stages, c->JQ, nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  CKA(cudaMemcpyAsync(A.b.traces, c->QF, nf * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  for (int n = b; n < e; ++n) {
+    const int i = n - b;
+    std::vector<double *> st, qf;
+    for (int k = 0; k < kord; ++k) {
+      st.push_back(A.b.stages + ((size_t)i * kord + k) * nq);
+      qf.push_back(A.b.traces + ((size_t)i * kord + k) * nf);
+    }
+    const bool last = n + 1 == e, win = A.in_window(n);
+    double *jq_next = last ? c->JQ : A.b.stages + (size_t)(i + 1) * kord * nq;
+    double *qf_next = last ? c->QF : A.b.traces + (size_t)(i + 1) * kord * nf;
+    double *part = (win && eps_part) ? eps_part + (size_t)(n - (A.nsteps - A.window)) * npart : nullptr;
+    double *evb = (win && A.b.evbw) ? A.b.evbw + (size_t)i * nevb : nullptr;
+    auto f = [&] { return forward_step(A, n, st.data(), part, qf.data(), jq_next, qf_next, evb); };
+    const int r = i == 0 ? f() : replay(c, &gx[win ? 1 : 0], f);
+    if (r) return r;
+  }
+  return DSEM_OK;
+}
+
+// Reverse of steps [e - 1 .. b] from the segment stash that seg_forward filled
+// (the end state in c->JQ).  Each step's viscosity reads gradients recomputed
+// from the previous step's stored last stage, except the segment's first step,
+// whose gradients keep_prev copied aside.  first: the first segment reversed.
+int seg_reverse(Adj &A, int b, int e, bool first, cudaGraphExec_t *gx) {
+  dsem_ctx *c = A.c;
+  const int kord = c->kord;
+  const size_t nq = c->nq, nf = c->nface;
+  const size_t nevb = (size_t)A.g->nel * 15 * A.g->G * A.g->G * A.g->G;
+  for (int m = e - 1; m >= b; --m) {
+    const int i = m - b;
+    std::vector<double *> st, qf;
+    for (int k = 0; k < kord; ++k) {
+      st.push_back(A.b.stages + ((size_t)i * kord + k) * nq);
+      qf.push_back(A.b.traces + ((size_t)i * kord + k) * nf);
+    }
+    const double *qend = m + 1 < e ? A.b.stages + (size_t)(i + 1) * kord * nq : c->JQ;
+    const double *qprev = m > b ? A.b.stages + ((size_t)(i - 1) * kord + kord - 1) * nq : nullptr;
+    const double *qfprev = m > b ? A.b.traces + ((size_t)(i - 1) * kord + kord - 1) * nf : nullptr;
+    const double *evb = A.ev ? A.g->EVB : ((A.in_window(m) && A.b.evbw) ? A.b.evbw + (size_t)i * nevb : nullptr);
+    auto f = [&] { return reverse_step(A, m, st.data(), qend, qf.data(), qprev, qfprev, evb); };
+    const int r = ((first && m == e - 1) || (A.ev && m == b)) ? f() : replay(c, &gx[A.in_window(m) ? 1 : 0], f);
+    if (r) return r;
+  }
+  return DSEM_OK;
+}
+
 }  // namespace
+
+extern "C" int dsem_set_adjoint_scheme(dsem_ctx *c, int scheme) {
+  if (!c) return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "null context");
+  if (scheme != DSEM_ADJ_REVOLVE && scheme != DSEM_ADJ_SEGMENTS)
+    return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "adjoint scheme: DSEM_ADJ_REVOLVE or DSEM_ADJ_SEGMENTS");
+  c->adj_scheme = scheme;
+  return DSEM_OK;
+}
 
 #ifdef DSEM_PHASE_TIMING
 extern "C" int dsem_debug_phase_cycles_adj(unsigned long long *out, int reset) {
@@ -628,22 +698,42 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
     }
   }
   CKA(cudaMalloc(&A.b.lr, sizeof(double)));
-  const size_t nstage = snapshots == 0 ? (size_t)nsteps * kord : (size_t)kord;
-  if (cudaMalloc(&A.b.stages, nstage * bq) != cudaSuccess) {
-    cudaGetLastError();
-    return dsem_int::fail(c, DSEM_ERR_NOMEM, "adjoint: not enough device memory for the stage states (use snapshots > 0)");
-  }
   // DSEM_ADJOINT_LEAN=1 takes the paths used when device memory is short: no
-  // optional trace or gradient slots (the same results, bit for bit, more work)
+  // optional trace or gradient slots and no segment stash (the same results,
+  // bit for bit, more work)
   const char *lean_env = std::getenv("DSEM_ADJOINT_LEAN");
   const bool lean = lean_env && lean_env[0] == '1';
-  // raw face traces of every kept stage state (with snapshots: of the step being reversed)
-  if (lean || cudaMalloc(&A.b.traces, nstage * bf) != cudaSuccess) {
-    cudaGetLastError();  // not enough memory: the reverse sweep recomputes the traces
-    A.b.traces = nullptr;
+  // two-level scheme: snapshots at the starts of segments of seg_k steps, and one
+  // segment's stage states and raw traces (the stash); revolve when they do not fit
+  int seg_k = 0, nseg = 0;
+  if (snapshots > 0 && c->adj_scheme == DSEM_ADJ_SEGMENTS && !lean) {
+    seg_k = (nsteps + snapshots - 1) / snapshots;
+    nseg = (nsteps + seg_k - 1) / seg_k;
+    if (cudaMalloc(&A.b.stages, (size_t)seg_k * kord * bq) != cudaSuccess ||
+        cudaMalloc(&A.b.traces, (size_t)seg_k * kord * bf) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(A.b.stages);
+      cudaFree(A.b.traces);
+      A.b.stages = A.b.traces = nullptr;
+      seg_k = nseg = 0;
+    }
+  }
+  A.seg_k = seg_k;
+  if (!seg_k) {
+    const size_t nstage = snapshots == 0 ? (size_t)nsteps * kord : (size_t)kord;
+    if (cudaMalloc(&A.b.stages, nstage * bq) != cudaSuccess) {
+      cudaGetLastError();
+      return dsem_int::fail(c, DSEM_ERR_NOMEM, "adjoint: not enough device memory for the stage states (use snapshots > 0)");
+    }
+    // raw face traces of every kept stage state (with snapshots: of the step being reversed)
+    if (lean || cudaMalloc(&A.b.traces, nstage * bf) != cudaSuccess) {
+      cudaGetLastError();  // not enough memory: the reverse sweep recomputes the traces
+      A.b.traces = nullptr;
+    }
   }
   A.ckpt = snapshots > 0;
-  for (int s = 0; s < snapshots; ++s) {
+  const int nslots = seg_k ? nseg : snapshots;
+  for (int s = 0; s < nslots; ++s) {
     double *p = nullptr, *pe = nullptr;
     if (cudaMalloc(&p, bq) != cudaSuccess || (A.ev && cudaMalloc(&pe, evb_bytes(A)) != cudaSuccess)) {
       cudaGetLastError();
@@ -685,6 +775,11 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
     cudaGetLastError();
     A.b.evbw = nullptr;
   }
+  if (seg_k && !A.ev && window > 0 &&  // segments: one slot per step of a segment
+      cudaMalloc(&A.b.evbw, (size_t)seg_k * nevb * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    A.b.evbw = nullptr;
+  }
   {
     // after the first (eager) step, steps are captured and replayed as CUDA
     // graphs, one per kind of step (inside or outside the window); the window's
@@ -696,12 +791,19 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
         if (x) cudaGraphExecDestroy(x);
     };
     std::vector<std::pair<int, int>> sp;
-    if (snapshots > 0) sp = spine(nsteps, snapshots);
+    if (snapshots > 0 && !seg_k) sp = spine(nsteps, snapshots);
     size_t ksp = 0;  // next snapshot of the spine
     for (int n = 0; n < nsteps; ++n) {
       if (ksp < sp.size() && sp[ksp].first == n) {  // the state after n steps, for the reverse sweep
         if ((r = save_slot(A, sp[ksp].second))) return drop(), r;
         ++ksp;
+      }
+      if (seg_k && n % seg_k == 0) {  // segments: the state at each segment's start
+        if (n > 0 && (r = save_slot(A, n / seg_k))) return drop(), r;
+        if (n / seg_k == nseg - 1) {  // the last segment runs through the stash, ready to reverse
+          if ((r = keep_prev(A)) || (r = seg_forward(A, n, nsteps, A.b.eps_part, gx))) return drop(), r;
+          break;
+        }
       }
       std::vector<double *> st, qf;
       if (snapshots == 0)
@@ -795,7 +897,24 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
         if (A.ev_valid0) CKA(cudaMemcpyAsync(A.b.slot_evb[0], A.b.evb0, evb_bytes(A), cudaMemcpyDeviceToDevice, c->st));
         A.b.slot_valid[0] = A.ev_valid0 ? 1 : 0;
       }
-      if ((r = revolve_spine(A, 0, nsteps, 0, 1))) return r;
+      if (seg_k) {
+        // segments, last first: recompute each from its snapshot into the stash, then reverse it
+        cudaGraphExec_t gf[2] = {nullptr, nullptr}, gr[2] = {nullptr, nullptr};
+        auto drop = [&]() {
+          for (auto *x : {&gf[0], &gf[1], &gr[0], &gr[1]})
+            if (*x) cudaGraphExecDestroy(*x);
+        };
+        for (int j = nseg - 1; j >= 0; --j) {
+          const int b = j * seg_k, e = std::min(nsteps, b + seg_k);
+          if (j < nseg - 1 &&
+              ((r = load_slot(A, j)) || (r = keep_prev(A)) || (r = seg_forward(A, b, e, nullptr, gf))))
+            return drop(), r;
+          if ((r = seg_reverse(A, b, e, j == nseg - 1, gr))) return drop(), r;
+        }
+        drop();
+      } else if ((r = revolve_spine(A, 0, nsteps, 0, 1))) {
+        return r;
+      }
     }
   }
   k_sum_into<<<1, 256, 0, c->st>>>(A.b.lrp, A.g->nel, A.b.lr);  // dJ/d(1/Re) of the volume terms

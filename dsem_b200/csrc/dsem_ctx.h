@@ -99,6 +99,7 @@ struct dsem_ctx {
   double *QLB = nullptr;  // [elem][3][5][L*G^2] per group at Group::l0
   bool keep_lob = false;  // the last stage of every step stores them (dsem_keep_lobatto)
   bool lob_valid = false; // QLB holds the arrays of the last stage run
+  int adj_scheme = 0;     // dsem_adjoint with snapshots > 0: DSEM_ADJ_REVOLVE or DSEM_ADJ_SEGMENTS
   cudaGraphExec_t gexec = nullptr;
   int graph_key = -1;
   long long graph_launches = 0;

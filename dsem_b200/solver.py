@@ -22,7 +22,7 @@ EXPORTS = ("dsem_create", "dsem_destroy", "dsem_last_error", "dsem_upload_q", "d
            "dsem_save_state", "dsem_load_state", "dsem_shard_info", "dsem_shard_stage", "dsem_diag_sums",
            "dsem_set_boundary", "dsem_autotune", "dsem_set_vol_variant", "dsem_shard_enqueue", "dsem_shard_finish",
            "dsem_get_stream", "dsem_keep_lobatto", "dsem_write_restart", "dsem_read_restart",
-           "dsem_set_les_sensors")
+           "dsem_set_les_sensors", "dsem_set_adjoint_scheme")
 
 
 class DsemError(RuntimeError):
@@ -78,6 +78,7 @@ def lib(path=None):
         L.dsem_diag_batch.argtypes = [vp, dp, C.c_int, dp, dp, dp]
         L.dsem_set_les.argtypes = [vp, C.c_double, C.c_double]
         L.dsem_set_les_sensors.argtypes = [vp, C.c_int, C.c_int]
+        L.dsem_set_adjoint_scheme.argtypes = [vp, C.c_int]
         L.dsem_set_boundary.argtypes = [vp, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]
         L.dsem_autotune.argtypes = [vp, C.c_int, C.POINTER(C.c_int), dp]
         L.dsem_set_vol_variant.argtypes = [vp, C.c_int, C.c_int]
@@ -257,9 +258,15 @@ class Solver:
         self._check(lib().dsem_get_nut(self.h, _dptr(m), self.ldx))
         return m
 
-    def adjoint(self, dt, nsteps, window, snapshots=0, want_grad=True):
+    ADJ_SCHEMES = {"revolve": 0, "segments": 1}
+
+    def adjoint(self, dt, nsteps, window, snapshots=0, want_grad=True, scheme="revolve"):
         """J = sum of eps*dt over the last `window` of `nsteps` steps and its
-        gradient: returns (J, dJ/dJQ0 in the upload layout or None, dJ/d(1/Re), ms)."""
+        gradient: returns (J, dJ/dJQ0 in the upload layout or None, dJ/d(1/Re), ms).
+        snapshots > 0 recomputes steps by `scheme`: "revolve" (binomial
+        checkpointing) or "segments" (snapshots at segment starts plus the stage
+        states of the segment being reversed); see dsem_set_adjoint_scheme."""
+        self._check(lib().dsem_set_adjoint_scheme(self.h, self.ADJ_SCHEMES[scheme]))
         J, lr, ms = C.c_double(), C.c_double(), C.c_double()
         g = np.zeros(self.qshape()) if want_grad else None
         self._check(lib().dsem_adjoint(self.h, float(dt), int(nsteps), int(window), int(snapshots), C.byref(J),

@@ -296,6 +296,21 @@ int dsem_diag_batch(dsem_ctx *ctx, const double *dt, int first, double *ke, doub
 int dsem_adjoint(dsem_ctx *ctx, double dt, int nsteps, int window, int snapshots, double *J, double *dJdQ0,
                  int ldx, double *dJdinvRe, double *ms);
 
+/* How dsem_adjoint recomputes steps when snapshots = s > 0.
+ * DSEM_ADJ_REVOLVE (the default): s step states, binomial checkpointing
+ *   (Griewank's revolve order): the fewest recomputed steps for s stored states.
+ * DSEM_ADJ_SEGMENTS: two levels.  The first sweep keeps the state at the start
+ *   of each of ceil(nsteps / K) segments of K = ceil(nsteps / s) steps; the
+ *   reverse sweep recomputes one segment at a time from its snapshot and keeps
+ *   that segment's K * kord stage states and their face traces in device memory
+ *   while it reverses the segment (the last segment is kept by the first sweep).
+ *   Every step is recomputed at most once, for K * kord more stage states of
+ *   device memory.  When those do not fit, the call falls back to revolve.
+ * Both give the store-all gradient (snapshots == 0) bit for bit. */
+#define DSEM_ADJ_REVOLVE 0
+#define DSEM_ADJ_SEGMENTS 1
+int dsem_set_adjoint_scheme(dsem_ctx *ctx, int scheme);
+
 /* Size of the static device array that holds the working buffers of
  * dsem_rhs_noalloc: 2^20 doubles (8 MiB) on every GPU that loads the library. */
 #define DSEM_NOALLOC_SCRATCH_DOUBLES (1 << 20)

@@ -81,6 +81,24 @@ def test_adjoint_checkpointing_gives_the_same_gradient():
     s.close()
 
 
+@pytest.mark.parametrize("snaps", [1, 2, 3, 6, 7, 10])
+def test_adjoint_segments_give_the_same_gradient(snaps):
+    """Two-level checkpointing (DSEM_ADJ_SEGMENTS: snapshots at segment starts, one
+    segment's stage states and traces kept while it is reversed): segments of 7, 4, 3, 2
+    and 1 steps, the last one shorter, the window (3 steps) across a segment boundary.
+    Same J, dJ/dJQ0 and dJ/d(1/Re) as store-all, bit for bit."""
+    from dsem_b200.solver import Solver
+    box, q, dt = _case(2, 4, 800.0, seed=5)
+    s = Solver(box.desc(), re=800.0)
+    s.upload(q)
+    J0, g0, lr0, _ = s.adjoint(dt, 7, 3, snapshots=0)
+    J1, g1, lr1, _ = s.adjoint(dt, 7, 3, snapshots=snaps, scheme="segments")
+    assert J1 == J0 and lr1 == lr0
+    assert np.array_equal(g1, g0)
+    assert np.array_equal(s.download(), q)  # the state is restored
+    s.close()
+
+
 @pytest.mark.parametrize("snaps", [0, 2])
 def test_adjoint_low_memory_paths_give_the_same_gradient(monkeypatch, snaps):
     """Without the optional trace and saved-gradient slots (DSEM_ADJOINT_LEAN=1,
@@ -185,9 +203,9 @@ def test_adjoint_with_entropy_viscosity(oracle_mod, n, p, nsteps, window, preste
 
 @pytest.mark.parametrize("prestep", [0, 2])
 def test_entropy_viscosity_adjoint_with_checkpoints(prestep):
-    """Binomial checkpointing with entropy viscosity: each checkpoint also keeps the gradients its
-    step's viscosity reads, and the step being reversed keeps its own copy before recomputation.
-    Every snapshot count gives the store-all gradient bit for bit."""
+    """Checkpointing with entropy viscosity, binomial and two-level: each checkpoint also keeps
+    the gradients its step's viscosity reads, and the step (or segment) being reversed keeps its
+    own copy before recomputation.  Every snapshot count gives the store-all gradient bit for bit."""
     from dsem_b200.solver import Solver
     box, q, dt = _case(2, 3, 400.0, seed=13)
     s = Solver(box.desc(), re=400.0, **EV)
@@ -198,14 +216,15 @@ def test_entropy_viscosity_adjoint_with_checkpoints(prestep):
     J0, g0, lr0, _ = s.adjoint(dt, 7, 3, snapshots=0)
     assert np.abs(g0).max() > 0
     for snaps in (1, 2, 3, 6):
-        s.upload(q0)
-        if prestep:  # the same gradients behind the first step's viscosity
-            s.upload(q)
-            s.step(dt, prestep)
-        J1, g1, lr1, _ = s.adjoint(dt, 7, 3, snapshots=snaps)
-        assert J1 == J0, snaps
-        assert lr1 == lr0, snaps
-        assert np.array_equal(g1, g0), snaps
+        for scheme in ("revolve", "segments"):
+            s.upload(q0)
+            if prestep:  # the same gradients behind the first step's viscosity
+                s.upload(q)
+                s.step(dt, prestep)
+            J1, g1, lr1, _ = s.adjoint(dt, 7, 3, snapshots=snaps, scheme=scheme)
+            assert J1 == J0, (snaps, scheme)
+            assert lr1 == lr0, (snaps, scheme)
+            assert np.array_equal(g1, g0), (snaps, scheme)
     s.close()
 
 
