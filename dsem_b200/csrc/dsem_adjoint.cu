@@ -78,6 +78,8 @@ struct Adj {
   int nsteps = 0, window = 0;
   long long launches = 0;
   bool ev = false;            // entropy viscosity on
+  bool les = false;           // static Smagorinsky on (never together with ev)
+  bool visc = false;          // ev or les: a viscosity from the previous step's saved gradients
   bool ev_valid0 = false;     // the gradients behind the first step's viscosity were valid on entry
   bool levb_pending = false;  // b.levb holds the demand on the next-to-reverse step's saved gradients
   bool ckpt = false;          // checkpoints (snapshots > 0): revolve or segments
@@ -86,6 +88,9 @@ struct Adj {
   bool in_window(int n) const { return n >= nsteps - window; }  // step n (0-based) ends inside the window
   double eps_w() const { return dt * 100.0 * c->P.r_re / s2; }
 };
+
+// The context's flag for "the saved gradients exist" that the step's viscosity model reads
+bool &grad_flag(Adj &A) { return A.les ? A.c->grad_valid : A.c->ev_grad_valid; }
 
 // Adjoint of one stage, the RK steps around it fused in: dJ/dQt += cdt dJ/dQ
 // before, dJ/dQ += R'^T dJ/dQt and dJ/dQt *= ark after.  eps_w != 0: the stage
@@ -124,7 +129,7 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, d
     using C = VolAdjCfg<G>;
     static std::atomic<unsigned long long> attr{0}, attr_ev{0};
     CKA(set_smem_once(k_vol_adj<G, false>, C::SMEM, attr));
-    if (A.ev) CKA(set_smem_once(k_vol_adj<G, true>, C::SMEM, attr_ev));
+    if (A.visc) CKA(set_smem_once(k_vol_adj<G, true>, C::SMEM, attr_ev));
     VolAdjArgs va{};
     va.JQ = Qs;
     va.jac = g.jac;
@@ -139,10 +144,11 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, d
     va.eps_w = eps_w;
     va.JQe = JQe;
     va.P = c->P;
-    if (A.ev) {
-      va.muhg = g.muhg;
+    if (A.visc) {
+      va.muhg = A.les ? g.nuhg : g.muhg;
       va.lmuhg = A.b.lmuhg;
       va.levb = levb;
+      va.les = A.les ? 1 : 0;
     }
     {  // one block per SM (shared memory): prefetch one wave ahead
       int nsm = 0;
@@ -157,7 +163,7 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, d
     }
     k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lff, c->P.re, A.b.lvf, ml.nrm, qraw, c->QF);
     CKA(cudaGetLastError());
-    if (A.ev)
+    if (A.visc)
       k_vol_adj<G, true><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
     else
       k_vol_adj<G, false><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
@@ -275,7 +281,7 @@ template <int G> int ev_forward_G(Adj &A, const double *Qn, const double *Qprev,
     constexpr int NG = G * G * G;
     bool ok = true;
     if (Qprev) {
-      const int r = saved_grads_G<G>(A, Qprev, qraw_prev, VOL_EV_SAVE);
+      const int r = saved_grads_G<G>(A, Qprev, qraw_prev, A.les ? VOL_SAVE : VOL_EV_SAVE);
       if (r) return r;
     } else if (A.ckpt) {  // kept before the step's recomputation overwrote them
       ok = A.prev_valid;
@@ -288,18 +294,37 @@ template <int G> int ev_forward_G(Adj &A, const double *Qn, const double *Qprev,
     } else {
       ok = false;
     }
-    EvArgs e{};
-    e.JQ = Qn;
-    e.sq = 5LL * NG;
-    e.jac = g.jac;
-    e.hd = g.hd;
-    e.EVB = g.EVB;
-    e.muhg = g.muhg;
-    e.valid = ok ? 1 : 0;
-    e.P = c->P;
-    e.ecase = g.ecase;
-    e.rec = c->d_rec;
-    CKA(Launch<G>::ev(e, g.nel, c->st));
+    if (A.les) {  // simpleSmag (k_les), into the group's nuhg
+      LesArgs a{};
+      a.JQ = Qn;
+      a.sq = 5LL * NG;
+      a.jac = g.jac;
+      a.hd = g.hd;
+      a.EVB = g.EVB;
+      a.nuhg = g.nuhg;
+      a.sens = g.sens;
+      a.sensors = 0;
+      a.valid = ok ? 1 : 0;
+      a.re = c->P.re;
+      a.cs = c->les_cs;
+      a.numax = c->les_numax;
+      a.ecase = g.ecase;
+      a.rec = c->d_rec;
+      CKA(Launch<G>::les(a, g.nel, c->st));
+    } else {
+      EvArgs e{};
+      e.JQ = Qn;
+      e.sq = 5LL * NG;
+      e.jac = g.jac;
+      e.hd = g.hd;
+      e.EVB = g.EVB;
+      e.muhg = g.muhg;
+      e.valid = ok ? 1 : 0;
+      e.P = c->P;
+      e.ecase = g.ecase;
+      e.rec = c->d_rec;
+      CKA(Launch<G>::ev(e, g.nel, c->st));
+    }
     CKA(cudaMemsetAsync(A.b.lmuhg, 0, (size_t)g.nel * NG * sizeof(double), c->st));
     ++A.launches;
     *valid = ok;
@@ -315,16 +340,33 @@ template <int G> int ev_adjoint_G(Adj &A, const double *Qn) {
     (void)Qn; (void)g;
     return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
   } else {
-    EvAdjArgs e{};
-    e.JQ = Qn;
-    e.jac = g.jac;
-    e.hd = g.hd;
-    e.EVB = g.EVB;
-    e.LMU = A.b.lmuhg;
-    e.LQ = A.b.lq;
-    e.LEVB = A.b.levb;
-    e.P = c->P;
-    k_ev_adj<G><<<g.nel, 128, 0, c->st>>>(e);
+    if (A.les) {
+      LesAdjArgs e{};
+      e.JQ = Qn;
+      e.jac = g.jac;
+      e.hd = g.hd;
+      e.EVB = g.EVB;
+      e.LNU = A.b.lmuhg;
+      e.LQ = A.b.lq;
+      e.LEVB = A.b.levb;
+      e.LR = A.b.lrp;
+      e.re = c->P.re;
+      e.cs = c->les_cs;
+      e.numax = c->les_numax;
+      e.valid = 1;
+      k_les_adj<G><<<g.nel, 128, 0, c->st>>>(e);
+    } else {
+      EvAdjArgs e{};
+      e.JQ = Qn;
+      e.jac = g.jac;
+      e.hd = g.hd;
+      e.EVB = g.EVB;
+      e.LMU = A.b.lmuhg;
+      e.LQ = A.b.lq;
+      e.LEVB = A.b.levb;
+      e.P = c->P;
+      k_ev_adj<G><<<g.nel, 128, 0, c->st>>>(e);
+    }
     CKA(cudaGetLastError());
     ++A.launches;
     return DSEM_OK;
@@ -363,19 +405,19 @@ int reverse_step(Adj &A, int n, double *const *st, const double *qend, double *c
     if (r) return r;
   }
   bool ev_valid = false;
-  if (A.ev) {
+  if (A.visc) {
     const int r = ev_forward(A, st[0], qprev, qfprev, &ev_valid);
     if (r) return r;
   }
   for (int kk = c->kord; kk >= 1; --kk) {
     const bool eps_here = win && kk == c->kord;
-    const double *levb = (A.ev && kk == c->kord && A.levb_pending) ? A.b.levb : nullptr;
+    const double *levb = (A.visc && kk == c->kord && A.levb_pending) ? A.b.levb : nullptr;
     int r = stage_adjoint(A, st[kk - 1], qend, eps_here ? A.eps_w() : 0.0, c->crk[kk - 1] * A.dt,
                           c->ark[kk - 1], qf ? qf[kk - 1] : nullptr, levb, kk == c->kord, kk > 1,
                           kk > 1 ? c->crk[kk - 2] * A.dt : 0.0);
     if (r) return r;
   }
-  if (A.ev) {  // the step's viscosity, from its start state and the previous step's gradients
+  if (A.visc) {  // the step's viscosity, from its start state and the previous step's gradients
     if (ev_valid) {
       const int r = ev_adjoint(A, st[0]);
       if (r) return r;
@@ -402,11 +444,11 @@ int forward_step(Adj &A, int n, double *const *st, double *eps_part, double *con
     if (!oop && st) CKA(cudaMemcpyAsync(st[kk - 1], c->JQ, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
     if (!oop && qf)
       CKA(cudaMemcpyAsync(qf[kk - 1], c->QF, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-    if (A.ev && kk == 1) {  // the step's entropy viscosity (tstep.f90:36-38)
-      const int r = dsem_int::ev(c, oop ? st[0] : nullptr);
+    if (A.visc && kk == 1) {  // the step's entropy or Smagorinsky viscosity (tstep.f90:36-43)
+      const int r = A.les ? dsem_int::les(c, oop ? st[0] : nullptr) : dsem_int::ev(c, oop ? st[0] : nullptr);
       if (r) return r;
     }
-    const bool save = (win || A.ev) && kk == c->kord;
+    const bool save = (win || A.visc) && kk == c->kord;
     int r;
     if (oop) {
       const bool last = kk == c->kord;
@@ -419,7 +461,7 @@ int forward_step(Adj &A, int n, double *const *st, double *eps_part, double *con
     if (r) return r;
     A.launches += 2 * (long long)c->groups.size() + 2 * (long long)c->mlists.size();
   }
-  if (A.ev) c->ev_grad_valid = true;  // the last stage saved the gradients of the next viscosity
+  if (A.visc) grad_flag(A) = true;  // the last stage saved the gradients of the next viscosity
   if (win && eps_part) {  // the step's enstrophy partials, summed on the host after the sweep
     int r = dsem_int::eps_enqueue(c, oop ? jq_next : nullptr, eps_part, oop ? evb_slot : nullptr);
     if (r) return r;
@@ -468,9 +510,9 @@ size_t evb_bytes(const Adj &A) {
 int load_slot(Adj &A, int si) {
   dsem_ctx *c = A.c;
   CKA(cudaMemcpyAsync(c->JQ, A.b.slots[si], c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-  if (A.ev) {
+  if (A.visc) {
     CKA(cudaMemcpyAsync(A.g->EVB, A.b.slot_evb[si], evb_bytes(A), cudaMemcpyDeviceToDevice, c->st));
-    c->ev_grad_valid = A.b.slot_valid[si] != 0;
+    grad_flag(A) = A.b.slot_valid[si] != 0;
   }
   return dsem_int::traces(c);
 }
@@ -480,9 +522,9 @@ int load_slot(Adj &A, int si) {
 int save_slot(Adj &A, int si) {
   dsem_ctx *c = A.c;
   CKA(cudaMemcpyAsync(A.b.slots[si], c->JQ, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-  if (A.ev) {
+  if (A.visc) {
     CKA(cudaMemcpyAsync(A.b.slot_evb[si], A.g->EVB, evb_bytes(A), cudaMemcpyDeviceToDevice, c->st));
-    A.b.slot_valid[si] = c->ev_grad_valid ? 1 : 0;
+    A.b.slot_valid[si] = grad_flag(A) ? 1 : 0;
   }
   return DSEM_OK;
 }
@@ -490,10 +532,10 @@ int save_slot(Adj &A, int si) {
 // Before the recomputation of a step about to be reversed: the gradients its
 // viscosity reads, which that step's last stage overwrites.
 int keep_prev(Adj &A) {
-  if (!A.ev) return DSEM_OK;
+  if (!A.visc) return DSEM_OK;
   dsem_ctx *c = A.c;
   CKA(cudaMemcpyAsync(A.b.evb_prev, A.g->EVB, evb_bytes(A), cudaMemcpyDeviceToDevice, c->st));
-  A.prev_valid = c->ev_grad_valid;
+  A.prev_valid = grad_flag(A);
   return DSEM_OK;
 }
 
@@ -631,9 +673,9 @@ int seg_reverse(Adj &A, int b, int e, bool first, cudaGraphExec_t *gx) {
     const double *qend = m + 1 < e ? A.b.stages + (size_t)(i + 1) * kord * nq : c->JQ;
     const double *qprev = m > b ? A.b.stages + ((size_t)(i - 1) * kord + kord - 1) * nq : nullptr;
     const double *qfprev = m > b ? A.b.traces + ((size_t)(i - 1) * kord + kord - 1) * nf : nullptr;
-    const double *evb = A.ev ? A.g->EVB : ((A.in_window(m) && A.b.evbw) ? A.b.evbw + (size_t)i * nevb : nullptr);
+    const double *evb = A.visc ? A.g->EVB : ((A.in_window(m) && A.b.evbw) ? A.b.evbw + (size_t)i * nevb : nullptr);
     auto f = [&] { return reverse_step(A, m, st.data(), qend, qf.data(), qprev, qfprev, evb); };
-    const int r = ((first && m == e - 1) || (A.ev && m == b)) ? f() : replay(c, &gx[A.in_window(m) ? 1 : 0], f);
+    const int r = ((first && m == e - 1) || (A.visc && m == b)) ? f() : replay(c, &gx[A.in_window(m) ? 1 : 0], f);
     if (r) return r;
   }
   return DSEM_OK;
@@ -666,10 +708,11 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   if (nsteps < 1 || window < 0 || window > nsteps || snapshots < 0 || !(dt > 0.0))
     return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "adjoint: need nsteps >= 1, 0 <= window <= nsteps, snapshots >= 0, dt > 0");
   if (c->ncase != 1 || c->groups.size() != 1 || c->mlists.size() != 1 || c->nnc > 0 || !c->groups[0].diag ||
-      c->P.ducros || c->les || c->ncut > 0 || c->nbnd > 0)
+      c->P.ducros || (c->les && (c->shock || c->les_sensors)) || c->ncut > 0 || c->nbnd > 0)
     return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED,
                           "adjoint: one case, one element order, conforming periodic mortars, axis-aligned elements, no "
-                          "Ducros sensor, LES, boundary faces or sharding");
+                          "Ducros sensor, no LES together with entropy viscosity or the LES sensors, no boundary faces "
+                          "or sharding");
   if (c->groups[0].G > 7) return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
   if (dJdQ0 && ldx < c->groups[0].G) return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "ldx smaller than the number of Gauss points");
   int r = upload_ops_here(c);
@@ -687,11 +730,13 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   for (double **p : {&A.b.qfr, &A.b.lff, &A.b.lvf, &A.b.lqf, &A.b.lqr}) CKA(cudaMalloc(p, bf));
   CKA(cudaMalloc(&A.b.lrp, (size_t)A.g->nel * sizeof(double)));
   A.ev = c->shock != 0;
-  if (A.ev) {
+  A.les = c->les != 0;
+  A.visc = A.ev || A.les;
+  if (A.visc) {
     const size_t ng = (size_t)A.g->nel * A.g->G * A.g->G * A.g->G;
     CKA(cudaMalloc(&A.b.lmuhg, ng * sizeof(double)));
     CKA(cudaMalloc(&A.b.levb, 15 * ng * sizeof(double)));
-    A.ev_valid0 = c->ev_grad_valid;
+    A.ev_valid0 = grad_flag(A);
     if (A.ev_valid0) {  // the gradients behind the first step's viscosity
       CKA(cudaMalloc(&A.b.evb0, 15 * ng * sizeof(double)));
       CKA(cudaMemcpyAsync(A.b.evb0, A.g->EVB, 15 * ng * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
@@ -735,18 +780,18 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   const int nslots = seg_k ? nseg : snapshots;
   for (int s = 0; s < nslots; ++s) {
     double *p = nullptr, *pe = nullptr;
-    if (cudaMalloc(&p, bq) != cudaSuccess || (A.ev && cudaMalloc(&pe, evb_bytes(A)) != cudaSuccess)) {
+    if (cudaMalloc(&p, bq) != cudaSuccess || (A.visc && cudaMalloc(&pe, evb_bytes(A)) != cudaSuccess)) {
       cudaGetLastError();
       cudaFree(p);
       return dsem_int::fail(c, DSEM_ERR_NOMEM, "adjoint: not enough device memory for the snapshots");
     }
     A.b.slots.push_back(p);
-    if (A.ev) {
+    if (A.visc) {
       A.b.slot_evb.push_back(pe);
       A.b.slot_valid.push_back(0);
     }
   }
-  if (A.ev && A.ckpt) CKA(cudaMalloc(&A.b.evb_prev, evb_bytes(A)));
+  if (A.visc && A.ckpt) CKA(cudaMalloc(&A.b.evb_prev, evb_bytes(A)));
   std::vector<double> tmp(1, dt);
   if ((r = dsem_int::set_dt(c, tmp.data()))) return r;
   cudaEvent_t e0, e1;
@@ -770,12 +815,12 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   // the gradients saved by each window step's last stage, for the reverse
   // sweep's direct enstrophy term (else recomputed there)
   const size_t nevb = (size_t)A.g->nel * 15 * A.g->G * A.g->G * A.g->G;
-  if (oop && !A.ev && window > 0 && !lean &&
+  if (oop && !A.visc && window > 0 && !lean &&
       cudaMalloc(&A.b.evbw, (size_t)window * nevb * sizeof(double)) != cudaSuccess) {
     cudaGetLastError();
     A.b.evbw = nullptr;
   }
-  if (seg_k && !A.ev && window > 0 &&  // segments: one slot per step of a segment
+  if (seg_k && !A.visc && window > 0 &&  // segments: one slot per step of a segment
       cudaMalloc(&A.b.evbw, (size_t)seg_k * nevb * sizeof(double)) != cudaSuccess) {
     cudaGetLastError();
     A.b.evbw = nullptr;
@@ -879,10 +924,10 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
         // the gradients step n's last stage saved: kept by the forward sweep, or with
         // entropy viscosity the group's EVB (the forward sweep's last step, then
         // each reverse step's recomputation for the step before it)
-        const double *evb = A.ev ? A.g->EVB
+        const double *evb = A.visc ? A.g->EVB
                                  : ((A.in_window(n) && A.b.evbw) ? A.b.evbw + (size_t)(n - (nsteps - window)) * nevb
                                                                  : nullptr);
-        if (n == nsteps - 1 || (A.ev && n == 0)) {  // launch sequences of their own: eager
+        if (n == nsteps - 1 || (A.visc && n == 0)) {  // launch sequences of their own: eager
           if ((r = reverse_step(A, n, st.data(), qend, qfp, qprev, qfprev, evb))) return drop(), r;
           continue;
         }
@@ -893,7 +938,7 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
       drop();
     } else {
       CKA(cudaMemcpyAsync(A.b.slots[0], A.b.q0, bq, cudaMemcpyDeviceToDevice, c->st));
-      if (A.ev) {  // the first step's viscosity reads the gradients from before the run
+      if (A.visc) {  // the first step's viscosity reads the gradients from before the run
         if (A.ev_valid0) CKA(cudaMemcpyAsync(A.b.slot_evb[0], A.b.evb0, evb_bytes(A), cudaMemcpyDeviceToDevice, c->st));
         A.b.slot_valid[0] = A.ev_valid0 ? 1 : 0;
       }

@@ -784,6 +784,116 @@ template <int G> __global__ void __launch_bounds__(128) k_ev_adj(EvAdjArgs A) {
   }
 }
 
+// Smagorinsky viscosity at a step's start (k_les: simpleSmag, staticSmag.f90:191-201),
+// transposed: nu = min(max(Re (Cs h)^2 |S|, 0), numax), |S| = sqrt(2 S_ij S_ij) from the
+// velocity gradients of the gradients saved by the previous step's last stage.  From
+// dJ/dnu (LNU) it adds dJ/dJQ of the step's start state into LQ, writes dJ/dEVB into
+// LEVB (fields 12..14, the temperature gradients, get 0) and adds the element's
+// dJ/d(1/Re) (nu depends on Re directly) into LR.  No shock or density sensor.
+struct LesAdjArgs {
+  const double *JQ, *jac, *hd, *EVB, *LNU;
+  double *LQ, *LEVB, *LR;
+  double re, cs, numax;
+  int valid;  // the saved gradients existed (else nu = 0 and nothing flows back)
+};
+
+template <int G> __global__ void __launch_bounds__(128) k_les_adj(LesAdjArgs A) {
+  constexpr int NG = G * G * G;
+  const int k = blockIdx.x;
+  const double *JQ = A.JQ + (long long)k * 5 * NG;
+  const double *E = A.EVB + (long long)k * 15 * NG;
+  const double jac0 = A.jac[(long long)k * NG];
+  double *LQ = A.LQ + (long long)k * 5 * NG;
+  double *LE = A.LEVB + (long long)k * 15 * NG;
+  double lr = 0.0;
+  for (int p = threadIdx.x; p < NG; p += blockDim.x) {
+    double g[3][4] = {}, lg[3][4] = {}, lJ[4] = {0.0, 0.0, 0.0, 0.0};
+    if (A.valid) {
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) g[d][v] = E[(v * 3 + d) * NG + p];
+      // forward, as k_les
+      const double rho = JQ[p] * jac0;
+      const double vel[3] = {JQ[NG + p] / rho, JQ[2 * NG + p] / rho, JQ[3 * NG + p] / rho};
+      double V[3][3];  // V[i][d] = d vel_i / d x_d
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) V[i][d] = (g[d][1 + i] - g[d][0] * vel[i]) / rho;
+      double Sm[3][3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Sm[i][j] = i == j ? V[i][i] : 0.5 * (V[i][j] + V[j][i]);
+      double X = 0.0;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) X += 2.0 * Sm[i][j] * Sm[i][j];
+      const double S = sqrt(X);
+      const double dg = A.hd[(long long)k * NG + p];
+      const double c2 = A.re * (A.cs * dg) * (A.cs * dg);
+      const double nu = c2 * S;
+      const double mx = nu >= 0.0 ? nu : 0.0;
+      const double lnu = (nu >= 0.0 && mx <= A.numax) ? A.LNU[(long long)k * NG + p] : 0.0;
+      lr += -lnu * A.re * nu;  // nu = Re (Cs h)^2 |S|: d nu / d(1/Re) = -Re nu
+      if (S > 0.0 && lnu != 0.0) {
+        const double lX = lnu * c2 * 0.5 / S;
+        double lV[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) lV[i][j] = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const double lS = lX * 4.0 * Sm[i][j];
+            if (i == j) {
+              lV[i][i] += lS;
+            } else {
+              lV[i][j] += 0.5 * lS;
+              lV[j][i] += 0.5 * lS;
+            }
+          }
+        double lrho = 0.0, lvel[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const double l = lV[i][d];
+            lg[d][1 + i] += l / rho;
+            lg[d][0] += -l * vel[i] / rho;
+            lvel[i] += -l * g[d][0] / rho;
+            lrho += -l * V[i][d] / rho;
+          }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          lJ[1 + i] += lvel[i] / rho;
+          lrho += -lvel[i] * vel[i] / rho;
+        }
+        lJ[0] += lrho * jac0;
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) LQ[v * NG + p] += lJ[v];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) LE[(v * 3 + d) * NG + p] = lg[d][v];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) LE[(12 + d) * NG + p] = 0.0;
+  }
+  // the element's dJ/d(1/Re): warp sums, then the four warps' sums in order
+  __shared__ double red[4];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lr += __shfl_xor_sync(0xffffffffu, lr, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = lr;
+  __syncthreads();
+  if (threadIdx.x == 0) A.LR[k] += red[0] + red[1] + red[2] + red[3];
+}
+
 struct VolAdjArgs {
   const double *JQ;
   const double *jac, *gg, *gm;  // diagonal metric layout
@@ -799,6 +909,7 @@ struct VolAdjArgs {
   const double *muhg;           // entropy viscosity at the Gauss points (null: none)
   double *lmuhg;                // in/out with muhg: dJ/dmu at the Gauss points, accumulated over stages
   const double *levb;           // dJ/d(gradients this stage saved for the next step's viscosity), or null
+  int les;                      // with muhg: it holds the Smagorinsky nu_t (amu = 1 + nu rho), not mu
   Phys P;
 };
 
@@ -1051,14 +1162,22 @@ template <int G, bool EVK> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1
       }
       const double gd = gm[D * NL + qi];
       // entropy viscosity at this Lobatto point (EV_Prolong, as k_vol_diag): amu = 1 + mu
+      // or Smagorinsky (nut_prolong, clipped at 0, as k_vol_diag): amu = 1 + nu rho
       constexpr bool ev = EVK;
-      double amu = 1.0, lam = 0.0;
+      double amu = 1.0, lam = 0.0, nuL = 0.0;
+      bool nu_on = false;
       if constexpr (ev) {
         const int g0 = gbase<G>(D, a, b);
         double acc = Op<G>::B(s, 0) * MU[g0];
 #pragma unroll
         for (int kk = 1; kk < G; ++kk) acc = __fma_rn(Op<G>::B(s, kk), MU[g0 + kk * xs], acc);
-        amu = 1.0 + acc;
+        if (A.les) {
+          nu_on = !(acc < 0.0);
+          nuL = nu_on ? acc : 0.0;
+          amu = amu + nuL * Q[0];
+        } else {
+          amu = 1.0 + acc;
+        }
       }
       double *lamp = ev ? &lam : nullptr;
       if (s == 0 || s == L - 1) {  // face point: VF = gd * fv
@@ -1104,7 +1223,14 @@ template <int G, bool EVK> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1
         const int fi = diag_field(D, jf);
         LG[jf * NL + qs] = lG[fi % 3][fi / 3];
       }
-      if constexpr (ev) LB[qs] = lam;  // dJ/d amu, in this point's (read) slot of field 0
+      if constexpr (ev) {  // dJ/d(prolonged viscosity), in this point's (read) slot of field 0
+        if (A.les) {
+          LL[qs] += lam * nuL;  // amu = 1 + nu rho: the density's share
+          LB[qs] = nu_on ? lam * Q[0] : 0.0;
+        } else {
+          LB[qs] = lam;
+        }
+      }
     }
     __syncthreads();
     PHASE_MARK(27);
@@ -1198,7 +1324,7 @@ template <int G, bool EVK> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1
   // ---- reverse of the temperature gradients this stage saved for the next
   // step's entropy viscosity (vol_diag_tgrad): T1_D = gmetg(D,D) D T(Lobatto
   // line of the state along D), T = gamma p / rho (RHS.f90:66-83)
-  if (EVK && A.levb) {
+  if (EVK && !A.les && A.levb) {
     const double *lt1 = A.levb + (long long)k * 15 * NG + 12 * NG;
     auto tgrad_dir = [&](auto Dc) {
       constexpr int D = decltype(Dc)::value;

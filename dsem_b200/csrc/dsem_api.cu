@@ -412,11 +412,12 @@ int enqueue_ev(dsem_ctx *c, long long *launches, const double *jq = nullptr) {
 }
 
 // Smagorinsky viscosity from the last Fluxes call's gradients (tstep.f90:40-43)
-int enqueue_les(dsem_ctx *c, long long *launches) {
+int enqueue_les(dsem_ctx *c, long long *launches, const double *jq = nullptr) {
+  if (!jq) jq = c->JQ;
   const int r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
     auto &g = c->groups[j];
     LesArgs a{};
-    a.JQ = c->JQ + g.q0;
+    a.JQ = jq + g.q0;
     a.sq = 5LL * g.G * g.G * g.G;
     a.jac = g.jac;
     a.hd = g.hd;
@@ -1880,6 +1881,10 @@ int traces(dsem_ctx *c) {
 int ev(dsem_ctx *c, const double *jq) {
   long long l = 0;
   return enqueue_ev(c, &l, jq);
+}
+int les(dsem_ctx *c, const double *jq) {
+  long long l = 0;
+  return enqueue_les(c, &l, jq);
 }
 // One RK stage of a single-group context with periodic conforming mortars only,
 // out of place: state io.jq_in and its raw face traces io.qf_in (both left

@@ -137,6 +137,7 @@ int fail(dsem_ctx *c, int code, const std::string &msg);
 int stage(dsem_ctx *c, int kk, bool save);  // one RK stage on c->JQ (eager launches)
 int traces(dsem_ctx *c);                    // face traces of c->JQ
 int ev(dsem_ctx *c, const double *jq = nullptr);  // entropy viscosity of jq (null: c->JQ; valid: c->ev_grad_valid)
+int les(dsem_ctx *c, const double *jq = nullptr);  // Smagorinsky viscosity of jq (null: c->JQ; valid: c->grad_valid)
 struct StageIO {
   double *jq_in;        // stage input state (read only)
   const double *qf_in;  // its raw face traces (read only)

@@ -237,3 +237,105 @@ def test_entropy_viscosity_adjoint_limits():
         s.adjoint(dt, 2, 1)
     assert e.value.code == -5
     s.close()
+
+
+LES = dict(cs=0.15, numax=1e3)
+
+
+@pytest.mark.parametrize("n,p,nsteps,window,prestep,numax", [(2, 3, 4, 2, 0, 1e3), (2, 4, 3, 3, 2, 1e3),
+                                                              (2, 3, 3, 2, 2, 30.0)])
+def test_adjoint_with_smagorinsky(oracle_mod, n, p, nsteps, window, prestep, numax):
+    """Static Smagorinsky LES (simpleSmag, nut_prolong, amu = 1 + nu_t rho,
+    staticSmag.f90:191-261, Vis_Fluxes_new.f90:123-125): each step's nu_t comes from
+    its start state and the gradients saved by the previous step's last stage; the
+    adjoint carries both dependencies, the density weight, the clip at 0 of the
+    prolonged nu_t and, with numax = 0.5, the cap at numax.  nu_t = Re (Cs h)^2 |S|
+    depends on Re itself, so dJ/d(1/Re) carries that term too."""
+    from dsem_b200.solver import Solver
+    re = 400.0
+    box, q, dt = _case(n, p, re, seed=17)
+    s = Solver(box.desc(), re=re)
+    s.set_les(LES["cs"], numax)
+    s.upload(q)
+    c = oracle_mod.Case.from_desc(box.desc())
+    c.set_phys(re=re)
+    c.set_les(LES["cs"], numax)
+    c.set_q(q)
+    if prestep:
+        s.step(dt, prestep)
+        c.step(0.0, dt, prestep)
+        assert np.array_equal(s.download(), c.get_q())
+        G = p + 1
+        nu = s.nut()[:, :G, :G, :G]
+        assert nu.max() > 0.0
+        if numax < 100.0:  # the cap is active at some points, not all
+            assert nu.max() == numax and nu.min() < numax
+    q0 = s.download()
+    J, g, lr, _ = s.adjoint(dt, nsteps, window, snapshots=0)
+    assert np.abs(g).max() > 0
+    for d in _directions(q, p + 1, 4, seed=p + 40):
+        Jc, dJ = c.objective_cs(dt, nsteps, window, d, 1e-30)
+        assert abs(J - Jc) <= 1e-12 * abs(Jc)
+        ga = float(np.sum(g * d))
+        assert abs(ga - dJ) <= TOL * abs(dJ), (ga, dJ)
+    if not prestep:  # d/d(1/Re): central differences of the oracle's J
+        r = 1.0 / re
+        h = 1e-5 * r
+        vals = []
+        for rr in (r + h, r - h):
+            cc = oracle_mod.Case.from_desc(box.desc())
+            cc.set_phys(re=1.0 / rr)
+            cc.set_les(LES["cs"], numax)
+            cc.set_q(q0)
+            vals.append(cc.objective_cs(dt, nsteps, window, None, 0.0)[0])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(lr - fd) <= TOL * abs(fd), (lr, fd)
+    s.close()
+
+
+@pytest.mark.parametrize("prestep", [0, 2])
+def test_smagorinsky_adjoint_with_checkpoints(prestep):
+    """Binomial and two-level checkpointing with LES: the same gradient as store-all, bit
+    for bit (each checkpoint keeps the gradients its step's nu_t reads)."""
+    from dsem_b200.solver import Solver
+    box, q, dt = _case(2, 3, 400.0, seed=19)
+    s = Solver(box.desc(), re=400.0)
+    s.set_les(LES["cs"], LES["numax"])
+
+    def start():
+        s.upload(q)
+        if prestep:
+            s.step(dt, prestep)
+
+    start()
+    J0, g0, lr0, _ = s.adjoint(dt, 7, 3, snapshots=0)
+    assert np.abs(g0).max() > 0
+    for snaps in (1, 2, 3, 6):
+        for scheme in ("revolve", "segments"):
+            start()
+            J1, g1, lr1, _ = s.adjoint(dt, 7, 3, snapshots=snaps, scheme=scheme)
+            assert J1 == J0, (snaps, scheme)
+            assert lr1 == lr0, (snaps, scheme)
+            assert np.array_equal(g1, g0), (snaps, scheme)
+    s.close()
+
+
+def test_smagorinsky_adjoint_limits():
+    """LES together with entropy viscosity, or with the shock / density sensors, is refused."""
+    from dsem_b200.solver import DsemError, Solver
+    box, q, dt = _case(2, 3, 400.0)
+    s = Solver(box.desc(), re=400.0, **EV)
+    s.set_les(LES["cs"], LES["numax"])
+    s.upload(q)
+    with pytest.raises(DsemError) as e:
+        s.adjoint(dt, 2, 1)
+    assert e.value.code == -5
+    s.close()
+    s = Solver(box.desc(), re=400.0)
+    s.set_les(LES["cs"], LES["numax"])
+    s.set_les_sensors(shock_sensor=True)
+    s.upload(q)
+    with pytest.raises(DsemError) as e:
+        s.adjoint(dt, 2, 1)
+    assert e.value.code == -5
+    s.close()
