@@ -708,11 +708,10 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   if (nsteps < 1 || window < 0 || window > nsteps || snapshots < 0 || !(dt > 0.0))
     return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "adjoint: need nsteps >= 1, 0 <= window <= nsteps, snapshots >= 0, dt > 0");
   if (c->ncase != 1 || c->groups.size() != 1 || c->mlists.size() != 1 || c->nnc > 0 || !c->groups[0].diag ||
-      c->P.ducros || (c->les && (c->shock || c->les_sensors)) || c->ncut > 0 || c->nbnd > 0)
+      (c->les && (c->shock || c->les_sensors)) || c->ncut > 0 || c->nbnd > 0)
     return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED,
                           "adjoint: one case, one element order, conforming periodic mortars, axis-aligned elements, no "
-                          "Ducros sensor, no LES together with entropy viscosity or the LES sensors, no boundary faces "
-                          "or sharding");
+                          "LES together with entropy viscosity or the LES sensors, no boundary faces or sharding");
   if (c->groups[0].G > 7) return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
   if (dJdQ0 && ldx < c->groups[0].G) return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "ldx smaller than the number of Gauss points");
   int r = upload_ops_here(c);

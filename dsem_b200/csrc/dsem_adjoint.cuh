@@ -675,8 +675,8 @@ __global__ void __launch_bounds__(256) k_trace_adj(const double *__restrict__ LQ
 
 // Entropy viscosity at a step's start (k_ev: RHS_ent_trans and Entropy_Viscosity,
 // RHS.f90:207-278, EViscosity_GL.f90:19-101), transposed:
-// mu = min(max(cmu Re rho h^2 |D|, 0), mumax) with D the entropy residual of
-// ev_residual (without the Ducros sensor).  From dJ/dmu (LMU) it adds
+// mu = min(max(cmu Re rho h^2 |D| [duc], 0), mumax) with D the entropy residual of
+// ev_residual and, with the Ducros variant (shock = 3), its sensor duc.  From dJ/dmu (LMU) it adds
 // dJ/dJQ of the step's start state into LQ and writes dJ/dEVB, the demand on
 // the gradients saved by the previous step's last stage, into LEVB.
 struct EvAdjArgs {
@@ -724,11 +724,18 @@ template <int G> __global__ void __launch_bounds__(128) k_ev_adj(EvAdjArgs A) {
     const double gam = t2 / den;
     const double biS = ((phi + gam) / Tt) / P.re;
     const double h2 = hd[p] * hd[p];
-    const double mur = P.cmu * P.re * rho * h2 * fabs(biS);
+    const double mur0 = P.cmu * P.re * rho * h2 * fabs(biS);
+    // Ducros sensor (shock = 3): duc = min(max(div^2 / (div^2 + |curl|^2 + 1e-9), 0), 1)
+    const double cw0 = Gv[2][1] - Gv[1][2], cw1 = Gv[0][2] - Gv[2][0], cw2 = Gv[1][0] - Gv[0][1];
+    const double c2 = cw0 * cw0 + cw1 * cw1 + cw2 * cw2, d2 = div * div, den_r = d2 + c2 + 1.0e-9;
+    const double rr = d2 / den_r;
+    const double duc = P.ducros ? (rr >= 1.0 ? 1.0 : (rr <= 0.0 ? 0.0 : rr)) : 1.0;
+    const double mur = P.ducros ? mur0 * duc : mur0;
     const bool active = isfinite(mur) && mur > 0.0 && mur < P.mumax;
     double lQ[NV] = {0.0, 0.0, 0.0, 0.0, 0.0}, lGq[3][4] = {}, lT1[3] = {0.0, 0.0, 0.0};
     if (active) {
-      const double lmur = A.LMU[(long long)k * NG + p];
+      const double lmur_in = A.LMU[(long long)k * NG + p];
+      const double lmur = P.ducros ? lmur_in * duc : lmur_in;  // d mur / d mur0
       double lrho = lmur * P.cmu * P.re * h2 * fabs(biS);
       const double lbiS = lmur * P.cmu * P.re * rho * h2 * (biS < 0.0 ? -1.0 : 1.0);
       const double lpg = lbiS / (Tt * P.re);  // d/d(phi + gam)
@@ -744,6 +751,19 @@ template <int G> __global__ void __launch_bounds__(128) k_ev_adj(EvAdjArgs A) {
       lGv[1][0] = lGv[0][1] = lpg * 2.0 * s01;
       lGv[0][2] = lGv[2][0] = lpg * 2.0 * s02;
       lGv[1][2] = lGv[2][1] = lpg * 2.0 * s12;
+      if (P.ducros && rr > 0.0 && rr < 1.0) {  // the sensor's share: mur = mur0 duc
+        const double lr = lmur_in * mur0;
+        const double ld2 = lr * (c2 + 1.0e-9) / (den_r * den_r), lc2 = -lr * d2 / (den_r * den_r);
+        const double ldiv = ld2 * 2.0 * div;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) lGv[i][i] += ldiv;
+        lGv[2][1] += lc2 * 2.0 * cw0;
+        lGv[1][2] -= lc2 * 2.0 * cw0;
+        lGv[0][2] += lc2 * 2.0 * cw1;
+        lGv[2][0] -= lc2 * 2.0 * cw1;
+        lGv[1][0] += lc2 * 2.0 * cw2;
+        lGv[0][1] -= lc2 * 2.0 * cw2;
+      }
       double lvel[3] = {0.0, 0.0, 0.0};
 #pragma unroll
       for (int i = 0; i < 3; ++i)
