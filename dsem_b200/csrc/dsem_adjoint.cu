@@ -60,9 +60,10 @@ struct AdjBuf {
   std::vector<double *> slot_evb;
   std::vector<char> slot_valid;
   double *evb_prev = nullptr;
+  double *lrb = nullptr;  // boundary faces: per boundary point, dJ/d(1/Re) of the external viscous flux
   ~AdjBuf() {
     for (double *p : {lq, lg, ljq, qfr, lff, lvf, lqf, lqr, lrp, lr, q0, stages, traces, lmuhg, levb, evb0,
-                      eps_part, evbw, evb_prev})
+                      eps_part, evbw, evb_prev, lrb})
       cudaFree(p);
     for (double *p : slots) cudaFree(p);
     for (double *p : slot_evb) cudaFree(p);
@@ -73,6 +74,7 @@ struct Adj {
   dsem_ctx *c;
   const Group *g;
   const MList *ml;
+  const BList *bl = nullptr;  // boundary faces of the order, or null
   AdjBuf b;
   double dt = 0.0, s2 = 0.0;
   int nsteps = 0, window = 0;
@@ -88,6 +90,26 @@ struct Adj {
   bool in_window(int n) const { return n >= nsteps - window; }  // step n (0-based) ends inside the window
   double eps_w() const { return dt * 100.0 * c->P.r_re / s2; }
 };
+
+BndPhys bnd_phys(const dsem_ctx *c) {  // as the forward's face launches
+  BndPhys P;
+  P.gamma = c->P.gamma;
+  P.twall = c->twall;
+  P.cv = c->P.mach * c->P.mach * c->P.gamma * (c->P.gamma - 1.0);
+  P.r_cv = 1.0 / P.cv;
+  return P;
+}
+
+// Boundary faces: their Dirichlet states (and fluxes, into c->FF) from the raw
+// traces now in c->QF's boundary slots, as the forward's k_face_bnd_inv.
+template <int G> int bnd_states(Adj &A) {
+  if (!A.bl) return DSEM_OK;
+  dsem_ctx *c = A.c;
+  const BList &bl = *A.bl;
+  CKA(Launch<G>::face_bnd_inv(bl.mb, bl.n, c->QF, c->FF, bl.nh, bl.nrm, bl.qext, bnd_phys(c), c->st));
+  ++A.launches;
+  return DSEM_OK;
+}
 
 // The context's flag for "the saved gradients exist" that the step's viscosity model reads
 bool &grad_flag(Adj &A) { return A.les ? A.c->grad_valid : A.c->ev_grad_valid; }
@@ -124,7 +146,10 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, d
       CKA(cudaMemcpyAsync(A.b.qfr, c->QF, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
       CKA(Launch<G>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st));
       A.launches += 2;
+      if (int r = bnd_states<G>(A)) return r;
       qfr = A.b.qfr;
+    } else if (A.bl) {  // the boundary slots' raw traces, turned into their states below
+      CKA(cudaMemcpyAsync(c->QF, qraw, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
     }
     using C = VolAdjCfg<G>;
     static std::atomic<unsigned long long> attr{0}, attr_ev{0};
@@ -163,6 +188,15 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, d
     }
     k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lff, c->P.re, A.b.lvf, ml.nrm, qraw, c->QF);
     CKA(cudaGetLastError());
+    if (A.bl) {
+      const BList &bl = *A.bl;
+      const unsigned nbb = (unsigned)(((long long)bl.n * G2 + 127) / 128);
+      if (qraw)
+        if (int r = bnd_states<G>(A)) return r;
+      k_face_bnd_vis_adj<G><<<nbb, 128, 0, c->st>>>(bl.mb, bl.n, A.b.lff, c->P.re, A.b.lvf, bl.nrm, bl.fvext, A.b.lrb);
+      CKA(cudaGetLastError());
+      ++A.launches;
+    }
     if (A.visc)
       k_vol_adj<G, true><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
     else
@@ -171,6 +205,14 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, d
     k_face_inv_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, qfr, A.b.lff, A.b.lqf, A.b.lqr, ml.nh, ml.nrm,
                                              c->P.gamma);
     CKA(cudaGetLastError());
+    if (A.bl) {
+      const BList &bl = *A.bl;
+      const unsigned nbb = (unsigned)(((long long)bl.n * G2 + 127) / 128);
+      k_face_bnd_inv_adj<G><<<nbb, 128, 0, c->st>>>(bl.mb, bl.n, qfr, A.b.lff, A.b.lqf, A.b.lqr, bl.nh, bl.nrm,
+                                                    bl.qext, bnd_phys(c));
+      CKA(cudaGetLastError());
+      ++A.launches;
+    }
     if (next)
       k_trace_adj<G, true><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq, A.b.lq, A.b.lg, ark, cdt_next, A.b.lff);
     else
@@ -201,6 +243,7 @@ template <int G> int saved_grads_G(Adj &A, const double *Qs, const double *qraw,
   const MList &ml = *A.ml;
   constexpr int G2 = G * G, NG = G * G * G;
   if (qraw) {
+    if (A.bl) CKA(cudaMemcpyAsync(c->QF, qraw, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
     const unsigned nbm = (unsigned)(((long long)ml.n * G2 + 127) / 128);
     k_face_avg<G><<<nbm, 128, 0, c->st>>>(ml.mc, ml.n, qraw, c->QF);
     CKA(cudaGetLastError());
@@ -213,6 +256,7 @@ template <int G> int saved_grads_G(Adj &A, const double *Qs, const double *qraw,
     CKA(Launch<G>::trace(ta, g.nel, c->st));
     CKA(Launch<G>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st));
   }
+  if (int r = bnd_states<G>(A)) return r;
   VolArgs a{};  // the volume kernel with saved gradients: EVB (its fluxes are not used)
   a.JQ = Qs;
   a.sq = 5LL * NG;
@@ -708,10 +752,11 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   if (nsteps < 1 || window < 0 || window > nsteps || snapshots < 0 || !(dt > 0.0))
     return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "adjoint: need nsteps >= 1, 0 <= window <= nsteps, snapshots >= 0, dt > 0");
   if (c->ncase != 1 || c->groups.size() != 1 || c->mlists.size() != 1 || c->nnc > 0 || !c->groups[0].diag ||
-      (c->les && (c->shock || c->les_sensors)) || c->ncut > 0 || c->nbnd > 0)
+      (c->les && (c->shock || c->les_sensors)) || c->ncut > 0 ||
+      (c->nbnd > 0 && (c->blists.size() != 1 || c->blists[0].G != c->groups[0].G)))
     return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED,
-                          "adjoint: one case, one element order, conforming periodic mortars, axis-aligned elements, no "
-                          "LES together with entropy viscosity or the LES sensors, no boundary faces or sharding");
+                          "adjoint: one case, one element order, conforming mortars, axis-aligned elements, no LES "
+                          "together with entropy viscosity or the LES sensors, no sharding");
   if (c->groups[0].G > 7) return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
   if (dJdQ0 && ldx < c->groups[0].G) return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "ldx smaller than the number of Gauss points");
   int r = upload_ops_here(c);
@@ -720,6 +765,7 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   A.c = c;
   A.g = &c->groups[0];
   A.ml = &c->mlists[0];
+  A.bl = c->nbnd > 0 ? &c->blists[0] : nullptr;
   A.dt = dt;
   A.nsteps = nsteps;
   A.window = window;
@@ -728,6 +774,11 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   for (double **p : {&A.b.lq, &A.b.lg, &A.b.ljq, &A.b.q0}) CKA(cudaMalloc(p, bq));
   for (double **p : {&A.b.qfr, &A.b.lff, &A.b.lvf, &A.b.lqf, &A.b.lqr}) CKA(cudaMalloc(p, bf));
   CKA(cudaMalloc(&A.b.lrp, (size_t)A.g->nel * sizeof(double)));
+  const size_t nbpt = A.bl ? (size_t)A.bl->n * A.g->G * A.g->G : 0;
+  if (A.bl) {
+    CKA(cudaMalloc(&A.b.lrb, nbpt * sizeof(double)));
+    CKA(cudaMemsetAsync(A.b.lrb, 0, nbpt * sizeof(double), c->st));
+  }
   A.ev = c->shock != 0;
   A.les = c->les != 0;
   A.visc = A.ev || A.les;
@@ -750,7 +801,7 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   // two-level scheme: snapshots at the starts of segments of seg_k steps, and one
   // segment's stage states and raw traces (the stash); revolve when they do not fit
   int seg_k = 0, nseg = 0;
-  if (snapshots > 0 && c->adj_scheme == DSEM_ADJ_SEGMENTS && !lean) {
+  if (snapshots > 0 && c->adj_scheme == DSEM_ADJ_SEGMENTS && !lean && !A.bl) {
     seg_k = (nsteps + snapshots - 1) / snapshots;
     nseg = (nsteps + seg_k - 1) / seg_k;
     if (cudaMalloc(&A.b.stages, (size_t)seg_k * kord * bq) != cudaSuccess ||
@@ -802,7 +853,7 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   if ((r = dsem_int::traces(c))) return r;
   // with every stage state and its raw traces kept, the sweep runs out of place
   // through the stash: its first slot starts with the initial state and traces
-  const bool oop = snapshots == 0 && A.b.traces;
+  const bool oop = snapshots == 0 && A.b.traces && !A.bl;  // out-of-place stages: periodic faces only
   if (oop) {
     CKA(cudaMemcpyAsync(A.b.stages, c->JQ, bq, cudaMemcpyDeviceToDevice, c->st));
     CKA(cudaMemcpyAsync(A.b.traces, c->QF, bf, cudaMemcpyDeviceToDevice, c->st));
@@ -963,6 +1014,10 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   }
   k_sum_into<<<1, 256, 0, c->st>>>(A.b.lrp, A.g->nel, A.b.lr);  // dJ/d(1/Re) of the volume terms
   CKA(cudaGetLastError());
+  if (A.bl) {  // ... and of the external viscous fluxes of inflow and outflow faces
+    k_sum_into<<<1, 256, 0, c->st>>>(A.b.lrb, (int)nbpt, A.b.lr);
+    CKA(cudaGetLastError());
+  }
   CKA(cudaEventRecord(e1, c->st));
   CKA(cudaEventSynchronize(e1));
   float t = 0.f;

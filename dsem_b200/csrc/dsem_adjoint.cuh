@@ -477,6 +477,204 @@ __device__ __forceinline__ void vort_vjp(const double *Qj, double jc, const doub
 
 // ---------------------------------------------------------------- kernels
 // Face terms of the divergence and the RK residual sign (k_update):
+// ------------------------------------------------------------ boundary faces
+// pow with a constant exponent on dual numbers
+__device__ __forceinline__ Dual dpow(Dual a, double e) {
+  const double pv = pow(a.v, e);
+  return {pv, a.d * e * pow(a.v, e - 1.0)};
+}
+
+// wall_mirror, osher_flux and riemann_state (dsem_stage.cuh) on dual numbers,
+// statement for statement; branches follow the values.
+__device__ __forceinline__ void wall_mirror_dual(const double *nh, const Dual *Q1, Dual *Q2) {
+  const Dual qnorm = nh[0] * Q1[1] + nh[1] * Q1[2] + nh[2] * Q1[3];
+  const Dual tx = Q1[1] - qnorm * nh[0], ty = Q1[2] - qnorm * nh[1], tz = Q1[3] - qnorm * nh[2];
+  Q2[0] = Q1[0];
+  Q2[1] = tx - qnorm * nh[0];
+  Q2[2] = ty - qnorm * nh[1];
+  Q2[3] = tz - qnorm * nh[2];
+  Q2[4] = Q1[4];
+}
+
+__device__ __noinline__ void osher_dual(const double *nh, double ds, const Dual *Ql, const Dual *Qr, double gamma,
+                                        Dual *flux) {
+  const double en1 = nh[0], en2 = nh[1], en3 = nh[2];
+  const Dual rho = Ql[0], rhou = Ql[1], rhov = Ql[2], rhow = Ql[3], rhoe = Ql[4];
+  const Dual rhon = Qr[0], rhoun = Qr[1], rhovn = Qr[2], rhown = Qr[3], rhoen = Qr[4];
+  const Dual qdotn = (en1 * rhou + en2 * rhov + en3 * rhow) / rho;
+  const Dual qdotnn = (en1 * rhoun + en2 * rhovn + en3 * rhown) / rhon;
+  const Dual p = (gamma - 1.0) * (rhoe - 0.5 / rho * (rhou * rhou + rhov * rhov + rhow * rhow));
+  const Dual a = dsqrt(gamma * p / rho);
+  Dual pn = (gamma - 1.0) * (rhoen - 0.5 / rhon * (rhoun * rhoun + rhovn * rhovn + rhown * rhown));
+  const Dual an = dsqrt(gamma * pn / rhon);
+  const Dual q_tanx = rhoun / rhon - qdotnn * en1;
+  const Dual q_tany = rhovn / rhon - qdotnn * en2;
+  const Dual q_tanz = rhown / rhon - qdotnn * en3;
+  const double z = (gamma - 1.0) / (2.0 * gamma);
+  Dual Ha = -qdotnn / an + 2.0 / (gamma - 1.0);
+  Ha = Ha / (qdotn / a + 2.0 / (gamma - 1.0));
+  pn = p / dpow(Ha, 1.0 / z);
+  Dual pstar = a + an - (qdotnn - qdotn) * ((gamma - 1.0) / 2.0);
+  pstar = pstar / (a / dpow(p, z) + an / dpow(pn, z));
+  pstar = dpow(pstar, 1.0 / z);
+  Dual ustar = Ha * qdotn / a + qdotnn / an + 2.0 * (Ha - 1.0) / (gamma - 1.0);
+  ustar = ustar / (Ha / a + 1.0 / an);
+  const Dual rs = pstar * gamma / (an * an);
+  const Dual u = q_tanx + en1 * ustar, v = q_tany + en2 * ustar, w = q_tanz + en3 * ustar;
+  const Dual Q0 = rs, Q1 = rs * u, Q2 = rs * v, Q3 = rs * w;
+  const Dual Q4 = pstar / (gamma - 1.0) + 0.5 * rs * (u * u + v * v + w * w);
+  const Dual uu = Q1 / Q0, vv = Q2 / Q0, ww = Q3 / Q0;
+  const Dual pp = (gamma - 1.0) * (Q4 - 0.5 * Q0 * (uu * uu + vv * vv + ww * ww));
+  const Dual f[NV] = {Q1, pp + Q1 * uu, Q1 * vv, Q1 * ww, uu * (Q4 + pp)};
+  const Dual g[NV] = {Q2, Q1 * vv, pp + Q2 * vv, Q3 * vv, vv * (Q4 + pp)};
+  const Dual h[NV] = {Q3, Q1 * ww, Q2 * ww, pp + Q3 * ww, ww * (Q4 + pp)};
+#pragma unroll
+  for (int k = 0; k < NV; ++k) flux[k] = ds * (en1 * f[k] + en2 * g[k] + en3 * h[k]);
+}
+
+__device__ __noinline__ void riemann_state_dual(const double *nh, const Dual *Ql, const Dual *Qr, double gamma, Dual *Q) {
+  const double en1 = nh[0], en2 = nh[1], en3 = nh[2];
+  const Dual rho = Ql[0], rhou = Ql[1], rhov = Ql[2], rhow = Ql[3], rhoe = Ql[4];
+  const Dual rhon = Qr[0], rhoun = Qr[1], rhovn = Qr[2], rhown = Qr[3], rhoen = Qr[4];
+  const Dual qdotn = (en1 * rhou + en2 * rhov + en3 * rhow) / rho;
+  const Dual qdotnn = (en1 * rhoun + en2 * rhovn + en3 * rhown) / rhon;
+  const Dual p = (gamma - 1.0) * (rhoe - 0.5 / rho * (rhou * rhou + rhov * rhov + rhow * rhow));
+  const Dual a = dsqrt(gamma * p / rho);
+  const Dual pn = (gamma - 1.0) * (rhoen - 0.5 / rhon * (rhoun * rhoun + rhovn * rhovn + rhown * rhown));
+  const Dual an = dsqrt(gamma * pn / rhon);
+  const Dual e0 = 0.5 * (qdotn + qdotnn);
+  const Dual eplus = e0 + 0.5 * (a + an);
+  const Dual eminus = e0 - 0.5 * (a + an);
+  Dual etos, q_tanx, q_tany, q_tanz;
+  if (e0.v > 0.0) {
+    etos = p / dpow(rho, gamma);
+    q_tanx = rhou / rho - qdotn * en1;
+    q_tany = rhov / rho - qdotn * en2;
+    q_tanz = rhow / rho - qdotn * en3;
+  } else {
+    etos = pn / dpow(rhon, gamma);
+    q_tanx = rhoun / rhon - qdotnn * en1;
+    q_tany = rhovn / rhon - qdotnn * en2;
+    q_tanz = rhown / rhon - qdotnn * en3;
+  }
+  const Dual rplus = eplus.v >= 0.0 ? qdotn + 2.0 / (gamma - 1.0) * a : qdotnn + 2.0 / (gamma - 1.0) * an;
+  const Dual rminus = eminus.v >= 0.0 ? qdotn - 2.0 / (gamma - 1.0) * a : qdotnn - 2.0 / (gamma - 1.0) * an;
+  const Dual qn = 0.5 * (rplus + rminus);
+  const Dual as = 0.25 * (gamma - 1.0) * (rplus - rminus);
+  const Dual rs = dpow(as * as / (gamma * etos), 1.0 / (gamma - 1.0));
+  const Dual ps = dpow(rs, gamma) * etos;
+  const Dual u = q_tanx + en1 * qn, v = q_tany + en2 * qn, w = q_tanz + en3 * qn;
+  Q[0] = rs;
+  Q[1] = rs * u;
+  Q[2] = rs * v;
+  Q[3] = rs * w;
+  Q[4] = ps / (gamma - 1.0) + 0.5 * rs * (u * u + v * v + w * w);
+}
+
+// Inviscid boundary faces (k_face_bnd_inv), transposed: from dJ/dFF (LFF) and
+// dJ/d(the face's Dirichlet state) (LQF) at each boundary point to dJ/d(its
+// raw trace) (LQR).  One forward-mode pass per trace component, through the
+// mirror state, the Roe or osher flux and the Dirichlet state.
+template <int G>
+__global__ void __launch_bounds__(128) k_face_bnd_inv_adj(const MortarB *__restrict__ mb, int nm,
+                                                           const double *__restrict__ QFR,
+                                                           const double *__restrict__ LFF,
+                                                           const double *__restrict__ LQF, double *__restrict__ LQR,
+                                                           const double *__restrict__ nh,
+                                                           const double *__restrict__ nrm,
+                                                           const double *__restrict__ qext, BndPhys P) {
+  constexpr int G2 = G * G;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nm * G2) return;
+  const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
+  const MortarB M = mb[m];
+  const int bc = M.flags & 7;
+  const bool low = (M.flags >> 3) & 1;
+  const long long gp = (long long)M.geo * G2 + pt;
+  const double n3[3] = {nh[gp * 3], nh[gp * 3 + 1], nh[gp * 3 + 2]};
+  const double ds = nrm[gp];
+  double Q1[NV], lf[NV], lq[NV], Qx[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    Q1[v] = QFR[M.ms + v * G2 + pt];
+    lf[v] = LFF[M.ms + v * G2 + pt];
+    lq[v] = LQF[M.ms + v * G2 + pt];
+    Qx[v] = (bc == BC_INFLOW || bc == BC_OUTFLOW) ? qext[(long long)M.geo * NV * G2 + v * G2 + pt] : 0.0;
+  }
+#pragma unroll 1
+  for (int j = 0; j < NV; ++j) {
+    Dual A[NV], B[NV], f[NV], qb[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) A[v] = {Q1[v], v == j ? 1.0 : 0.0};
+    if (bc == BC_WALLADIAB || bc == BC_WALLISOTH) {
+      wall_mirror_dual(n3, A, B);
+      if (bc == BC_WALLADIAB) {
+        riemann_dual(n3, ds, low ? B : A, low ? A : B, P.gamma, f);
+        qb[4] = A[4];
+      } else {
+        const Dual rho = B[0];
+        const Dual u = B[1] / rho, v = B[2] / rho, w = B[3] / rho;
+        B[4] = (rho * P.twall) / P.cv + 0.5 * rho * (u * u + v * v + w * w);
+        if (low) {
+          const double mn[3] = {-n3[0], -n3[1], -n3[2]};
+          osher_dual(mn, -ds, A, B, P.gamma, f);
+        } else {
+          osher_dual(n3, ds, A, B, P.gamma, f);
+        }
+        qb[4] = (A[0] * P.twall) / P.cv;
+      }
+      qb[0] = A[0];
+      qb[1] = qb[2] = qb[3] = Dual{0.0, 0.0};
+    } else {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) B[v] = {Qx[v], 0.0};
+      riemann_dual(n3, ds, low ? B : A, low ? A : B, P.gamma, f);
+      riemann_state_dual(n3, low ? B : A, low ? A : B, P.gamma, qb);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s += lf[v] * f[v].d + lq[v] * qb[v].d;
+    LQR[M.ms + j * G2 + pt] = s;
+  }
+}
+
+// Viscous boundary faces (k_face_bnd_vis), transposed: from dJ/dVF after the
+// boundary condition (-LFF/Re) to dJ/dVF before it (LVF).  Inflow and outflow
+// add the external flux (0.5 fv_ext |n|), whose 1/Re term the volume adjoint's
+// Re * LVF . VF does not see: it goes to LRB, one slot per boundary point,
+// accumulated over the sweep and summed at its end.
+template <int G>
+__global__ void __launch_bounds__(128) k_face_bnd_vis_adj(const MortarB *__restrict__ mb, int nm,
+                                                           const double *__restrict__ LFF, double re,
+                                                           double *__restrict__ LVF, const double *__restrict__ nrm,
+                                                           const double *__restrict__ fvext, double *__restrict__ LRB) {
+  constexpr int G2 = G * G;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nm * G2) return;
+  const int m = (int)(t / G2), pt = (int)(t - (long long)m * G2);
+  const MortarB M = mb[m];
+  const int bc = M.flags & 7;
+  const bool neg_n = (M.flags >> 4) & 1;
+  const long long gp = (long long)M.geo * G2 + pt;
+  const double nm_m = nrm[gp];
+  double lr = 0.0;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double lb = -LFF[M.ms + v * G2 + pt] / re;  // dJ/d(boundary VF)
+    double lfv1;
+    if (bc == BC_WALLADIAB || bc == BC_WALLISOTH) {
+      lfv1 = (v == 4 && bc == BC_WALLADIAB) ? 0.0 : lb * nm_m;
+    } else {
+      const double fx = fvext[(long long)M.geo * NV * G2 + v * G2 + pt];
+      const double Qs = neg_n ? -fx : fx;
+      lfv1 = 0.5 * nm_m * lb;
+      lr += re * lb * (0.5 * Qs * nm_m);
+    }
+    LVF[M.ms + v * G2 + pt] = lfv1 / nm_m;
+  }
+  if (bc == BC_INFLOW || bc == BC_OUTFLOW) LRB[t] += lr;
+}
+
 // Qt = -(QTI + sum_faces D_edge FB), FB = FF - VF/Re, transposed for one element
 // from its dJ/dQt (lam, shared) to dJ/dFF (LFF).  dJ/dVF is -LFF/Re, formed by
 // k_face_vis_adj.

@@ -292,8 +292,10 @@ int dsem_diag_batch(dsem_ctx *ctx, const double *dt, int first, double *ke, doub
  * axis-aligned elements, conforming periodic mortars, shock = 0, 1 or 3
  * (entropy viscosity, with or without the Ducros sensor) or static Smagorinsky LES without the
  * shock and density sensors (not both models at once; with snapshots > 0
- * each snapshot also keeps the gradients its step's viscosity reads), no
- * boundary faces or sharding (DSEM_ERR_UNSUPPORTED otherwise). */
+ * each snapshot also keeps the gradients its step's viscosity reads),
+ * boundary faces of every kind (walls, inflow, outflow; with them
+ * DSEM_ADJ_SEGMENTS falls back to revolve), no sharding
+ * (DSEM_ERR_UNSUPPORTED otherwise). */
 int dsem_adjoint(dsem_ctx *ctx, double dt, int nsteps, int window, int snapshots, double *J, double *dJdQ0,
                  int ldx, double *dJdinvRe, double *ms);
 

@@ -1980,11 +1980,15 @@ template <class T> Case<T> *convert_case(const Case<double> &c) {
       B.Qm[a] = cv(A.Qm[a]);
       B.fv[a] = cv(A.fv[a]);
     }
+    B.bc = A.bc;  // boundary mortars: condition and external states
+    B.Qx = A.Qx;
+    B.fvx = A.fvx;
   }
   o->gamma = c.gamma;
   o->re = c.re;
   o->pr = c.pr;
   o->mach = c.mach;
+  o->twall = c.twall;
   o->cmu = c.cmu;
   o->mumax = c.mumax;
   o->shock = c.shock;

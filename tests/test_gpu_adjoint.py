@@ -372,3 +372,79 @@ def test_smagorinsky_adjoint_limits():
         s.adjoint(dt, 2, 1)
     assert e.value.code == -5
     s.close()
+
+
+BND_CASES = [
+    {"y": ("walladiab", "walladiab")},
+    {"y": ("wallisoth", "walladiab")},
+    {"x": ("inflow", "outflow")},
+    {"z": ("outflow", "wallisoth"), "x": ("inflow", "walladiab")},
+]
+
+
+def _bnd_pair(oracle_mod, bc, p, re, **phys):
+    from dsem_b200.solver import Solver
+    box = mesh.Box(2, 3, 2, p, bc=bc)
+    q = mesh.random_isotropic(box, seed=5, k0=2.0, mach_t=0.3)
+    dt = 0.3 * mesh.dtcalc(box, q)
+    qx = mesh.boundary_state(box, 1.0, (0.3, 0.1, -0.2), 100.0 / 1.4, seed=3, amp=0.05)
+    fx = 0.01 * np.random.default_rng(4).standard_normal(qx.shape)
+    s = Solver(box.desc(), re=re, **phys)
+    s.upload(q)
+    s.set_boundary(100.0, qx, fx)
+    c = oracle_mod.Case.from_desc(box.desc())
+    c.set_phys(re=re, **phys)
+    c.set_q(q)
+    c.set_boundary(100.0, qx, fx)
+    return box, q, dt, s, c
+
+
+@pytest.mark.parametrize("bc", BND_CASES)
+def test_adjoint_with_boundary_faces(oracle_mod, bc):
+    """Walls (adiabatic: Roe against the mirror state; isothermal: osher), inflow and outflow
+    (Roe against the external state, riemann_solution's Dirichlet state) and their viscous
+    conditions (boundary_flux, DirichletBC, Vis_Neumann; ViscousBC_slide.f90:9-420), reversed
+    by forward-mode passes through each boundary point's flux and state.  Against
+    complex-step derivatives of the oracle, d/d(1/Re) against its central differences (the
+    external viscous flux of inflow and outflow faces carries its own 1/Re term), and bit for
+    bit across the storage schemes."""
+    re = 500.0
+    box, q, dt, s, c = _bnd_pair(oracle_mod, bc, 3, re)
+    nsteps, window = 3, 2
+    J, g, lr, _ = s.adjoint(dt, nsteps, window, snapshots=0)
+    assert np.abs(g).max() > 0
+    for d in _directions(q, 4, 3, seed=70):
+        Jc, dJ = c.objective_cs(dt, nsteps, window, d, 1e-30)
+        assert abs(J - Jc) <= 1e-10 * abs(Jc)
+        ga = float(np.sum(g * d))
+        assert abs(ga - dJ) <= TOL * abs(dJ), (ga, dJ)
+    r = 1.0 / re
+    h = 1e-5 * r
+    vals = []
+    for rr in (r + h, r - h):
+        _, _, _, _, cc = _bnd_pair(oracle_mod, bc, 3, 1.0 / rr)
+        vals.append(cc.objective_cs(dt, nsteps, window, None, 0.0)[0])
+    fd = (vals[0] - vals[1]) / (2 * h)
+    assert abs(lr - fd) <= TOL * abs(fd), (lr, fd)
+    for snaps, scheme in ((1, "revolve"), (2, "revolve"), (2, "segments")):
+        s.upload(q)
+        J1, g1, lr1, _ = s.adjoint(dt, nsteps, window, snapshots=snaps, scheme=scheme)
+        assert J1 == J and lr1 == lr and np.array_equal(g1, g), (snaps, scheme)
+    s.close()
+
+
+def test_adjoint_with_boundary_faces_and_entropy_viscosity(oracle_mod):
+    """Walls with entropy viscosity: the saved gradients the viscosity reads are recomputed
+    with the boundary faces' Dirichlet states at the element ends."""
+    re = 400.0
+    box, q, dt, s, c = _bnd_pair(oracle_mod, {"y": ("walladiab", "walladiab")}, 3, re, **EV)
+    s.step(dt, 2)
+    c.step(0.0, dt, 2)
+    assert np.array_equal(s.download(), c.get_q())
+    J, g, lr, _ = s.adjoint(dt, 3, 2, snapshots=0)
+    for d in _directions(q, 4, 3, seed=71):
+        Jc, dJ = c.objective_cs(dt, 3, 2, d, 1e-30)
+        assert abs(J - Jc) <= 1e-12 * abs(Jc)
+        ga = float(np.sum(g * d))
+        assert abs(ga - dJ) <= TOL * abs(dJ), (ga, dJ)
+    s.close()
