@@ -61,9 +61,10 @@ struct AdjBuf {
   std::vector<char> slot_valid;
   double *evb_prev = nullptr;
   double *lrb = nullptr;  // boundary faces: per boundary point, dJ/d(1/Re) of the external viscous flux
+  double *volscr = nullptr;  // p = 7, 8: the volume adjoint's per element scratch (VolAdjCfg::SCR)
   ~AdjBuf() {
     for (double *p : {lq, lg, ljq, qfr, lff, lvf, lqf, lqr, lrp, lr, q0, stages, traces, lmuhg, levb, evb0,
-                      eps_part, evbw, evb_prev, lrb})
+                      eps_part, evbw, evb_prev, lrb, volscr})
       cudaFree(p);
     for (double *p : slots) cudaFree(p);
     for (double *p : slot_evb) cudaFree(p);
@@ -128,99 +129,94 @@ int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, d
   dsem_ctx *c = A.c;
   const Group &g = *A.g;
   const MList &ml = *A.ml;
-  if constexpr (G > 7) {
-    (void)Qs; (void)JQe; (void)eps_w; (void)g; (void)ml; (void)cdt; (void)ark; (void)qraw;
-    (void)levb; (void)upd; (void)next; (void)cdt_next;
-    return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
-  } else {
-    constexpr int G2 = G * G;
-    // forward prerequisites: raw traces (qfr), averaged traces (c->QF)
-    const double *qfr = qraw;  // given: the viscous-face adjoint writes the averages
-    if (!qraw) {
-      TraceArgs ta{};
-      ta.JQ = Qs;
-      ta.sq = 5LL * G * G * G;
-      ta.jac = g.jac;
-      ta.QF = c->QF;
-      CKA(Launch<G>::trace(ta, g.nel, c->st));
-      CKA(cudaMemcpyAsync(A.b.qfr, c->QF, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-      CKA(Launch<G>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st));
-      A.launches += 2;
-      if (int r = bnd_states<G>(A)) return r;
-      qfr = A.b.qfr;
-    } else if (A.bl) {  // the boundary slots' raw traces, turned into their states below
-      CKA(cudaMemcpyAsync(c->QF, qraw, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-    }
-    using C = VolAdjCfg<G>;
-    static std::atomic<unsigned long long> attr{0}, attr_ev{0};
-    CKA(set_smem_once(k_vol_adj<G, false>, C::SMEM, attr));
-    if (A.visc) CKA(set_smem_once(k_vol_adj<G, true>, C::SMEM, attr_ev));
-    VolAdjArgs va{};
-    va.JQ = Qs;
-    va.jac = g.jac;
-    va.gg = g.gg;
-    va.gm = g.gm;
-    va.QF = c->QF;
-    va.LQT = A.b.lg;
-    va.LVF = A.b.lvf;
-    va.LJQ = A.b.ljq;
-    va.LQF = A.b.lqf;
-    va.lr = A.b.lrp;
-    va.eps_w = eps_w;
-    va.JQe = JQe;
-    va.P = c->P;
-    if (A.visc) {
-      va.muhg = A.les ? g.nuhg : g.muhg;
-      va.lmuhg = A.b.lmuhg;
-      va.levb = levb;
-      va.les = A.les ? 1 : 0;
-    }
-    {  // one block per SM (shared memory): prefetch one wave ahead
-      int nsm = 0;
-      CKA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->dev));
-      va.pf = nsm;
-    }
-    const unsigned nb = (unsigned)(((long long)ml.n * G2 + 127) / 128);
-    if (upd) {
-      k_upd_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lg, A.b.lq, cdt, A.b.lff);
-      CKA(cudaGetLastError());
-      ++A.launches;
-    }
-    k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lff, c->P.re, A.b.lvf, ml.nrm, qraw, c->QF);
-    CKA(cudaGetLastError());
-    if (A.bl) {
-      const BList &bl = *A.bl;
-      const unsigned nbb = (unsigned)(((long long)bl.n * G2 + 127) / 128);
-      if (qraw)
-        if (int r = bnd_states<G>(A)) return r;
-      k_face_bnd_vis_adj<G><<<nbb, 128, 0, c->st>>>(bl.mb, bl.n, A.b.lff, c->P.re, A.b.lvf, bl.nrm, bl.fvext, A.b.lrb);
-      CKA(cudaGetLastError());
-      ++A.launches;
-    }
-    if (A.visc)
-      k_vol_adj<G, true><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
-    else
-      k_vol_adj<G, false><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
-    CKA(cudaGetLastError());
-    k_face_inv_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, qfr, A.b.lff, A.b.lqf, A.b.lqr, ml.nh, ml.nrm,
-                                             c->P.gamma);
-    CKA(cudaGetLastError());
-    if (A.bl) {
-      const BList &bl = *A.bl;
-      const unsigned nbb = (unsigned)(((long long)bl.n * G2 + 127) / 128);
-      k_face_bnd_inv_adj<G><<<nbb, 128, 0, c->st>>>(bl.mb, bl.n, qfr, A.b.lff, A.b.lqf, A.b.lqr, bl.nh, bl.nrm,
-                                                    bl.qext, bnd_phys(c));
-      CKA(cudaGetLastError());
-      ++A.launches;
-    }
-    if (next)
-      k_trace_adj<G, true><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq, A.b.lq, A.b.lg, ark, cdt_next, A.b.lff);
-    else
-      k_trace_adj<G, false><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq, A.b.lq, A.b.lg, ark, 0.0, nullptr);
-    CKA(cudaGetLastError());
-    A.launches += 4;
-    return DSEM_OK;
+  constexpr int G2 = G * G;
+  // forward prerequisites: raw traces (qfr), averaged traces (c->QF)
+  const double *qfr = qraw;  // given: the viscous-face adjoint writes the averages
+  if (!qraw) {
+    TraceArgs ta{};
+    ta.JQ = Qs;
+    ta.sq = 5LL * G * G * G;
+    ta.jac = g.jac;
+    ta.QF = c->QF;
+    CKA(Launch<G>::trace(ta, g.nel, c->st));
+    CKA(cudaMemcpyAsync(A.b.qfr, c->QF, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    CKA(Launch<G>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st));
+    A.launches += 2;
+    if (int r = bnd_states<G>(A)) return r;
+    qfr = A.b.qfr;
+  } else if (A.bl) {  // the boundary slots' raw traces, turned into their states below
+    CKA(cudaMemcpyAsync(c->QF, qraw, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
   }
+  using C = VolAdjCfg<G>;
+  static std::atomic<unsigned long long> attr{0}, attr_ev{0};
+  CKA(set_smem_once(k_vol_adj<G, false>, C::SMEM, attr));
+  if (A.visc) CKA(set_smem_once(k_vol_adj<G, true>, C::SMEM, attr_ev));
+  VolAdjArgs va{};
+  va.JQ = Qs;
+  va.jac = g.jac;
+  va.gg = g.gg;
+  va.gm = g.gm;
+  va.QF = c->QF;
+  va.LQT = A.b.lg;
+  va.LVF = A.b.lvf;
+  va.LJQ = A.b.ljq;
+  va.LQF = A.b.lqf;
+  va.lr = A.b.lrp;
+  va.eps_w = eps_w;
+  va.JQe = JQe;
+  va.P = c->P;
+  if (A.visc) {
+    va.muhg = A.les ? g.nuhg : g.muhg;
+    va.lmuhg = A.b.lmuhg;
+    va.levb = levb;
+    va.les = A.les ? 1 : 0;
+  }
+  va.scr = A.b.volscr;
+  {  // one block per SM (shared memory): prefetch one wave ahead
+    int nsm = 0;
+    CKA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->dev));
+    va.pf = nsm;
+  }
+  const unsigned nb = (unsigned)(((long long)ml.n * G2 + 127) / 128);
+  if (upd) {
+    k_upd_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lg, A.b.lq, cdt, A.b.lff);
+    CKA(cudaGetLastError());
+    ++A.launches;
+  }
+  k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lff, c->P.re, A.b.lvf, ml.nrm, qraw, c->QF);
+  CKA(cudaGetLastError());
+  if (A.bl) {
+    const BList &bl = *A.bl;
+    const unsigned nbb = (unsigned)(((long long)bl.n * G2 + 127) / 128);
+    if (qraw)
+      if (int r = bnd_states<G>(A)) return r;
+    k_face_bnd_vis_adj<G><<<nbb, 128, 0, c->st>>>(bl.mb, bl.n, A.b.lff, c->P.re, A.b.lvf, bl.nrm, bl.fvext, A.b.lrb);
+    CKA(cudaGetLastError());
+    ++A.launches;
+  }
+  if (A.visc)
+    k_vol_adj<G, true><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
+  else
+    k_vol_adj<G, false><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
+  CKA(cudaGetLastError());
+  k_face_inv_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, qfr, A.b.lff, A.b.lqf, A.b.lqr, ml.nh, ml.nrm,
+                                           c->P.gamma);
+  CKA(cudaGetLastError());
+  if (A.bl) {
+    const BList &bl = *A.bl;
+    const unsigned nbb = (unsigned)(((long long)bl.n * G2 + 127) / 128);
+    k_face_bnd_inv_adj<G><<<nbb, 128, 0, c->st>>>(bl.mb, bl.n, qfr, A.b.lff, A.b.lqf, A.b.lqr, bl.nh, bl.nrm,
+                                                  bl.qext, bnd_phys(c));
+    CKA(cudaGetLastError());
+    ++A.launches;
+  }
+  if (next)
+    k_trace_adj<G, true><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq, A.b.lq, A.b.lg, ark, cdt_next, A.b.lff);
+  else
+    k_trace_adj<G, false><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq, A.b.lq, A.b.lg, ark, 0.0, nullptr);
+  CKA(cudaGetLastError());
+  A.launches += 4;
+  return DSEM_OK;
 }
 
 int stage_adjoint(Adj &A, const double *Qs, const double *JQe, double eps_w, double cdt, double ark,
@@ -282,20 +278,15 @@ template <int G> int saved_grads_G(Adj &A, const double *Qs, const double *qraw,
 template <int G> int eps_direct_G(Adj &A, const double *Qs, const double *qraw, const double *qend, const double *evb) {
   dsem_ctx *c = A.c;
   const Group &g = *A.g;
-  if constexpr (G > 7) {
-    (void)Qs; (void)qraw; (void)qend; (void)evb; (void)g;
-    return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
-  } else {
-    if (!evb) {
-      const int r = saved_grads_G<G>(A, Qs, qraw, VOL_SAVE);
-      if (r) return r;
-      evb = g.EVB;
-    }
-    k_eps_dir<G><<<g.nel, 128, 0, c->st>>>(qend, g.jac, evb, A.eps_w(), A.b.lq);
-    CKA(cudaGetLastError());
-    ++A.launches;
-    return DSEM_OK;
+  if (!evb) {
+    const int r = saved_grads_G<G>(A, Qs, qraw, VOL_SAVE);
+    if (r) return r;
+    evb = g.EVB;
   }
+  k_eps_dir<G><<<g.nel, 128, 0, c->st>>>(qend, g.jac, evb, A.eps_w(), A.b.lq);
+  CKA(cudaGetLastError());
+  ++A.launches;
+  return DSEM_OK;
 }
 
 int eps_direct(Adj &A, const double *Qs, const double *qraw, const double *qend, const double *evb) {
@@ -318,103 +309,93 @@ template <int G> int ev_forward_G(Adj &A, const double *Qn, const double *Qprev,
   dsem_ctx *c = A.c;
   const Group &g = *A.g;
   const MList &ml = *A.ml;
-  if constexpr (G > 7) {
-    (void)Qn; (void)Qprev; (void)qraw_prev; (void)valid; (void)g; (void)ml;
-    return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
-  } else {
-    constexpr int NG = G * G * G;
-    bool ok = true;
-    if (Qprev) {
-      const int r = saved_grads_G<G>(A, Qprev, qraw_prev, A.les ? VOL_SAVE : VOL_EV_SAVE);
-      if (r) return r;
-    } else if (A.ckpt) {  // kept before the step's recomputation overwrote them
-      ok = A.prev_valid;
-      if (ok)
-        CKA(cudaMemcpyAsync(g.EVB, A.b.evb_prev, (size_t)g.nel * 15 * NG * sizeof(double), cudaMemcpyDeviceToDevice,
-                            c->st));
-    } else if (A.ev_valid0) {
-      CKA(cudaMemcpyAsync(g.EVB, A.b.evb0, (size_t)g.nel * 15 * NG * sizeof(double), cudaMemcpyDeviceToDevice,
+  constexpr int NG = G * G * G;
+  bool ok = true;
+  if (Qprev) {
+    const int r = saved_grads_G<G>(A, Qprev, qraw_prev, A.les ? VOL_SAVE : VOL_EV_SAVE);
+    if (r) return r;
+  } else if (A.ckpt) {  // kept before the step's recomputation overwrote them
+    ok = A.prev_valid;
+    if (ok)
+      CKA(cudaMemcpyAsync(g.EVB, A.b.evb_prev, (size_t)g.nel * 15 * NG * sizeof(double), cudaMemcpyDeviceToDevice,
                           c->st));
-    } else {
-      ok = false;
-    }
-    if (A.les) {  // simpleSmag (k_les), into the group's nuhg
-      LesArgs a{};
-      a.JQ = Qn;
-      a.sq = 5LL * NG;
-      a.jac = g.jac;
-      a.hd = g.hd;
-      a.EVB = g.EVB;
-      a.nuhg = g.nuhg;
-      a.sens = g.sens;
-      a.sensors = 0;
-      a.valid = ok ? 1 : 0;
-      a.re = c->P.re;
-      a.cs = c->les_cs;
-      a.numax = c->les_numax;
-      a.ecase = g.ecase;
-      a.rec = c->d_rec;
-      CKA(Launch<G>::les(a, g.nel, c->st));
-    } else {
-      EvArgs e{};
-      e.JQ = Qn;
-      e.sq = 5LL * NG;
-      e.jac = g.jac;
-      e.hd = g.hd;
-      e.EVB = g.EVB;
-      e.muhg = g.muhg;
-      e.valid = ok ? 1 : 0;
-      e.P = c->P;
-      e.ecase = g.ecase;
-      e.rec = c->d_rec;
-      CKA(Launch<G>::ev(e, g.nel, c->st));
-    }
-    CKA(cudaMemsetAsync(A.b.lmuhg, 0, (size_t)g.nel * NG * sizeof(double), c->st));
-    ++A.launches;
-    *valid = ok;
-    return DSEM_OK;
+  } else if (A.ev_valid0) {
+    CKA(cudaMemcpyAsync(g.EVB, A.b.evb0, (size_t)g.nel * 15 * NG * sizeof(double), cudaMemcpyDeviceToDevice,
+                        c->st));
+  } else {
+    ok = false;
   }
+  if (A.les) {  // simpleSmag (k_les), into the group's nuhg
+    LesArgs a{};
+    a.JQ = Qn;
+    a.sq = 5LL * NG;
+    a.jac = g.jac;
+    a.hd = g.hd;
+    a.EVB = g.EVB;
+    a.nuhg = g.nuhg;
+    a.sens = g.sens;
+    a.sensors = 0;
+    a.valid = ok ? 1 : 0;
+    a.re = c->P.re;
+    a.cs = c->les_cs;
+    a.numax = c->les_numax;
+    a.ecase = g.ecase;
+    a.rec = c->d_rec;
+    CKA(Launch<G>::les(a, g.nel, c->st));
+  } else {
+    EvArgs e{};
+    e.JQ = Qn;
+    e.sq = 5LL * NG;
+    e.jac = g.jac;
+    e.hd = g.hd;
+    e.EVB = g.EVB;
+    e.muhg = g.muhg;
+    e.valid = ok ? 1 : 0;
+    e.P = c->P;
+    e.ecase = g.ecase;
+    e.rec = c->d_rec;
+    CKA(Launch<G>::ev(e, g.nel, c->st));
+  }
+  CKA(cudaMemsetAsync(A.b.lmuhg, 0, (size_t)g.nel * NG * sizeof(double), c->st));
+  ++A.launches;
+  *valid = ok;
+  return DSEM_OK;
 }
 
 // dJ/dmu of the reversed step into dJ/dQn (b.lq) and the previous step's saved gradients (b.levb)
 template <int G> int ev_adjoint_G(Adj &A, const double *Qn) {
   dsem_ctx *c = A.c;
   const Group &g = *A.g;
-  if constexpr (G > 7) {
-    (void)Qn; (void)g;
-    return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
+  if (A.les) {
+    LesAdjArgs e{};
+    e.JQ = Qn;
+    e.jac = g.jac;
+    e.hd = g.hd;
+    e.EVB = g.EVB;
+    e.LNU = A.b.lmuhg;
+    e.LQ = A.b.lq;
+    e.LEVB = A.b.levb;
+    e.LR = A.b.lrp;
+    e.re = c->P.re;
+    e.cs = c->les_cs;
+    e.numax = c->les_numax;
+    e.valid = 1;
+    k_les_adj<G><<<g.nel, 128, 0, c->st>>>(e);
   } else {
-    if (A.les) {
-      LesAdjArgs e{};
-      e.JQ = Qn;
-      e.jac = g.jac;
-      e.hd = g.hd;
-      e.EVB = g.EVB;
-      e.LNU = A.b.lmuhg;
-      e.LQ = A.b.lq;
-      e.LEVB = A.b.levb;
-      e.LR = A.b.lrp;
-      e.re = c->P.re;
-      e.cs = c->les_cs;
-      e.numax = c->les_numax;
-      e.valid = 1;
-      k_les_adj<G><<<g.nel, 128, 0, c->st>>>(e);
-    } else {
-      EvAdjArgs e{};
-      e.JQ = Qn;
-      e.jac = g.jac;
-      e.hd = g.hd;
-      e.EVB = g.EVB;
-      e.LMU = A.b.lmuhg;
-      e.LQ = A.b.lq;
-      e.LEVB = A.b.levb;
-      e.P = c->P;
-      k_ev_adj<G><<<g.nel, 128, 0, c->st>>>(e);
-    }
-    CKA(cudaGetLastError());
-    ++A.launches;
-    return DSEM_OK;
+    EvAdjArgs e{};
+    e.JQ = Qn;
+    e.jac = g.jac;
+    e.hd = g.hd;
+    e.EVB = g.EVB;
+    e.LMU = A.b.lmuhg;
+    e.LQ = A.b.lq;
+    e.LEVB = A.b.levb;
+    e.P = c->P;
+    k_ev_adj<G><<<g.nel, 128, 0, c->st>>>(e);
   }
+  CKA(cudaGetLastError());
+  ++A.launches;
+  return DSEM_OK;
 }
 
 int ev_forward(Adj &A, const double *Qn, const double *Qprev, const double *qraw_prev, bool *valid) {
@@ -757,7 +738,6 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
     return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED,
                           "adjoint: one case, one element order, conforming mortars, axis-aligned elements, no LES "
                           "together with entropy viscosity or the LES sensors, no sharding");
-  if (c->groups[0].G > 7) return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED, "adjoint: p > 6 is not supported");
   if (dJdQ0 && ldx < c->groups[0].G) return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "ldx smaller than the number of Gauss points");
   int r = upload_ops_here(c);
   if (r) return r;
@@ -774,6 +754,17 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   for (double **p : {&A.b.lq, &A.b.lg, &A.b.ljq, &A.b.q0}) CKA(cudaMalloc(p, bq));
   for (double **p : {&A.b.qfr, &A.b.lff, &A.b.lvf, &A.b.lqf, &A.b.lqr}) CKA(cudaMalloc(p, bf));
   CKA(cudaMalloc(&A.b.lrp, (size_t)A.g->nel * sizeof(double)));
+  {  // p = 7, 8: the volume adjoint's arrays that do not fit shared memory
+    size_t scr = 0;
+    with_G(A.g->G, [&](auto gc) -> cudaError_t {
+      scr = VolAdjCfg<decltype(gc)::value>::SCR;
+      return cudaSuccess;
+    });
+    if (scr && cudaMalloc(&A.b.volscr, scr * A.g->nel * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return dsem_int::fail(c, DSEM_ERR_NOMEM, "adjoint: not enough device memory for the volume scratch");
+    }
+  }
   const size_t nbpt = A.bl ? (size_t)A.bl->n * A.g->G * A.g->G : 0;
   if (A.bl) {
     CKA(cudaMalloc(&A.b.lrb, nbpt * sizeof(double)));

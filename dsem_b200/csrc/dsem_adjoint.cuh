@@ -1128,17 +1128,25 @@ struct VolAdjArgs {
   double *lmuhg;                // in/out with muhg: dJ/dmu at the Gauss points, accumulated over stages
   const double *levb;           // dJ/d(gradients this stage saved for the next step's viscosity), or null
   int les;                      // with muhg: it holds the Smagorinsky nu_t (amu = 1 + nu rho), not mu
+  double *scr;                  // G >= 8: per element scratch of VolAdjCfg<G>::SCR doubles
   Phys P;
 };
 
 
 template <int G> struct VolAdjCfg {
   static constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G;
-  // one element per SM (shared memory); at least one thread per Lobatto point of a grid
-  static constexpr int NT = NL <= 256 ? 256 : ((NL + 31) / 32) * 32;
-  static constexpr size_t NDBL = 5 * NG + 15 * NG + 15 * NG + 5 * NL + 5 * NL + 11 * NL + 5 * NG + 5 * NG + 30 * G2 +
-                                 NT + 3 * NG + 30 * G2 + 2 * NG;
+  // One element per SM (shared memory).  p <= 6: every array in shared memory, at least
+  // one thread per Lobatto point of a grid.  p = 7, 8 (G >= 8): the element's working set
+  // (471 KB at p = 8) is twice an SM's shared memory, so the Gauss gradients, their
+  // adjoints and the interpolated-gradient adjoints (GLOB: 30 G^3 + 11 L G^2 doubles) live
+  // in a per-element device scratch (L2-resident while the element runs), 512 threads.
+  static constexpr bool GLOB = G >= 8;
+  static constexpr int NT = GLOB ? 512 : (NL <= 256 ? 256 : ((NL + 31) / 32) * 32);
+  static constexpr size_t SCR = GLOB ? (size_t)30 * NG + 11 * NL : 0;
+  static constexpr size_t NDBL = 5 * NG + (GLOB ? 0 : 15 * NG + 15 * NG) + 5 * NL + 5 * NL + (GLOB ? 0 : 11 * NL) +
+                                 5 * NG + 5 * NG + 30 * G2 + NT + 3 * NG + 30 * G2 + 2 * NG;
   static constexpr size_t SMEM = sizeof(double) * NDBL;
+  static_assert(SMEM <= 227 * 1024, "one element's shared arrays must fit one CTA");
 };
 
 // Volume adjoint of one element (diagonal metrics): recomputes the Lobatto
@@ -1149,12 +1157,21 @@ template <int G, bool EVK> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G, NT = C::NT;
   extern __shared__ double sm[];
   double *q = sm;               // [5][NG] physical state
-  double *GR = q + 5 * NG;      // [15][NG] Gauss gradients, field f*3 + direction
-  double *LGR = GR + 15 * NG;   // [15][NG] their adjoints
-  double *LB = LGR + 15 * NG;   // [5][NL] Lobatto arrays of the current grid
+  double *GR, *LGR, *LG, *LB;
+  if constexpr (C::GLOB) {
+    double *x = A.scr + (long long)blockIdx.x * C::SCR;
+    GR = x;
+    LGR = x + 15 * NG;
+    LG = x + 30 * NG;
+    LB = q + 5 * NG;
+  } else {
+    GR = q + 5 * NG;   // [15][NG] Gauss gradients, field f*3 + direction
+    LGR = GR + 15 * NG;  // [15][NG] their adjoints
+    LB = LGR + 15 * NG;  // [5][NL] Lobatto arrays of the current grid
+  }
   double *LL = LB + 5 * NL;     // [5][NL] their adjoints
-  double *LG = LL + 5 * NL;     // [11][NL] adjoints of the interpolated gradient fields
-  double *LQ = LG + 11 * NL;    // [5][NG] dJ/dq
+  if constexpr (!C::GLOB) LG = LL + 5 * NL;  // [11][NL] adjoints of the interpolated gradient fields
+  double *LQ = LL + 5 * NL + (C::GLOB ? 0 : 11 * NL);  // [5][NG] dJ/dq
   double *LAM = LQ + 5 * NG;    // [5][NG] dJ/dQt
   double *LQFs = LAM + 5 * NG;  // [30][G2] dJ/dQF
   double *red = LQFs + 30 * G2;  // [NT]

@@ -288,7 +288,7 @@ int dsem_diag_batch(dsem_ctx *ctx, const double *dt, int first, double *ke, doub
  * states and recomputes steps in binomial checkpointing order.  Outputs (each
  * may be NULL): J; dJ/d(JQ at the start) in the ldx layout of dsem_upload_q;
  * dJ/d(1/Re); the device milliseconds of the whole call.  The state is
- * restored on return.  Supported: one case, one element order with p <= 6,
+ * restored on return.  Supported: one case, one element order (p <= 8),
  * axis-aligned elements, conforming periodic mortars, shock = 0, 1 or 3
  * (entropy viscosity, with or without the Ducros sensor) or static Smagorinsky LES without the
  * shock and density sensors (not both models at once; with snapshots > 0

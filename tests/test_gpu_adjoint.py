@@ -139,14 +139,15 @@ def test_adjoint_objective_is_the_diagnostic_sum():
 
 
 def test_adjoint_rejects_unsupported_cases():
-    from dsem_b200.solver import DsemError, Solver
-    box = mesh.Box(2, 2, 2, 8)
-    s = Solver(box.desc(), re=400.0)
-    s.upload(mesh.taylor_green(box))
+    from dsem_b200.solver import DsemError, Ensemble, Solver
+    boxes = [mesh.Box(2, 2, 2, 3), mesh.Box(2, 2, 2, 4)]
+    ens = Ensemble([b.desc() for b in boxes], [400.0, 800.0])  # several cases
+    for k, b in enumerate(boxes):
+        ens.upload_case(k, mesh.taylor_green(b))
     with pytest.raises(DsemError) as e:
-        s.adjoint(1e-3, 2, 1)
+        ens.adjoint(1e-3, 2, 1)
     assert e.value.code == -5
-    s.close()
+    ens.close()
     rot = [0] * 27
     rot[13] = 7
     box = mesh.Box(3, 3, 3, 3, rot=rot)
@@ -447,4 +448,37 @@ def test_adjoint_with_boundary_faces_and_entropy_viscosity(oracle_mod):
         assert abs(J - Jc) <= 1e-12 * abs(Jc)
         ga = float(np.sum(g * d))
         assert abs(ga - dJ) <= TOL * abs(dJ), (ga, dJ)
+    s.close()
+
+
+@pytest.mark.parametrize("p,ev", [(7, False), (8, False), (8, True)])
+def test_adjoint_high_order(oracle_mod, p, ev):
+    """p = 7 and 8: the volume adjoint keeps its element's Gauss gradients, their adjoints
+    and the interpolated-gradient adjoints in a per-element device scratch (the working set
+    is twice an SM's shared memory).  Against complex-step derivatives of the oracle, with
+    and without entropy viscosity, and bit for bit under checkpointing."""
+    from dsem_b200.solver import Solver
+    re = 600.0
+    phys = dict(EV) if ev else {}
+    box, q, dt = _case(2, p, re, seed=23)
+    s = Solver(box.desc(), re=re, **phys)
+    s.upload(q)
+    c = oracle_mod.Case.from_desc(box.desc())
+    c.set_phys(re=re, **phys)
+    c.set_q(q)
+    if ev:
+        s.step(dt, 1)
+        c.step(0.0, dt, 1)
+    q0 = s.download()
+    J, g, lr, _ = s.adjoint(dt, 2, 2, snapshots=0)
+    for d in _directions(q, p + 1, 3, seed=p + 80):
+        Jc, dJ = c.objective_cs(dt, 2, 2, d, 1e-30)
+        assert abs(J - Jc) <= 1e-12 * abs(Jc)
+        ga = float(np.sum(g * d))
+        assert abs(ga - dJ) <= TOL * abs(dJ), (ga, dJ)
+    s.upload(q0 if not ev else q)
+    if ev:
+        s.step(dt, 1)
+    J1, g1, lr1, _ = s.adjoint(dt, 2, 2, snapshots=1, scheme="segments")
+    assert J1 == J and lr1 == lr and np.array_equal(g1, g)
     s.close()
