@@ -532,6 +532,7 @@ namespace {
 struct MeshSet {
   std::vector<const dsem_mesh_desc *> m;
   std::vector<int> el0, mo0;  // first element / mortar of each case (+ totals)
+  double snap = 0.0;          // off-diagonal metric entries up to snap x the point's largest diagonal count as 0
   int case_of(int e) const {
     return (int)(std::upper_bound(el0.begin(), el0.end(), e) - el0.begin()) - 1;
   }
@@ -622,6 +623,21 @@ int dsem_create(const dsem_mesh_desc *m, const dsem_phys *ph, dsem_ctx **out) {
   return create_ctx(ms, ph, {ph->re}, out);
 }
 
+int dsem_create_snapped(const dsem_mesh_desc *m, const dsem_phys *ph, double metric_snap, dsem_ctx **out) {
+  if (!m || !ph || !out) return fail(nullptr, DSEM_ERR_INVALID_ARG, "null argument");
+  if (!(metric_snap >= 0.0 && metric_snap < 1e-6))
+    return fail(nullptr, DSEM_ERR_INVALID_ARG, "metric_snap must lie in [0, 1e-6)");
+  *out = nullptr;
+  int r = check_desc(m);
+  if (r) return r;
+  MeshSet ms;
+  ms.m = {m};
+  ms.el0 = {0, m->ngrid};
+  ms.mo0 = {0, m->nmort};
+  ms.snap = metric_snap;
+  return create_ctx(ms, ph, {ph->re}, out);
+}
+
 int dsem_create_batch(int ncase, const dsem_mesh_desc *meshes, const dsem_phys *phys, dsem_ctx **out) {
   if (!meshes || !phys || !out || ncase <= 0) return fail(nullptr, DSEM_ERR_INVALID_ARG, "null argument or ncase < 1");
   *out = nullptr;
@@ -673,8 +689,15 @@ int setup_ctx(dsem_ctx *c, const MeshSet &ms) {
     g.q0 = q0;
     g.f0 = f0;
     const int L = G + 1, NG = G * G * G, NL = L * G * G;
-    // metric layout: diagonal when every off-diagonal entry is exactly zero
+    // metric layout: diagonal when every off-diagonal entry is zero (with ms.snap > 0: at
+    // most snap times the largest diagonal entry of its point, dsem_create_snapped)
     bool diag = true;
+    auto off_zero = [&](const double *g3, int i, int j) {
+      const double x = std::fabs(g3[i + 3 * j]);
+      if (ms.snap <= 0.0) return x == 0.0;
+      const double scale = std::max(std::fabs(g3[0]), std::max(std::fabs(g3[4]), std::fabs(g3[8])));
+      return x <= ms.snap * scale;
+    };
     for (int e : ids) {
       for (int l = 0; l < L && diag; ++l)
         for (int mm = 0; mm < L && diag; ++mm)
@@ -684,7 +707,7 @@ int setup_ctx(dsem_ctx *c, const MeshSet &ms) {
             if (n < G && mm < G && l < G)
               for (int i = 0; i < 3; ++i)
                 for (int j = 0; j < 3; ++j)
-                  if (i != j && m->gmetg[q * 9 + i + 3 * j] != 0.0) diag = false;
+                  if (i != j && !off_zero(m->gmetg + q * 9, i, j)) diag = false;
             const int idx[3] = {n, mm, l};
             for (int d = 0; d < 3; ++d) {
               bool ok = true;
@@ -692,7 +715,7 @@ int setup_ctx(dsem_ctx *c, const MeshSet &ms) {
                 if (idx[a] >= (a == d ? L : G)) ok = false;
               if (!ok) continue;
               for (int j = 0; j < 3; ++j)
-                if (j != d && m->gmet[q * 9 + d + 3 * j] != 0.0) diag = false;
+                if (j != d && !off_zero(m->gmet + q * 9, d, j)) diag = false;
             }
           }
       if (!diag) break;

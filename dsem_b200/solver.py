@@ -22,7 +22,7 @@ EXPORTS = ("dsem_create", "dsem_destroy", "dsem_last_error", "dsem_upload_q", "d
            "dsem_save_state", "dsem_load_state", "dsem_shard_info", "dsem_shard_stage", "dsem_diag_sums",
            "dsem_set_boundary", "dsem_autotune", "dsem_set_vol_variant", "dsem_shard_enqueue", "dsem_shard_finish",
            "dsem_get_stream", "dsem_keep_lobatto", "dsem_write_restart", "dsem_read_restart",
-           "dsem_set_les_sensors", "dsem_set_adjoint_scheme")
+           "dsem_set_les_sensors", "dsem_set_adjoint_scheme", "dsem_create_snapped")
 
 
 class DsemError(RuntimeError):
@@ -58,6 +58,7 @@ def lib(path=None):
         vp = C.c_void_p
         dp = C.POINTER(C.c_double)
         L.dsem_create.argtypes = [C.POINTER(MeshDesc), C.POINTER(Phys), C.POINTER(vp)]
+        L.dsem_create_snapped.argtypes = [C.POINTER(MeshDesc), C.POINTER(Phys), C.c_double, C.POINTER(vp)]
         L.dsem_destroy.argtypes = [vp]
         L.dsem_last_error.argtypes = [vp]
         L.dsem_last_error.restype = C.c_char_p
@@ -124,13 +125,19 @@ def _mesh_desc(desc):
 class Solver:
     """One device context: geometry + state resident in HBM."""
 
-    def __init__(self, desc, gamma=1.4, re=1600.0, pr=0.72, mach=1.0, cmu=0.0, mumax=0.0, shock=0, iord=4):
+    def __init__(self, desc, gamma=1.4, re=1600.0, pr=0.72, mach=1.0, cmu=0.0, mumax=0.0, shock=0, iord=4,
+                 metric_snap=0.0):
+        """metric_snap > 0: dsem_create_snapped (metric rounding noise up to that relative
+        size is treated as zero, so noisy axis-aligned elements take the diagonal kernel)."""
         L = lib()
         md, self._arrays = _mesh_desc(desc)
         self.ngrid, self.nmort, self.ldx = int(desc["ngrid"]), int(desc["nmort"]), int(desc["ldx"])
         ph = Phys(gamma, re, pr, mach, cmu, mumax, int(shock), int(iord))
         h = C.c_void_p()
-        rc = L.dsem_create(C.byref(md), C.byref(ph), C.byref(h))
+        if metric_snap:
+            rc = L.dsem_create_snapped(C.byref(md), C.byref(ph), float(metric_snap), C.byref(h))
+        else:
+            rc = L.dsem_create(C.byref(md), C.byref(ph), C.byref(h))
         if rc != DSEM_OK:
             raise DsemError(rc, L.dsem_last_error(None).decode())
         self.h = h

@@ -87,6 +87,15 @@ typedef struct {
  * Replaces nothing in DSEM itself: it is the one-time upload that precedes the
  * time loop (3DDriver_parfmdf.f90:307). */
 int dsem_create(const dsem_mesh_desc *mesh, const dsem_phys *phys, dsem_ctx **out);
+/* dsem_create for meshes whose axis-aligned elements carry rounding noise in their
+ * metrics: DSEM's trilinear map (grad_hex8_map, GeomLib3D.f90) leaves off-diagonal
+ * entries of ~1e-14 relative on most box sizes (28^3 and up), which send every element
+ * to the general-metric volume kernel (2.2x slower per element at p = 8).  Entries of a
+ * point whose magnitude is at most metric_snap times the point's largest diagonal entry
+ * count as zero, so such elements take the diagonal kernel; the right-hand side then
+ * differs from DSEM's by about metric_snap relative.  metric_snap = 0 is dsem_create;
+ * values must lie in [0, 1e-6). */
+int dsem_create_snapped(const dsem_mesh_desc *mesh, const dsem_phys *phys, double metric_snap, dsem_ctx **out);
 void dsem_destroy(dsem_ctx *ctx);
 const char *dsem_last_error(const dsem_ctx *ctx); /* ctx may be NULL (creation errors) */
 
