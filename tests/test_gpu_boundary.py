@@ -139,14 +139,16 @@ def test_boundary_state_is_required():
         with pytest.raises(DsemError) as e:
             s.step(1e-4, 1)
         assert e.value.code == -1
+        with pytest.raises(DsemError) as e:  # the adjoint's forward sweep needs the same data
+            s.adjoint(1e-4, 2, 1)
+        assert e.value.code == -1
         s.close()
     box = mesh.Box(2, 2, 2, 3, bc={"y": ("walladiab", "walladiab")})
     s = Solver(box.desc(), re=500.0)
     s.upload(mesh.random_isotropic(box, seed=1, k0=1.0, mach_t=0.2))
     s.step(1e-4, 1)  # adiabatic walls need no boundary data
-    with pytest.raises(DsemError) as e:
-        s.adjoint(1e-4, 2, 1)
-    assert e.value.code == -5
+    J, g, _, _ = s.adjoint(1e-4, 2, 1)
+    assert np.isfinite(J) and np.isfinite(g).all()
     s.close()
 
 
