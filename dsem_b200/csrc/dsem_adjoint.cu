@@ -308,7 +308,6 @@ int eps_direct(Adj &A, const double *Qs, const double *qraw, const double *qend,
 template <int G> int ev_forward_G(Adj &A, const double *Qn, const double *Qprev, const double *qraw_prev, bool *valid) {
   dsem_ctx *c = A.c;
   const Group &g = *A.g;
-  const MList &ml = *A.ml;
   constexpr int NG = G * G * G;
   bool ok = true;
   if (Qprev) {

@@ -1399,8 +1399,9 @@ template <int G, bool EVK> __global__ void __launch_bounds__(VolAdjCfg<G>::NT, 1
       // entropy viscosity at this Lobatto point (EV_Prolong, as k_vol_diag): amu = 1 + mu
       // or Smagorinsky (nut_prolong, clipped at 0, as k_vol_diag): amu = 1 + nu rho
       constexpr bool ev = EVK;
-      double amu = 1.0, lam = 0.0, nuL = 0.0;
-      bool nu_on = false;
+      double amu = 1.0, lam = 0.0;
+      [[maybe_unused]] double nuL = 0.0;
+      [[maybe_unused]] bool nu_on = false;
       if constexpr (ev) {
         const int g0 = gbase<G>(D, a, b);
         double acc = Op<G>::B(s, 0) * MU[g0];
