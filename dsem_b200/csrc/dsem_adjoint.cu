@@ -71,11 +71,20 @@ struct AdjBuf {
   }
 };
 
+// Where a group's slices of the adjoint's buffers start (doubles, or elements for e0)
+struct GOff {
+  long long q0 = 0, f0 = 0, e0 = 0;  // state, face slots, elements (as the context's)
+  long long gq = 0;                  // Gauss points: q0 / 5 (lmuhg)
+  long long ev = 0;                  // saved-gradient slots: 3 q0 (levb, evb copies)
+  long long scr = 0;                 // the volume adjoint's scratch (VolAdjCfg::SCR per element)
+};
+
 struct Adj {
   dsem_ctx *c;
-  const Group *g;
-  const MList *ml;
-  const BList *bl = nullptr;  // boundary faces of the order, or null
+  std::vector<GOff> off;      // per order group
+  std::vector<long long> boff;  // per boundary list: first point in b.lrb
+  bool single = true;         // one order group, no p-nonconforming mortars: the fused and out-of-place paths
+  const BList *bl = nullptr;  // boundary faces (single group): the list, or null
   AdjBuf b;
   double dt = 0.0, s2 = 0.0;
   int nsteps = 0, window = 0;
@@ -101,15 +110,82 @@ BndPhys bnd_phys(const dsem_ctx *c) {  // as the forward's face launches
   return P;
 }
 
+// f(gc, group, its offsets) for every order group (gc: the order as a type)
+template <class F> int each_group(Adj &A, F &&f) {
+  for (size_t j = 0; j < A.c->groups.size(); ++j) {
+    int r = DSEM_OK;
+    const cudaError_t e = with_G(A.c->groups[j].G, [&](auto gc) -> cudaError_t {
+      r = f(gc, A.c->groups[j], A.off[j]);
+      return cudaSuccess;
+    });
+    if (e != cudaSuccess) return dsem_int::fail(A.c, DSEM_ERR_UNSUPPORTED, "adjoint: element order not supported");
+    if (r) return r;
+  }
+  return DSEM_OK;
+}
+template <class L, class F> int each_list(Adj &A, const std::vector<L> &lists, F &&f) {
+  for (size_t j = 0; j < lists.size(); ++j) {
+    const cudaError_t e = with_G(lists[j].G, [&](auto gc) -> cudaError_t { return f(gc, lists[j], j); });
+    if (e != cudaSuccess) return dsem_int::fail(A.c, DSEM_ERR_CUDA, "adjoint: face launch failed");
+  }
+  return DSEM_OK;
+}
+
+// Stands for "each group's own EVB" where a function takes saved gradients (evb)
+const double g_evb_groups = 0.0;
+#define EVB_GROUPS (&g_evb_groups)
+// a group's slice of saved gradients: its own EVB, a slice of a buffer laid out like b.levb, or null
+const double *evb_of(const double *evb, const Group &g, const GOff &o) {
+  if (evb == EVB_GROUPS) return g.EVB;
+  return evb ? evb + o.ev : nullptr;
+}
+
 // Boundary faces: their Dirichlet states (and fluxes, into c->FF) from the raw
 // traces now in c->QF's boundary slots, as the forward's k_face_bnd_inv.
-template <int G> int bnd_states(Adj &A) {
-  if (!A.bl) return DSEM_OK;
+int bnd_states(Adj &A) {
   dsem_ctx *c = A.c;
-  const BList &bl = *A.bl;
-  CKA(Launch<G>::face_bnd_inv(bl.mb, bl.n, c->QF, c->FF, bl.nh, bl.nrm, bl.qext, bnd_phys(c), c->st));
-  ++A.launches;
-  return DSEM_OK;
+  const BndPhys BP = bnd_phys(c);
+  A.launches += (long long)c->blists.size();
+  return each_list(A, c->blists, [&](auto gc, const BList &bl, size_t) -> cudaError_t {
+    return Launch<decltype(gc)::value>::face_bnd_inv(bl.mb, bl.n, c->QF, c->FF, bl.nh, bl.nrm, bl.qext, BP, c->st);
+  });
+}
+
+// The forward face inputs of the volume kernels into c->QF: with raw = null the stage
+// state Qs's raw traces (a copy kept in b.qfr when keep_raw), else a copy of raw; then the
+// averaged states of every interior mortar (conforming and p-nonconforming) and the
+// boundary faces' Dirichlet states (fluxes into c->FF).
+int face_states(Adj &A, const double *Qs, const double *raw, bool keep_raw) {
+  dsem_ctx *c = A.c;
+  int r;
+  if (!raw) {
+    r = each_group(A, [&](auto gc, const Group &g, const GOff &o) -> int {
+      constexpr int G = decltype(gc)::value;
+      TraceArgs ta{};
+      ta.JQ = Qs + o.q0;
+      ta.sq = 5LL * G * G * G;
+      ta.jac = g.jac;
+      ta.QF = c->QF + o.f0;
+      CKA(Launch<G>::trace(ta, g.nel, c->st));
+      ++A.launches;
+      return DSEM_OK;
+    });
+    if (r) return r;
+    if (keep_raw) CKA(cudaMemcpyAsync(A.b.qfr, c->QF, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  } else {
+    CKA(cudaMemcpyAsync(c->QF, raw, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  }
+  r = each_list(A, c->mlists, [&](auto gc, const MList &ml, size_t) -> cudaError_t {
+    return Launch<decltype(gc)::value>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st);
+  });
+  if (r) return r;
+  A.launches += (long long)c->mlists.size();
+  if (c->nnc > 0) {
+    k_face_nc_inv<<<c->nnc, 128, 0, c->st>>>(c->nc, c->QF, c->FF, c->nc_nh, c->nc_nrm, c->nc_mats, c->P.gamma);
+    CKA(cudaGetLastError());
+    ++A.launches;
+  }
+  return bnd_states(A);
 }
 
 // The context's flag for "the saved gradients exist" that the step's viscosity model reads
@@ -122,297 +198,315 @@ bool &grad_flag(Adj &A) { return A.les ? A.c->grad_valid : A.c->ev_grad_valid; }
 // The first part (dJ/dQt += cdt dJ/dQ and the face terms) runs here only when
 // upd; otherwise the previous stage of the reverse sweep ran it.  With next,
 // this stage's last kernel also runs that first part of the stage reversed
-// next, with its coefficient cdt_next.
-template <int G>
-int stage_adjoint_G(Adj &A, const double *Qs, const double *JQe, double eps_w, double cdt, double ark,
-                    const double *qraw, const double *levb, bool upd, bool next, double cdt_next) {
+// next, with its coefficient cdt_next.  Per order group: the RK parts, the
+// volume adjoint and the trace adjoint; per face list: the face adjoints.
+int stage_adjoint(Adj &A, const double *Qs, const double *JQe, double eps_w, double cdt, double ark,
+                  const double *qraw, const double *levb, bool upd, bool next, double cdt_next) {
   dsem_ctx *c = A.c;
-  const Group &g = *A.g;
-  const MList &ml = *A.ml;
-  constexpr int G2 = G * G;
-  // forward prerequisites: raw traces (qfr), averaged traces (c->QF)
-  const double *qfr = qraw;  // given: the viscous-face adjoint writes the averages
-  if (!qraw) {
-    TraceArgs ta{};
-    ta.JQ = Qs;
-    ta.sq = 5LL * G * G * G;
-    ta.jac = g.jac;
-    ta.QF = c->QF;
-    CKA(Launch<G>::trace(ta, g.nel, c->st));
-    CKA(cudaMemcpyAsync(A.b.qfr, c->QF, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-    CKA(Launch<G>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st));
-    A.launches += 2;
-    if (int r = bnd_states<G>(A)) return r;
-    qfr = A.b.qfr;
+  // forward prerequisites: raw traces (qfr), averaged and boundary states (c->QF).  One
+  // group with kept traces: the viscous-face adjoint writes the averages as it goes.
+  const bool fused = qraw && A.single;
+  const double *qfr = qraw;
+  int r;
+  if (!fused) {
+    if ((r = face_states(A, Qs, qraw, !qraw))) return r;
+    if (!qraw) qfr = A.b.qfr;
   } else if (A.bl) {  // the boundary slots' raw traces, turned into their states below
     CKA(cudaMemcpyAsync(c->QF, qraw, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
   }
-  using C = VolAdjCfg<G>;
-  static std::atomic<unsigned long long> attr{0}, attr_ev{0};
-  CKA(set_smem_once(k_vol_adj<G, false>, C::SMEM, attr));
-  if (A.visc) CKA(set_smem_once(k_vol_adj<G, true>, C::SMEM, attr_ev));
-  VolAdjArgs va{};
-  va.JQ = Qs;
-  va.jac = g.jac;
-  va.gg = g.gg;
-  va.gm = g.gm;
-  va.QF = c->QF;
-  va.LQT = A.b.lg;
-  va.LVF = A.b.lvf;
-  va.LJQ = A.b.ljq;
-  va.LQF = A.b.lqf;
-  va.lr = A.b.lrp;
-  va.eps_w = eps_w;
-  va.JQe = JQe;
-  va.P = c->P;
-  if (A.visc) {
-    va.muhg = A.les ? g.nuhg : g.muhg;
-    va.lmuhg = A.b.lmuhg;
-    va.levb = levb;
-    va.les = A.les ? 1 : 0;
-  }
-  va.scr = A.b.volscr;
-  {  // one block per SM (shared memory): prefetch one wave ahead
-    int nsm = 0;
-    CKA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->dev));
-    va.pf = nsm;
-  }
-  const unsigned nb = (unsigned)(((long long)ml.n * G2 + 127) / 128);
+  int nsm = 0;  // one volume block per SM (shared memory): prefetch one wave ahead
+  CKA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->dev));
   if (upd) {
-    k_upd_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lg, A.b.lq, cdt, A.b.lff);
-    CKA(cudaGetLastError());
-    ++A.launches;
+    r = each_group(A, [&](auto gc, const Group &g, const GOff &o) -> int {
+      constexpr int G = decltype(gc)::value;
+      k_upd_adj<G><<<g.nel, 256, 0, c->st>>>(A.b.lg + o.q0, A.b.lq + o.q0, cdt, A.b.lff + o.f0);
+      CKA(cudaGetLastError());
+      ++A.launches;
+      return DSEM_OK;
+    });
+    if (r) return r;
   }
-  k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lff, c->P.re, A.b.lvf, ml.nrm, qraw, c->QF);
-  CKA(cudaGetLastError());
-  if (A.bl) {
-    const BList &bl = *A.bl;
-    const unsigned nbb = (unsigned)(((long long)bl.n * G2 + 127) / 128);
-    if (qraw)
-      if (int r = bnd_states<G>(A)) return r;
-    k_face_bnd_vis_adj<G><<<nbb, 128, 0, c->st>>>(bl.mb, bl.n, A.b.lff, c->P.re, A.b.lvf, bl.nrm, bl.fvext, A.b.lrb);
-    CKA(cudaGetLastError());
-    ++A.launches;
-  }
-  if (A.visc)
-    k_vol_adj<G, true><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
-  else
-    k_vol_adj<G, false><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
-  CKA(cudaGetLastError());
-  k_face_inv_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, qfr, A.b.lff, A.b.lqf, A.b.lqr, ml.nh, ml.nrm,
-                                           c->P.gamma);
-  CKA(cudaGetLastError());
-  if (A.bl) {
-    const BList &bl = *A.bl;
-    const unsigned nbb = (unsigned)(((long long)bl.n * G2 + 127) / 128);
-    k_face_bnd_inv_adj<G><<<nbb, 128, 0, c->st>>>(bl.mb, bl.n, qfr, A.b.lff, A.b.lqf, A.b.lqr, bl.nh, bl.nrm,
-                                                  bl.qext, bnd_phys(c));
-    CKA(cudaGetLastError());
-    ++A.launches;
-  }
-  if (next)
-    k_trace_adj<G, true><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq, A.b.lq, A.b.lg, ark, cdt_next, A.b.lff);
-  else
-    k_trace_adj<G, false><<<g.nel, 256, 0, c->st>>>(A.b.lqr, g.jac, A.b.ljq, A.b.lq, A.b.lg, ark, 0.0, nullptr);
-  CKA(cudaGetLastError());
-  A.launches += 4;
-  return DSEM_OK;
-}
-
-int stage_adjoint(Adj &A, const double *Qs, const double *JQe, double eps_w, double cdt, double ark,
-                  const double *qraw, const double *levb, bool upd, bool next, double cdt_next) {
-  int r = DSEM_OK;
-  cudaError_t e = with_G(A.g->G, [&](auto gc) -> cudaError_t {
-    r = stage_adjoint_G<decltype(gc)::value>(A, Qs, JQe, eps_w, cdt, ark, qraw, levb, upd, next, cdt_next);
-    return cudaSuccess;
+  r = each_list(A, c->mlists, [&](auto gc, const MList &ml, size_t) -> cudaError_t {
+    constexpr int G = decltype(gc)::value;
+    const unsigned nb = (unsigned)(((long long)ml.n * G * G + 127) / 128);
+    k_face_vis_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, A.b.lff, c->P.re, A.b.lvf, ml.nrm, fused ? qraw : nullptr,
+                                             c->QF);
+    return cudaGetLastError();
   });
-  if (e != cudaSuccess) return dsem_int::fail(A.c, DSEM_ERR_UNSUPPORTED, "adjoint: element order not supported");
-  return r;
+  if (r) return r;
+  A.launches += (long long)c->mlists.size();
+  if (c->nnc > 0) {
+    k_face_nc_vis_adj<<<c->nnc, 128, 0, c->st>>>(c->nc, A.b.lff, c->P.re, A.b.lvf, c->nc_nrm, c->nc_mats);
+    CKA(cudaGetLastError());
+    ++A.launches;
+  }
+  if (c->nbnd > 0) {
+    if (fused && (r = bnd_states(A))) return r;
+    r = each_list(A, c->blists, [&](auto gc, const BList &bl, size_t j) -> cudaError_t {
+      constexpr int G = decltype(gc)::value;
+      const unsigned nbb = (unsigned)(((long long)bl.n * G * G + 127) / 128);
+      k_face_bnd_vis_adj<G><<<nbb, 128, 0, c->st>>>(bl.mb, bl.n, A.b.lff, c->P.re, A.b.lvf, bl.nrm, bl.fvext,
+                                                    A.b.lrb + A.boff[j]);
+      return cudaGetLastError();
+    });
+    if (r) return r;
+    A.launches += (long long)c->blists.size();
+  }
+  r = each_group(A, [&](auto gc, const Group &g, const GOff &o) -> int {
+    constexpr int G = decltype(gc)::value;
+    using C = VolAdjCfg<G>;
+    static std::atomic<unsigned long long> attr{0}, attr_ev{0};
+    CKA(set_smem_once(k_vol_adj<G, false>, C::SMEM, attr));
+    if (A.visc) CKA(set_smem_once(k_vol_adj<G, true>, C::SMEM, attr_ev));
+    VolAdjArgs va{};
+    va.JQ = Qs + o.q0;
+    va.jac = g.jac;
+    va.gg = g.gg;
+    va.gm = g.gm;
+    va.QF = c->QF + o.f0;
+    va.LQT = A.b.lg + o.q0;
+    va.LVF = A.b.lvf + o.f0;
+    va.LJQ = A.b.ljq + o.q0;
+    va.LQF = A.b.lqf + o.f0;
+    va.lr = A.b.lrp + o.e0;
+    va.eps_w = eps_w;
+    va.JQe = JQe ? JQe + o.q0 : nullptr;
+    va.P = c->P;
+    if (A.visc) {
+      va.muhg = A.les ? g.nuhg : g.muhg;
+      va.lmuhg = A.b.lmuhg + o.gq;
+      va.levb = levb ? levb + o.ev : nullptr;
+      va.les = A.les ? 1 : 0;
+    }
+    va.scr = A.b.volscr ? A.b.volscr + o.scr : nullptr;
+    va.pf = nsm;
+    if (A.visc)
+      k_vol_adj<G, true><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
+    else
+      k_vol_adj<G, false><<<g.nel, C::NT, C::SMEM, c->st>>>(va);
+    CKA(cudaGetLastError());
+    ++A.launches;
+    return DSEM_OK;
+  });
+  if (r) return r;
+  r = each_list(A, c->mlists, [&](auto gc, const MList &ml, size_t) -> cudaError_t {
+    constexpr int G = decltype(gc)::value;
+    const unsigned nb = (unsigned)(((long long)ml.n * G * G + 127) / 128);
+    k_face_inv_adj<G><<<nb, 128, 0, c->st>>>(ml.mc, ml.n, qfr, A.b.lff, A.b.lqf, A.b.lqr, ml.nh, ml.nrm, c->P.gamma);
+    return cudaGetLastError();
+  });
+  if (r) return r;
+  A.launches += (long long)c->mlists.size();
+  if (c->nnc > 0) {
+    k_face_nc_inv_adj<<<c->nnc, 128, 0, c->st>>>(c->nc, qfr, A.b.lff, A.b.lqf, A.b.lqr, c->nc_nh, c->nc_nrm,
+                                                 c->nc_mats, c->P.gamma);
+    CKA(cudaGetLastError());
+    ++A.launches;
+  }
+  if (c->nbnd > 0) {
+    const BndPhys BP = bnd_phys(c);
+    r = each_list(A, c->blists, [&](auto gc, const BList &bl, size_t) -> cudaError_t {
+      constexpr int G = decltype(gc)::value;
+      const unsigned nbb = (unsigned)(((long long)bl.n * G * G + 127) / 128);
+      k_face_bnd_inv_adj<G><<<nbb, 128, 0, c->st>>>(bl.mb, bl.n, qfr, A.b.lff, A.b.lqf, A.b.lqr, bl.nh, bl.nrm,
+                                                    bl.qext, BP);
+      return cudaGetLastError();
+    });
+    if (r) return r;
+    A.launches += (long long)c->blists.size();
+  }
+  return each_group(A, [&](auto gc, const Group &g, const GOff &o) -> int {
+    constexpr int G = decltype(gc)::value;
+    if (next)
+      k_trace_adj<G, true><<<g.nel, 256, 0, c->st>>>(A.b.lqr + o.f0, g.jac, A.b.ljq + o.q0, A.b.lq + o.q0,
+                                                      A.b.lg + o.q0, ark, cdt_next, A.b.lff + o.f0);
+    else
+      k_trace_adj<G, false><<<g.nel, 256, 0, c->st>>>(A.b.lqr + o.f0, g.jac, A.b.ljq + o.q0, A.b.lq + o.q0,
+                                                       A.b.lg + o.q0, ark, 0.0, nullptr);
+    CKA(cudaGetLastError());
+    ++A.launches;
+    return DSEM_OK;
+  });
 }
 
-// The gradients a forward step's last stage saves (into the group's EVB),
-// recomputed by the forward volume kernel itself (mode VOL_SAVE or VOL_EV_SAVE)
+// The gradients a forward step's last stage saves (into the groups' EVB),
+// recomputed by the forward volume kernels themselves (mode VOL_SAVE or VOL_EV_SAVE)
 // from that stage's input state Qs and its raw face traces qraw (null: recomputed).
-template <int G> int saved_grads_G(Adj &A, const double *Qs, const double *qraw, int mode) {
+int saved_grads(Adj &A, const double *Qs, const double *qraw, int mode) {
   dsem_ctx *c = A.c;
-  const Group &g = *A.g;
-  const MList &ml = *A.ml;
-  constexpr int G2 = G * G, NG = G * G * G;
-  if (qraw) {
+  int r;
+  if (qraw && A.single) {  // the averages from the kept traces
     if (A.bl) CKA(cudaMemcpyAsync(c->QF, qraw, c->nface * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-    const unsigned nbm = (unsigned)(((long long)ml.n * G2 + 127) / 128);
-    k_face_avg<G><<<nbm, 128, 0, c->st>>>(ml.mc, ml.n, qraw, c->QF);
-    CKA(cudaGetLastError());
-  } else {
-    TraceArgs ta{};
-    ta.JQ = Qs;
-    ta.sq = 5LL * NG;
-    ta.jac = g.jac;
-    ta.QF = c->QF;
-    CKA(Launch<G>::trace(ta, g.nel, c->st));
-    CKA(Launch<G>::face_inv(ml.mc, ml.n, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st));
+    r = each_list(A, c->mlists, [&](auto gc, const MList &ml, size_t) -> cudaError_t {
+      constexpr int G = decltype(gc)::value;
+      const unsigned nbm = (unsigned)(((long long)ml.n * G * G + 127) / 128);
+      k_face_avg<G><<<nbm, 128, 0, c->st>>>(ml.mc, ml.n, qraw, c->QF);
+      return cudaGetLastError();
+    });
+    if (r) return r;
+    A.launches += (long long)c->mlists.size();
+    if ((r = bnd_states(A))) return r;
+  } else if ((r = face_states(A, Qs, qraw, false))) {
+    return r;
   }
-  if (int r = bnd_states<G>(A)) return r;
-  VolArgs a{};  // the volume kernel with saved gradients: EVB (its fluxes are not used)
-  a.JQ = Qs;
-  a.sq = 5LL * NG;
-  a.jac = g.jac;
-  a.gg = g.gg;
-  a.gm = g.gm;
-  a.muhg = g.muhg;
-  a.QF = c->QF;
-  a.VF = c->VF;
-  a.QTI = c->QTI;
-  a.EVB = g.EVB;
-  a.P = c->P;
-  a.ecase = g.ecase;
-  a.rec = c->d_rec;
-  CKA(Launch<G>::vol(a, g.nel, true, mode, c->st));
-  A.launches += qraw ? 2 : 3;
-  return DSEM_OK;
+  return each_group(A, [&](auto gc, const Group &g, const GOff &o) -> int {
+    constexpr int G = decltype(gc)::value;
+    constexpr int NG = G * G * G;
+    VolArgs a{};  // the volume kernel with saved gradients: EVB (its fluxes are not used)
+    a.JQ = Qs + o.q0;
+    a.sq = 5LL * NG;
+    a.jac = g.jac;
+    a.gg = g.gg;
+    a.gm = g.gm;
+    a.muhg = g.muhg;
+    a.QF = c->QF + o.f0;
+    a.VF = c->VF + o.f0;
+    a.QTI = c->QTI + o.q0;
+    a.EVB = g.EVB;
+    a.P = c->P;
+    a.ecase = g.ecase;
+    a.rec = c->d_rec;
+    CKA(Launch<G>::vol(a, g.nel, true, mode, c->st));
+    ++A.launches;
+    return DSEM_OK;
+  });
 }
 
 // Direct part of a window step's enstrophy term into dJ/dQ of its end state
-// qend, from the gradients its last stage saved: evb, or (null) recomputed
-// from that stage's input state Qs and raw traces qraw into the group's EVB.
-template <int G> int eps_direct_G(Adj &A, const double *Qs, const double *qraw, const double *qend, const double *evb) {
-  dsem_ctx *c = A.c;
-  const Group &g = *A.g;
-  if (!evb) {
-    const int r = saved_grads_G<G>(A, Qs, qraw, VOL_SAVE);
-    if (r) return r;
-    evb = g.EVB;
-  }
-  k_eps_dir<G><<<g.nel, 128, 0, c->st>>>(qend, g.jac, evb, A.eps_w(), A.b.lq);
-  CKA(cudaGetLastError());
-  ++A.launches;
-  return DSEM_OK;
-}
-
+// qend, from the gradients its last stage saved: evb (EVB_GROUPS: the groups'
+// own; else a buffer laid out like b.levb), or (null) recomputed from that
+// stage's input state Qs and raw traces qraw into the groups' EVB.
 int eps_direct(Adj &A, const double *Qs, const double *qraw, const double *qend, const double *evb) {
-  int r = DSEM_OK;
-  with_G(A.g->G, [&](auto gc) -> cudaError_t {
-    r = eps_direct_G<decltype(gc)::value>(A, Qs, qraw, qend, evb);
-    return cudaSuccess;
+  dsem_ctx *c = A.c;
+  if (!evb) {
+    const int r = saved_grads(A, Qs, qraw, VOL_SAVE);
+    if (r) return r;
+    evb = EVB_GROUPS;
+  }
+  return each_group(A, [&](auto gc, const Group &g, const GOff &o) -> int {
+    constexpr int G = decltype(gc)::value;
+    k_eps_dir<G><<<g.nel, 128, 0, c->st>>>(qend + o.q0, g.jac, evb_of(evb, g, o), A.eps_w(), A.b.lq + o.q0);
+    CKA(cudaGetLastError());
+    ++A.launches;
+    return DSEM_OK;
   });
-  return r;
 }
 
-// Entropy viscosity for the reverse sweep of a step whose start state is Qn:
+// Copies between the groups' EVB and a buffer laid out like b.levb
+int evb_copy(Adj &A, double *buf, bool to_buf) {
+  dsem_ctx *c = A.c;
+  return each_group(A, [&](auto gc, const Group &g, const GOff &o) -> int {
+    constexpr int G = decltype(gc)::value;
+    const size_t n = (size_t)g.nel * 15 * G * G * G * sizeof(double);
+    if (to_buf)
+      CKA(cudaMemcpyAsync(buf + o.ev, g.EVB, n, cudaMemcpyDeviceToDevice, c->st));
+    else
+      CKA(cudaMemcpyAsync(g.EVB, buf + o.ev, n, cudaMemcpyDeviceToDevice, c->st));
+    return DSEM_OK;
+  });
+}
+
+// Entropy viscosity (or Smagorinsky) for the reverse sweep of a step whose start state is Qn:
 // first the gradients that fed it, saved by the previous step's last stage
 // (when that stage's input state Qprev is kept: recomputed from it and its raw
 // face traces; else with checkpoints: copied aside before the step's
 // recomputation, keep_prev; else kept from entry for the first step), then
-// the viscosity itself (k_ev, into the group's muhg).  *valid: whether those
+// the viscosity itself (k_ev / k_les, into the groups' muhg / nuhg).  *valid: whether those
 // gradients existed.
-template <int G> int ev_forward_G(Adj &A, const double *Qn, const double *Qprev, const double *qraw_prev, bool *valid) {
+int ev_forward(Adj &A, const double *Qn, const double *Qprev, const double *qraw_prev, bool *valid) {
   dsem_ctx *c = A.c;
-  const Group &g = *A.g;
-  constexpr int NG = G * G * G;
   bool ok = true;
+  int r;
   if (Qprev) {
-    const int r = saved_grads_G<G>(A, Qprev, qraw_prev, A.les ? VOL_SAVE : VOL_EV_SAVE);
-    if (r) return r;
+    if ((r = saved_grads(A, Qprev, qraw_prev, A.les ? VOL_SAVE : VOL_EV_SAVE))) return r;
   } else if (A.ckpt) {  // kept before the step's recomputation overwrote them
     ok = A.prev_valid;
-    if (ok)
-      CKA(cudaMemcpyAsync(g.EVB, A.b.evb_prev, (size_t)g.nel * 15 * NG * sizeof(double), cudaMemcpyDeviceToDevice,
-                          c->st));
+    if (ok && (r = evb_copy(A, A.b.evb_prev, false))) return r;
   } else if (A.ev_valid0) {
-    CKA(cudaMemcpyAsync(g.EVB, A.b.evb0, (size_t)g.nel * 15 * NG * sizeof(double), cudaMemcpyDeviceToDevice,
-                        c->st));
+    if ((r = evb_copy(A, A.b.evb0, false))) return r;
   } else {
     ok = false;
   }
-  if (A.les) {  // simpleSmag (k_les), into the group's nuhg
-    LesArgs a{};
-    a.JQ = Qn;
-    a.sq = 5LL * NG;
-    a.jac = g.jac;
-    a.hd = g.hd;
-    a.EVB = g.EVB;
-    a.nuhg = g.nuhg;
-    a.sens = g.sens;
-    a.sensors = 0;
-    a.valid = ok ? 1 : 0;
-    a.re = c->P.re;
-    a.cs = c->les_cs;
-    a.numax = c->les_numax;
-    a.ecase = g.ecase;
-    a.rec = c->d_rec;
-    CKA(Launch<G>::les(a, g.nel, c->st));
-  } else {
-    EvArgs e{};
-    e.JQ = Qn;
-    e.sq = 5LL * NG;
-    e.jac = g.jac;
-    e.hd = g.hd;
-    e.EVB = g.EVB;
-    e.muhg = g.muhg;
-    e.valid = ok ? 1 : 0;
-    e.P = c->P;
-    e.ecase = g.ecase;
-    e.rec = c->d_rec;
-    CKA(Launch<G>::ev(e, g.nel, c->st));
-  }
-  CKA(cudaMemsetAsync(A.b.lmuhg, 0, (size_t)g.nel * NG * sizeof(double), c->st));
-  ++A.launches;
+  r = each_group(A, [&](auto gc, const Group &g, const GOff &o) -> int {
+    constexpr int G = decltype(gc)::value;
+    constexpr int NG = G * G * G;
+    if (A.les) {  // simpleSmag (k_les), into the group's nuhg
+      LesArgs a{};
+      a.JQ = Qn + o.q0;
+      a.sq = 5LL * NG;
+      a.jac = g.jac;
+      a.hd = g.hd;
+      a.EVB = g.EVB;
+      a.nuhg = g.nuhg;
+      a.sens = g.sens;
+      a.sensors = 0;
+      a.valid = ok ? 1 : 0;
+      a.re = c->P.re;
+      a.cs = c->les_cs;
+      a.numax = c->les_numax;
+      a.ecase = g.ecase;
+      a.rec = c->d_rec;
+      CKA(Launch<G>::les(a, g.nel, c->st));
+    } else {
+      EvArgs e{};
+      e.JQ = Qn + o.q0;
+      e.sq = 5LL * NG;
+      e.jac = g.jac;
+      e.hd = g.hd;
+      e.EVB = g.EVB;
+      e.muhg = g.muhg;
+      e.valid = ok ? 1 : 0;
+      e.P = c->P;
+      e.ecase = g.ecase;
+      e.rec = c->d_rec;
+      CKA(Launch<G>::ev(e, g.nel, c->st));
+    }
+    ++A.launches;
+    return DSEM_OK;
+  });
+  if (r) return r;
+  CKA(cudaMemsetAsync(A.b.lmuhg, 0, (size_t)(c->nq / 5) * sizeof(double), c->st));
   *valid = ok;
   return DSEM_OK;
 }
 
-// dJ/dmu of the reversed step into dJ/dQn (b.lq) and the previous step's saved gradients (b.levb)
-template <int G> int ev_adjoint_G(Adj &A, const double *Qn) {
-  dsem_ctx *c = A.c;
-  const Group &g = *A.g;
-  if (A.les) {
-    LesAdjArgs e{};
-    e.JQ = Qn;
-    e.jac = g.jac;
-    e.hd = g.hd;
-    e.EVB = g.EVB;
-    e.LNU = A.b.lmuhg;
-    e.LQ = A.b.lq;
-    e.LEVB = A.b.levb;
-    e.LR = A.b.lrp;
-    e.re = c->P.re;
-    e.cs = c->les_cs;
-    e.numax = c->les_numax;
-    e.valid = 1;
-    k_les_adj<G><<<g.nel, 128, 0, c->st>>>(e);
-  } else {
-    EvAdjArgs e{};
-    e.JQ = Qn;
-    e.jac = g.jac;
-    e.hd = g.hd;
-    e.EVB = g.EVB;
-    e.LMU = A.b.lmuhg;
-    e.LQ = A.b.lq;
-    e.LEVB = A.b.levb;
-    e.P = c->P;
-    k_ev_adj<G><<<g.nel, 128, 0, c->st>>>(e);
-  }
-  CKA(cudaGetLastError());
-  ++A.launches;
-  return DSEM_OK;
-}
-
-int ev_forward(Adj &A, const double *Qn, const double *Qprev, const double *qraw_prev, bool *valid) {
-  int r = DSEM_OK;
-  with_G(A.g->G, [&](auto gc) -> cudaError_t {
-    r = ev_forward_G<decltype(gc)::value>(A, Qn, Qprev, qraw_prev, valid);
-    return cudaSuccess;
-  });
-  return r;
-}
-
+// dJ/dmu (or dJ/dnu_t) of the reversed step into dJ/dQn (b.lq) and the previous step's saved
+// gradients (b.levb)
 int ev_adjoint(Adj &A, const double *Qn) {
-  int r = DSEM_OK;
-  with_G(A.g->G, [&](auto gc) -> cudaError_t {
-    r = ev_adjoint_G<decltype(gc)::value>(A, Qn);
-    return cudaSuccess;
+  dsem_ctx *c = A.c;
+  return each_group(A, [&](auto gc, const Group &g, const GOff &o) -> int {
+    constexpr int G = decltype(gc)::value;
+    if (A.les) {
+      LesAdjArgs e{};
+      e.JQ = Qn + o.q0;
+      e.jac = g.jac;
+      e.hd = g.hd;
+      e.EVB = g.EVB;
+      e.LNU = A.b.lmuhg + o.gq;
+      e.LQ = A.b.lq + o.q0;
+      e.LEVB = A.b.levb + o.ev;
+      e.LR = A.b.lrp + o.e0;
+      e.re = c->P.re;
+      e.cs = c->les_cs;
+      e.numax = c->les_numax;
+      e.valid = 1;
+      k_les_adj<G><<<g.nel, 128, 0, c->st>>>(e);
+    } else {
+      EvAdjArgs e{};
+      e.JQ = Qn + o.q0;
+      e.jac = g.jac;
+      e.hd = g.hd;
+      e.EVB = g.EVB;
+      e.LMU = A.b.lmuhg + o.gq;
+      e.LQ = A.b.lq + o.q0;
+      e.LEVB = A.b.levb + o.ev;
+      e.P = c->P;
+      k_ev_adj<G><<<g.nel, 128, 0, c->st>>>(e);
+    }
+    CKA(cudaGetLastError());
+    ++A.launches;
+    return DSEM_OK;
   });
-  return r;
 }
 
 // Reverse of step n, its stage input states at st[0..kord) and its end state at
@@ -524,10 +618,8 @@ template <class F> int replay(dsem_ctx *c, cudaGraphExec_t *gx, F &&f) {
   return DSEM_OK;
 }
 
-size_t evb_bytes(const Adj &A) {
-  const Group &g = *A.g;
-  return (size_t)g.nel * 15 * g.G * g.G * g.G * sizeof(double);
-}
+// bytes of all groups' saved gradients (15 G^3 doubles per element: 3 nq)
+size_t evb_bytes(const Adj &A) { return (size_t)3 * A.c->nq * sizeof(double); }
 
 // The state of slot si into the context; with entropy viscosity also the
 // gradients behind the viscosity of the slot's step and their validity.
@@ -535,7 +627,7 @@ int load_slot(Adj &A, int si) {
   dsem_ctx *c = A.c;
   CKA(cudaMemcpyAsync(c->JQ, A.b.slots[si], c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
   if (A.visc) {
-    CKA(cudaMemcpyAsync(A.g->EVB, A.b.slot_evb[si], evb_bytes(A), cudaMemcpyDeviceToDevice, c->st));
+    if (int r = evb_copy(A, A.b.slot_evb[si], false)) return r;
     grad_flag(A) = A.b.slot_valid[si] != 0;
   }
   return dsem_int::traces(c);
@@ -547,7 +639,7 @@ int save_slot(Adj &A, int si) {
   dsem_ctx *c = A.c;
   CKA(cudaMemcpyAsync(A.b.slots[si], c->JQ, c->nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
   if (A.visc) {
-    CKA(cudaMemcpyAsync(A.b.slot_evb[si], A.g->EVB, evb_bytes(A), cudaMemcpyDeviceToDevice, c->st));
+    if (int r = evb_copy(A, A.b.slot_evb[si], true)) return r;
     A.b.slot_valid[si] = grad_flag(A) ? 1 : 0;
   }
   return DSEM_OK;
@@ -557,8 +649,7 @@ int save_slot(Adj &A, int si) {
 // viscosity reads, which that step's last stage overwrites.
 int keep_prev(Adj &A) {
   if (!A.visc) return DSEM_OK;
-  dsem_ctx *c = A.c;
-  CKA(cudaMemcpyAsync(A.b.evb_prev, A.g->EVB, evb_bytes(A), cudaMemcpyDeviceToDevice, c->st));
+  if (int r = evb_copy(A, A.b.evb_prev, true)) return r;
   A.prev_valid = grad_flag(A);
   return DSEM_OK;
 }
@@ -611,7 +702,7 @@ int revolve(Adj &A, int i, int j, int si, int sfree) {
     int r = load_slot(A, si);
     if (r) return r;
     if ((r = keep_prev(A)) || (r = forward_step(A, i, st.data(), nullptr, qfp))) return r;
-    return reverse_step(A, i, st.data(), c->JQ, qfp, nullptr, nullptr, A.g->EVB);
+    return reverse_step(A, i, st.data(), c->JQ, qfp, nullptr, nullptr, EVB_GROUPS);
   }
   if (nfree == 0) {  // no free slot: re-advance from slot si for every step
     for (int m = j - 1; m >= i; --m) {
@@ -620,7 +711,7 @@ int revolve(Adj &A, int i, int j, int si, int sfree) {
       for (int n = i; n < m; ++n)
         if ((r = forward_step(A, n, nullptr, nullptr))) return r;
       if ((r = keep_prev(A)) || (r = forward_step(A, m, st.data(), nullptr, qfp))) return r;
-      if ((r = reverse_step(A, m, st.data(), c->JQ, qfp, nullptr, nullptr, A.g->EVB))) return r;
+      if ((r = reverse_step(A, m, st.data(), c->JQ, qfp, nullptr, nullptr, EVB_GROUPS))) return r;
     }
     return DSEM_OK;
   }
@@ -656,7 +747,7 @@ int seg_forward(Adj &A, int b, int e, double *eps_part, cudaGraphExec_t *gx) {
   dsem_ctx *c = A.c;
   const int kord = c->kord;
   const size_t nq = c->nq, nf = c->nface, npart = (size_t)c->ngrid * 5;
-  const size_t nevb = (size_t)A.g->nel * 15 * A.g->G * A.g->G * A.g->G;
+  const size_t nevb = (size_t)3 * c->nq;
   CKA(cudaMemcpyAsync(A.b.stages, c->JQ, nq * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
   CKA(cudaMemcpyAsync(A.b.traces, c->QF, nf * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
   for (int n = b; n < e; ++n) {
@@ -686,7 +777,7 @@ int seg_reverse(Adj &A, int b, int e, bool first, cudaGraphExec_t *gx) {
   dsem_ctx *c = A.c;
   const int kord = c->kord;
   const size_t nq = c->nq, nf = c->nface;
-  const size_t nevb = (size_t)A.g->nel * 15 * A.g->G * A.g->G * A.g->G;
+  const size_t nevb = (size_t)3 * c->nq;
   for (int m = e - 1; m >= b; --m) {
     const int i = m - b;
     std::vector<double *> st, qf;
@@ -697,7 +788,7 @@ int seg_reverse(Adj &A, int b, int e, bool first, cudaGraphExec_t *gx) {
     const double *qend = m + 1 < e ? A.b.stages + (size_t)(i + 1) * kord * nq : c->JQ;
     const double *qprev = m > b ? A.b.stages + ((size_t)(i - 1) * kord + kord - 1) * nq : nullptr;
     const double *qfprev = m > b ? A.b.traces + ((size_t)(i - 1) * kord + kord - 1) * nf : nullptr;
-    const double *evb = A.visc ? A.g->EVB : ((A.in_window(m) && A.b.evbw) ? A.b.evbw + (size_t)i * nevb : nullptr);
+    const double *evb = A.visc ? EVB_GROUPS : ((A.in_window(m) && A.b.evbw) ? A.b.evbw + (size_t)i * nevb : nullptr);
     auto f = [&] { return reverse_step(A, m, st.data(), qend, qf.data(), qprev, qfprev, evb); };
     const int r = ((first && m == e - 1) || (A.visc && m == b)) ? f() : replay(c, &gx[A.in_window(m) ? 1 : 0], f);
     if (r) return r;
@@ -731,20 +822,45 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   if (!c) return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "null context");
   if (nsteps < 1 || window < 0 || window > nsteps || snapshots < 0 || !(dt > 0.0))
     return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "adjoint: need nsteps >= 1, 0 <= window <= nsteps, snapshots >= 0, dt > 0");
-  if (c->ncase != 1 || c->groups.size() != 1 || c->mlists.size() != 1 || c->nnc > 0 || !c->groups[0].diag ||
-      (c->les && (c->shock || c->les_sensors)) || c->ncut > 0 ||
-      (c->nbnd > 0 && (c->blists.size() != 1 || c->blists[0].G != c->groups[0].G)))
+  bool diag = true;
+  int gmax = 0;
+  for (const Group &g : c->groups) {
+    diag = diag && g.diag;
+    gmax = std::max(gmax, g.G);
+  }
+  if (c->ncase != 1 || !diag || (c->les && (c->shock || c->les_sensors)) || c->ncut > 0)
     return dsem_int::fail(c, DSEM_ERR_UNSUPPORTED,
-                          "adjoint: one case, one element order, conforming mortars, axis-aligned elements, no LES "
-                          "together with entropy viscosity or the LES sensors, no sharding");
-  if (dJdQ0 && ldx < c->groups[0].G) return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "ldx smaller than the number of Gauss points");
+                          "adjoint: one case, axis-aligned elements, no LES together with entropy viscosity or the "
+                          "LES sensors, no sharding");
+  if (dJdQ0 && ldx < gmax) return dsem_int::fail(c, DSEM_ERR_INVALID_ARG, "ldx smaller than the number of Gauss points");
   int r = upload_ops_here(c);
   if (r) return r;
   Adj A;
   A.c = c;
-  A.g = &c->groups[0];
-  A.ml = &c->mlists[0];
-  A.bl = c->nbnd > 0 ? &c->blists[0] : nullptr;
+  A.single = c->groups.size() == 1 && c->nnc == 0;
+  A.bl = (A.single && c->nbnd > 0) ? &c->blists[0] : nullptr;
+  {  // the groups' slices of the buffers
+    long long scr = 0;
+    for (const Group &g : c->groups) {
+      GOff o;
+      o.q0 = g.q0;
+      o.f0 = g.f0;
+      o.e0 = g.e0;
+      o.gq = g.q0 / 5;
+      o.ev = 3 * g.q0;
+      o.scr = scr;
+      with_G(g.G, [&](auto gc) -> cudaError_t {
+        scr += (long long)VolAdjCfg<decltype(gc)::value>::SCR * g.nel;
+        return cudaSuccess;
+      });
+      A.off.push_back(o);
+    }
+    // p = 7, 8: the volume adjoint's arrays that do not fit shared memory
+    if (scr && cudaMalloc(&A.b.volscr, (size_t)scr * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return dsem_int::fail(c, DSEM_ERR_NOMEM, "adjoint: not enough device memory for the volume scratch");
+    }
+  }
   A.dt = dt;
   A.nsteps = nsteps;
   A.window = window;
@@ -752,20 +868,13 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   const int kord = c->kord;
   for (double **p : {&A.b.lq, &A.b.lg, &A.b.ljq, &A.b.q0}) CKA(cudaMalloc(p, bq));
   for (double **p : {&A.b.qfr, &A.b.lff, &A.b.lvf, &A.b.lqf, &A.b.lqr}) CKA(cudaMalloc(p, bf));
-  CKA(cudaMalloc(&A.b.lrp, (size_t)A.g->nel * sizeof(double)));
-  {  // p = 7, 8: the volume adjoint's arrays that do not fit shared memory
-    size_t scr = 0;
-    with_G(A.g->G, [&](auto gc) -> cudaError_t {
-      scr = VolAdjCfg<decltype(gc)::value>::SCR;
-      return cudaSuccess;
-    });
-    if (scr && cudaMalloc(&A.b.volscr, scr * A.g->nel * sizeof(double)) != cudaSuccess) {
-      cudaGetLastError();
-      return dsem_int::fail(c, DSEM_ERR_NOMEM, "adjoint: not enough device memory for the volume scratch");
-    }
+  CKA(cudaMalloc(&A.b.lrp, (size_t)c->ngrid * sizeof(double)));
+  size_t nbpt = 0;  // boundary points, per list
+  for (const BList &bl : c->blists) {
+    A.boff.push_back((long long)nbpt);
+    nbpt += (size_t)bl.n * bl.G * bl.G;
   }
-  const size_t nbpt = A.bl ? (size_t)A.bl->n * A.g->G * A.g->G : 0;
-  if (A.bl) {
+  if (nbpt) {
     CKA(cudaMalloc(&A.b.lrb, nbpt * sizeof(double)));
     CKA(cudaMemsetAsync(A.b.lrb, 0, nbpt * sizeof(double), c->st));
   }
@@ -773,13 +882,12 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   A.les = c->les != 0;
   A.visc = A.ev || A.les;
   if (A.visc) {
-    const size_t ng = (size_t)A.g->nel * A.g->G * A.g->G * A.g->G;
-    CKA(cudaMalloc(&A.b.lmuhg, ng * sizeof(double)));
-    CKA(cudaMalloc(&A.b.levb, 15 * ng * sizeof(double)));
+    CKA(cudaMalloc(&A.b.lmuhg, (nq / 5) * sizeof(double)));
+    CKA(cudaMalloc(&A.b.levb, evb_bytes(A)));
     A.ev_valid0 = grad_flag(A);
     if (A.ev_valid0) {  // the gradients behind the first step's viscosity
-      CKA(cudaMalloc(&A.b.evb0, 15 * ng * sizeof(double)));
-      CKA(cudaMemcpyAsync(A.b.evb0, A.g->EVB, 15 * ng * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+      CKA(cudaMalloc(&A.b.evb0, evb_bytes(A)));
+      if ((r = evb_copy(A, A.b.evb0, true))) return r;
     }
   }
   CKA(cudaMalloc(&A.b.lr, sizeof(double)));
@@ -791,7 +899,7 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   // two-level scheme: snapshots at the starts of segments of seg_k steps, and one
   // segment's stage states and raw traces (the stash); revolve when they do not fit
   int seg_k = 0, nseg = 0;
-  if (snapshots > 0 && c->adj_scheme == DSEM_ADJ_SEGMENTS && !lean && !A.bl) {
+  if (snapshots > 0 && c->adj_scheme == DSEM_ADJ_SEGMENTS && !lean && A.single && c->nbnd == 0) {
     seg_k = (nsteps + snapshots - 1) / snapshots;
     nseg = (nsteps + seg_k - 1) / seg_k;
     if (cudaMalloc(&A.b.stages, (size_t)seg_k * kord * bq) != cudaSuccess ||
@@ -843,7 +951,7 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   if ((r = dsem_int::traces(c))) return r;
   // with every stage state and its raw traces kept, the sweep runs out of place
   // through the stash: its first slot starts with the initial state and traces
-  const bool oop = snapshots == 0 && A.b.traces && !A.bl;  // out-of-place stages: periodic faces only
+  const bool oop = snapshots == 0 && A.b.traces && A.single && c->nbnd == 0;  // out-of-place stages: one group, periodic faces
   if (oop) {
     CKA(cudaMemcpyAsync(A.b.stages, c->JQ, bq, cudaMemcpyDeviceToDevice, c->st));
     CKA(cudaMemcpyAsync(A.b.traces, c->QF, bf, cudaMemcpyDeviceToDevice, c->st));
@@ -854,7 +962,7 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   if (window > 0) CKA(cudaMalloc(&A.b.eps_part, (size_t)window * npart * sizeof(double)));
   // the gradients saved by each window step's last stage, for the reverse
   // sweep's direct enstrophy term (else recomputed there)
-  const size_t nevb = (size_t)A.g->nel * 15 * A.g->G * A.g->G * A.g->G;
+  const size_t nevb = (size_t)3 * c->nq;
   if (oop && !A.visc && window > 0 && !lean &&
       cudaMalloc(&A.b.evbw, (size_t)window * nevb * sizeof(double)) != cudaSuccess) {
     cudaGetLastError();
@@ -938,7 +1046,7 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
   CKA(cudaMemsetAsync(A.b.lq, 0, bq, c->st));
   CKA(cudaMemsetAsync(A.b.lg, 0, bq, c->st));
   CKA(cudaMemsetAsync(A.b.lr, 0, sizeof(double), c->st));
-  CKA(cudaMemsetAsync(A.b.lrp, 0, (size_t)A.g->nel * sizeof(double), c->st));  // per element, summed over stages
+  CKA(cudaMemsetAsync(A.b.lrp, 0, (size_t)c->ngrid * sizeof(double), c->st));  // per element, summed over stages
   if (window > 0) {
     if (snapshots == 0) {
       // Every reverse step launches the same kernels with other stage pointers:
@@ -964,7 +1072,7 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
         // the gradients step n's last stage saved: kept by the forward sweep, or with
         // entropy viscosity the group's EVB (the forward sweep's last step, then
         // each reverse step's recomputation for the step before it)
-        const double *evb = A.visc ? A.g->EVB
+        const double *evb = A.visc ? EVB_GROUPS
                                  : ((A.in_window(n) && A.b.evbw) ? A.b.evbw + (size_t)(n - (nsteps - window)) * nevb
                                                                  : nullptr);
         if (n == nsteps - 1 || (A.visc && n == 0)) {  // launch sequences of their own: eager
@@ -1002,9 +1110,9 @@ extern "C" int dsem_adjoint(dsem_ctx *c, double dt, int nsteps, int window, int 
       }
     }
   }
-  k_sum_into<<<1, 256, 0, c->st>>>(A.b.lrp, A.g->nel, A.b.lr);  // dJ/d(1/Re) of the volume terms
+  k_sum_into<<<1, 256, 0, c->st>>>(A.b.lrp, c->ngrid, A.b.lr);  // dJ/d(1/Re) of the volume terms
   CKA(cudaGetLastError());
-  if (A.bl) {  // ... and of the external viscous fluxes of inflow and outflow faces
+  if (nbpt) {  // ... and of the external viscous fluxes of inflow and outflow faces
     k_sum_into<<<1, 256, 0, c->st>>>(A.b.lrb, (int)nbpt, A.b.lr);
     CKA(cudaGetLastError());
   }

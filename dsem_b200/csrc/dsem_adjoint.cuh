@@ -675,6 +675,252 @@ __global__ void __launch_bounds__(128) k_face_bnd_vis_adj(const MortarB *__restr
   if (bc == BC_INFLOW || bc == BC_OUTFLOW) LRB[t] += lr;
 }
 
+// ------------------------------------------------- p-nonconforming mortars
+// Transposes of the projections of k_face_nc_inv / k_face_nc_vis (dsem_stage.cuh:
+// nc_to_mortar, nc_to_face, nc_rotate_to_*), on [var][j*NMX + i] arrays in shared memory.
+
+// x[k] = sum_{i < nout} A[i*nin + k] y[i*ys]: the transpose of nc_apply
+static __device__ __forceinline__ double nc_apply_t(const double *A, int nin, int nout, int k, const double *y, int ys) {
+  double acc = A[k] * y[0];
+  for (int i = 1; i < nout; ++i) acc = acc + A[i * nin + k] * y[i * ys];
+  return acc;
+}
+
+// nc_to_mortar transposed: a (mortar extents) -> a (face extents), in place via tmp
+static __device__ void nc_to_mortar_t(const MortarNC &M, int side, const double *mats, double *a, double *tmp, int tid,
+                                      int nt) {
+  const bool c1 = M.conf[2 * side], c2 = M.conf[2 * side + 1];
+  if (c1 && c2) return;
+  const int n = side == 0 ? M.gm : M.gs;
+  const int m1 = c1 ? n : M.lm1;
+  if (!c2) {  // the j step: out[j][i] = sum_k A[j*n + k] in[k][i], j < lm2, k < n, i < m1
+    const double *A = mats + M.P[side][1];
+    for (int t = tid; t < NV * m1 * n; t += nt) {
+      const int v = t / (m1 * n), r = t - v * m1 * n, i = r % m1, k = r / m1;
+      tmp[v * NMX * NMX + k * NMX + i] = nc_apply_t(A, n, M.lm2, k, a + v * NMX * NMX + i, NMX);
+    }
+    __syncthreads();
+    for (int t = tid; t < NV * m1 * n; t += nt) {
+      const int v = t / (m1 * n), r = t - v * m1 * n, i = r % m1, k = r / m1;
+      a[v * NMX * NMX + k * NMX + i] = tmp[v * NMX * NMX + k * NMX + i];
+    }
+    __syncthreads();
+  }
+  if (!c1) {  // the i step: out[j][i] = sum_k A[i*n + k] in[j][k], i < lm1, j < n, k < n
+    const double *A = mats + M.P[side][0];
+    for (int t = tid; t < NV * n * n; t += nt) {
+      const int v = t / (n * n), r = t - v * n * n, k = r % n, j = r / n;
+      tmp[v * NMX * NMX + j * NMX + k] = nc_apply_t(A, n, M.lm1, k, a + v * NMX * NMX + j * NMX, 1);
+    }
+    __syncthreads();
+    for (int t = tid; t < NV * n * n; t += nt) {
+      const int v = t / (n * n), r = t - v * n * n, k = r % n, j = r / n;
+      a[v * NMX * NMX + j * NMX + k] = tmp[v * NMX * NMX + j * NMX + k];
+    }
+    __syncthreads();
+  }
+}
+
+// nc_to_face transposed: a (face extents) -> a (mortar extents), in place via tmp
+static __device__ void nc_to_face_t(const MortarNC &M, int side, const double *mats, double *a, double *tmp, int tid,
+                                    int nt) {
+  const bool c1 = M.conf[2 * side], c2 = M.conf[2 * side + 1];
+  if (c1 && c2) return;
+  const int n = side == 0 ? M.gm : M.gs;
+  const int m1 = c1 ? M.lm1 : n;
+  if (!c2) {  // the j step: out[j][i] = sum_k R[j*lm2 + k] in[k][i], j < n, k < lm2, i < m1
+    const double *A = mats + M.R[side][1];
+    for (int t = tid; t < NV * m1 * M.lm2; t += nt) {
+      const int v = t / (m1 * M.lm2), r = t - v * m1 * M.lm2, i = r % m1, k = r / m1;
+      tmp[v * NMX * NMX + k * NMX + i] = nc_apply_t(A, M.lm2, n, k, a + v * NMX * NMX + i, NMX);
+    }
+    __syncthreads();
+    for (int t = tid; t < NV * m1 * M.lm2; t += nt) {
+      const int v = t / (m1 * M.lm2), r = t - v * m1 * M.lm2, i = r % m1, k = r / m1;
+      a[v * NMX * NMX + k * NMX + i] = tmp[v * NMX * NMX + k * NMX + i];
+    }
+    __syncthreads();
+  }
+  if (!c1) {  // the i step: out[j][i] = sum_k R[i*lm1 + k] in[j][k], i < n, k < lm1, j < lm2
+    const double *A = mats + M.R[side][0];
+    for (int t = tid; t < NV * M.lm1 * M.lm2; t += nt) {
+      const int v = t / (M.lm1 * M.lm2), r = t - v * M.lm1 * M.lm2, k = r % M.lm1, j = r / M.lm1;
+      tmp[v * NMX * NMX + j * NMX + k] = nc_apply_t(A, M.lm1, n, k, a + v * NMX * NMX + j * NMX, 1);
+    }
+    __syncthreads();
+    for (int t = tid; t < NV * M.lm1 * M.lm2; t += nt) {
+      const int v = t / (M.lm1 * M.lm2), r = t - v * M.lm1 * M.lm2, k = r % M.lm1, j = r / M.lm1;
+      a[v * NMX * NMX + j * NMX + k] = tmp[v * NMX * NMX + j * NMX + k];
+    }
+    __syncthreads();
+  }
+}
+
+// face slot (var-major, n x n) <-> [var][j*NMX + i] array, with a factor on load
+static __device__ __forceinline__ void nc_load(double *dst, const double *src, int n, double f, int tid, int nt) {
+  for (int t = tid; t < NV * NMX * NMX; t += nt) dst[t] = 0.0;
+  __syncthreads();
+  const int n2 = n * n;
+  for (int t = tid; t < NV * n2; t += nt) {
+    const int v = t / n2, p = t - v * n2;
+    dst[v * NMX * NMX + (p / n) * NMX + p % n] = f * src[t];
+  }
+  __syncthreads();
+}
+static __device__ __forceinline__ void nc_store(double *dst, const double *src, int n, int tid, int nt) {
+  const int n2 = n * n;
+  for (int t = tid; t < NV * n2; t += nt) {
+    const int v = t / n2, p = t - v * n2;
+    dst[t] = src[v * NMX * NMX + (p / n) * NMX + p % n];
+  }
+}
+// b <- a (all of it); then a <- rotated b when the mortar has an orientation
+static __device__ __forceinline__ void nc_rot_mortar_inplace(const MortarNC &M, double *a, double *b, int tid, int nt) {
+  if (!M.orient) return;
+  for (int t = tid; t < NV * NMX * NMX; t += nt) b[t] = 0.0;
+  __syncthreads();
+  nc_rotate_to_mortar(M, a, b, tid, nt);
+  __syncthreads();
+  for (int t = tid; t < NV * NMX * NMX; t += nt) a[t] = b[t];
+  __syncthreads();
+}
+static __device__ __forceinline__ void nc_rot_face_inplace(const MortarNC &M, double *a, double *b, int tid, int nt) {
+  if (!M.orient) return;
+  for (int t = tid; t < NV * NMX * NMX; t += nt) b[t] = 0.0;
+  __syncthreads();
+  nc_rotate_to_face(M, a, b, tid, nt);
+  __syncthreads();
+  for (int t = tid; t < NV * NMX * NMX; t += nt) a[t] = b[t];
+  __syncthreads();
+}
+
+// k_face_nc_inv transposed, one CTA per nonconforming mortar: from dJ/dFF (LFF) and dJ/d(the
+// averaged state) (LQF) at both face slots to dJ/d(raw traces) (LQR).  The mortar-space states
+// are recomputed from the raw traces QFR; rotations transpose to their inverses.
+static __global__ void __launch_bounds__(128) k_face_nc_inv_adj(const MortarNC *__restrict__ mn,
+                                                                 const double *__restrict__ QFR,
+                                                                 const double *__restrict__ LFF,
+                                                                 const double *__restrict__ LQF,
+                                                                 double *__restrict__ LQR, const double *__restrict__ nh,
+                                                                 const double *__restrict__ nrm,
+                                                                 const double *__restrict__ mats, double gamma) {
+  __shared__ double A1[NV * NMX * NMX], A2[NV * NMX * NMX], T0[NV * NMX * NMX], LF[NV * NMX * NMX],
+      LA[NV * NMX * NMX], X[NV * NMX * NMX];
+  const MortarNC M = mn[blockIdx.x];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  // forward: the two sides' states on the mortar points
+  nc_load(A1, QFR + M.ms, M.gm, 1.0, tid, nt);
+  nc_load(A2, QFR + M.ss, M.gs, 1.0, tid, nt);
+  nc_rot_mortar_inplace(M, A2, T0, tid, nt);
+  nc_to_mortar(M, 0, mats, A1, T0, tid, nt);
+  nc_to_mortar(M, 1, mats, A2, T0, tid, nt);
+  // dJ/d(mortar flux) and dJ/d(mortar average) from both faces
+  nc_load(LF, LFF + M.ms, M.gm, 1.0, tid, nt);
+  nc_to_face_t(M, 0, mats, LF, T0, tid, nt);
+  nc_load(X, LFF + M.ss, M.gs, (double)M.sign, tid, nt);
+  nc_rot_mortar_inplace(M, X, T0, tid, nt);
+  nc_to_face_t(M, 1, mats, X, T0, tid, nt);
+  for (int t = tid; t < NV * NMX * NMX; t += nt) LF[t] += X[t];
+  __syncthreads();
+  nc_load(LA, LQF + M.ms, M.gm, 1.0, tid, nt);
+  nc_to_face_t(M, 0, mats, LA, T0, tid, nt);
+  nc_load(X, LQF + M.ss, M.gs, 1.0, tid, nt);
+  nc_rot_mortar_inplace(M, X, T0, tid, nt);
+  nc_to_face_t(M, 1, mats, X, T0, tid, nt);
+  for (int t = tid; t < NV * NMX * NMX; t += nt) LA[t] += X[t];
+  __syncthreads();
+  // Roe flux and average at each mortar point, reversed; the states' adjoints replace them
+  for (int t = tid; t < M.lm1 * M.lm2; t += nt) {
+    const int i = t % M.lm1, j = t / M.lm1;
+    double Q1[NV], Q2[NV], lf[NV], l1[NV], l2[NV];
+    for (int v = 0; v < NV; ++v) {
+      const int q = v * NMX * NMX + j * NMX + i;
+      Q1[v] = A1[q];
+      Q2[v] = A2[q];
+      lf[v] = LF[q];
+      l1[v] = 0.5 * LA[q];
+      l2[v] = l1[v];
+    }
+    const long long gp = (long long)M.geo + t;
+    const double n3[3] = {nh[gp * 3], nh[gp * 3 + 1], nh[gp * 3 + 2]};
+    if (M.low)
+      roe_vjp_rev(n3, nrm[gp], Q2, Q1, gamma, lf, l2, l1);
+    else
+      roe_vjp_rev(n3, nrm[gp], Q1, Q2, gamma, lf, l1, l2);
+    for (int v = 0; v < NV; ++v) {
+      const int q = v * NMX * NMX + j * NMX + i;
+      A1[q] = l1[v];
+      A2[q] = l2[v];
+    }
+  }
+  __syncthreads();
+  // back to the faces: prolongations transposed, the slave's rotation inverted
+  nc_to_mortar_t(M, 0, mats, A1, T0, tid, nt);
+  nc_store(LQR + M.ms, A1, M.gm, tid, nt);
+  nc_to_mortar_t(M, 1, mats, A2, T0, tid, nt);
+  nc_rot_face_inplace(M, A2, T0, tid, nt);
+  nc_store(LQR + M.ss, A2, M.gs, tid, nt);
+}
+
+// k_face_nc_vis transposed: from dJ/dVF after the average (-LFF/Re at both faces) to dJ/dVF
+// before it (LVF).
+static __global__ void __launch_bounds__(128) k_face_nc_vis_adj(const MortarNC *__restrict__ mn,
+                                                                 const double *__restrict__ LFF, double re,
+                                                                 double *__restrict__ LVF,
+                                                                 const double *__restrict__ nrm,
+                                                                 const double *__restrict__ mats) {
+  __shared__ double QB[NV * NMX * NMX], X[NV * NMX * NMX], T0[NV * NMX * NMX];
+  const MortarNC M = mn[blockIdx.x];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const bool conf1 = M.conf[0] && M.conf[1], conf2 = M.conf[2] && M.conf[3];
+  const double *nm = nrm + M.geo;  // mortar points, index i + lm1*j
+  nc_load(QB, LFF + M.ms, M.gm, -1.0 / re, tid, nt);
+  nc_to_face_t(M, 0, mats, QB, T0, tid, nt);
+  nc_load(X, LFF + M.ss, M.gs, -1.0 / re, tid, nt);
+  nc_rot_mortar_inplace(M, X, T0, tid, nt);
+  nc_to_face_t(M, 1, mats, X, T0, tid, nt);
+  const double sg = M.sign == -1 ? -1.0 : 1.0;
+  for (int t = tid; t < NV * NMX * NMX; t += nt) QB[t] += sg * X[t];
+  __syncthreads();
+  // QB = 0.5 (fv1 + nsign fv2) |n| at the mortar points: dJ/dfv1 into QB, dJ/dfv2 into X
+  for (int t = tid; t < NV * NMX * NMX; t += nt) X[t] = 0.0;
+  __syncthreads();
+  for (int t = tid; t < NV * M.lm1 * M.lm2; t += nt) {
+    const int v = t / (M.lm1 * M.lm2), r = t - v * M.lm1 * M.lm2, i = r % M.lm1, j = r / M.lm1;
+    const int q = v * NMX * NMX + j * NMX + i;
+    const double l = 0.5 * nm[i + M.lm1 * j] * QB[q];
+    QB[q] = l;
+    X[q] = M.nsign == -1 ? -l : l;
+  }
+  __syncthreads();
+  // master: fv1 = P0(VF) / |n|
+  for (int t = tid; t < NV * M.lm1 * M.lm2; t += nt) {
+    const int v = t / (M.lm1 * M.lm2), r = t - v * M.lm1 * M.lm2, i = r % M.lm1, j = r / M.lm1;
+    QB[v * NMX * NMX + j * NMX + i] = QB[v * NMX * NMX + j * NMX + i] / nm[i + M.lm1 * j];
+  }
+  __syncthreads();
+  if (!conf1) nc_to_mortar_t(M, 0, mats, QB, T0, tid, nt);
+  nc_store(LVF + M.ms, QB, M.gm, tid, nt);
+  // slave: conforming, fv2 = rotate(VF / |n| in face indexing); else fv2 = P1(rotate(VF)) / |n|
+  if (conf2) {
+    nc_rot_face_inplace(M, X, T0, tid, nt);
+    for (int t = tid; t < NV * M.gs * M.gs; t += nt) {
+      const int v = t / (M.gs * M.gs), r = t - v * M.gs * M.gs, i = r % M.gs, j = r / M.gs;
+      X[v * NMX * NMX + j * NMX + i] = X[v * NMX * NMX + j * NMX + i] / nm[i + M.lm1 * j];
+    }
+    __syncthreads();
+  } else {
+    for (int t = tid; t < NV * M.lm1 * M.lm2; t += nt) {
+      const int v = t / (M.lm1 * M.lm2), r = t - v * M.lm1 * M.lm2, i = r % M.lm1, j = r / M.lm1;
+      X[v * NMX * NMX + j * NMX + i] = X[v * NMX * NMX + j * NMX + i] / nm[i + M.lm1 * j];
+    }
+    __syncthreads();
+    nc_to_mortar_t(M, 1, mats, X, T0, tid, nt);
+    nc_rot_face_inplace(M, X, T0, tid, nt);
+  }
+  nc_store(LVF + M.ss, X, M.gs, tid, nt);
+}
+
 // Qt = -(QTI + sum_faces D_edge FB), FB = FF - VF/Re, transposed for one element
 // from its dJ/dQt (lam, shared) to dJ/dFF (LFF).  dJ/dVF is -LFF/Re, formed by
 // k_face_vis_adj.

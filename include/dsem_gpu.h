@@ -297,8 +297,8 @@ int dsem_diag_batch(dsem_ctx *ctx, const double *dt, int first, double *ke, doub
  * states and recomputes steps in binomial checkpointing order.  Outputs (each
  * may be NULL): J; dJ/d(JQ at the start) in the ldx layout of dsem_upload_q;
  * dJ/d(1/Re); the device milliseconds of the whole call.  The state is
- * restored on return.  Supported: one case, one element order (p <= 8),
- * axis-aligned elements, conforming periodic mortars, shock = 0, 1 or 3
+ * restored on return.  Supported: one case, any element orders (p <= 8, with
+ * the p-nonconforming mortars between them), axis-aligned elements, shock = 0, 1 or 3
  * (entropy viscosity, with or without the Ducros sensor) or static Smagorinsky LES without the
  * shock and density sensors (not both models at once; with snapshots > 0
  * each snapshot also keeps the gradients its step's viscosity reads),

@@ -482,3 +482,65 @@ def test_adjoint_high_order(oracle_mod, p, ev):
     J1, g1, lr1, _ = s.adjoint(dt, 2, 2, snapshots=1, scheme="segments")
     assert J1 == J and lr1 == lr and np.array_equal(g1, g)
     s.close()
+
+
+def _band(n, p_out, p_in):
+    """Orders of an n^3 box: p_out, with the middle third in x at p_in (p-nonconforming mortars
+    between the two)."""
+    orders = np.full(n ** 3, p_out)
+    for iz in range(n):
+        for ix in range(n):
+            for iy in range(n):
+                if n // 3 <= ix < n - n // 3:
+                    orders[iy + n * (ix + n * iz)] = p_in
+    return orders
+
+
+@pytest.mark.parametrize("p_out,p_in,phys,bc", [(3, 4, {}, None), (4, 6, {}, None), (3, 4, EV, None),
+                                                 (3, 4, {}, {"y": ("walladiab", "walladiab")})])
+def test_adjoint_nonconforming_band(oracle_mod, p_out, p_in, phys, bc):
+    """Two element orders joined by p-nonconforming mortars (mortar_operations.f90:151-758:
+    prolongation to the mortar, Roe flux and average there, restriction back): the stage
+    adjoint runs per order group and per face list, and k_face_nc_inv_adj / k_face_nc_vis_adj
+    transpose the projections.  Against complex-step derivatives of the oracle, and bit for
+    bit under checkpointing."""
+    from dsem_b200.solver import Solver
+    re = 500.0
+    box = mesh.Box(3, 3, 3, _band(3, p_out, p_in), bc=bc)
+    assert (~box.mortar[:, 13:17].all(axis=1)).sum() > 0  # nonconforming mortars present
+    q = mesh.random_isotropic(box, seed=29, k0=2.0, mach_t=0.2)
+    dt = 0.4 * mesh.dtcalc(box, q)
+    s = Solver(box.desc(), re=re, **phys)
+    c = oracle_mod.Case.from_desc(box.desc())
+    c.set_phys(re=re, **phys)
+    c.set_q(q)
+    s.upload(q)
+    if phys:
+        s.step(dt, 1)
+        c.step(0.0, dt, 1)
+    q0 = s.download()
+    J, g, lr, _ = s.adjoint(dt, 3, 2, snapshots=0)
+    assert np.abs(g).max() > 0
+    for d in _directions(q, p_in + 1, 3, seed=p_out + 90):
+        Jc, dJ = c.objective_cs(dt, 3, 2, d, 1e-30)
+        assert abs(J - Jc) <= 1e-12 * abs(Jc)
+        ga = float(np.sum(g * d))
+        assert abs(ga - dJ) <= TOL * abs(dJ), (ga, dJ)
+    if not phys:  # d/d(1/Re): central differences of the oracle's J
+        r = 1.0 / re
+        h = 1e-5 * r
+        vals = []
+        for rr in (r + h, r - h):
+            cc = oracle_mod.Case.from_desc(box.desc())
+            cc.set_phys(re=1.0 / rr)
+            cc.set_q(q0)
+            vals.append(cc.objective_cs(dt, 3, 2, None, 0.0)[0])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(lr - fd) <= TOL * abs(fd), (lr, fd)
+    for snaps in (1, 2):
+        s.upload(q)
+        if phys:
+            s.step(dt, 1)
+        J1, g1, lr1, _ = s.adjoint(dt, 3, 2, snapshots=snaps)
+        assert J1 == J and lr1 == lr and np.array_equal(g1, g), snaps
+    s.close()
