@@ -32,7 +32,9 @@ static cudaError_t vol_diag_one(const VolArgs &a, int nel, cudaStream_t s) {
   cudaError_t e = set_smem_once(kern, C::SMEM, attr);
   if (e != cudaSuccess) return e;
   if (nel <= 0) return cudaSuccess;
-  kern<<<nel, C::NT, C::SMEM, s>>>(a);
+  VolArgs b = a;
+  b.nel = nel;
+  kern<<<(nel + C::EPB - 1) / C::EPB, C::NT, C::SMEM, s>>>(b);
   return cudaGetLastError();
 }
 
@@ -56,6 +58,8 @@ template <int G> int Launch<G>::vol_variant_threads(int v) {
   switch (v) {
     case 1: return VolDiagShape<G, 1>::NT;
     case 2: return VolDiagShape<G, 2>::NT;
+    case 3: return VolDiagShape<G, 3>::NT;
+    case 4: return VolDiagShape<G, 4>::NT;
     default: return VolDiagShape<G, 0>::NT;
   }
 }
@@ -63,10 +67,14 @@ template <int G> int Launch<G>::vol_variant_threads(int v) {
 template <int G>
 cudaError_t Launch<G>::vol(const VolArgs &a, int nel, bool diag, int mode, cudaStream_t s, int variant) {
   if constexpr (G == 5 || G == 7 || G == 9) {  // variants of the diagonal kernel without entropy viscosity
-    if (diag && (variant == 1 || variant == 2) && (mode == VOL_PLAIN || mode == VOL_SAVE)) {
-      if (mode == VOL_SAVE)
-        return variant == 1 ? vol_diag_one<G, false, 1, 1>(a, nel, s) : vol_diag_one<G, false, 1, 2>(a, nel, s);
-      return variant == 1 ? vol_diag_one<G, false, 0, 1>(a, nel, s) : vol_diag_one<G, false, 0, 2>(a, nel, s);
+    if (diag && variant >= 1 && variant < VOL_VARIANTS && (mode == VOL_PLAIN || mode == VOL_SAVE)) {
+      const bool sv = mode == VOL_SAVE;
+      switch (variant) {
+        case 1: return sv ? vol_diag_one<G, false, 1, 1>(a, nel, s) : vol_diag_one<G, false, 0, 1>(a, nel, s);
+        case 2: return sv ? vol_diag_one<G, false, 1, 2>(a, nel, s) : vol_diag_one<G, false, 0, 2>(a, nel, s);
+        case 3: return sv ? vol_diag_one<G, false, 1, 3>(a, nel, s) : vol_diag_one<G, false, 0, 3>(a, nel, s);
+        default: return sv ? vol_diag_one<G, false, 1, 4>(a, nel, s) : vol_diag_one<G, false, 0, 4>(a, nel, s);
+      }
     }
   }
   switch (mode) {

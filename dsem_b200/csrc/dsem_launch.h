@@ -37,7 +37,7 @@ cudaError_t set_smem_once(K kern, size_t smem, std::atomic<unsigned long long> &
 // volume kernel variants: metric layout x entropy viscosity x saved gradients
 enum VolMode { VOL_PLAIN = 0, VOL_SAVE = 1, VOL_EV = 2, VOL_EV_SAVE = 3 };
 // launch shapes of the diagonal volume kernel the autotuner chooses from
-constexpr int VOL_VARIANTS = 3;
+constexpr int VOL_VARIANTS = 5;
 
 template <int G> struct Launch {
   static cudaError_t set_ops(const double *host_ops, int n);  // copies the operator table to constant memory

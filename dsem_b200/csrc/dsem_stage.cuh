@@ -798,6 +798,7 @@ struct VolArgs {
   Phys P;
   const int *ecase;             // optional: case of each element (ensembles)
   const double *rec;            // optional: per case {re, 1/re}
+  int nel;                      // elements of the launch (set by the launcher)
 };
 
 template <int G, bool DIAG, bool EV, int SAVE> struct VolCfg {

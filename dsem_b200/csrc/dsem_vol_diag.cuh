@@ -27,18 +27,24 @@
 
 namespace dsem {
 
-// Launch shapes of k_vol_diag: threads per element (NT) and the elements an SM
-// must hold at once (MINB, which sets the register budget).  Variant 0 is the
-// default; the autotuner (dsem_autotune) times variants 1 and 2 against it for
-// p = 4, 6, 8.  Every variant evaluates each value with the same FMA chain, so
-// all give identical results.
+// Launch shapes of k_vol_diag: threads per element (NT), the elements an SM
+// must hold at once (MINB, which sets the register budget), elements per block
+// (EPB: a block advances EPB elements one after another) and the Lobatto points
+// per flux task (PPT: 2, two points of a line sharing each gradient-line load, or
+// 1).  Variant 0 is the default; the autotuner (dsem_autotune) times variants
+// 1..4 against it for p = 4, 6, 8: 1 and 2 change the threads and register
+// budget, 3 takes two elements per block, 4 the other points-per-task.  Every
+// variant evaluates each value with the same FMA chain, so all give identical
+// results.
 #ifndef DSEM_VOL_DIAG_NT8
 #define DSEM_VOL_DIAG_NT8 192  // 2 CTAs x 6 warps per SM leave 168 registers per thread: no spills at p = 8
 #endif
-template <int G, int V> struct VolDiagShape {
+template <int G, int VV> struct VolDiagShape {
   // p >= 7: 192 / 128 / 256 threads, two elements per SM (168 / 255 / 128 registers)
   // p = 5, 6: 96 / 64 / 128 threads, four elements per SM (168 / 255 / 128 registers)
   // p <= 4: 64 / 64 / 128 threads, eight / six / four elements per SM
+  // variants 3 and 4: the threads and register budget of variant 0
+  static constexpr int V = VV >= 3 ? 0 : VV;
   static constexpr int NT = G >= 8 ? (V == 0 ? DSEM_VOL_DIAG_NT8 : (V == 1 ? 128 : 256))
                                    : G >= 6 ? (V == 0 ? 96 : (V == 1 ? 64 : 128))
                                             : G >= 4 ? (V == 2 ? 128 : 64) : 32;
@@ -47,6 +53,11 @@ template <int G, int V> struct VolDiagShape {
 #else
   static constexpr int MINB = G >= 8 ? 2 : (G >= 6 ? 4 : (G >= 4 ? (V == 0 ? 8 : (V == 1 ? 6 : 4)) : 16));
 #endif
+  static constexpr int EPB = VV == 3 ? 2 : 1;
+  // points per flux task: p = 8 (G = 9) two by default, lower orders one (measured: 12 % faster
+  // at p = 6); variant 4 takes the other
+  static constexpr int PPT_DEFAULT = G >= 8 ? 2 : 1;
+  static constexpr int PPT = VV == 4 ? 3 - PPT_DEFAULT : PPT_DEFAULT;
 };
 
 template <int G, bool EV, int SAVE, int V = 0> struct VolDiagCfg {
@@ -54,6 +65,7 @@ template <int G, bool EV, int SAVE, int V = 0> struct VolDiagCfg {
   static constexpr int NT = VolDiagShape<G, V>::NT;
   static constexpr int NPT = (NG + NT - 1) / NT;       // Gauss points per thread (divergence)
   static constexpr int MINB = VolDiagShape<G, V>::MINB;
+  static constexpr int EPB = VolDiagShape<G, V>::EPB, PPT = VolDiagShape<G, V>::PPT;
   static constexpr int NGR = 12;                        // Gauss gradients of fields 0..3
   static constexpr int NWORK = (6 * NL > 5 * NG) ? 6 * NL : 5 * NG;  // state (pass 1) / Lobatto arrays (pass 2)
   static constexpr size_t SMEM = sizeof(double) * (size_t)(NGR * NG + NWORK + 2 * G * L);
@@ -321,7 +333,9 @@ __device__ __forceinline__ void vol_diag_dir(const VolArgs &A, const Phys &P, co
     }
     vol_diag_point<G, D>(l0 + s0 * ls, s0, a, b, c0, les, nu0, EV, mu0, P, gm, LB, VF);
   };
-  if constexpr (SPLITB) {
+  if constexpr (C::PPT == 1) {  // one point per task
+    for (int u = tid; u < 2 * NTB; u += NT) b_point(u >> 1, u & 1);
+  } else if constexpr (SPLITB) {
     for (int t = tid; t < RB * NT; t += NT) b_task(t);
     if (tid < 2 * LEFTB) b_point(RB * NT + (tid >> 1), tid & 1);
   } else {
@@ -364,19 +378,18 @@ __device__ __forceinline__ void vol_diag_dir(const VolArgs &A, const Phys &P, co
   PHASE_MARK(4 + 3 * (2 - D));
 }
 
-template <int G, bool EV, int SAVE, int V = 0>
-__global__ void __launch_bounds__(VolDiagCfg<G, EV, SAVE, V>::NT, VolDiagCfg<G, EV, SAVE, V>::MINB)
-    k_vol_diag(VolArgs A) {
+// One element k of the volume kernel (its block's threads, shared memory sm).
+template <int G, bool EV, int SAVE, int V>
+__device__ __forceinline__ void vol_diag_element(const VolArgs &A, const int k, double *sm) {
   using C = VolDiagCfg<G, EV, SAVE, V>;
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G, NT = C::NT, NPT = C::NPT;
-  extern __shared__ double sm[];
   double *GR = sm;                  // [12][NG] Gauss gradients, field f*3 + direction
   double *WK = GR + C::NGR * NG;    // pass 1: state q [5][NG]; pass 2: LB [5][NL] + T4 [NL]
   double *LB = WK;
   double *T4 = WK + 5 * NL;         // energy gradient along D on grid D
   double *Bm = WK + C::NWORK;       // bx [L][G]
   double *Dm = Bm + L * G;          // dmx [G][L]
-  const int k = blockIdx.x, tid = threadIdx.x;
+  const int tid = threadIdx.x;
   const double *JQ = A.JQ + (long long)k * A.sq;
   const double *jac = A.jac + (long long)k * NG;
   const double *QF = A.QF + (long long)k * 30 * G2;
@@ -466,6 +479,23 @@ __global__ void __launch_bounds__(VolDiagCfg<G, EV, SAVE, V>::NT, VolDiagCfg<G, 
   vol_diag_dir<G, EV, SAVE, 1, V>(A, P, JQ, jac, QF, gg, gm, muhg, nuhg, GR, LB, T4, Bm, Dm, VF, QTI, tid, t_ph_);
   vol_diag_dir<G, EV, SAVE, 0, V>(A, P, JQ, jac, QF, gg, gm, muhg, nuhg, GR, LB, T4, Bm, Dm, VF, QTI, tid, t_ph_);
   PHASE_MARK(20);
+}
+
+template <int G, bool EV, int SAVE, int V = 0>
+__global__ void __launch_bounds__(VolDiagCfg<G, EV, SAVE, V>::NT, VolDiagCfg<G, EV, SAVE, V>::MINB)
+    k_vol_diag(VolArgs A) {
+  using C = VolDiagCfg<G, EV, SAVE, V>;
+  extern __shared__ double sm[];
+  if constexpr (C::EPB == 1) {
+    vol_diag_element<G, EV, SAVE, V>(A, blockIdx.x, sm);
+  } else {  // the block's elements one after another (each ends with a block barrier)
+#pragma unroll 1
+    for (int e = 0; e < C::EPB; ++e) {
+      const int k = blockIdx.x * C::EPB + e;
+      if (k >= A.nel) break;
+      vol_diag_element<G, EV, SAVE, V>(A, k, sm);
+    }
+  }
 }
 
 }  // namespace dsem

@@ -15,6 +15,7 @@ LIB = os.path.join(HERE, "libdsem_b200.so")
 
 DSEM_OK = 0
 ERRORS = {-1: "INVALID_ARG", -2: "CUDA", -3: "NONFINITE", -4: "TIMEOUT", -5: "UNSUPPORTED", -6: "NOMEM"}
+VOL_VARIANTS = 5  # DSEM_VOL_VARIANTS: launch shapes of the volume kernel per order
 EXPORTS = ("dsem_create", "dsem_destroy", "dsem_last_error", "dsem_upload_q", "dsem_download_q", "dsem_step",
            "dsem_stage", "dsem_rhs", "dsem_diag", "dsem_get_muhg", "dsem_last_timing", "dsem_profile_rhs",
            "dsem_create_batch", "dsem_batch_size", "dsem_upload_q_case", "dsem_download_q_case", "dsem_step_batch",
@@ -244,7 +245,7 @@ class Solver:
         """Times the volume kernel's launch shapes per element order and keeps the
         fastest: returns {p: chosen shape} and ms[p-1][shape] (-1: not timed)."""
         choice = np.zeros(8, dtype=np.int32)
-        ms = np.zeros((8, 3))
+        ms = np.zeros((8, VOL_VARIANTS))
         self._check(lib().dsem_autotune(self.h, int(reps), choice.ctypes.data_as(C.POINTER(C.c_int)), _dptr(ms)))
         orders = sorted({p for p in range(1, 9) if ms[p - 1, 0] >= 0})
         return {p: int(choice[p - 1]) for p in orders}, ms

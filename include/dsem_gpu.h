@@ -180,7 +180,7 @@ int dsem_load_state(dsem_ctx *ctx, const void *buf, long long nbytes);
  * either may be NULL.  Call it after dsem_upload_q.  dsem_set_vol_variant
  * sets a shape by hand. */
 #define DSEM_MAX_ORDER 8
-#define DSEM_VOL_VARIANTS 3
+#define DSEM_VOL_VARIANTS 5
 int dsem_autotune(dsem_ctx *ctx, int reps, int *choice, double *ms);
 int dsem_set_vol_variant(dsem_ctx *ctx, int p, int variant);
 
