@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--adj-steps", type=int, default=400, help="adjoint workload: steps of the run")
     ap.add_argument("--adj-window", type=int, default=100, help="adjoint workload: steps in the objective")
+    ap.add_argument("--shape", type=int, default=-1,
+                    help="default workload: the volume kernel's launch shape (0..4) instead of the autotuner's")
     return ap.parse_args()
 
 
@@ -530,7 +532,11 @@ def main():
     dof = 5 * box.nel * G ** 3
     s = Solver(desc, re=RE)
     s.upload(q)
-    shapes, shape_ms = s.autotune(reps=3)  # launch shape of the volume kernel (untimed)
+    if args.shape >= 0:  # a given launch shape (profiling one shape), no tuning
+        s.set_vol_variant(args.p, args.shape)
+        shapes, shape_ms = {args.p: args.shape}, np.full((8, 5), -1.0)
+    else:
+        shapes, shape_ms = s.autotune(reps=3)  # launch shape of the volume kernel (untimed)
 
     def barrier():
         torch.cuda.synchronize()
