@@ -347,10 +347,19 @@ UpdArgs upd_args(const dsem_ctx *c, const Group &g, int kk, double *qt_out) {
   return u;
 }
 
-int enqueue_update(dsem_ctx *c, int kk, double *qt_out, long long *launches) {
+// fuse_vis: the update kernel averages the raw viscous face fluxes itself (c->fuse_vis
+// contexts; no enqueue_face_vis before it)
+int enqueue_update(dsem_ctx *c, int kk, double *qt_out, long long *launches, bool fuse_vis = false) {
   int r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
     auto &g = c->groups[j];
-    const UpdArgs u = upd_args(c, g, kk, qt_out);
+    UpdArgs u = upd_args(c, g, kk, qt_out);
+    if (fuse_vis)
+      for (const auto &ml : c->mlists)
+        if (ml.G == g.G) {
+          u.fmc = g.fmc;
+          u.VFr = c->VF;
+          u.vnrm = ml.nrm;
+        }
     CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::update(u, g.nel, st); }));
     return DSEM_OK;
   });
@@ -378,13 +387,16 @@ int enqueue_lob_keep(dsem_ctx *c, long long *launches) {
   return DSEM_OK;
 }
 
-int enqueue_stage(dsem_ctx *c, int kk, bool save, double *qt_out, long long *launches) {
+// fuse_vis (dsem_step): on c->fuse_vis contexts the update kernel averages the viscous
+// face fluxes and k_face_vis is not launched (VF keeps the raw fluxes after the stage)
+int enqueue_stage(dsem_ctx *c, int kk, bool save, double *qt_out, long long *launches, bool fuse_vis = false) {
   int r;
+  fuse_vis = fuse_vis && c->fuse_vis;
   if ((r = enqueue_face_inv(c, launches))) return r;
   if (kk == c->kord && c->keep_lob && (r = enqueue_lob_keep(c, launches))) return r;
   if ((r = enqueue_vol(c, save, launches))) return r;
-  if ((r = enqueue_face_vis(c, launches))) return r;
-  return enqueue_update(c, kk, qt_out, launches);
+  if (!fuse_vis && (r = enqueue_face_vis(c, launches))) return r;
+  return enqueue_update(c, kk, qt_out, launches, fuse_vis);
 }
 
 int enqueue_ev(dsem_ctx *c, long long *launches, const double *jq = nullptr) {
@@ -467,7 +479,7 @@ int enqueue_step(dsem_ctx *c, bool save_last, long long *launches) {
     if (r) return r;
   }
   for (int kk = 1; kk <= c->kord; ++kk) {
-    int r = enqueue_stage(c, kk, save_last && kk == c->kord, nullptr, launches);
+    int r = enqueue_stage(c, kk, save_last && kk == c->kord, nullptr, launches, true);
     if (r) return r;
   }
   return DSEM_OK;
@@ -1021,6 +1033,51 @@ int setup_ctx(dsem_ctx *c, const MeshSet &ms) {
     if (!mats.empty()) CK(cudaMemcpy(c->nc_mats, mats.data(), mats.size() * sizeof(double), cudaMemcpyHostToDevice));
   }
 
+  // the mortar of each element face, for the update kernel that averages the viscous face
+  // fluxes itself (dsem_step): only when every face is one side of exactly one conforming
+  // mortar (no boundary, p-nonconforming or cut faces)
+  if (ncs.empty() && cuts.empty() && c->blists.empty() && !c->groups.empty()) {
+    const size_t ng = c->groups.size();
+    std::vector<std::vector<MortarC>> fm(ng);
+    std::vector<std::vector<char>> seen(ng);
+    for (size_t gi = 0; gi < ng; ++gi) {
+      fm[gi].resize(6 * (size_t)c->groups[gi].nel);
+      seen[gi].assign(6 * (size_t)c->groups[gi].nel, 0);
+    }
+    bool ok = true;
+    for (int G = GMIN; G <= GMAX && ok; ++G)
+      for (const MortarC &m : mcs[G]) {
+        const long long G2 = (long long)G * G;
+        for (int side = 0; side < 2 && ok; ++side) {
+          const long long off = side ? m.ss : m.ms;
+          ok = false;
+          for (size_t gi = 0; gi < ng; ++gi) {
+            const Group &g = c->groups[gi];
+            if (g.G != G || off < g.f0 || off >= g.f0 + (long long)g.nel * 30 * G2) continue;
+            const long long rel = off - g.f0, slot = rel / (5 * G2);
+            if (rel % (5 * G2) != 0 || seen[gi][slot]) break;
+            seen[gi][slot] = 1;
+            MortarC e = m;
+            e.flags |= side << 8;
+            fm[gi][slot] = e;
+            ok = true;
+            break;
+          }
+        }
+        if (!ok) break;
+      }
+    for (size_t gi = 0; gi < ng && ok; ++gi)
+      for (char s : seen[gi]) ok = ok && s;
+    if (ok) {
+      for (size_t gi = 0; gi < ng; ++gi) {
+        Group &g = c->groups[gi];
+        CK(cudaMalloc(&g.fmc, fm[gi].size() * sizeof(MortarC)));
+        CK(cudaMemcpy(g.fmc, fm[gi].data(), fm[gi].size() * sizeof(MortarC), cudaMemcpyHostToDevice));
+      }
+      c->fuse_vis = true;
+    }
+  }
+
   // ---- state and face buffers
   CK(cudaMalloc(&c->JQ, c->nq * sizeof(double)));
   CK(cudaMalloc(&c->gQ, c->nq * sizeof(double)));
@@ -1091,6 +1148,7 @@ void dsem_destroy(dsem_ctx *c) {
     cudaFree(g.ecase);
     cudaFree(g.nuhg);
     cudaFree(g.sens);
+    cudaFree(g.fmc);
   }
   cudaFree(c->d_rec);
   cudaFree(c->d_dtc);
@@ -1845,8 +1903,9 @@ int dsem_profile_rhs(dsem_ctx *c, int reps, double *ms) {
       }));
     }
     CK(cudaEventRecord(ev[2], c->st));
-    for (auto &ml : c->mlists)
-      CK(with_G(ml.G, [&](auto g) { return Launch<decltype(g)::value>::face_vis(ml.mc, ml.n, c->VF, ml.nrm, c->st); }));
+    for (auto &ml : c->mlists)  // (the update kernel averages the viscous fluxes on fuse_vis contexts)
+      if (!c->fuse_vis)
+        CK(with_G(ml.G, [&](auto g) { return Launch<decltype(g)::value>::face_vis(ml.mc, ml.n, c->VF, ml.nrm, c->st); }));
     for (auto &bl : c->blists)
       CK(with_G(bl.G, [&](auto g) {
         return Launch<decltype(g)::value>::face_bnd_vis(bl.mb, bl.n, c->VF, bl.nrm, bl.fvext, c->st);
@@ -1866,6 +1925,13 @@ int dsem_profile_rhs(dsem_ctx *c, int reps, double *ms) {
       u.re = c->P.re;
       u.r_re = c->P.r_re;
       u.update = 0;
+      if (c->fuse_vis)
+        for (const auto &ml : c->mlists)
+          if (ml.G == g.G) {
+            u.fmc = g.fmc;
+            u.VFr = c->VF;
+            u.vnrm = ml.nrm;
+          }
       CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::update(u, g.nel, c->st); }));
     }
     CK(cudaEventRecord(ev[4], c->st));
@@ -1895,7 +1961,7 @@ namespace dsem_int {
 int fail(dsem_ctx *c, int code, const std::string &msg) { return ::fail(c, code, msg); }
 int stage(dsem_ctx *c, int kk, bool save) {
   long long l = 0;
-  return enqueue_stage(c, kk, save, nullptr, &l);
+  return enqueue_stage(c, kk, save, nullptr, &l, true);
 }
 int traces(dsem_ctx *c) {
   long long l = 0;
@@ -1925,12 +1991,17 @@ int stage_io(dsem_ctx *c, int kk, bool save, const StageIO &io) {
   u.JQ = io.jq_in;
   u.JQo = io.jq_out;
   u.QF = io.qf_out;
+  if (c->fuse_vis) {  // the update kernel averages the viscous face fluxes (no k_face_vis)
+    u.fmc = g.fmc;
+    u.VFr = c->VF;
+    u.vnrm = ml.nrm;
+  }
   const int mode = vol_mode(c, save);
   CK(with_G(g.G, [&](auto gg) -> cudaError_t {
     using Lg = Launch<decltype(gg)::value>;
     cudaError_t e = Lg::face_inv_from(ml.mc, ml.n, io.qf_in, c->QF, c->FF, ml.nh, ml.nrm, c->P.gamma, c->st);
     if (e == cudaSuccess) e = Lg::vol(a, g.nel, g.diag, mode, c->st, c->vol_variant[g.G]);
-    if (e == cudaSuccess) e = Lg::face_vis(ml.mc, ml.n, c->VF, ml.nrm, c->st);
+    if (e == cudaSuccess && !c->fuse_vis) e = Lg::face_vis(ml.mc, ml.n, c->VF, ml.nrm, c->st);
     if (e == cudaSuccess) e = Lg::update(u, g.nel, c->st);
     return e;
   }));

@@ -39,6 +39,7 @@ struct Group {
   double *sens = nullptr;  // [elem][2][G^3] Ducros and density sensors (Smagorinsky sensors on)
   int *int2ext = nullptr;  // device: caller element id of each group element
   int *ecase = nullptr;    // device: case of each group element
+  MortarC *fmc = nullptr;  // device: [elem][6] mortar of each face, bit 8 of flags on a slave side (fuse_vis)
   std::vector<int> case_lo, case_hi;  // group elements [lo, hi) of each case
 };
 
@@ -77,6 +78,9 @@ struct dsem_ctx {
   double ark[5] = {}, brk[5] = {}, crk[5] = {};
   std::vector<Group> groups;
   std::vector<MList> mlists;
+  // every element face is one side of one conforming mortar: dsem_step's update kernel
+  // averages the viscous face fluxes itself (Group::fmc) and no k_face_vis runs
+  bool fuse_vis = false;
   int vol_variant[dsem::GMAX + 1] = {};  // launch shape of the volume kernel per order G (dsem_autotune)
   std::vector<BList> blists;  // boundary faces; their conditions need dsem_set_boundary first
   int nbnd = 0;

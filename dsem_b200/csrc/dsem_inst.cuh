@@ -88,7 +88,10 @@ cudaError_t Launch<G>::vol(const VolArgs &a, int nel, bool diag, int mode, cudaS
 template <int G> cudaError_t Launch<G>::update(const UpdArgs &a, int nel, cudaStream_t s) {
   if (nel <= 0) return cudaSuccess;
   const size_t smem = sizeof(double) * (30 * G * G + 5 * G * G * G + 2 * G);
-  k_update<G><<<nel, 256, smem, s>>>(a);
+  if (a.fmc)
+    k_update<G, true><<<nel, 256, smem, s>>>(a);
+  else
+    k_update<G, false><<<nel, 256, smem, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -1102,9 +1102,29 @@ struct UpdArgs {
   const int *ecase;           // optional: case of each element (ensembles)
   const double *rec, *dtc;    // optional: per case {re, 1/re} and dt; cdt = crk * dt
   double crk;
+  // optional (k_update<G, true>): the BR1 average of the viscous face fluxes (k_face_vis)
+  // done here from both sides' raw fluxes, so that no k_face_vis runs before.  fmc[6k + f]
+  // is the conforming mortar on face f + 1 of element k, bit 8 of its flags set when that
+  // face is the mortar's slave side; VFr is the base of the face slots its offsets index
+  // (VF then holds raw fluxes) and vnrm the norms of its order's mortars.
+  const MortarC *fmc;
+  const double *VFr, *vnrm;
 };
 
-template <int G> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
+// BR1 average at mortar point pt of field v (k_face_vis, send_flux_to_mortars), the
+// value that face side (0 master, 1 slave) receives: the same operations in the same order.
+__device__ __forceinline__ double vis_avg_point(const MortarC &M, int side, double vm, double vs, double nm_m,
+                                                double nm_s) {
+  const double rm = 1.0 / nm_m, rs = 1.0 / nm_s;
+  const bool neg_n = (M.flags >> 4) & 1, neg_s = (M.flags >> 3) & 1;
+  const double fv1 = ddiv(vm, nm_m, rm);
+  const double fv2 = ddiv(vs, nm_s, rs);
+  const double Qs = neg_n ? -fv2 : fv2;
+  const double qb = 0.5 * (fv1 + Qs) * nm_m;
+  return side ? (neg_s ? -qb : qb) : qb;
+}
+
+template <int G, bool FV = false> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G;
   extern __shared__ double sm[];
   double *FB = sm;            // 30*G2 face fluxes
@@ -1123,21 +1143,61 @@ template <int G> __global__ void __launch_bounds__(256) k_update(UpdArgs A) {
     }
     if (A.dtc) cdt = A.crk * A.dtc[cs];
   }
-  // send_flux_to_faces_add; four items per thread in flight (HBM latency)
-  for (int i0 = tid; i0 < 30 * G2; i0 += 4 * nt) {
-    double ff[4], vf[4];
+  if constexpr (!FV) {
+    // send_flux_to_faces_add; four items per thread in flight (HBM latency)
+    for (int i0 = tid; i0 < 30 * G2; i0 += 4 * nt) {
+      double ff[4], vf[4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int i = i0 + u * nt;
-      if (i < 30 * G2) {
-        ff[u] = FF[i];
-        vf[u] = VF[i];
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u * nt;
+        if (i < 30 * G2) {
+          ff[u] = FF[i];
+          vf[u] = VF[i];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u * nt;
+        if (i < 30 * G2) FB[i] = ff[u] - ddiv(vf[u], re, rre);
       }
     }
+  } else {
+    // the element's six mortars, then per item (face f, field v, mortar point pt) the
+    // BR1 average of k_face_vis into this face's slot (pt on a master face, the point
+    // sp that the orientation maps pt to on a slave face); four items per thread in flight
+    __shared__ MortarC FM[6];
+    if (tid < 6) FM[tid] = A.fmc[6LL * k + tid];
+    __syncthreads();
+    constexpr int UF = 4;
+    for (int i0 = tid; i0 < 30 * G2; i0 += UF * nt) {
+      double ff[UF], vm[UF], vs[UF], nm[UF], ns[UF];
+      int own[UF];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int i = i0 + u * nt;
-      if (i < 30 * G2) FB[i] = ff[u] - ddiv(vf[u], re, rre);
+      for (int u = 0; u < UF; ++u) {
+        const int i = i0 + u * nt;
+        own[u] = -1;
+        if (i < 30 * G2) {
+          const int f = i / (5 * G2), r = i - f * 5 * G2, v = r / G2, pt = r - v * G2;
+          const MortarC &M = FM[f];
+          int si, sj;
+          slave_index<G>(M.flags & 7, pt % G, pt / G, si, sj);
+          const int sp = si + G * sj;
+          own[u] = f * 5 * G2 + v * G2 + (((M.flags >> 8) & 1) ? sp : pt);
+          const long long g0 = (long long)M.geo * G2;
+          ff[u] = FF[own[u]];
+          vm[u] = A.VFr[M.ms + v * G2 + pt];
+          vs[u] = A.VFr[M.ss + v * G2 + sp];
+          nm[u] = A.vnrm[g0 + pt];
+          ns[u] = A.vnrm[g0 + sp];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < UF; ++u) {
+        if (own[u] < 0) continue;
+        const MortarC &M = FM[own[u] / (5 * G2)];
+        const double vf = vis_avg_point(M, (M.flags >> 8) & 1, vm[u], vs[u], nm[u], ns[u]);
+        FB[own[u]] = ff[u] - ddiv(vf, re, rre);
+      }
     }
   }
   for (int i = tid; i < G; i += nt) {

@@ -135,7 +135,10 @@ int dsem_last_timing(const dsem_ctx *ctx, double *ms, long long *launches);
 /* Benchmark hook (no DSEM counterpart): times reps evaluations of each
  * kernel of a right-hand side with CUDA events on the context's stream and
  * returns the mean milliseconds per evaluation in ms[4] = {inviscid face,
- * volume, viscous face, divergence + update}.  The state is left unchanged. */
+ * volume, viscous face, divergence + update}.  The state is left unchanged.
+ * The kernels are those dsem_step runs: where every element face is one side
+ * of a conforming mortar, the update kernel averages the viscous face fluxes
+ * itself, so ms[2] is then about zero and ms[3] includes that average. */
 int dsem_profile_rhs(dsem_ctx *ctx, int reps, double *ms);
 
 /* Static Smagorinsky LES (tstep.f90:40-43, turbulence/staticSmago/staticSmag.f90):
