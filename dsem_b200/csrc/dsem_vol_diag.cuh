@@ -213,7 +213,6 @@ __device__ __forceinline__ void vol_diag_dir(const VolArgs &A, const Phys &P, co
                                              const double *Dm, double *VF, double *QTI, int tid, long long &t_ph_) {
   using C = VolDiagCfg<G, EV, SAVE, V>;
   constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G, NT = C::NT, NPT = C::NPT;
-  const double gamma = P.gamma;
   const int xs = D == 0 ? 1 : (D == 1 ? G : G2);
   const int ls = xs;  // Lobatto-grid stride along D (lstride)
   // (a) Lobatto arrays of grid D; the energy gradient along D on grid D (round robin, the
@@ -382,7 +381,7 @@ __device__ __forceinline__ void vol_diag_dir(const VolArgs &A, const Phys &P, co
 template <int G, bool EV, int SAVE, int V>
 __device__ __forceinline__ void vol_diag_element(const VolArgs &A, const int k, double *sm) {
   using C = VolDiagCfg<G, EV, SAVE, V>;
-  constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G, NT = C::NT, NPT = C::NPT;
+  constexpr int L = G + 1, G2 = G * G, NG = G * G * G, NL = L * G * G, NT = C::NT;
   double *GR = sm;                  // [12][NG] Gauss gradients, field f*3 + direction
   double *WK = GR + C::NGR * NG;    // pass 1: state q [5][NG]; pass 2: LB [5][NL] + T4 [NL]
   double *LB = WK;
