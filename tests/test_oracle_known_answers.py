@@ -5,7 +5,10 @@ be built here, so the restatement is pinned by properties of the mathematics
 the reference implements: exactness of the spectral operators, the mortar L2
 projections and the quadrature; Roe-flux consistency and symmetry; freestream
 preservation and discrete conservation of the full right-hand side; invariance
-under rotated element frames; analytic Taylor-Green invariants.
+under rotated element frames; analytic Taylor-Green invariants; spectral
+convergence of the full right-hand side to the exact time derivatives of an
+advected density wave (convection, heat conduction) and of a viscous shear
+wave (viscous stress and its work).
 """
 import math
 
@@ -243,3 +246,67 @@ def test_entropy_viscosity_bounds(oracle_mod):
     c.step(0.0, dt, 2)
     mu = c.muhg()[:, :5, :5, :5]
     assert mu.max() > 0.0 and mu.min() >= 0.0 and mu.max() <= 0.5
+
+
+def _rhs_dqdt(oracle_mod, box, rho, u, p, re, gamma=1.4):
+    """dQ/dt at the Gauss points from the oracle's right-hand side (Qt is d(Q/jacob)/dt)."""
+    c = _case(oracle_mod, box, re=re)
+    c.set_q(mesh._jq(box, rho, u, p, gamma))
+    qt = c.rhs().reshape(box.nel, 5, -1)
+    return qt * box.jacob[:, None, :], box.jacob != 0
+
+
+def test_density_wave_spectral_convergence(oracle_mod):
+    """A density wave advected at uniform velocity and pressure, rho = 1 + a sin(x + y + z):
+    the exact time derivatives are d rho/dt = -u.grad rho, d(rho u)/dt = u d rho/dt (the
+    viscous stress of a uniform velocity vanishes, whatever Re is) and
+    dE/dt = -|u|^2/2 u.grad rho + gamma/(Pr (gamma - 1)) lap(p/rho) / Re (heat conduction;
+    the Mach number cancels between T = gamma M^2 p/rho and the conductivity).  On a periodic
+    3^3 box the full right-hand side (Int_fluxes, Vis_Fluxes, the Roe and BR1 mortars,
+    update_interior) converges to them spectrally as p grows."""
+    gamma, pr, re, a, p0 = 1.4, 0.72, 100.0, 0.2, 1.0 / 1.4
+    U = np.array([0.3, -0.2, 0.1])
+    e_cm, e_en = [], []
+    for p in (2, 4, 6, 8):
+        box = mesh.Box(3, 3, 3, p)
+        s = box.xg[..., 0] + box.xg[..., 1] + box.xg[..., 2]
+        rho = 1.0 + a * np.sin(s)
+        u = np.broadcast_to(U, rho.shape + (3,)).copy()
+        dq, m = _rhs_dqdt(oracle_mod, box, rho, u, np.full_like(rho, p0), re)
+        drho = -a * np.cos(s) * U.sum()
+        lap = 3.0 * p0 * (a * np.sin(s) / rho ** 2 + 2.0 * a * a * np.cos(s) ** 2 / rho ** 3)
+        de = -0.5 * (U @ U) * a * np.cos(s) * U.sum() + gamma / (pr * (gamma - 1.0)) * lap / re
+        e_cm.append(max(np.abs(dq[:, v][m] - ex[m]).max() for v, ex in
+                        enumerate([drho, U[0] * drho, U[1] * drho, U[2] * drho])) / np.abs(drho[m]).max())
+        e_en.append(np.abs(dq[:, 4][m] - de[m]).max() / np.abs(de[m]).max())
+    for k in range(1, 4):
+        assert e_cm[k] <= 0.1 * e_cm[k - 1], e_cm
+        assert e_en[k] <= 0.2 * e_en[k - 1], e_en
+    assert e_cm[-1] <= 1e-5 and e_en[-1] <= 1e-3, (e_cm, e_en)
+
+
+def test_shear_wave_viscous_stress(oracle_mod):
+    """A divergence-free shear wave at uniform density and pressure, u = A sin(x + y) (1, -1, 0):
+    the convective terms and the heat flux vanish, so d rho/dt = 0, d(rho u)/dt = -(2/Re) u
+    (mu lap u with |k|^2 = 2) and dE/dt = div(tau.u)/Re = 4 A^2 cos(2(x + y))/Re.  The viscous
+    stress, its work and the BR1 viscous mortars of the full right-hand side converge to them
+    spectrally; the z momentum, untouched by the wave, stays zero to rounding."""
+    gamma, re, A = 1.4, 50.0, 0.1
+    d = np.array([1.0, -1.0, 0.0])
+    errs = []
+    for p in (2, 4, 6, 8):
+        box = mesh.Box(3, 3, 3, p)
+        s = box.xg[..., 0] + box.xg[..., 1]
+        rho = np.ones_like(s)
+        u = A * np.sin(s)[..., None] * d
+        dq, m = _rhs_dqdt(oracle_mod, box, rho, u, np.full_like(rho, 1.0 / gamma), re)
+        sm, se = 2.0 * A / re, 4.0 * A * A / re
+        e_rho = np.abs(dq[:, 0][m]).max() / sm
+        e_mom = max(np.abs(dq[:, 1 + i][m] + 2.0 / re * A * np.sin(s[m]) * d[i]).max() for i in (0, 1)) / sm
+        e_en = np.abs(dq[:, 4][m] - se * np.cos(2.0 * s[m])).max() / se
+        assert np.abs(dq[:, 3][m]).max() <= 1e-10 * sm
+        errs.append((e_rho, e_mom, e_en))
+    errs = np.array(errs)
+    for k in range(1, 4):
+        assert np.all(errs[k] <= 0.1 * errs[k - 1]), errs
+    assert np.all(errs[-1] <= [1e-3, 1e-3, 1e-2]), errs
