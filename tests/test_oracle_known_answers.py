@@ -256,6 +256,24 @@ def _rhs_dqdt(oracle_mod, box, rho, u, p, re, gamma=1.4):
     return qt * box.jacob[:, None, :], box.jacob != 0
 
 
+def _density_wave_errors(oracle_mod, box, re=100.0, a=0.2, gamma=1.4, pr=0.72):
+    """Max errors of the oracle's dQ/dt against the exact derivatives of the advected density
+    wave (test_density_wave_spectral_convergence): (continuity and momentum, energy), each
+    relative to the largest exact value."""
+    p0 = 1.0 / gamma
+    U = np.array([0.3, -0.2, 0.1])
+    s = box.xg[..., 0] + box.xg[..., 1] + box.xg[..., 2]
+    rho = 1.0 + a * np.sin(s)
+    u = np.broadcast_to(U, rho.shape + (3,)).copy()
+    dq, m = _rhs_dqdt(oracle_mod, box, rho, u, np.full_like(rho, p0), re)
+    drho = -a * np.cos(s) * U.sum()
+    lap = 3.0 * p0 * (a * np.sin(s) / rho ** 2 + 2.0 * a * a * np.cos(s) ** 2 / rho ** 3)
+    de = -0.5 * (U @ U) * a * np.cos(s) * U.sum() + gamma / (pr * (gamma - 1.0)) * lap / re
+    e_cm = max(np.abs(dq[:, v][m] - ex[m]).max() for v, ex in
+               enumerate([drho, U[0] * drho, U[1] * drho, U[2] * drho])) / np.abs(drho[m]).max()
+    return e_cm, np.abs(dq[:, 4][m] - de[m]).max() / np.abs(de[m]).max()
+
+
 def test_density_wave_spectral_convergence(oracle_mod):
     """A density wave advected at uniform velocity and pressure, rho = 1 + a sin(x + y + z):
     the exact time derivatives are d rho/dt = -u.grad rho, d(rho u)/dt = u d rho/dt (the
@@ -264,21 +282,7 @@ def test_density_wave_spectral_convergence(oracle_mod):
     the Mach number cancels between T = gamma M^2 p/rho and the conductivity).  On a periodic
     3^3 box the full right-hand side (Int_fluxes, Vis_Fluxes, the Roe and BR1 mortars,
     update_interior) converges to them spectrally as p grows."""
-    gamma, pr, re, a, p0 = 1.4, 0.72, 100.0, 0.2, 1.0 / 1.4
-    U = np.array([0.3, -0.2, 0.1])
-    e_cm, e_en = [], []
-    for p in (2, 4, 6, 8):
-        box = mesh.Box(3, 3, 3, p)
-        s = box.xg[..., 0] + box.xg[..., 1] + box.xg[..., 2]
-        rho = 1.0 + a * np.sin(s)
-        u = np.broadcast_to(U, rho.shape + (3,)).copy()
-        dq, m = _rhs_dqdt(oracle_mod, box, rho, u, np.full_like(rho, p0), re)
-        drho = -a * np.cos(s) * U.sum()
-        lap = 3.0 * p0 * (a * np.sin(s) / rho ** 2 + 2.0 * a * a * np.cos(s) ** 2 / rho ** 3)
-        de = -0.5 * (U @ U) * a * np.cos(s) * U.sum() + gamma / (pr * (gamma - 1.0)) * lap / re
-        e_cm.append(max(np.abs(dq[:, v][m] - ex[m]).max() for v, ex in
-                        enumerate([drho, U[0] * drho, U[1] * drho, U[2] * drho])) / np.abs(drho[m]).max())
-        e_en.append(np.abs(dq[:, 4][m] - de[m]).max() / np.abs(de[m]).max())
+    e_cm, e_en = zip(*[_density_wave_errors(oracle_mod, mesh.Box(3, 3, 3, p)) for p in (2, 4, 6, 8)])
     for k in range(1, 4):
         assert e_cm[k] <= 0.1 * e_cm[k - 1], e_cm
         assert e_en[k] <= 0.2 * e_en[k - 1], e_en
@@ -310,3 +314,33 @@ def test_shear_wave_viscous_stress(oracle_mod):
     for k in range(1, 4):
         assert np.all(errs[k] <= 0.1 * errs[k - 1]), errs
     assert np.all(errs[-1] <= [1e-3, 1e-3, 1e-2]), errs
+
+
+def test_density_wave_general_curved_and_nonconforming(oracle_mod):
+    """The density wave's exact derivatives hold in physical coordinates, so the same
+    convergence pins the general-metric path, curved elements and p-nonconforming mortars:
+    a rotated middle element reproduces the axis-aligned box's errors (the scheme is
+    invariant under the element's frame); curved elements (a smooth periodic warp of every
+    element's map, as general_hex_map gives DSEM's curved meshes) converge spectrally; a
+    middle-third band of order p_in inside order p_out (L2 mortar projections,
+    mortar_operations.f90:249-758) stays within 2.5x of the uniform order p_out."""
+    rot = [0] * 27
+    rot[13] = 17
+    e_warp = []
+    for p in (2, 4, 6, 8):
+        plain = _density_wave_errors(oracle_mod, mesh.Box(3, 3, 3, p))
+        rotated = _density_wave_errors(oracle_mod, mesh.Box(3, 3, 3, p, rot=rot))
+        assert np.allclose(rotated, plain, rtol=1e-6, atol=1e-12), (p, rotated, plain)
+        e_warp.append(_density_wave_errors(oracle_mod, mesh.Box(3, 3, 3, p, warp=0.03)))
+    e_warp = np.array(e_warp)
+    for k in range(1, 4):
+        assert np.all(e_warp[k] <= 0.3 * e_warp[k - 1]), e_warp
+    assert np.all(e_warp[-1] <= [2e-3, 5e-3]), e_warp
+    for p_out, p_in in ((4, 6), (6, 8)):
+        orders = np.full(27, p_out)
+        for iz in range(3):
+            for iy in range(3):
+                orders[iy + 3 * (1 + 3 * iz)] = p_in  # ix = 1, the middle third in x
+        band = _density_wave_errors(oracle_mod, mesh.Box(3, 3, 3, orders))
+        uniform = _density_wave_errors(oracle_mod, mesh.Box(3, 3, 3, p_out))
+        assert np.all(np.array(band) <= 2.5 * np.array(uniform)), (p_out, p_in, band, uniform)
