@@ -9,7 +9,9 @@ with NS/BCs/stac3m) that hold for the reference algorithm itself:
   right-hand side up to rounding;
 * a wall without normal velocity passes no mass: the Roe flux of two equal
   states has a zero mass component, so the domain's mass changes only by
-  rounding."""
+  rounding;
+* a parallel shear flow decaying between no-slip walls has exact time
+  derivatives, and the full right-hand side converges to them spectrally."""
 import numpy as np
 import pytest
 
@@ -108,6 +110,39 @@ def test_wall_without_normal_velocity_passes_no_mass(oracle_mod):
     scale = float((np.abs(qt) * W).sum())
     assert scale > 1.0
     assert abs(total) <= 1e-13 * scale, (total, scale)
+
+
+@pytest.mark.parametrize("wall", ["walladiab", "wallisoth"])
+def test_wall_shear_decay_spectral_convergence(oracle_mod, wall):
+    """u = A sin(y/2) along x between no-slip walls at y = 0 and 2 pi (uniform density and
+    pressure, the walls' temperature): u vanishes on both walls, so the walls' Roe flux, wall
+    state and viscous wall flux (wallbc_Inv / wallbc_isoth, wall_vis_flux) see the exact
+    solution, whose time derivatives are d(rho u)/dt = -A sin(y/2)/(4 Re) (mu u_yy),
+    dE/dt = A^2 cos(y)/(4 Re) (the stress's work) and zero for the other components.  On
+    2 x 3 x 2 elements the right-hand side converges to them spectrally as p grows."""
+    re, A = 50.0, 0.5
+    errs = []
+    for p in (2, 4, 6, 8):
+        box = mesh.Box(2, 3, 2, p, bc={"y": (wall, wall)})
+        y = box.xg[..., 1]
+        u = np.zeros(y.shape + (3,))
+        u[..., 0] = A * np.sin(y / 2.0)
+        c = oracle_mod.Case.from_desc(box.desc())
+        c.set_phys(re=re)
+        c.set_q(mesh._jq(box, np.ones_like(y), u, np.full_like(y, TWALL / GAMMA), GAMMA))
+        c.set_boundary(TWALL)
+        dq = c.rhs().reshape(box.nel, 5, -1) * box.jacob[:, None, :]
+        m = box.jacob != 0
+        sm, se = A / (4.0 * re), A * A / (4.0 * re)
+        assert np.abs(dq[:, 3][m]).max() <= 1e-8 * sm  # z momentum: rounding only
+        errs.append([np.abs(dq[:, 0][m]).max() / sm,
+                     np.abs(dq[:, 1][m] + sm * np.sin(y[m] / 2.0)).max() / sm,
+                     np.abs(dq[:, 2][m]).max() / sm,
+                     np.abs(dq[:, 4][m] - se * np.cos(y[m])).max() / se])
+    errs = np.array(errs)
+    for k in range(1, 4):
+        assert np.all(errs[k] <= 0.1 * errs[k - 1]), errs
+    assert np.all(errs[-1] <= [1e-5, 1e-5, 1e-4, 1e-3]), errs
 
 
 def test_boundary_needs_its_condition(oracle_mod):
