@@ -10,8 +10,10 @@ with NS/BCs/stac3m) that hold for the reference algorithm itself:
 * a wall without normal velocity passes no mass: the Roe flux of two equal
   states has a zero mass component, so the domain's mass changes only by
   rounding;
-* a parallel shear flow decaying between no-slip walls has exact time
-  derivatives, and the full right-hand side converges to them spectrally."""
+* a parallel shear flow decaying between no-slip walls, and a density wave
+  convected through inflow and outflow faces that carry the exact external
+  state, have exact time derivatives, and the full right-hand side converges
+  to them spectrally."""
 import numpy as np
 import pytest
 
@@ -143,6 +145,47 @@ def test_wall_shear_decay_spectral_convergence(oracle_mod, wall):
     for k in range(1, 4):
         assert np.all(errs[k] <= 0.1 * errs[k - 1]), errs
     assert np.all(errs[-1] <= [1e-5, 1e-5, 1e-4, 1e-3]), errs
+
+
+def test_inflow_outflow_density_wave_convergence(oracle_mod):
+    """A density wave rho = 1 + a sin(x + 2y + z) convected at uniform velocity and pressure
+    through an inflow face (x = 0) and an outflow face (x = 2 pi) whose external states are the
+    exact solution at each mortar point (mrtr%Q(:,:,:,2), filled point by point in the
+    mortar_xyz layout): continuity and momentum have the exact derivatives d rho/dt =
+    -u.grad rho and d(rho u)/dt = u d rho/dt (no viscous stress), and the full right-hand
+    side, inflow_specAll / outflow_specAll Riemann fluxes included, converges to them
+    spectrally as p grows."""
+    a, re = 0.2, 400.0
+    U = np.array([0.4, 0.1, -0.1])
+    p0 = TWALL / GAMMA
+
+    def wave(xyz):
+        s = xyz[..., 0] + 2.0 * xyz[..., 1] + xyz[..., 2]
+        return 1.0 + a * np.sin(s), s
+
+    errs = []
+    for p in (2, 4, 6, 8):
+        box = mesh.Box(3, 3, 2, p, bc={"x": ("inflow", "outflow")})
+        rho, s = wave(box.xg)
+        u = np.broadcast_to(U, rho.shape + (3,)).copy()
+        c = oracle_mod.Case.from_desc(box.desc())
+        c.set_phys(re=re)
+        c.set_q(mesh._jq(box, rho, u, np.full_like(rho, p0), GAMMA))
+        mx = box.mortar_xyz()
+        qext = np.zeros((box.nmort, 5, box.ldx, box.ldx))
+        for j in box.boundary_mortars():
+            G = int(box.mortar[j, 8])
+            r, _ = wave(mx[j, :G, :G])
+            qext[j, :, :G, :G] = [r, r * U[0], r * U[1], r * U[2], p0 / (GAMMA - 1.0) + 0.5 * r * (U @ U)]
+        c.set_boundary(TWALL, qext, None)
+        dq = c.rhs().reshape(box.nel, 5, -1) * box.jacob[:, None, :]
+        m = box.jacob != 0
+        drho = -a * np.cos(s) * (U[0] + 2.0 * U[1] + U[2])
+        errs.append(max(np.abs(dq[:, v][m] - ex[m]).max() for v, ex in
+                        enumerate([drho, U[0] * drho, U[1] * drho, U[2] * drho])) / np.abs(drho[m]).max())
+    for k in range(1, 4):
+        assert errs[k] <= 0.15 * errs[k - 1], errs
+    assert errs[-1] <= 5e-4, errs
 
 
 def test_boundary_needs_its_condition(oracle_mod):
