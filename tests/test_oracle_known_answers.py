@@ -393,3 +393,38 @@ def test_kinetic_energy_budget(oracle_mod):
     h = np.array(h)[1:]  # the first call has no previous KE
     assert np.all(h[:, 1] > 0)
     assert np.abs(100.0 * h[:, 1] / h[:, 2] - 1.0).max() <= 1e-4
+
+
+def test_smagorinsky_viscosity_of_a_shear_wave(oracle_mod):
+    """Static Smagorinsky (simpleSmag, staticSmag.f90:32-118) on the shear wave
+    u = A sin(x + y) (1, -1, 0) at uniform density: |S| = sqrt(2 S_ij S_ij) = 2 A |cos(x + y)|
+    exactly, so the subgrid viscosity (in units of 1/Re) is Re (Cs Delta)^2 2 A |cos(x + y)|
+    with Delta = J^(1/3) / G (delta_g, :191-201).  It is formed at a step's start from the
+    previous right-hand side's Lobatto arrays and converges to that spectrally; values above
+    numax are capped at numax."""
+    gamma, re, A, cs = 1.4, 400.0, 0.1, 0.17
+    d = np.array([1.0, -1.0, 0.0])
+
+    def nut(p, numax):
+        box = mesh.Box(3, 3, 3, p)
+        s = box.xg[..., 0] + box.xg[..., 1]
+        c = _case(oracle_mod, box, re=re)
+        c.set_les(cs, numax)
+        c.set_q(mesh._jq(box, np.ones_like(s), A * np.sin(s)[..., None] * d, np.full_like(s, 1.0 / gamma), gamma))
+        c.rhs()
+        c.step(0.0, 1e-6, 1)
+        m = box.jacob != 0
+        delta = np.abs(1.0 / box.jacob[m]) ** (1.0 / 3.0) / (p + 1)
+        return c.nut().reshape(box.nel, -1)[m], re * (cs * delta) ** 2 * 2.0 * A * np.abs(np.cos(s[m]))
+
+    errs = []
+    for p in (2, 4, 6, 8):
+        got, ex = nut(p, 1e6)
+        errs.append(np.abs(got - ex).max() / ex.max())
+    for k in range(1, 4):
+        assert errs[k] <= 0.05 * errs[k - 1], errs
+    assert errs[-1] <= 1e-5, errs
+    got, ex = nut(8, 0.06)
+    assert got.max() == 0.06 and np.all(got >= 0.0)
+    low = ex < 0.05
+    assert np.abs(got[low] - ex[low]).max() <= 1e-5 * ex.max()
