@@ -289,27 +289,32 @@ def test_density_wave_spectral_convergence(oracle_mod):
     assert e_cm[-1] <= 1e-5 and e_en[-1] <= 1e-3, (e_cm, e_en)
 
 
+def _shear_wave_errors(oracle_mod, box, re=50.0, A=0.1, gamma=1.4):
+    """Errors of the oracle's dQ/dt against the shear wave's exact derivatives
+    (test_shear_wave_viscous_stress): (density, x/y momentum, energy) relative to 2A/Re,
+    2A/Re and 4A^2/Re, and the largest z-momentum rate relative to 2A/Re."""
+    d = np.array([1.0, -1.0, 0.0])
+    s = box.xg[..., 0] + box.xg[..., 1]
+    u = A * np.sin(s)[..., None] * d
+    dq, m = _rhs_dqdt(oracle_mod, box, np.ones_like(s), u, np.full_like(s, 1.0 / gamma), re)
+    sm, se = 2.0 * A / re, 4.0 * A * A / re
+    e = (np.abs(dq[:, 0][m]).max() / sm,
+         max(np.abs(dq[:, 1 + i][m] + 2.0 / re * A * np.sin(s[m]) * d[i]).max() for i in (0, 1)) / sm,
+         np.abs(dq[:, 4][m] - se * np.cos(2.0 * s[m])).max() / se)
+    return np.array(e), np.abs(dq[:, 3][m]).max() / sm
+
+
 def test_shear_wave_viscous_stress(oracle_mod):
     """A divergence-free shear wave at uniform density and pressure, u = A sin(x + y) (1, -1, 0):
     the convective terms and the heat flux vanish, so d rho/dt = 0, d(rho u)/dt = -(2/Re) u
     (mu lap u with |k|^2 = 2) and dE/dt = div(tau.u)/Re = 4 A^2 cos(2(x + y))/Re.  The viscous
     stress, its work and the BR1 viscous mortars of the full right-hand side converge to them
     spectrally; the z momentum, untouched by the wave, stays zero to rounding."""
-    gamma, re, A = 1.4, 50.0, 0.1
-    d = np.array([1.0, -1.0, 0.0])
     errs = []
     for p in (2, 4, 6, 8):
-        box = mesh.Box(3, 3, 3, p)
-        s = box.xg[..., 0] + box.xg[..., 1]
-        rho = np.ones_like(s)
-        u = A * np.sin(s)[..., None] * d
-        dq, m = _rhs_dqdt(oracle_mod, box, rho, u, np.full_like(rho, 1.0 / gamma), re)
-        sm, se = 2.0 * A / re, 4.0 * A * A / re
-        e_rho = np.abs(dq[:, 0][m]).max() / sm
-        e_mom = max(np.abs(dq[:, 1 + i][m] + 2.0 / re * A * np.sin(s[m]) * d[i]).max() for i in (0, 1)) / sm
-        e_en = np.abs(dq[:, 4][m] - se * np.cos(2.0 * s[m])).max() / se
-        assert np.abs(dq[:, 3][m]).max() <= 1e-10 * sm
-        errs.append((e_rho, e_mom, e_en))
+        e, ez = _shear_wave_errors(oracle_mod, mesh.Box(3, 3, 3, p))
+        assert ez <= 1e-10
+        errs.append(e)
     errs = np.array(errs)
     for k in range(1, 4):
         assert np.all(errs[k] <= 0.1 * errs[k - 1]), errs
@@ -323,7 +328,8 @@ def test_density_wave_general_curved_and_nonconforming(oracle_mod):
     invariant under the element's frame); curved elements (a smooth periodic warp of every
     element's map, as general_hex_map gives DSEM's curved meshes) converge spectrally; a
     middle-third band of order p_in inside order p_out (L2 mortar projections,
-    mortar_operations.f90:249-758) stays within 2.5x of the uniform order p_out."""
+    mortar_operations.f90:249-758) stays within 2.5x of the uniform order p_out, for the
+    density wave and for the viscous shear wave."""
     rot = [0] * 27
     rot[13] = 17
     e_warp = []
@@ -344,6 +350,10 @@ def test_density_wave_general_curved_and_nonconforming(oracle_mod):
         band = _density_wave_errors(oracle_mod, mesh.Box(3, 3, 3, orders))
         uniform = _density_wave_errors(oracle_mod, mesh.Box(3, 3, 3, p_out))
         assert np.all(np.array(band) <= 2.5 * np.array(uniform)), (p_out, p_in, band, uniform)
+        # the viscous mortar projections (k_face_nc_vis's restatement): the shear wave too
+        band, _ = _shear_wave_errors(oracle_mod, mesh.Box(3, 3, 3, orders))
+        uniform, _ = _shear_wave_errors(oracle_mod, mesh.Box(3, 3, 3, p_out))
+        assert np.all(band <= 2.5 * uniform), (p_out, p_in, band, uniform)
 
 
 @pytest.mark.parametrize("iord,lo,hi", [(4, 12.0, 20.0), (3, 6.5, 10.0)])
