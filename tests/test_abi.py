@@ -48,3 +48,31 @@ def test_invalid_descriptor_rejected():
     rc = L.dsem_create(None, None, ctypes.byref(h))
     assert rc == -1
     assert b"null" in L.dsem_last_error(None)
+
+
+def test_header_is_strict_c_and_links(tmp_path):
+    """A C caller (what DSEM's iso_c_binding interface binds to): include/dsem_gpu.h compiles
+    as strict C99 and as C++11 (-pedantic -Werror), every declared function links against the
+    library, and the program runs a call that needs no device."""
+    import shutil
+    import subprocess
+    if not shutil.which("gcc") or not shutil.which("g++"):
+        pytest.skip("no host C compiler")
+    from dsem_b200 import solver
+    solver.lib()  # builds the library if it is missing
+    libdir = os.path.dirname(solver.LIB)
+    fns = header_functions()
+    src = tmp_path / "caller.c"
+    src.write_text('#include "dsem_gpu.h"\n#include <stdio.h>\nint main(void) {\n'
+                   "  void (*fp[])(void) = {\n" + ",\n".join(f"    (void (*)(void))&{f}" for f in fns) +
+                   "\n  };\n  const char *e = dsem_last_error(NULL);\n"
+                   '  printf("%d %s\\n", (int)(sizeof fp / sizeof fp[0]), e ? "ok" : "null");\n  return 0;\n}\n')
+    inc = os.path.join(ROOT, "include")
+    for cc, std, lang in (("gcc", "-std=c99", []), ("g++", "-std=c++11", ["-x", "c++"])):
+        exe = tmp_path / f"caller_{cc}"
+        r = subprocess.run([cc, std, "-Wall", "-Wextra", "-pedantic", "-Werror", *lang, "-I", inc, str(src),
+                            "-x", "none", "-L", libdir, "-ldsem_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+        assert out.returncode == 0 and out.stdout.split() == [str(len(fns)), "ok"], (out.stdout, out.stderr)
