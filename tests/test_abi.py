@@ -76,3 +76,61 @@ def test_header_is_strict_c_and_links(tmp_path):
         assert r.returncode == 0, r.stderr
         out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
         assert out.returncode == 0 and out.stdout.split() == [str(len(fns)), "ok"], (out.stdout, out.stderr)
+
+
+def _c_kind(decl):
+    decl = decl.strip()
+    if "*" in decl:
+        return "ptr"
+    return "double" if re.match(r"(const\s+)?double\b", decl) else ("int" if re.match(r"(const\s+)?int\b", decl)
+                                                                    else decl)
+
+
+def _header_structs_and_functions():
+    txt = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "dsem_gpu.h")).read(), flags=re.S)
+    structs = {}
+    for body, name in re.findall(r"typedef struct\s*\{(.*?)\}\s*(\w+)\s*;", txt, flags=re.S):
+        fields = []
+        for stmt in body.split(";"):
+            stmt = stmt.strip()
+            if not stmt:
+                continue
+            m = re.match(r"((?:const\s+)?\w+)\s*(.*)", stmt)
+            base, names = m.group(1), m.group(2)
+            for nm in names.split(","):
+                nm = nm.strip()
+                fields.append((nm.lstrip("*").strip(), "ptr" if nm.startswith("*") else _c_kind(base)))
+        structs[name] = fields
+    funcs = {}
+    for ret, name, params in re.findall(r"([\w\s\*]+?)\b(dsem_\w+)\s*\(([^)]*)\)\s*;", txt):
+        ps = [x for x in params.split(",") if x.strip() and x.strip() != "void"]
+        funcs[name] = ("ptr" if "*" in ret else ret.strip().split()[-1], len(ps))
+    return structs, funcs
+
+
+def test_integration_fortran_binding_matches_header():
+    """The iso_c_binding module a DSEM maintainer adds agrees with
+    include/dsem_gpu.h: its BIND(C) derived types list the C structs' fields in the same order
+    with matching kinds (c_int / c_double / c_ptr), and each interface binds a declared
+    function with the same number of arguments and the same kind of result."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    block = re.search(r"```fortran\n(MODULE dsem_cuda.*?END MODULE dsem_cuda)\n```", text, flags=re.S).group(1)
+    block = re.sub(r"!.*", "", block)
+    structs, funcs = _header_structs_and_functions()
+    kinds = {"INTEGER(c_int)": "int", "REAL(c_double)": "double", "TYPE(c_ptr)": "ptr"}
+    types = re.findall(r"TYPE, BIND\(C\) :: (\w+)\n(.*?)END TYPE", block, flags=re.S)
+    assert {t for t, _ in types} == {"dsem_mesh_desc", "dsem_phys"}
+    for tname, body in types:
+        fields = []
+        for line in body.strip().splitlines():
+            decl, names = line.split("::")
+            fields += [(n.strip(), kinds[decl.strip()]) for n in names.split(",")]
+        assert fields == structs[tname], (tname, fields, structs[tname])
+    bound = re.findall(r"(INTEGER\(c_int\) FUNCTION|TYPE\(c_ptr\) FUNCTION|SUBROUTINE) (\w+)\(([^)]*)\) "
+                       r"BIND\(C, name='(\w+)'\)", block)
+    assert len(bound) >= 7
+    for kind, fname, args, cname in bound:
+        assert fname == cname and cname in funcs, cname
+        ret, nparams = funcs[cname]
+        assert nparams == len([a for a in args.split(",") if a.strip()]), cname
+        assert ret == {"INTEGER(c_int) FUNCTION": "int", "TYPE(c_ptr) FUNCTION": "ptr", "SUBROUTINE": "void"}[kind], cname
