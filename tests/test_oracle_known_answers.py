@@ -95,6 +95,39 @@ def test_roe_consistency_and_symmetry(oracle_mod):
         assert np.allclose(a, -b, rtol=1e-11, atol=1e-12)
 
 
+def test_roe_upwinds_supersonic_states(oracle_mod):
+    """When both states move through the face faster than sound (normal Mach 2-3, any
+    tangential velocity), every Roe wave speed has one sign, so the Roe flux (riemann,
+    PhysLib.f90:231-320; the entropy fix only touches near-zero speeds) is the physical flux
+    of the upstream state: ds n.F(QL) for flow along n, ds n.F(QR) against it."""
+    g = 1.4
+    rng = np.random.default_rng(5)
+
+    def cons(rho, u, p):
+        return np.array([rho, rho * u[0], rho * u[1], rho * u[2], p / (g - 1.0) + 0.5 * rho * (u @ u)])
+
+    def flux(n, ds, Q):
+        f, gf, h = oracle_mod.euler(Q)
+        return ds * (n[0] * f + n[1] * gf + n[2] * h)
+
+    for _ in range(100):
+        n = rng.standard_normal(3)
+        n /= np.linalg.norm(n)
+        ds = 0.5 + rng.random()
+        (rl, rr), (pl, pr) = 0.5 + rng.random(2), 0.5 + rng.random(2)
+        un = (2.0 + rng.random()) * max(math.sqrt(g * pl / rl), math.sqrt(g * pr / rr))
+        tl, tr = rng.standard_normal(3), rng.standard_normal(3)
+        tl -= (tl @ n) * n
+        tr -= (tr @ n) * n
+        ul, ur = un * n + 0.3 * tl, un * (1.0 + 0.1 * rng.random()) * n + 0.3 * tr
+        QL, QR = cons(rl, ul, pl), cons(rr, ur, pr)
+        ref = flux(n, ds, QL)
+        assert np.abs(oracle_mod.riemann(n, ds, QL, QR) - ref).max() <= 1e-14 * np.abs(ref).max()
+        QL, QR = cons(rl, -ul, pl), cons(rr, -ur, pr)
+        ref = flux(n, ds, QR)
+        assert np.abs(oracle_mod.riemann(n, ds, QL, QR) - ref).max() <= 1e-14 * np.abs(ref).max()
+
+
 def _case(oracle_mod, box, re=400.0):
     c = oracle_mod.Case.from_desc(box.desc())
     c.set_phys(re=re)
