@@ -347,19 +347,24 @@ UpdArgs upd_args(const dsem_ctx *c, const Group &g, int kk, double *qt_out) {
   return u;
 }
 
+// the update kernel of group g averages the raw viscous face fluxes itself (k_update<G, true>;
+// c->fuse_vis contexts, no k_face_vis before it)
+void fuse_vis_args(const dsem_ctx *c, const Group &g, UpdArgs &u) {
+  for (const auto &ml : c->mlists)
+    if (ml.G == g.G) {
+      u.fmc = g.fmc;
+      u.VFr = c->VF;
+      u.vnrm = ml.nrm;
+    }
+}
+
 // fuse_vis: the update kernel averages the raw viscous face fluxes itself (c->fuse_vis
 // contexts; no enqueue_face_vis before it)
 int enqueue_update(dsem_ctx *c, int kk, double *qt_out, long long *launches, bool fuse_vis = false) {
   int r = fork_jobs(c, c->groups.size(), [&](size_t j, cudaStream_t st) -> int {
     auto &g = c->groups[j];
     UpdArgs u = upd_args(c, g, kk, qt_out);
-    if (fuse_vis)
-      for (const auto &ml : c->mlists)
-        if (ml.G == g.G) {
-          u.fmc = g.fmc;
-          u.VFr = c->VF;
-          u.vnrm = ml.nrm;
-        }
+    if (fuse_vis) fuse_vis_args(c, g, u);
     CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::update(u, g.nel, st); }));
     return DSEM_OK;
   });
@@ -1925,13 +1930,7 @@ int dsem_profile_rhs(dsem_ctx *c, int reps, double *ms) {
       u.re = c->P.re;
       u.r_re = c->P.r_re;
       u.update = 0;
-      if (c->fuse_vis)
-        for (const auto &ml : c->mlists)
-          if (ml.G == g.G) {
-            u.fmc = g.fmc;
-            u.VFr = c->VF;
-            u.vnrm = ml.nrm;
-          }
+      if (c->fuse_vis) fuse_vis_args(c, g, u);
       CK(with_G(g.G, [&](auto gg) { return Launch<decltype(gg)::value>::update(u, g.nel, c->st); }));
     }
     CK(cudaEventRecord(ev[4], c->st));
@@ -1991,11 +1990,7 @@ int stage_io(dsem_ctx *c, int kk, bool save, const StageIO &io) {
   u.JQ = io.jq_in;
   u.JQo = io.jq_out;
   u.QF = io.qf_out;
-  if (c->fuse_vis) {  // the update kernel averages the viscous face fluxes (no k_face_vis)
-    u.fmc = g.fmc;
-    u.VFr = c->VF;
-    u.vnrm = ml.nrm;
-  }
+  if (c->fuse_vis) fuse_vis_args(c, g, u);  // the update kernel averages the viscous face fluxes
   const int mode = vol_mode(c, save);
   CK(with_G(g.G, [&](auto gg) -> cudaError_t {
     using Lg = Launch<decltype(gg)::value>;

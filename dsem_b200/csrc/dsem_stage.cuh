@@ -1111,8 +1111,10 @@ struct UpdArgs {
   const double *VFr, *vnrm;
 };
 
-// BR1 average at mortar point pt of field v (k_face_vis, send_flux_to_mortars), the
-// value that face side (0 master, 1 slave) receives: the same operations in the same order.
+// BR1 average of one field at one mortar point (k_face_vis, send_flux_to_mortars) from the
+// master's and the slave's raw viscous fluxes vm, vs and the mortar norms at the point and
+// at its slave image: the value that the face on side `side` (0 master, 1 slave) receives,
+// with k_face_vis's operations in k_face_vis's order.
 __device__ __forceinline__ double vis_avg_point(const MortarC &M, int side, double vm, double vs, double nm_m,
                                                 double nm_s) {
   const double rm = 1.0 / nm_m, rs = 1.0 / nm_s;
