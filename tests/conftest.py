@@ -18,3 +18,10 @@ def oracle_mod():
     from oracle import oracle
     oracle.set_threads(os.cpu_count() or 1)
     return oracle
+
+
+@pytest.fixture(scope="session")
+def box22():
+    """The 22^3, p = 8 Taylor-Green box (built once per session for the tests that need it)."""
+    from dsem_b200 import mesh
+    return mesh.Box(22, 22, 22, 8)

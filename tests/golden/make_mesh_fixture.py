@@ -1,11 +1,14 @@
 """Writes tests/golden/mesh_22cube_p8.json from the reference checkout's 22^3 Taylor-Green
 case folder (p8-22x22x22): the METIS graph's header, the elements that list themselves as a
-neighbour, a SHA-256 of every element's sorted neighbour list, and the corner coordinates of a
-sample of elements from the shipped mesh file.  tests/test_mesh.py checks the mesh builder
+neighbour, a SHA-256 of every element's sorted neighbour list, the corner coordinates of a
+sample of elements from the shipped mesh file, and the shipped 100-way METIS partition
+(DNS-22p8.graph.part.100, one part id per element, base64 of one byte each).
+tests/test_mesh.py and tests/test_shard_plan.py check the mesh builder and the shard planner
 against it without the checkout.
 
     python tests/golden/make_mesh_fixture.py <reference checkout>   (or DSEM_REFERENCE_DIR)
 """
+import base64
 import hashlib
 import json
 import os
@@ -42,13 +45,17 @@ def main():
     while not lines[i].startswith("end"):
         elems.append((int(lines[i].split()[0]), [int(x) for x in lines[i + 1].split()]))
         i += 2
+    with open(os.path.join(case, "DNS-22p8.graph.part.100")) as f:
+        part = [int(x) for x in f.read().split()]
+    assert len(part) == ne and 0 <= min(part) and max(part) < 256
     out = {
-        "source": "p8-22x22x22/DNS-22p8.graph and p8-22x22x22/tgv-22x22x22-p8.mesh of the reference",
+        "source": "p8-22x22x22/DNS-22p8.graph, tgv-22x22x22-p8.mesh and DNS-22p8.graph.part.100 of the reference",
         "graph_header": [ne, nm],
         "self_listed": [e + 1 for e in range(ne) if e + 1 in nbs[e]],
         "adjacency_sha256": adjacency_digest(nbs),
         "elements_in_mesh_file": len(elems),
         "corner_sample": {str(eid): [nodes[k] for k in conn] for eid, conn in elems[::SAMPLE]},
+        "metis_part_100_b64": base64.b64encode(bytes(part)).decode(),
     }
     with open(os.path.join(HERE, "mesh_22cube_p8.json"), "w") as f:
         json.dump(out, f, indent=0)

@@ -14,12 +14,6 @@ REF = os.path.join(os.environ.get("DSEM_REFERENCE_DIR", ""), "p8-22x22x22") \
 KEYS = ("ncg", "jacob", "gmetg", "gmet", "mortar", "n_hat", "norm")
 
 
-@pytest.fixture(scope="module")
-def box22():
-    """The 22^3, p = 8 Taylor-Green box (built once for the tests that need it)."""
-    return mesh.Box(22, 22, 22, 8)
-
-
 @pytest.mark.parametrize("n,p,rot", [(4, 4, None), (3, 2, {13: 5}), (3, 6, {13: 22}), (2, 3, None)])
 def test_builder_matches_oracle_bitwise(oracle_mod, n, p, rot):
     r = None

@@ -63,3 +63,36 @@ def test_exchange_plans_agree_across_two_gloo_ranks():
     for p in procs:
         p.join(timeout=60)
     assert res == {0: True, 1: True}
+
+
+def test_plan_of_dsem_metis_partition(box22):
+    """The planner on DSEM's own partition of the 22^3 case: the 100-way METIS split it ships
+    (DNS-22p8.graph.part.100, read by metis_file.f90; kept in tests/golden/mesh_22cube_p8.json).
+    Every element lands in exactly one part, every mortar whose elements share a part appears
+    once and every mortar between parts on both sides, as one ghost face each, and for every
+    pair of neighbouring parts the block one sends lists the same mortars, in the same order,
+    as the block the other receives."""
+    import base64
+    import json
+
+    from dsem_b200.shard import partition
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "mesh_22cube_p8.json")) as f:
+        part = np.frombuffer(base64.b64decode(json.load(f)["metis_part_100_b64"]), dtype=np.uint8).astype(np.int64)
+    assert part.shape == (box22.nel,) and part.max() == 99
+    parts = partition(box22.desc(), part)
+    els = np.concatenate([p["elements"] for p in parts])
+    assert np.array_equal(np.sort(els), np.arange(box22.nel))
+    m = box22.mortar
+    crossing = part[m[:, 0] - 1] != part[m[:, 1] - 1]
+    count = np.zeros(box22.nmort, dtype=int)
+    for p in parts:
+        count[p["mortars"]] += 1
+    assert np.all(count[~crossing] == 1) and np.all(count[crossing] == 2)
+    assert sum(len(p["ghosts"]) for p in parts) == 2 * int(crossing.sum())
+    for r, p in enumerate(parts):
+        assert sorted(p["ghosts"]) == sorted(np.where(crossing & ((part[m[:, 0] - 1] == r) |
+                                                                  (part[m[:, 1] - 1] == r)))[0].tolist())
+        for nb, g0, n in p["plan"]:
+            back = [x for x in parts[nb]["plan"] if x[0] == r]
+            assert len(back) == 1 and back[0][2] == n
+            assert p["ghosts"][g0:g0 + n] == parts[nb]["ghosts"][back[0][1]:back[0][1] + n]
