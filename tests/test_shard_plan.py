@@ -71,17 +71,25 @@ def test_plan_of_dsem_metis_partition(box22):
     Every element lands in exactly one part, every mortar whose elements share a part appears
     once and every mortar between parts on both sides, as one ghost face each, and for every
     pair of neighbouring parts the block one sends lists the same mortars, in the same order,
-    as the block the other receives."""
+    as the block the other receives.  Each part numbers its elements as DSEM's ranks do: the
+    local indices equal grid_distribution.dat, which DSEM wrote for this partition
+    (read_restart, restart.f90:486-496)."""
     import base64
     import json
 
     from dsem_b200.shard import partition
     with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "mesh_22cube_p8.json")) as f:
-        part = np.frombuffer(base64.b64decode(json.load(f)["metis_part_100_b64"]), dtype=np.uint8).astype(np.int64)
+        fx = json.load(f)
+    decode = lambda k: np.frombuffer(base64.b64decode(fx[k]), dtype=np.uint8).astype(np.int64)
+    part, dsem_local = decode("metis_part_100_b64"), decode("grid_distribution_local_b64")
     assert part.shape == (box22.nel,) and part.max() == 99
     parts = partition(box22.desc(), part)
     els = np.concatenate([p["elements"] for p in parts])
     assert np.array_equal(np.sort(els), np.arange(box22.nel))
+    local = np.zeros(box22.nel, dtype=np.int64)
+    for p in parts:
+        local[p["elements"]] = np.arange(1, len(p["elements"]) + 1)
+    assert np.array_equal(local, dsem_local)
     m = box22.mortar
     crossing = part[m[:, 0] - 1] != part[m[:, 1] - 1]
     count = np.zeros(box22.nmort, dtype=int)
