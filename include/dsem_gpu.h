@@ -79,7 +79,9 @@ typedef struct {
   double gamma, re, pr, mach; /* NS_data.f90:51-201                                    */
   double cmu, mumax;          /* entropy-viscosity coefficients                        */
   int shock;                  /* 1: entropy viscosity (tstep.f90:36-38); 3: also the
-                                 Ducros sensor (input keyword `ducros`)                */
+                                 Ducros sensor (input keyword `ducrosSens`, logical
+                                 ducrosSensor: input_lib.f90:166, 442-443; applied at
+                                 EViscosity_GL.f90:84)                                 */
   int iord;                   /* rkcoefs order: 3 (3 stages) or 4 (5 stages)           */
 } dsem_phys;
 
