@@ -498,21 +498,18 @@ void contract(int d, const double *A, int nout, int nin, const T *in, const int 
   // generic index helpers with explicit extents
   if (k1 < 0) k1 = nin;
   int e[3] = {eout[0], eout[1], eout[2]};
+  // stride of the input along d, and the input index of (a, b, c) with its d-th index 0
+  const size_t sd = d == 0 ? 1 : (d == 1 ? (size_t)ein[0] : (size_t)ein[0] * ein[1]);
   for (int c = 0; c < e[2]; ++c)
     for (int b = 0; b < e[1]; ++b)
       for (int a = 0; a < e[0]; ++a) {
-        int o[3] = {a, b, c};
-        int r = o[d];
         int ii[3] = {a, b, c};
-        T acc = T(0.0);
-        for (int k = k0; k < k1; ++k) {
-          ii[d] = k;
-          size_t pin = ii[0] + (size_t)ein[0] * (ii[1] + (size_t)ein[1] * ii[2]);
-          if (k == k0)
-            acc = A[r * nin + k] * in[pin];
-          else
-            acc = fmac(A[r * nin + k], in[pin], acc);
-        }
+        const int r = ii[d];
+        ii[d] = 0;
+        const T *x = in + ii[0] + (size_t)ein[0] * (ii[1] + (size_t)ein[1] * ii[2]);
+        const double *row = A + (size_t)r * nin;
+        T acc = k0 < k1 ? row[k0] * x[k0 * sd] : T(0.0);
+        for (int k = k0 + 1; k < k1; ++k) acc = fmac(row[k], x[k * sd], acc);
         out[a + (size_t)eout[0] * (b + (size_t)eout[1] * c)] = acc;
       }
 }
