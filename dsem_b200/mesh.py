@@ -100,7 +100,8 @@ def hex8(c, cx, cy, cz):
 def invert_metric(gx):
     """Invert_Metric_Tensor: returns grad_cx[..., i, j] = dX_i/dx_j and J."""
     small = 100 * np.finfo(float).eps
-    g = lambda i, j: gx[..., i, j]
+    comp = {(i, j): np.ascontiguousarray(gx[..., i, j]) for i in range(3) for j in range(3)}
+    g = lambda i, j: comp[i, j]
     J = (g(0, 0) * g(1, 1) * g(2, 2) - g(0, 1) * g(1, 0) * g(2, 2) - g(0, 0) * g(1, 2) * g(2, 1)
          + g(0, 2) * g(1, 0) * g(2, 1) + g(0, 1) * g(1, 2) * g(2, 0) - g(0, 2) * g(1, 1) * g(2, 0))
     gc = np.empty_like(gx)
@@ -312,44 +313,63 @@ class Box:
                 q = np.broadcast_to(nn + ldx * (mm + ldx * ll), (ext[2], ext[1], ext[0])).ravel()
                 for b in range(3):
                     self.gmet[ids[:, None], q[None, :], d + 3 * b] = row[..., b].reshape(len(ids), -1)
-        # mortars
+        # mortars (their geometry is evaluated per group of equal master face and size, the
+        # face normals per face and order, with the same elementwise arithmetic per point)
         nm = len(self.mort_raw)
         self.nmort = nm
         self.mortar = np.zeros((nm, 17), dtype=np.int32)
         self.n_hat = np.zeros((nm, ldx, ldx, 3))
         self.norm = np.zeros((nm, ldx, ldx))
+        jobs = {}  # (master face, lenmortar) -> ([mortar], [master element])
+        normals = {}
         for j, (id1, id2, f1, f2, orient, sign) in enumerate(self.mort_raw):
             if id2 < 0:  # boundary mortar: master face only, nsign = 1 (set_mortars.f90:361)
                 Gm = int(self.G[id1])
                 self.mortar[j] = [id1 + 1, 0, f1, 0, Gm, Gm, Gm, Gm, Gm, Gm, 0, 1, 1, 1, 1, 1, 1]
-                self._mortar_geometry(j, id1, f1, [Gm, Gm])
+                job = jobs.setdefault((f1, Gm, Gm), ([], []))
+                job[0].append(j)
+                job[1].append(id1)
                 continue
             Gm, Gs = int(self.G[id1]), int(self.G[id2])
             j1, j2 = (1, 0) if orient >= 4 else (0, 1)
             lens = [[Gm, Gs], [Gm, Gs]]
             lm = [max(lens[0][0], lens[j1][1]), max(lens[1][0], lens[j2][1])]
             conf = [lm[0] == lens[0][0], lm[1] == lens[1][0], lm[0] == lens[j1][1], lm[1] == lens[j2][1]]
-            n1 = self._face_normal(id1, f1)
-            n2 = self._face_normal(id2, f2)
+            for f in (f1, f2):
+                if f not in normals:
+                    normals[f] = self._face_normals(f)
+            n1, n2 = normals[f1][id1], normals[f2][id2]
             nsign = 1 if float(np.dot(n1, n2)) >= 0 else -1
             self.mortar[j] = [id1 + 1, id2 + 1, f1, f2, Gm, Gm, Gs, Gs, lm[0], lm[1], orient, sign, nsign] + \
                 [int(x) for x in conf]
-            self._mortar_geometry(j, id1, f1, lm)
+            job = jobs.setdefault((f1, lm[0], lm[1]), ([], []))
+            job[0].append(j)
+            job[1].append(id1)
+        for (f1, l0, l1), (js, es) in jobs.items():
+            self._mortar_geometry(np.array(js), np.array(es), f1, [l0, l1])
 
-    def _face_normal(self, e, face):
-        G = int(self.G[e])
-        L = G + 1
+    def _face_normals(self, face):
+        """Unit normal J grad X_d of face `face` of every element [nel][3], at the face's
+        first Gauss point pair (the Lobatto end along d); its sign against the other side's
+        gives nsign."""
+        out = np.zeros((self.nel, 3))
         d = FACE_DIR[face]
-        cx = lobatto_points(L)
-        cxg = gauss_points(G)
-        pt = [cxg[0], cxg[0], cxg[0]]
-        pt[d] = cx[-1] if face in (2, 4, 5) else cx[0]
-        gx = self._map(self.corner[e], np.float64(pt[0]), np.float64(pt[1]), np.float64(pt[2]))[1]
-        gc, J = invert_metric(gx)
-        g = J * gc[d, :]
-        return g / math.sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2])
+        for G in np.unique(self.G):
+            G = int(G)
+            ids = np.where(self.G == G)[0]
+            cx = lobatto_points(G + 1)
+            cxg = gauss_points(G)
+            pt = [cxg[0], cxg[0], cxg[0]]
+            pt[d] = cx[-1] if face in (2, 4, 5) else cx[0]
+            gx = self._map(self.corner[ids], np.float64(pt[0]), np.float64(pt[1]), np.float64(pt[2]))[1]
+            gc, J = invert_metric(gx)
+            g = J[:, None] * gc[:, d, :]
+            out[ids] = g / np.sqrt(g[:, 0] * g[:, 0] + g[:, 1] * g[:, 1] + g[:, 2] * g[:, 2])[:, None]
+        return out
 
-    def _mortar_geometry(self, j, e, face, lm):
+    def _mortar_geometry(self, js, es, face, lm):
+        """n_hat and norm of the mortars js, whose master faces `face` of elements es have
+        lenmortar lm."""
         d = FACE_DIR[face]
         c1, c2 = gauss_points(lm[0]), gauss_points(lm[1])
         A = c1[None, :]
@@ -361,12 +381,12 @@ class Box:
             X, Y, Z = A, B, np.full_like(A * B, end)
         else:
             X, Y, Z = np.full_like(A * B, end), A, B
-        gx = self._map(self.corner[e], X + 0 * B, Y + 0 * A, Z + 0 * A)[1]
+        gx = self._map(self.corner[es][:, None, None, :, :], X + 0 * B, Y + 0 * A, Z + 0 * A)[1]
         gc, J = invert_metric(gx)
         r = gc[..., d, :]
         sqr = np.sqrt(r[..., 0] * r[..., 0] + r[..., 1] * r[..., 1] + r[..., 2] * r[..., 2])
-        self.n_hat[j, :lm[1], :lm[0], :] = r / sqr[..., None]
-        self.norm[j, :lm[1], :lm[0]] = J * sqr
+        self.n_hat[js, :lm[1], :lm[0], :] = r / sqr[..., None]
+        self.norm[js, :lm[1], :lm[0]] = J * sqr
 
     # ------------------------------------------------------------ exports
     def desc(self):
